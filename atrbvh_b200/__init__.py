@@ -1,0 +1,473 @@
+"""atrbvh_b200 -- ATRBVH build-and-traverse on NVIDIA B200 (sm_100a).
+
+Python mirror of the reference's BVHRT-Core builder interface over the C ABI in
+include/atrbvh.h (libatrbvh.so, built in-tree by ``python -m atrbvh_b200.build``).
+Class and method names follow the reference:
+
+    scene = SceneWrapper(ctx, vertices, bbmin, bbmax)     # BVHRT::SceneWrapper
+    tree = LBVHBuilder(False).BuildTree(scene)            # BVHRT::LBVHBuilder
+    AgglomerativeTreeletOptimizer(9, 2).Optimize(tree)    # BVHRT::AgglomerativeTreeletOptimizer
+    TRBVHOptimizer(7, 3).Optimize(tree)                   # BVHRT::TRBVHOptimizer
+    collapsed, sah = BVHTreeCollapser().Collapse(tree)    # BVHRT::BVHTreeCollapser
+    host = BVHTreeInstanceManager().DeviceToHostTree(tree)
+    bvh = CudaBVH(collapsed, scene)                       # Compact2 + Woop layout
+    bvh.trace(rays_ptr, num_rays, results_ptr)            # kepler_dynamic_fetch trace()
+
+Errors raise AtrError (the reference exits the process instead).  There is no
+CPU fallback: without the library or a B200 every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libatrbvh.so"
+
+ATR_OK = 0
+SCENE_UNIFORM = 0
+SCENE_CLUSTERED = 1
+
+
+class AtrError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"atrbvh status {status}: {msg}")
+        self.status = status
+
+
+_lib: C.CDLL | None = None
+
+_p = C.c_void_p
+_i32p = C.POINTER(C.c_int32)
+_f32p = C.POINTER(C.c_float)
+
+
+class TreeView(C.Structure):
+    _fields_ = [("num_triangles", C.c_uint32), ("root", C.c_int32), ("parent", _p), ("left", _p),
+                ("right", _p), ("data", _p), ("bbox_min", _p), ("bbox_max", _p), ("area", _p)]
+
+
+class CollapsedView(C.Structure):
+    _fields_ = [("num_triangles", C.c_uint32), ("root", C.c_int32), ("parent", _p), ("left", _p),
+                ("right", _p), ("data", _p), ("triangle_count", _p), ("bbox_min", _p), ("bbox_max", _p),
+                ("triangle_indices", _p)]
+
+
+class CompactView(C.Structure):
+    _fields_ = [("num_nodes", C.c_int64), ("num_woop", C.c_int64), ("nodes", _p), ("woop", _p),
+                ("tri_index", _p), ("max_depth", C.c_int32)]
+
+
+# (name, restype, argtypes) for every exported entry point of include/atrbvh.h.
+_SIGS = [
+    ("atr_last_error", C.c_char_p, []),
+    ("atr_version", C.c_char_p, []),
+    ("atr_ctx_create", C.c_int, [C.c_int, _p, C.POINTER(_p)]),
+    ("atr_ctx_destroy", C.c_int, [_p]),
+    ("atr_ctx_synchronize", C.c_int, [_p]),
+    ("atr_ctx_get_stream", C.c_int, [_p, C.POINTER(_p)]),
+    ("atr_ctx_set_timing", C.c_int, [_p, C.c_int]),
+    ("atr_ctx_phase_times", C.c_int, [_p, _f32p, C.c_int, C.POINTER(C.c_int)]),
+    ("atr_scene_create", C.c_int, [_p, _p, C.c_uint32, _f32p, _f32p, C.c_int, C.POINTER(_p)]),
+    ("atr_scene_destroy", C.c_int, [_p]),
+    ("atr_scene_bounds", C.c_int, [_p, _p, _f32p, _f32p]),
+    ("atr_scene_device_vertices", C.c_int, [_p, C.POINTER(_p), C.POINTER(C.c_uint32)]),
+    ("atr_scene_set_vertices", C.c_int, [_p, _p, _p, C.c_int]),
+    ("atr_build_lbvh", C.c_int, [_p, _p, C.c_int, C.POINTER(_p)]),
+    ("atr_tree_destroy", C.c_int, [_p]),
+    ("atr_tree_view_get", C.c_int, [_p, C.POINTER(TreeView)]),
+    ("atr_tree_download", C.c_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    ("atr_tree_sah", C.c_int, [_p, _p, C.c_float, C.c_float, _f32p]),
+    ("atr_tree_sorted_keys", C.c_int, [_p, _p, _p, _p]),
+    ("atr_device_morton", C.c_int, [_p, _p, C.c_uint32, _f32p, _f32p, C.c_int, _p]),
+    ("atr_device_sort_pairs", C.c_int, [_p, _p, _p, C.c_uint32, C.c_int]),
+    ("atr_optimize_atrbvh", C.c_int, [_p, _p, C.c_int, C.c_int, C.c_float, C.c_float]),
+    ("atr_optimize_trbvh", C.c_int, [_p, _p, C.c_int, C.c_int, C.c_float, C.c_float]),
+    ("atr_refit", C.c_int, [_p, _p, _p]),
+    ("atr_collapse", C.c_int, [_p, _p, C.c_float, C.c_float, C.c_int, C.POINTER(_p), _f32p]),
+    ("atr_collapsed_destroy", C.c_int, [_p]),
+    ("atr_collapsed_view_get", C.c_int, [_p, C.POINTER(CollapsedView)]),
+    ("atr_collapsed_download", C.c_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p]),
+    ("atr_flatten_compact2", C.c_int, [_p, _p, _p, C.POINTER(_p)]),
+    ("atr_compact_destroy", C.c_int, [_p]),
+    ("atr_compact_view_get", C.c_int, [_p, C.POINTER(CompactView)]),
+    ("atr_trace", C.c_int, [_p, _p, _p, C.c_int64, C.c_int, _p]),
+    ("atr_gen_scene", C.c_int, [C.c_int, C.c_uint32, C.c_uint64, _p]),
+    ("atr_gen_batch_sizes", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _p]),
+    ("atr_gen_batch_scene", C.c_int, [C.c_uint32, _p, C.c_uint64, _p]),
+    ("atr_gen_rays_pinhole", C.c_int, [C.c_uint32, C.c_uint32, _f32p, C.c_float, _p]),
+    ("atr_gen_rays_random", C.c_int, [C.c_uint64, C.c_uint64, _f32p, _f32p, _p]),
+]
+
+EXPORTED = [name for name, _, _ in _SIGS]
+
+
+def lib() -> C.CDLL:
+    """Load libatrbvh.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise AtrError(-1, f"{LIB_PATH} is missing; run `python -m atrbvh_b200.build`")
+        l = C.CDLL(str(LIB_PATH))
+        for name, res, args in _SIGS:
+            f = getattr(l, name, None)
+            if f is None:
+                continue
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != ATR_OK:
+        raise AtrError(status, lib().atr_last_error().decode(errors="replace"))
+
+
+def _f3(v) -> C.Array:
+    a = (C.c_float * 3)(*[float(x) for x in v])
+    return a
+
+
+def _ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+# ---- synthetic workloads ------------------------------------------------------
+
+def gen_scene(kind: int, n: int, seed: int = 0) -> np.ndarray:
+    """Triangle soup (n, 3, 4) float32 of the given distribution."""
+    out = np.empty((n, 3, 4), dtype=np.float32)
+    check(lib().atr_gen_scene(kind, n, seed, _ptr(out)))
+    return out
+
+
+def gen_batch_sizes(count: int, lo: int, hi: int, seed: int = 0) -> np.ndarray:
+    out = np.empty(count, dtype=np.uint32)
+    check(lib().atr_gen_batch_sizes(count, lo, hi, seed, _ptr(out)))
+    return out
+
+
+def gen_batch_scene(sizes: np.ndarray, seed: int = 0) -> np.ndarray:
+    sizes = np.ascontiguousarray(sizes, dtype=np.uint32)
+    out = np.empty((int(sizes.sum()), 3, 4), dtype=np.float32)
+    check(lib().atr_gen_batch_scene(len(sizes), _ptr(sizes), seed, _ptr(out)))
+    return out
+
+
+def gen_rays_pinhole(w: int, h: int, eye=(0.5, 0.5, -1.5), fov_deg: float = 60.0) -> np.ndarray:
+    out = np.empty((w * h, 2, 4), dtype=np.float32)
+    check(lib().atr_gen_rays_pinhole(w, h, _f3(eye), fov_deg, _ptr(out)))
+    return out
+
+
+def gen_rays_random(n: int, bbmin, bbmax, seed: int = 0) -> np.ndarray:
+    out = np.empty((n, 2, 4), dtype=np.float32)
+    check(lib().atr_gen_rays_random(n, seed, _f3(bbmin), _f3(bbmax), _ptr(out)))
+    return out
+
+
+# ---- runtime objects -----------------------------------------------------------
+
+class Context:
+    """One CUDA stream plus scratch pool (atr_ctx)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        h = C.c_void_p()
+        check(lib().atr_ctx_create(device, C.c_void_p(stream) if stream else None, C.byref(h)))
+        self.handle = h
+
+    def synchronize(self) -> None:
+        check(lib().atr_ctx_synchronize(self.handle))
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib().atr_ctx_get_stream(self.handle, C.byref(s)))
+        return s.value or 0
+
+    def set_timing(self, on: bool) -> None:
+        check(lib().atr_ctx_set_timing(self.handle, 1 if on else 0))
+
+    def phase_times(self) -> list[float]:
+        buf = (C.c_float * 64)()
+        n = C.c_int()
+        check(lib().atr_ctx_phase_times(self.handle, buf, 64, C.byref(n)))
+        return [buf[i] for i in range(min(n.value, 64))]
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().atr_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SceneWrapper:
+    """BVHRT::SceneWrapper: device copy of the triangle soup and its box."""
+
+    def __init__(self, ctx: Context, vertices, bbmin=None, bbmax=None, device_ptr: int | None = None,
+                 num_triangles: int | None = None):
+        self.ctx = ctx
+        h = C.c_void_p()
+        if device_ptr is not None:
+            n = int(num_triangles)
+            src, on_dev = C.c_void_p(device_ptr), 1
+        else:
+            v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3, 4)
+            n = v.shape[0]
+            src, on_dev = _ptr(v), 0
+            self._host = v
+        bmin = _f3(bbmin) if bbmin is not None else None
+        bmax = _f3(bbmax) if bbmax is not None else None
+        check(lib().atr_scene_create(ctx.handle, src, n, bmin, bmax, on_dev, C.byref(h)))
+        self.handle = h
+        self.n = n
+
+    def bounds(self) -> tuple[np.ndarray, np.ndarray]:
+        a = (C.c_float * 3)()
+        b = (C.c_float * 3)()
+        check(lib().atr_scene_bounds(self.ctx.handle, self.handle, a, b))
+        return np.array(a[:], np.float32), np.array(b[:], np.float32)
+
+    def set_vertices(self, vertices=None, device_ptr: int | None = None) -> None:
+        if device_ptr is not None:
+            check(lib().atr_scene_set_vertices(self.ctx.handle, self.handle, C.c_void_p(device_ptr), 1))
+        else:
+            v = np.ascontiguousarray(vertices, dtype=np.float32)
+            check(lib().atr_scene_set_vertices(self.ctx.handle, self.handle, _ptr(v), 0))
+            self.ctx.synchronize()
+
+    def device_vertices(self) -> int:
+        p = C.c_void_p()
+        check(lib().atr_scene_device_vertices(self.handle, C.byref(p), None))
+        return p.value
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().atr_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class HostTree:
+    """Host mirror of a device tree (SoABVHTree after DeviceToHostTree)."""
+    parent: np.ndarray
+    left: np.ndarray
+    right: np.ndarray
+    data: np.ndarray
+    bbox_min: np.ndarray  # (2N-1, 4)
+    bbox_max: np.ndarray
+    area: np.ndarray
+
+    @property
+    def num_triangles(self) -> int:
+        return (len(self.parent) + 1) // 2
+
+    def RootIndex(self) -> int:
+        return 0
+
+    def SAH(self, ci: float = 1.2, ct: float = 1.0) -> float:
+        """SoABVHTree::SAH with the reference's sequential float32 sums."""
+        a = self.area.astype(np.float32)
+        n = self.num_triangles
+        si = np.float32(a[0])
+        for x in a[1:n - 1]:
+            si = np.float32(si + x)
+        sl = np.float32(0.0)
+        for x in a[n - 1:]:
+            sl = np.float32(sl + x)
+        return float(np.float32(np.float32(np.float32(ci) * si) + np.float32(np.float32(ct) * sl)) / a[0])
+
+
+class BVHTree:
+    """Device tree handle (atr_tree); arrays in the reference's SoA layout."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p, n: int):
+        self.ctx = ctx
+        self.handle = handle
+        self.n = n
+
+    def view(self) -> TreeView:
+        v = TreeView()
+        check(lib().atr_tree_view_get(self.handle, C.byref(v)))
+        return v
+
+    def NumberOfTriangles(self) -> int:
+        return self.n
+
+    def sah(self, ci: float = 1.2, ct: float = 1.0) -> float:
+        s = C.c_float()
+        check(lib().atr_tree_sah(self.ctx.handle, self.handle, ci, ct, C.byref(s)))
+        return s.value
+
+    def sorted_keys(self) -> tuple[np.ndarray, np.ndarray]:
+        k = np.empty(self.n, np.uint64)
+        i = np.empty(self.n, np.uint32)
+        check(lib().atr_tree_sorted_keys(self.ctx.handle, self.handle, _ptr(k), _ptr(i)))
+        return k, i
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().atr_tree_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LBVHBuilder:
+    """BVHRT::LBVHBuilder(use64BitMortonCodes)."""
+
+    def __init__(self, use64BitMortonCodes: bool = False):
+        self.bits = 63 if use64BitMortonCodes else 30
+
+    def BuildTree(self, scene: SceneWrapper) -> BVHTree:
+        h = C.c_void_p()
+        check(lib().atr_build_lbvh(scene.ctx.handle, scene.handle, self.bits, C.byref(h)))
+        return BVHTree(scene.ctx, h, scene.n)
+
+
+class AgglomerativeTreeletOptimizer:
+    """BVHRT::AgglomerativeTreeletOptimizer(treeletSize=9, iterations=2)."""
+
+    def __init__(self, treeletSize: int = 9, iterations: int = 2, ci: float = 1.2, ct: float = 1.0):
+        self.treelet, self.iterations, self.ci, self.ct = treeletSize, iterations, ci, ct
+
+    def Optimize(self, tree: BVHTree) -> None:
+        check(lib().atr_optimize_atrbvh(tree.ctx.handle, tree.handle, self.treelet, self.iterations,
+                                        self.ci, self.ct))
+
+
+class TRBVHOptimizer:
+    """BVHRT::TRBVHOptimizer(treeletSize=7, iterations=3)."""
+
+    def __init__(self, treeletSize: int = 7, iterations: int = 3, ci: float = 1.2, ct: float = 1.0):
+        self.treelet, self.iterations, self.ci, self.ct = treeletSize, iterations, ci, ct
+
+    def Optimize(self, tree: BVHTree) -> None:
+        check(lib().atr_optimize_trbvh(tree.ctx.handle, tree.handle, self.treelet, self.iterations,
+                                       self.ci, self.ct))
+
+
+def Refit(tree: BVHTree, scene: SceneWrapper) -> None:
+    """Bottom-up box refit of a resident tree from the scene's current vertices."""
+    check(lib().atr_refit(tree.ctx.handle, tree.handle, scene.handle))
+
+
+@dataclass
+class HostCollapsedTree:
+    parent: np.ndarray
+    left: np.ndarray
+    right: np.ndarray
+    data: np.ndarray
+    triangle_count: np.ndarray
+    bbox_min: np.ndarray
+    bbox_max: np.ndarray
+    triangle_indices: np.ndarray
+
+
+class BVHCollapsedTree:
+    def __init__(self, ctx: Context, handle: C.c_void_p, n: int):
+        self.ctx, self.handle, self.n = ctx, handle, n
+
+    def view(self) -> CollapsedView:
+        v = CollapsedView()
+        check(lib().atr_collapsed_view_get(self.handle, C.byref(v)))
+        return v
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().atr_collapsed_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BVHTreeCollapser:
+    """BVHRT::BVHTreeCollapser::Collapse(tree, &sah, ci, ct); max_leaf=0 is the reference."""
+
+    def Collapse(self, tree: BVHTree, ci: float = 1.2, ct: float = 1.0, max_leaf: int = 0):
+        h = C.c_void_p()
+        s = C.c_float()
+        check(lib().atr_collapse(tree.ctx.handle, tree.handle, ci, ct, max_leaf, C.byref(h), C.byref(s)))
+        return BVHCollapsedTree(tree.ctx, h, tree.n), s.value
+
+
+class BVHTreeInstanceManager:
+    """Host copies of device trees (BVHRT::BVHTreeInstanceManager)."""
+
+    def DeviceToHostTree(self, tree: BVHTree) -> HostTree:
+        nn = 2 * tree.n - 1
+        ht = HostTree(*(np.empty(nn, np.int32) for _ in range(4)), np.empty((nn, 4), np.float32),
+                      np.empty((nn, 4), np.float32), np.empty(nn, np.float32))
+        check(lib().atr_tree_download(tree.ctx.handle, tree.handle, _ptr(ht.parent), _ptr(ht.left),
+                                      _ptr(ht.right), _ptr(ht.data), _ptr(ht.bbox_min), _ptr(ht.bbox_max),
+                                      _ptr(ht.area)))
+        return ht
+
+    def DeviceToHostCollapsedTree(self, c: BVHCollapsedTree) -> HostCollapsedTree:
+        nn = 2 * c.n - 1
+        h = HostCollapsedTree(*(np.empty(nn, np.int32) for _ in range(5)), np.empty((nn, 4), np.float32),
+                              np.empty((nn, 4), np.float32), np.empty(c.n, np.int32))
+        check(lib().atr_collapsed_download(c.ctx.handle, c.handle, _ptr(h.parent), _ptr(h.left),
+                                           _ptr(h.right), _ptr(h.data), _ptr(h.triangle_count),
+                                           _ptr(h.bbox_min), _ptr(h.bbox_max), _ptr(h.triangle_indices)))
+        return h
+
+    def FreeDeviceTree(self, tree: BVHTree) -> None:
+        tree.close()
+
+    def FreeDeviceCollapsedTree(self, c: BVHCollapsedTree) -> None:
+        c.close()
+
+
+class CudaBVH:
+    """Compact2 layout + Woop triangles of a collapsed tree, and its traversal."""
+
+    def __init__(self, collapsed: BVHCollapsedTree, scene: SceneWrapper):
+        h = C.c_void_p()
+        check(lib().atr_flatten_compact2(scene.ctx.handle, collapsed.handle, scene.handle, C.byref(h)))
+        self.ctx = scene.ctx
+        self.handle = h
+
+    def view(self) -> CompactView:
+        v = CompactView()
+        check(lib().atr_compact_view_get(self.handle, C.byref(v)))
+        return v
+
+    def trace(self, rays_ptr: int, num_rays: int, results_ptr: int, any_hit: bool = False) -> None:
+        """rays: device float4 pairs; results: device int4 per ray."""
+        check(lib().atr_trace(self.ctx.handle, self.handle, C.c_void_p(rays_ptr), num_rays,
+                              1 if any_hit else 0, C.c_void_p(results_ptr)))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().atr_compact_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

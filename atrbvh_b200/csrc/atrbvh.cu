@@ -1,0 +1,326 @@
+// ATRBVH: agglomerative treelet restructuring on sm_100a.
+//
+// Semantics follow BVHRT-Core/src/AgglomerativeTreelet.cu:392-554 (bottom-up
+// pass, one thread per leaf; the second child to arrive processes a node; a
+// warp restructures the treelets of its lanes' nodes whose subtree holds at
+// least gamma triangles) and AgglomerativeTreeletOptimizer.cpp:73-92 (gamma
+// starts at the treelet size and doubles per iteration).  The treelet state
+// lives in registers, one treelet leaf per lane; only the distance matrix is
+// in shared memory.  Every reduction keeps the reference's shuffle-down tree
+// and strict comparisons, so ties resolve as in the reference.
+//
+// Memory ordering: a node's data is published by the thread that finished it
+// (plain stores, fence, atomic); the second arrival fences after its atomic
+// and reads descendants through L2 (ld.cg), and __syncwarp orders the other
+// lanes of the warp behind it.
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace atr {
+namespace {
+
+constexpr int kMaxTreelet = 20;
+constexpr int kMaxDist = kMaxTreelet * (kMaxTreelet - 1) / 2;  // 190
+constexpr int kAtrWarps = 4;
+
+__device__ __forceinline__ bool is_internal(int idx, uint32_t n) { return (uint32_t)idx < n - 1u; }
+
+// Row/column of flat index k of the strictly lower triangular matrix stored
+// row by row (r(r-1)/2 + c): BVHRT-Core/src/TriangularMatrix.cuh:150-168.
+__device__ __forceinline__ void trm_rc(int k, int& r, int& c) {
+    r = (int)__fmul_rn(__fadd_rn(1.0f, __fsqrt_rn((float)(8 * k + 1))), 0.5f);
+    if (r * (r - 1) / 2 > k) --r;
+    if ((r + 1) * r / 2 <= k) ++r;
+    c = k - r * (r - 1) / 2;
+}
+__device__ __forceinline__ int trm_idx(int r, int c) { return r * (r - 1) / 2 + c; }
+
+struct Box {
+    float mnx, mny, mnz, mxx, mxy, mxz;
+};
+
+__device__ __forceinline__ Box shfl_box(const Box& b, int src) {
+    Box o;
+    o.mnx = __shfl_sync(kFull, b.mnx, src);
+    o.mny = __shfl_sync(kFull, b.mny, src);
+    o.mnz = __shfl_sync(kFull, b.mnz, src);
+    o.mxx = __shfl_sync(kFull, b.mxx, src);
+    o.mxy = __shfl_sync(kFull, b.mxy, src);
+    o.mxz = __shfl_sync(kFull, b.mxz, src);
+    return o;
+}
+
+// Surface area of the union of two boxes (Commons.cuh:156-164).
+__device__ __forceinline__ float union_area(const Box& a, const Box& b) {
+    return sa3(__fsub_rn(fmaxf(a.mxx, b.mxx), fminf(a.mnx, b.mnx)),
+               __fsub_rn(fmaxf(a.mxy, b.mxy), fminf(a.mny, b.mny)),
+               __fsub_rn(fmaxf(a.mxz, b.mxz), fminf(a.mnz, b.mnz)));
+}
+
+struct TreeRefs {
+    uint32_t n;
+    int32_t* parent;
+    int32_t* left;
+    int32_t* right;
+    float4* bmin;
+    float4* bmax;
+    float* area;
+    float* nsah;
+};
+
+// Lane-held treelet leaf with everything later steps need, loaded as soon as
+// the lane receives the node.
+struct LeafSlot {
+    int node;
+    float area;
+    int cl = -1, cr = -1;  // children (internal nodes only)
+    float cal, car;  // children's areas
+    float4 mn, mx;   // box
+    float sah;       // nodesSah
+};
+
+__device__ __forceinline__ void load_slot(const TreeRefs& t, LeafSlot& s, int node, float area) {
+    s.node = node;
+    s.area = area;
+    s.mn = ld_cg(t.bmin + node);
+    s.mx = ld_cg(t.bmax + node);
+    s.sah = ld_cg(t.nsah + node);
+    if (is_internal(node, t.n)) {
+        s.cl = ld_cg(t.left + node);
+        s.cr = ld_cg(t.right + node);
+        s.cal = ld_cg(t.area + s.cl);
+        s.car = ld_cg(t.area + s.cr);
+    }
+}
+
+// One treelet rooted at `root`, processed by the whole warp.
+__device__ bool process_treelet(const TreeRefs& t, int root, float root_sah, int tsize, float ci,
+                                float* dist) {
+    const int lane = threadIdx.x & 31;
+
+    // ---- formTreelet (Treelet.cuh:57-114) ----
+    int internal_node = lane == 0 ? root : -1;  // lane k holds treeletInternalNodes[k]
+    LeafSlot slot;
+    slot.node = -1;
+    {
+        const int l0 = ld_cg(t.left + root), r0 = ld_cg(t.right + root);
+        if (lane < 2) {
+            const int nd = lane == 0 ? l0 : r0;
+            load_slot(t, slot, nd, ld_cg(t.area + nd));
+        }
+    }
+    for (int it = 0; it < tsize - 2; ++it) {
+        const int m = 2 + it;
+        float v = -FLT_MAX;
+        int ix = lane;
+        if (lane < m) v = is_internal(slot.node, t.n) ? slot.area : -FLT_MAX;
+        // findLeafToExpand: shuffle-down tree over m lanes, strict >.
+        int c = m, sh = m / 2;
+        while (c > 1) {
+            const float ov = __shfl_down_sync(kFull, v, sh);
+            const int oi = __shfl_down_sync(kFull, ix, sh);
+            if (lane < c - sh && ov > v) { v = ov; ix = oi; }
+            c = (c + 1) / 2;
+            sh = c / 2;
+        }
+        const int largest = __shfl_sync(kFull, ix, 0);
+        const int rep = __shfl_sync(kFull, slot.node, largest);
+        if (!is_internal(rep, t.n)) return false;  // only reachable with a malformed tree
+        const int L = __shfl_sync(kFull, slot.cl, largest);
+        const int R = __shfl_sync(kFull, slot.cr, largest);
+        const float aL = __shfl_sync(kFull, slot.cal, largest);
+        const float aR = __shfl_sync(kFull, slot.car, largest);
+        if (lane == it + 1) internal_node = rep;
+        if (lane == largest) load_slot(t, slot, L, aL);
+        if (lane == it + 2) load_slot(t, slot, R, aR);
+    }
+
+    // ---- agglomerative merge (AgglomerativeTreelet.cu:476-532) ----
+    Box box;
+    box.mnx = slot.mn.x; box.mny = slot.mn.y; box.mnz = slot.mn.z;
+    box.mxx = slot.mx.x; box.mxy = slot.mx.y; box.mxz = slot.mx.z;
+    int node = slot.node;
+    float sah = slot.sah;
+    int right_node = -1;  // treeletLeaves[lane] after the merge that fills this lane
+    float la = 0.0f;      // treeletLeavesAreas[lane]
+
+    const int npairs = tsize * (tsize - 1) / 2;
+    for (int base = 0; base < npairs; base += 32) {
+        const int j = base + lane;
+        int r = 0, c = 0;
+        if (j < npairs) trm_rc(j, r, c);
+        const Box a = shfl_box(box, r);
+        const Box b = shfl_box(box, c);
+        if (j < npairs) dist[j] = union_area(a, b);
+    }
+    __syncwarp();
+
+    for (int last = tsize - 1; last > 0; --last) {
+        // findMinimumDistance (:83-99): strided scan, strict <, shuffle-down reduce.
+        const int msize = last * (last + 1) / 2;
+        float best = FLT_MAX;
+        int bi = 0;
+        for (int j = lane; j < msize; j += 32) {
+            const float d = dist[j];
+            if (d < best) { best = d; bi = j; }
+        }
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) {
+            const float ob = __shfl_down_sync(kFull, best, sh);
+            const int oi = __shfl_down_sync(kFull, bi, sh);
+            if (ob < best) { best = ob; bi = oi; }
+        }
+        const int mi = __shfl_sync(kFull, bi, 0);
+        int jr, jc;
+        trm_rc(mi, jr, jc);
+
+        // updateState (:101-150).
+        const float sah_new = __fadd_rn(__shfl_sync(kFull, sah, jr), __shfl_sync(kFull, sah, jc));
+        const int left_index = __shfl_sync(kFull, node, jr);
+        const int right_index = __shfl_sync(kFull, node, jc);
+        const Box bjr = shfl_box(box, jr);
+        const Box bjc = shfl_box(box, jc);
+        Box A;
+        A.mnx = fminf(bjc.mnx, bjr.mnx); A.mny = fminf(bjc.mny, bjr.mny); A.mnz = fminf(bjc.mnz, bjr.mnz);
+        A.mxx = fmaxf(bjc.mxx, bjr.mxx); A.mxy = fmaxf(bjc.mxy, bjr.mxy); A.mxz = fmaxf(bjc.mxz, bjr.mxz);
+        const int new_internal = __shfl_sync(kFull, internal_node, last - 1);
+        const float la_new = __fadd_rn(sah_new, __fmul_rn(ci, box_area(A.mnx, A.mny, A.mnz, A.mxx, A.mxy, A.mxz)));
+        if (lane == jc) {
+            node = new_internal;
+            box = A;
+            sah = la_new;
+        }
+        if (lane == last) la = la_new;
+        const int last_index = __shfl_sync(kFull, node, last);
+        const float sah_last = __shfl_sync(kFull, sah, last);
+        const Box blast = shfl_box(box, last);
+        if (lane == jr) {
+            node = last_index;
+            sah = sah_last;
+            box = blast;
+        }
+        if (lane == last) {
+            node = left_index;
+            right_node = right_index;
+            box = A;
+        }
+
+        // updateDistancesMatrix (:152-188).
+        if (last > 1) {
+            float moved = 0.0f;
+            const bool mv = lane < last && lane != jr;
+            if (mv) moved = dist[trm_idx(last, lane)];
+            __syncwarp();
+            if (mv) dist[trm_idx(max(jr, lane), min(jr, lane))] = moved;
+            __syncwarp();
+            int r = lane, c = lane;
+            const bool up = lane < last && lane != jc;
+            if (up) { r = max(jc, lane); c = min(jc, lane); }
+            const Box br = shfl_box(box, r);
+            const Box bc = shfl_box(box, c);
+            const float d = union_area(br, bc);
+            if (up) dist[trm_idx(r, c)] = d;
+            __syncwarp();
+        }
+    }
+
+    // ---- updateTreelet (:190-212) ----
+    const float la1 = __shfl_sync(kFull, la, 1);
+    const int ni = __shfl_sync(kFull, internal_node, lane > 0 ? lane - 1 : 0);
+    if (la1 < root_sah && lane >= 1 && lane < tsize) {
+        t.left[ni] = node;
+        t.right[ni] = right_node;
+        t.parent[node] = ni;
+        t.parent[right_node] = ni;
+        t.nsah[ni] = la;
+        const float4 mn = make_float4(box.mnx, box.mny, box.mnz, 0.0f);
+        const float4 mx = make_float4(box.mxx, box.mxy, box.mxz, 0.0f);
+        t.bmin[ni] = mn;
+        t.bmax[ni] = mx;
+        t.area[ni] = box_area(mn, mx);
+    }
+    __syncwarp();
+    return true;
+}
+
+__global__ void __launch_bounds__(kAtrWarps * 32) k_atrbvh(TreeRefs t, int32_t* __restrict__ subtree,
+                                                           uint32_t* __restrict__ counters, int tsize,
+                                                           int gamma, float ci, float ct, uint32_t* err) {
+    __shared__ float s_dist[kAtrWarps][kMaxDist];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int cur = -1;
+    if (i < t.n) {
+        const int leaf = (int)i + (int)t.n - 1;
+        subtree[leaf] = 1;
+        t.nsah[leaf] = __fmul_rn(ct, t.area[leaf]);
+        cur = t.parent[leaf];
+    }
+    while (__any_sync(kFull, cur >= 0)) {
+        bool second = false;
+        if (cur >= 0) {
+            __threadfence();
+            if (atomicAdd(&counters[cur], 1u) == 0u) cur = -1;
+            else { second = true; __threadfence(); }
+        }
+        int cnt = 0;
+        float my_sah = 0.0f;
+        if (second) {
+            const int l = ld_cg(t.left + cur), r = ld_cg(t.right + cur);
+            const float a = ld_cg(t.area + cur);
+            cnt = ld_cg(subtree + l) + ld_cg(subtree + r);
+            my_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), ld_cg(t.nsah + l)), ld_cg(t.nsah + r));
+            subtree[cur] = cnt;
+            t.nsah[cur] = my_sah;
+        }
+        unsigned vote = __ballot_sync(kFull, cnt >= gamma);
+        if (vote) __syncwarp();
+        while (vote) {
+            const int rl = __ffs(vote) - 1;
+            const int root = __shfl_sync(kFull, cur, rl);
+            const float rsah = __shfl_sync(kFull, my_sah, rl);
+            if (!process_treelet(t, root, rsah, tsize, ci, s_dist[w]) && lane == 0)
+                set_error_bits(err, kErrTreeletClimb);
+            vote &= vote - 1;
+        }
+        if (cur >= 0) cur = ld_cg(t.parent + cur);
+    }
+}
+
+}  // namespace
+}  // namespace atr
+
+using namespace atr;
+
+extern "C" int atr_optimize_atrbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int iterations, float ci, float ct) {
+    ATR_REQUIRE(ctx && tree, ATR_ERR_INVALID_ARG, "atr_optimize_atrbvh: NULL argument");
+    ATR_REQUIRE(tsize >= 3 && tsize <= kMaxTreelet, ATR_ERR_UNSUPPORTED,
+                "atr_optimize_atrbvh: treelet size %d outside [3, %d]", tsize, kMaxTreelet);
+    ATR_REQUIRE(iterations >= 0, ATR_ERR_INVALID_ARG, "atr_optimize_atrbvh: iterations %d", iterations);
+    const uint32_t n = tree->n;
+    if (iterations == 0) return ATR_OK;
+    const size_t nn = 2 * (size_t)n - 1;
+    void* scratch = nullptr;
+    const size_t b_sub = align256(nn * 4), b_sah = align256(nn * 4), b_ctr = align256((size_t)(n - 1) * 4);
+    ATR_TRY(ctx->alloc(&scratch, b_sub + b_sah + b_ctr));
+    char* p = static_cast<char*>(scratch);
+    int32_t* subtree = reinterpret_cast<int32_t*>(p);
+    float* nsah = reinterpret_cast<float*>(p + b_sub);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(p + b_sub + b_sah);
+    TreeRefs t{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nsah};
+    const int threads = kAtrWarps * 32;
+    const uint32_t blocks = (n + threads - 1) / threads;
+    int gamma = tsize;
+    ctx->phase_begin("atrbvh");
+    for (int it = 0; it < iterations; ++it) {
+        cudaMemsetAsync(counters, 0, (size_t)(n - 1) * 4, ctx->stream);
+        k_atrbvh<<<blocks, threads, 0, ctx->stream>>>(t, subtree, counters, tsize, gamma, ci, ct, ctx->d_error);
+        gamma *= 2;
+    }
+    ctx->phase_end();
+    cudaError_t e = cudaGetLastError();
+    ctx->release(scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "k_atrbvh launch", __FILE__, __LINE__);
+    return ATR_OK;
+}

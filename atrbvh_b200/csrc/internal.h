@@ -1,0 +1,124 @@
+// Internal definitions shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/atrbvh.h"
+
+namespace atr {
+
+void set_error(const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define ATR_CUDA(call)                                                             \
+    do {                                                                           \
+        cudaError_t _e = (call);                                                   \
+        if (_e != cudaSuccess) return ::atr::cuda_fail(_e, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define ATR_REQUIRE(cond, code, ...)           \
+    do {                                       \
+        if (!(cond)) {                         \
+            ::atr::set_error(__VA_ARGS__);     \
+            return (code);                     \
+        }                                      \
+    } while (0)
+
+#define ATR_TRY(expr)                 \
+    do {                              \
+        int _s = (expr);              \
+        if (_s != ATR_OK) return _s;  \
+    } while (0)
+
+// Device-side error bits (ORed into atr_ctx::d_error by kernels whose bounded
+// waits give up).
+enum : uint32_t {
+    kErrSortLookback = 1u,
+    kErrBuildClimb = 2u,
+    kErrTreeletClimb = 4u,
+    kErrTraceStack = 8u,
+    kErrCollapse = 16u,
+};
+
+constexpr int kNumSms = 148;  // B200
+
+// Round up to a multiple of 256 bytes (alignment of every sub-array).
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace atr
+
+struct atr_ctx {
+    int device = 0;
+    int num_sms = atr::kNumSms;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint32_t* d_error = nullptr;  // device error bits
+    bool timing = false;
+    struct Phase {
+        std::string name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Phase> phases;
+    std::vector<float> phase_ms;
+
+    // Stream-ordered allocation from the device's default pool.
+    int alloc(void** p, size_t bytes);
+    void release(void* p);
+    // Phase timing helpers (no-ops unless timing is enabled).
+    void phase_begin(const char* name);
+    void phase_end();
+};
+
+struct atr_scene {
+    atr_ctx* ctx = nullptr;
+    uint32_t n = 0;
+    float4* verts = nullptr;  // 3 per triangle
+    float* d_bounds = nullptr;  // min.xyz, max.xyz on the device
+};
+
+struct atr_tree {
+    atr_ctx* ctx = nullptr;
+    uint32_t n = 0;
+    void* block = nullptr;
+    int32_t *parent = nullptr, *left = nullptr, *right = nullptr, *data = nullptr;
+    float4 *bmin = nullptr, *bmax = nullptr;
+    float* area = nullptr;
+    // Sort output kept from the build (keys as stored: uint32 or uint64).
+    void* sorted_keys = nullptr;
+    uint32_t* sorted_idx = nullptr;
+    int morton_bits = 30;
+};
+
+struct atr_collapsed {
+    atr_ctx* ctx = nullptr;
+    uint32_t n = 0;
+    void* block = nullptr;
+    int32_t *parent = nullptr, *left = nullptr, *right = nullptr, *data = nullptr, *count = nullptr;
+    float4 *bmin = nullptr, *bmax = nullptr;
+    int32_t* tri_indices = nullptr;
+};
+
+struct atr_compact {
+    atr_ctx* ctx = nullptr;
+    int64_t num_nodes = 0;
+    int64_t num_woop = 0;
+    int32_t max_depth = 0;
+    int4* nodes = nullptr;
+    float4* woop = nullptr;
+    int32_t* tri_index = nullptr;
+};
+
+namespace atr {
+
+// Allocate the SoA arrays of a tree with n triangles in one block.
+int tree_alloc(atr_ctx* ctx, uint32_t n, atr_tree** out);
+
+// LBVH internals used by the batched path.
+int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds,
+                    int morton_bits, atr_tree* t);
+
+}  // namespace atr

@@ -1,0 +1,629 @@
+// LBVH construction on sm_100a:
+//   scene bounds  -> Morton codes (+ all radix-digit histograms in the same pass)
+//   -> onesweep LSD radix sort of (key, triangle index)
+//   -> one bottom-up pass that builds the Karras radix tree and refits its
+//      boxes at the same time.
+//
+// The tree is bit-identical to the reference's two-kernel build
+// (BVHRT-Core/src/LBVH.cu:208-316 topology, :465-570 refit): the binary radix
+// tree over the (key, index) pairs is unique, and internal node numbering
+// follows Karras (a node covering [l, r] is stored at r when it is its
+// parent's left child and at l when it is the right child; the root at 0).
+
+#include <cstdio>
+#include <utility>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace atr {
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr uint32_t kFlagAgg = 0x40000000u;
+constexpr uint32_t kFlagInc = 0x80000000u;
+constexpr uint32_t kValueMask = 0x3fffffffu;
+constexpr uint32_t kLookbackLimit = 1u << 26;
+
+template <typename K> struct KeyTraits;
+template <> struct KeyTraits<uint32_t> { static constexpr int kPasses = 4; };
+template <> struct KeyTraits<uint64_t> { static constexpr int kPasses = 8; };
+
+// ---- scene bounds (SceneConverter.cpp:28-60 on the device) -----------------
+__global__ void __launch_bounds__(256) k_bounds_partial(const float4* __restrict__ v, uint64_t nv,
+                                                         float* __restrict__ partial) {
+    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+    float mx[3] = {FLT_MIN, FLT_MIN, FLT_MIN};
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nv;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float4 p = __ldg(v + i);
+        mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
+        mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = fminf(mn[k], __shfl_xor_sync(kFull, mn[k], o));
+            mx[k] = fmaxf(mx[k], __shfl_xor_sync(kFull, mx[k], o));
+        }
+    __shared__ float s[8][6];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+        for (int k = 0; k < 3; ++k) { s[w][k] = mn[k]; s[w][3 + k] = mx[k]; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 1; j < (int)(blockDim.x >> 5); ++j)
+            for (int k = 0; k < 3; ++k) {
+                s[0][k] = fminf(s[0][k], s[j][k]);
+                s[0][3 + k] = fmaxf(s[0][3 + k], s[j][3 + k]);
+            }
+        for (int k = 0; k < 6; ++k) partial[blockIdx.x * 6 + k] = s[0][k];
+    }
+}
+
+__global__ void k_bounds_final(const float* __restrict__ partial, int np, float* __restrict__ out) {
+    if (threadIdx.x != 0) return;
+    float r[6] = {FLT_MAX, FLT_MAX, FLT_MAX, FLT_MIN, FLT_MIN, FLT_MIN};
+    for (int j = 0; j < np; ++j)
+        for (int k = 0; k < 3; ++k) {
+            r[k] = fminf(r[k], partial[j * 6 + k]);
+            r[3 + k] = fmaxf(r[3 + k], partial[j * 6 + 3 + k]);
+        }
+    for (int k = 0; k < 6; ++k) out[k] = r[k];
+}
+
+// ---- Morton codes (LBVH.cu:14-97, Commons.cuh:426-510,606-662) ---------------
+__device__ __forceinline__ uint32_t expand10(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+__device__ __forceinline__ uint64_t expand21(uint64_t v) {
+    v &= 0x1fffffull;
+    v = (v | v << 32) & 0x1f00000000ffffull;
+    v = (v | v << 16) & 0x1f0000ff0000ffull;
+    v = (v | v << 8) & 0x100f00f00f00f00full;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+    v = (v | v << 2) & 0x1249249249249249ull;
+    return v;
+}
+
+template <typename K>
+__device__ __forceinline__ K morton_code(float cx, float cy, float cz, const float* b);
+
+template <>
+__device__ __forceinline__ uint32_t morton_code<uint32_t>(float cx, float cy, float cz, const float* b) {
+    const float c[3] = {cx, cy, cz};
+    uint32_t q[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float nrm = __fdiv_rn(__fsub_rn(c[k], b[k]), __fsub_rn(b[3 + k], b[k]));
+        q[k] = expand10(__float2uint_rz(fminf(fmaxf(__fmul_rn(nrm, 1024.0f), 0.0f), 1023.0f)));
+    }
+    return q[0] * 4u + q[1] * 2u + q[2];
+}
+template <>
+__device__ __forceinline__ uint64_t morton_code<uint64_t>(float cx, float cy, float cz, const float* b) {
+    const float c[3] = {cx, cy, cz};
+    uint64_t q[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float nrm = __fdiv_rn(__fsub_rn(c[k], b[k]), __fsub_rn(b[3 + k], b[k]));
+        q[k] = expand21(__float2ull_rz(fminf(fmaxf(__fmul_rn(nrm, 2097152.0f), 0.0f), 2097151.0f)));
+    }
+    return q[0] * 4u + q[1] * 2u + q[2];
+}
+
+// One triangle per iteration of a grid-stride loop; histograms of every
+// 8-bit digit are accumulated in shared memory and flushed once per block.
+template <typename K>
+__global__ void __launch_bounds__(256) k_morton(const float4* __restrict__ v, uint32_t n,
+                                                 const float* __restrict__ bounds, K* __restrict__ keys,
+                                                 uint32_t* __restrict__ hist) {
+    constexpr int P = KeyTraits<K>::kPasses;
+    __shared__ uint32_t sh[P * 256];
+    __shared__ float sb[6];
+    for (int j = threadIdx.x; j < P * 256; j += blockDim.x) sh[j] = 0;
+    if (threadIdx.x < 6) sb[threadIdx.x] = bounds[threadIdx.x];
+    __syncthreads();
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const float4 a = __ldg(v + 3 * (size_t)t), b = __ldg(v + 3 * (size_t)t + 1), c = __ldg(v + 3 * (size_t)t + 2);
+        const float cx = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.x, b.x), c.x), fminf(fminf(a.x, b.x), c.x)), 0.5f);
+        const float cy = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.y, b.y), c.y), fminf(fminf(a.y, b.y), c.y)), 0.5f);
+        const float cz = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.z, b.z), c.z), fminf(fminf(a.z, b.z), c.z)), 0.5f);
+        const K code = morton_code<K>(cx, cy, cz, sb);
+        keys[t] = code;
+        if (hist) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) atomicAdd(&sh[p * 256 + (uint32_t)((code >> (8 * p)) & 255u)], 1u);
+        }
+    }
+    if (!hist) return;
+    __syncthreads();
+    for (int j = threadIdx.x; j < P * 256; j += blockDim.x)
+        if (sh[j]) atomicAdd(&hist[j], sh[j]);
+}
+
+// Digit histogram of arbitrary keys (used by the generic sort entry point).
+template <typename K>
+__global__ void __launch_bounds__(256) k_histogram(const K* __restrict__ keys, uint32_t n,
+                                                    uint32_t* __restrict__ hist) {
+    constexpr int P = KeyTraits<K>::kPasses;
+    __shared__ uint32_t sh[P * 256];
+    for (int j = threadIdx.x; j < P * 256; j += blockDim.x) sh[j] = 0;
+    __syncthreads();
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const K code = keys[t];
+#pragma unroll
+        for (int p = 0; p < P; ++p) atomicAdd(&sh[p * 256 + (uint32_t)((code >> (8 * p)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < P * 256; j += blockDim.x)
+        if (sh[j]) atomicAdd(&hist[j], sh[j]);
+}
+
+// Exclusive scan of 256 values held one per thread of a 256-thread block.
+__device__ __forceinline__ uint32_t block_exclusive_scan256(uint32_t x, uint32_t* s_warp) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[w] = inc;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int j = 0; j < w; ++j) wbase += s_warp[j];
+    __syncthreads();
+    return wbase + inc - x;
+}
+
+// ---- onesweep radix sort pass ------------------------------------------------
+// Stable: keys of one digit keep their input order (tiles are numbered by an
+// atomic ticket so that every tile's predecessors are already running; each
+// warp ranks a contiguous run of the tile in order).  The per-tile digit
+// counts are combined across tiles by decoupled look-back; a wait that does
+// not resolve within kLookbackLimit polls sets kErrSortLookback and gives up.
+template <typename K, bool kIota>
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(
+        const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
+        uint32_t* __restrict__ vout, uint32_t n, int shift, const uint32_t* __restrict__ hist,
+        uint32_t* __restrict__ status, uint32_t* __restrict__ ticket, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K* s_keys = reinterpret_cast<K*>(smem_raw);
+    uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_keys + kSortTile);
+    __shared__ uint32_t s_wh[kSortWarps][256];
+    __shared__ uint32_t s_dstart[256];
+    __shared__ uint32_t s_gbase[256];
+    __shared__ uint32_t s_scan[kSortWarps];
+    __shared__ uint32_t s_tile;
+
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    for (int j = threadIdx.x; j < kSortWarps * 256; j += kSortThreads) (&s_wh[0][0])[j] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t base = (uint64_t)tile * kSortTile;
+    const uint32_t valid_n = (uint32_t)min((uint64_t)kSortTile, (uint64_t)n - base);
+
+    K key[kSortItems];
+    uint32_t val[kSortItems];
+    uint32_t rank[kSortItems];
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const uint64_t idx = base + (uint64_t)w * (kSortItems * 32) + r * 32 + lane;
+        const bool valid = idx < n;
+        key[r] = valid ? kin[idx] : (K)0;
+        val[r] = kIota ? (uint32_t)idx : (valid ? vin[idx] : 0u);
+        const uint32_t d = valid ? (uint32_t)((key[r] >> shift) & 255u) : 256u;
+        const uint32_t peers = __match_any_sync(kFull, d);
+        const uint32_t before = __popc(peers & lt);
+        uint32_t cnt = 0;
+        if (valid) cnt = s_wh[w][d];
+        __syncwarp();
+        if (valid && before == 0) s_wh[w][d] = cnt + __popc(peers);
+        __syncwarp();
+        rank[r] = valid ? cnt + before : 0xffffffffu;
+    }
+    __syncthreads();
+
+    // Per-digit exclusive offsets across warps, tile totals, digit starts.
+    const uint32_t d = threadIdx.x;
+    uint32_t run = 0;
+#pragma unroll
+    for (int j = 0; j < kSortWarps; ++j) {
+        const uint32_t c = s_wh[j][d];
+        s_wh[j][d] = run;
+        run += c;
+    }
+    const uint32_t count = run;
+    s_dstart[d] = block_exclusive_scan256(count, s_scan);
+    const uint32_t gdigit = block_exclusive_scan256(hist[d], s_scan);
+
+    // Decoupled look-back for digit d.
+    uint32_t* st = status + (size_t)tile * 256 + d;
+    uint32_t prefix = 0;
+    if (tile == 0) {
+        __stcg(st, kFlagInc | count);
+    } else {
+        __stcg(st, kFlagAgg | count);
+        int64_t k = (int64_t)tile - 1;
+        uint32_t polls = 0;
+        while (k >= 0) {
+            const uint32_t s = *reinterpret_cast<volatile uint32_t*>(status + (size_t)k * 256 + d);
+            if (s & kFlagInc) { prefix += s & kValueMask; break; }
+            if (s & kFlagAgg) { prefix += s & kValueMask; --k; continue; }
+            if (++polls > kLookbackLimit) { set_error_bits(err, kErrSortLookback); break; }
+        }
+        __threadfence();
+        __stcg(st, kFlagInc | (prefix + count));
+    }
+    s_gbase[d] = gdigit + prefix - s_dstart[d];
+    __syncthreads();
+
+    // Scatter into shared memory in digit order, then write out coalesced.
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        if (rank[r] == 0xffffffffu) continue;
+        const uint32_t dd = (uint32_t)((key[r] >> shift) & 255u);
+        const uint32_t p = s_dstart[dd] + s_wh[w][dd] + rank[r];
+        s_keys[p] = key[r];
+        s_vals[p] = val[r];
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < valid_n; i += kSortThreads) {
+        const K kk = s_keys[i];
+        const uint32_t dd = (uint32_t)((kk >> shift) & 255u);
+        const uint32_t dst = s_gbase[dd] + i;
+        if (dst < n) {  // holds whenever hist matches the keys
+            kout[dst] = kk;
+            vout[dst] = s_vals[i];
+        }
+    }
+}
+
+// ---- fused Karras build + refit ------------------------------------------------
+// Common prefix of the adjacent sorted pairs (k, k+1) with the reference's
+// index tie-break (LBVH.cu:163-201).
+__device__ __forceinline__ int delta_adj(const uint32_t* keys, int k) {
+    const uint32_t a = keys[k], b = keys[k + 1];
+    return a == b ? 32 + __clz(k ^ (k + 1)) : __clz(a ^ b);
+}
+__device__ __forceinline__ int delta_adj(const uint64_t* keys, int k) {
+    const uint64_t a = keys[k], b = keys[k + 1];
+    return a == b ? 64 + __clzll((long long)(k ^ (k + 1))) : __clzll((long long)(a ^ b));
+}
+
+// One thread per sorted leaf climbs while it is the second of two siblings to
+// arrive (an atomic exchange on the parent's split position carries the
+// first arrival's far range end).  Each node's record is written once.
+template <typename K>
+__global__ void __launch_bounds__(256) k_build(const K* __restrict__ keys, const uint32_t* __restrict__ sidx,
+                                                const float4* __restrict__ verts, uint32_t n,
+                                                int32_t* __restrict__ parent, int32_t* __restrict__ left,
+                                                int32_t* __restrict__ right, int32_t* __restrict__ data,
+                                                float4* __restrict__ bmin, float4* __restrict__ bmax,
+                                                float* __restrict__ area, int32_t* __restrict__ slot) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t tri = sidx[i];
+    const float4 a = __ldg(verts + 3 * (size_t)tri), b = __ldg(verts + 3 * (size_t)tri + 1),
+                 c = __ldg(verts + 3 * (size_t)tri + 2);
+    float4 mn = make_float4(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z), 0.0f);
+    float4 mx = make_float4(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z), 0.0f);
+    const int leaf = (int)i + (int)n - 1;
+    left[leaf] = -1;
+    right[leaf] = -1;
+    data[leaf] = (int32_t)tri;
+    bmin[leaf] = mn;
+    bmax[leaf] = mx;
+    area[leaf] = box_area(mn, mx);
+
+    const int last = (int)n - 1;
+    int l = (int)i, r = (int)i;
+    int dl = l > 0 ? delta_adj(keys, l - 1) : -1;
+    int dr = r < last ? delta_adj(keys, r) : -1;
+    while (true) {
+        const bool is_left = dr > dl;
+        const int split = is_left ? r : l - 1;
+        __threadfence();
+        const int other = atomicExch(&slot[split], is_left ? l : r);
+        if (other < 0) return;  // first of the two children: the sibling finishes the parent
+        __threadfence();
+        const int pl = is_left ? l : other;
+        const int pr = is_left ? other : r;
+        const int lc = split == pl ? split + last : split;
+        const int rc = split + 1 == pr ? split + 1 + last : split + 1;
+        const int sib = is_left ? rc : lc;
+        const float4 smn = ld_cg(bmin + sib), smx = ld_cg(bmax + sib);
+        mn = make_float4(fminf(mn.x, smn.x), fminf(mn.y, smn.y), fminf(mn.z, smn.z), 0.0f);
+        mx = make_float4(fmaxf(mx.x, smx.x), fmaxf(mx.y, smx.y), fmaxf(mx.z, smx.z), 0.0f);
+        const bool root = pl == 0 && pr == last;
+        int p = 0;
+        if (!root) {
+            dl = pl > 0 ? delta_adj(keys, pl - 1) : -1;
+            dr = pr < last ? delta_adj(keys, pr) : -1;
+            p = dr > dl ? pr : pl;
+        }
+        left[p] = lc;
+        right[p] = rc;
+        data[p] = -1;
+        parent[lc] = p;
+        parent[rc] = p;
+        bmin[p] = mn;
+        bmax[p] = mx;
+        area[p] = box_area(mn, mx);
+        if (root) {
+            parent[0] = -1;
+            return;
+        }
+        l = pl;
+        r = pr;
+    }
+}
+
+// ---- refit of an existing topology ---------------------------------------------
+__global__ void __launch_bounds__(256) k_refit(const float4* __restrict__ verts, uint32_t n,
+                                                const int32_t* __restrict__ parent,
+                                                const int32_t* __restrict__ left,
+                                                const int32_t* __restrict__ right,
+                                                const int32_t* __restrict__ data,
+                                                float4* __restrict__ bmin, float4* __restrict__ bmax,
+                                                float* __restrict__ area, uint32_t* __restrict__ counters) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int leaf = (int)i + (int)n - 1;
+    const uint32_t tri = (uint32_t)data[leaf];
+    const float4 a = __ldg(verts + 3 * (size_t)tri), b = __ldg(verts + 3 * (size_t)tri + 1),
+                 c = __ldg(verts + 3 * (size_t)tri + 2);
+    float4 mn = make_float4(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z), 0.0f);
+    float4 mx = make_float4(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z), 0.0f);
+    bmin[leaf] = mn;
+    bmax[leaf] = mx;
+    area[leaf] = box_area(mn, mx);
+    int cur = parent[leaf];
+    while (cur >= 0) {
+        __threadfence();
+        if (atomicAdd(&counters[cur], 1u) == 0u) return;
+        __threadfence();
+        const int l = left[cur], r = right[cur];
+        const float4 lm = ld_cg(bmin + l), lx = ld_cg(bmax + l), rm = ld_cg(bmin + r), rx = ld_cg(bmax + r);
+        mn = make_float4(fminf(lm.x, rm.x), fminf(lm.y, rm.y), fminf(lm.z, rm.z), 0.0f);
+        mx = make_float4(fmaxf(lx.x, rx.x), fmaxf(lx.y, rx.y), fmaxf(lx.z, rx.z), 0.0f);
+        bmin[cur] = mn;
+        bmax[cur] = mx;
+        area[cur] = box_area(mn, mx);
+        cur = parent[cur];
+    }
+}
+
+int grid_for(atr_ctx* ctx, uint64_t work, int per_sm_blocks, int threads) {
+    const uint64_t need = (work + threads - 1) / threads;
+    const uint64_t cap = (uint64_t)ctx->num_sms * per_sm_blocks;
+    return (int)(need < cap ? (need ? need : 1) : cap);
+}
+
+// Sort (key, value) pairs in place.  keys/vals hold the input and receive the
+// output (every key width uses an even number of passes).  hist must hold the
+// digit histograms of every pass (P x 256) when hist_ready; otherwise it is
+// computed here.  kIota passes generate the initial values.
+template <typename K>
+int sort_pairs(atr_ctx* ctx, K* keys, uint32_t* vals, uint32_t n, uint32_t* hist, bool hist_ready,
+               bool iota) {
+    constexpr int P = KeyTraits<K>::kPasses;
+    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    const size_t sbytes = (size_t)P * tiles * 256 * 4;
+    void* tmp = nullptr;
+    const size_t kb = align256((size_t)n * sizeof(K)), vb = align256((size_t)n * 4);
+    const size_t hb = hist ? 0 : align256(P * 256 * 4);
+    ATR_TRY(ctx->alloc(&tmp, kb + vb + align256(sbytes) + 256 + hb));
+    char* p = static_cast<char*>(tmp);
+    K* k2 = reinterpret_cast<K*>(p); p += kb;
+    uint32_t* v2 = reinterpret_cast<uint32_t*>(p); p += vb;
+    uint32_t* status = reinterpret_cast<uint32_t*>(p); p += align256(sbytes);
+    uint32_t* tickets = reinterpret_cast<uint32_t*>(p); p += 256;
+    if (!hist) hist = reinterpret_cast<uint32_t*>(p);
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaMemsetAsync(status, 0, align256(sbytes) + 256, s);
+    if (e != cudaSuccess) { ctx->release(tmp); return cuda_fail(e, "cudaMemsetAsync", __FILE__, __LINE__); }
+    if (!hist_ready) {
+        cudaMemsetAsync(hist, 0, P * 256 * 4, s);
+        k_histogram<K><<<grid_for(ctx, n, 4, 256), 256, 0, s>>>(keys, n, hist);
+    }
+    const size_t smem = (size_t)kSortTile * (sizeof(K) + 4);
+    cudaFuncSetAttribute(k_onesweep<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_onesweep<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    K* ka = keys; K* kb2 = k2;
+    uint32_t* va = vals; uint32_t* vb2 = v2;
+    for (int pass = 0; pass < P; ++pass) {
+        uint32_t* st = status + (size_t)pass * tiles * 256;
+        if (pass == 0 && iota)
+            k_onesweep<K, true><<<tiles, kSortThreads, smem, s>>>(ka, va, kb2, vb2, n, 8 * pass,
+                                                                  hist + pass * 256, st, tickets + pass, ctx->d_error);
+        else
+            k_onesweep<K, false><<<tiles, kSortThreads, smem, s>>>(ka, va, kb2, vb2, n, 8 * pass,
+                                                                   hist + pass * 256, st, tickets + pass, ctx->d_error);
+        std::swap(ka, kb2);
+        std::swap(va, vb2);
+    }
+    e = cudaGetLastError();
+    ctx->release(tmp);
+    if (e != cudaSuccess) return cuda_fail(e, "k_onesweep launch", __FILE__, __LINE__);
+    return ATR_OK;
+}
+
+template <typename K>
+int build_typed(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds, atr_tree* t) {
+    constexpr int P = KeyTraits<K>::kPasses;
+    cudaStream_t s = ctx->stream;
+    void* keys = nullptr;
+    void* idx = nullptr;
+    void* aux = nullptr;
+    ATR_TRY(ctx->alloc(&keys, (size_t)n * sizeof(K)));
+    int st = ctx->alloc(&idx, (size_t)n * 4);
+    if (st == ATR_OK) st = ctx->alloc(&aux, align256(P * 256 * 4) + align256((size_t)(n - 1) * 4));
+    if (st != ATR_OK) { ctx->release(keys); ctx->release(idx); return st; }
+    uint32_t* hist = static_cast<uint32_t*>(aux);
+    int32_t* slot = reinterpret_cast<int32_t*>(static_cast<char*>(aux) + align256(P * 256 * 4));
+    cudaMemsetAsync(hist, 0, P * 256 * 4, s);
+    cudaMemsetAsync(slot, 0xff, (size_t)(n - 1) * 4, s);
+
+    ctx->phase_begin("morton");
+    k_morton<K><<<grid_for(ctx, n, 8, 256), 256, 0, s>>>(verts, n, d_bounds, static_cast<K*>(keys), hist);
+    ctx->phase_end();
+    ctx->phase_begin("sort");
+    st = sort_pairs<K>(ctx, static_cast<K*>(keys), static_cast<uint32_t*>(idx), n, hist, true, true);
+    ctx->phase_end();
+    if (st == ATR_OK) {
+        ctx->phase_begin("build");
+        k_build<K><<<(n + 255) / 256, 256, 0, s>>>(static_cast<K*>(keys), static_cast<uint32_t*>(idx), verts, n,
+                                                  t->parent, t->left, t->right, t->data, t->bmin, t->bmax,
+                                                  t->area, slot);
+        ctx->phase_end();
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "k_build launch", __FILE__, __LINE__);
+    }
+    ctx->release(aux);
+    if (st != ATR_OK) { ctx->release(keys); ctx->release(idx); return st; }
+    ctx->release(t->sorted_keys);
+    ctx->release(t->sorted_idx);
+    t->sorted_keys = keys;
+    t->sorted_idx = static_cast<uint32_t*>(idx);
+    return ATR_OK;
+}
+
+}  // namespace
+
+int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds, int morton_bits,
+                    atr_tree* t) {
+    t->morton_bits = morton_bits;
+    if (morton_bits == 30) return build_typed<uint32_t>(ctx, verts, n, d_bounds, t);
+    return build_typed<uint64_t>(ctx, verts, n, d_bounds, t);
+}
+
+int refit_tree(atr_ctx* ctx, atr_tree* t, const float4* verts) {
+    const uint32_t n = t->n;
+    void* ctr = nullptr;
+    ATR_TRY(ctx->alloc(&ctr, (size_t)(n - 1) * 4));
+    cudaMemsetAsync(ctr, 0, (size_t)(n - 1) * 4, ctx->stream);
+    k_refit<<<(n + 255) / 256, 256, 0, ctx->stream>>>(verts, n, t->parent, t->left, t->right, t->data, t->bmin,
+                                                      t->bmax, t->area, static_cast<uint32_t*>(ctr));
+    cudaError_t e = cudaGetLastError();
+    ctx->release(ctr);
+    if (e != cudaSuccess) return cuda_fail(e, "k_refit launch", __FILE__, __LINE__);
+    return ATR_OK;
+}
+
+int scene_bounds_device(atr_ctx* ctx, const float4* verts, uint32_t n, float* d_out) {
+    const uint64_t nv = 3ull * n;
+    const int blocks = grid_for(ctx, nv, 2, 256);
+    void* part = nullptr;
+    ATR_TRY(ctx->alloc(&part, (size_t)blocks * 6 * 4));
+    k_bounds_partial<<<blocks, 256, 0, ctx->stream>>>(verts, nv, static_cast<float*>(part));
+    k_bounds_final<<<1, 32, 0, ctx->stream>>>(static_cast<float*>(part), blocks, d_out);
+    cudaError_t e = cudaGetLastError();
+    ctx->release(part);
+    if (e != cudaSuccess) return cuda_fail(e, "k_bounds launch", __FILE__, __LINE__);
+    return ATR_OK;
+}
+
+}  // namespace atr
+
+using namespace atr;
+
+extern "C" {
+
+int atr_scene_create(atr_ctx* ctx, const float* vertices, uint32_t n, const float* bbmin, const float* bbmax,
+                     int on_device, atr_scene** out) {
+    ATR_REQUIRE(ctx && vertices && out, ATR_ERR_INVALID_ARG, "atr_scene_create: NULL argument");
+    ATR_REQUIRE(n >= 2 && n < (1u << 30), ATR_ERR_INVALID_ARG,
+                "atr_scene_create: triangle count %u outside [2, 2^30)", n);
+    ATR_REQUIRE((bbmin == nullptr) == (bbmax == nullptr), ATR_ERR_INVALID_ARG,
+                "atr_scene_create: give both bounds or neither");
+    *out = nullptr;
+    atr_scene* s = new atr_scene();
+    s->ctx = ctx;
+    s->n = n;
+    int st = ctx->alloc(reinterpret_cast<void**>(&s->verts), (size_t)n * 48);
+    if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&s->d_bounds), 256);
+    if (st != ATR_OK) { atr_scene_destroy(s); return st; }
+    cudaError_t e = cudaMemcpyAsync(s->verts, vertices, (size_t)n * 48,
+                                    on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) { atr_scene_destroy(s); return cuda_fail(e, "cudaMemcpyAsync(vertices)", __FILE__, __LINE__); }
+    if (bbmin) {
+        float h[6] = {bbmin[0], bbmin[1], bbmin[2], bbmax[0], bbmax[1], bbmax[2]};
+        e = cudaMemcpyAsync(s->d_bounds, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // h is a stack array
+        if (e != cudaSuccess) { atr_scene_destroy(s); return cuda_fail(e, "cudaMemcpyAsync(bounds)", __FILE__, __LINE__); }
+    } else {
+        st = scene_bounds_device(ctx, s->verts, n, s->d_bounds);
+        if (st != ATR_OK) { atr_scene_destroy(s); return st; }
+    }
+    *out = s;
+    return ATR_OK;
+}
+
+int atr_scene_set_vertices(atr_ctx* ctx, atr_scene* s, const float* vertices, int on_device) {
+    ATR_REQUIRE(ctx && s && vertices, ATR_ERR_INVALID_ARG, "atr_scene_set_vertices: NULL argument");
+    ATR_CUDA(cudaMemcpyAsync(s->verts, vertices, (size_t)s->n * 48,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    return ATR_OK;
+}
+
+int atr_build_lbvh(atr_ctx* ctx, const atr_scene* scene, int morton_bits, atr_tree** out) {
+    ATR_REQUIRE(ctx && scene && out, ATR_ERR_INVALID_ARG, "atr_build_lbvh: NULL argument");
+    ATR_REQUIRE(morton_bits == 30 || morton_bits == 63, ATR_ERR_UNSUPPORTED,
+                "atr_build_lbvh: morton_bits must be 30 or 63 (got %d)", morton_bits);
+    *out = nullptr;
+    atr_tree* t = nullptr;
+    ATR_TRY(tree_alloc(ctx, scene->n, &t));
+    int st = lbvh_build_into(ctx, scene->verts, scene->n, scene->d_bounds, morton_bits, t);
+    if (st != ATR_OK) { atr_tree_destroy(t); return st; }
+    *out = t;
+    return ATR_OK;
+}
+
+int atr_refit(atr_ctx* ctx, atr_tree* tree, const atr_scene* scene) {
+    ATR_REQUIRE(ctx && tree && scene, ATR_ERR_INVALID_ARG, "atr_refit: NULL argument");
+    ATR_REQUIRE(tree->n == scene->n, ATR_ERR_INVALID_ARG, "atr_refit: tree has %u triangles, scene %u",
+                tree->n, scene->n);
+    return refit_tree(ctx, tree, scene->verts);
+}
+
+int atr_device_morton(atr_ctx* ctx, const float* vertices, uint32_t n, const float* bbmin, const float* bbmax,
+                      int morton_bits, void* keys) {
+    ATR_REQUIRE(ctx && vertices && bbmin && bbmax && keys, ATR_ERR_INVALID_ARG, "atr_device_morton: NULL argument");
+    ATR_REQUIRE(morton_bits == 30 || morton_bits == 63, ATR_ERR_UNSUPPORTED, "atr_device_morton: bits %d", morton_bits);
+    ATR_REQUIRE(n > 0, ATR_ERR_INVALID_ARG, "atr_device_morton: no triangles");
+    void* b = nullptr;
+    ATR_TRY(ctx->alloc(&b, 32));
+    float h[6] = {bbmin[0], bbmin[1], bbmin[2], bbmax[0], bbmax[1], bbmax[2]};
+    cudaMemcpyAsync(b, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream);
+    const float4* v = reinterpret_cast<const float4*>(vertices);
+    if (morton_bits == 30)
+        k_morton<uint32_t><<<grid_for(ctx, n, 8, 256), 256, 0, ctx->stream>>>(v, n, static_cast<float*>(b),
+                                                                               static_cast<uint32_t*>(keys), nullptr);
+    else
+        k_morton<uint64_t><<<grid_for(ctx, n, 8, 256), 256, 0, ctx->stream>>>(v, n, static_cast<float*>(b),
+                                                                               static_cast<uint64_t*>(keys), nullptr);
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);  // h is a stack array
+    ctx->release(b);
+    if (e != cudaSuccess) return cuda_fail(e, "k_morton", __FILE__, __LINE__);
+    return ATR_OK;
+}
+
+int atr_device_sort_pairs(atr_ctx* ctx, void* keys, uint32_t* values, uint32_t count, int key_bits) {
+    ATR_REQUIRE(ctx && keys && values, ATR_ERR_INVALID_ARG, "atr_device_sort_pairs: NULL argument");
+    ATR_REQUIRE(count < (1u << 30), ATR_ERR_INVALID_ARG, "atr_device_sort_pairs: count %u >= 2^30", count);
+    if (count == 0) return ATR_OK;
+    if (key_bits <= 32) return sort_pairs<uint32_t>(ctx, static_cast<uint32_t*>(keys), values, count, nullptr, false, false);
+    return sort_pairs<uint64_t>(ctx, static_cast<uint64_t*>(keys), values, count, nullptr, false, false);
+}
+
+}  // extern "C"

@@ -1,0 +1,211 @@
+/*
+ * atrbvh.h -- C ABI of the B200 ATRBVH build-and-traverse library.
+ *
+ * Every entry point returns an int status (ATR_OK = 0); atr_last_error()
+ * gives a message for the calling thread.  Nothing calls exit().  All device
+ * work is enqueued on the context's CUDA stream; functions that return host
+ * data synchronise that stream.  Plain pointers and sizes only: vertices are
+ * three float4 per triangle (x, y, z, w; w ignored), node boxes are float4.
+ *
+ * Each declaration names the reference interface it replaces
+ * (leonardo-domingues/atrbvh, paths relative to the project root).
+ */
+#ifndef ATRBVH_H
+#define ATRBVH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum atr_status {
+    ATR_OK = 0,
+    ATR_ERR_INVALID_ARG = 1,  /* bad size, pointer or parameter */
+    ATR_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    ATR_ERR_OOM = 3,          /* device allocation failed */
+    ATR_ERR_UNSUPPORTED = 4,  /* parameter outside the supported range */
+    ATR_ERR_DEVICE_WAIT = 5,  /* a bounded device-side wait gave up */
+    ATR_ERR_NO_DEVICE = 6     /* no CUDA device / wrong architecture */
+};
+
+enum atr_scene_kind { ATR_SCENE_UNIFORM = 0, ATR_SCENE_CLUSTERED = 1 };
+
+typedef struct atr_ctx atr_ctx;
+typedef struct atr_scene atr_scene;
+typedef struct atr_tree atr_tree;
+typedef struct atr_collapsed atr_collapsed;
+typedef struct atr_compact atr_compact;
+typedef struct atr_batch atr_batch;
+
+/* Device-resident tree in the reference's structure-of-arrays layout
+ * (BVHRT-Core/src/SoABVHTree.h:21-34): 2N-1 nodes, internal nodes [0, N-2],
+ * leaves [N-1, 2N-2], root 0.  Leaves have left = right = -1 and data = the
+ * triangle index; internal nodes have data = -1; the root's parent is -1. */
+typedef struct atr_tree_view {
+    uint32_t num_triangles;
+    int32_t root;
+    int32_t* parent;
+    int32_t* left;
+    int32_t* right;
+    int32_t* data;
+    float* bbox_min; /* float4 per node */
+    float* bbox_max; /* float4 per node */
+    float* area;
+} atr_tree_view;
+
+/* Collapsed tree (BVHRT-Core/src/BVHCollapsedTree.h:9-58).  A node with
+ * data >= 0 is a leaf: with triangle_count > 1, data is the offset of its
+ * triangle list in triangle_indices; otherwise data is the triangle index. */
+typedef struct atr_collapsed_view {
+    uint32_t num_triangles;
+    int32_t root;
+    int32_t* parent;
+    int32_t* left;
+    int32_t* right;
+    int32_t* data;
+    int32_t* triangle_count;
+    float* bbox_min;
+    float* bbox_max;
+    int32_t* triangle_indices; /* num_triangles entries */
+} atr_collapsed_view;
+
+/* Compact2 traversal layout (gpu-ray-traversal/src/rt/cuda/CudaBVH.hpp:41-55):
+ * 64-byte nodes of child boxes (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y),
+ * (c1 ...), (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z), (child0, child1, 0, 0) where
+ * an inner child is its float4 offset and a leaf child is ~(float4 offset of
+ * its first Woop triangle); three float4 per Woop triangle and a float4 of
+ * 0x80000000 after each leaf; tri_index holds the triangle id at each
+ * triangle's first float4. */
+typedef struct atr_compact_view {
+    int64_t num_nodes;
+    int64_t num_woop;
+    int32_t* nodes;     /* 16 int32 per node */
+    float* woop;        /* 4 floats per entry */
+    int32_t* tri_index; /* one per Woop float4 entry */
+    int32_t max_depth;  /* deepest inner-node level (root = 1) */
+} atr_compact_view;
+
+/* ---- errors, version ------------------------------------------------- */
+const char* atr_last_error(void);
+const char* atr_version(void);
+
+/* ---- context: one per host thread; owns a stream and scratch ---------
+ * Replaces the reference's implicit legacy default stream
+ * (BVHRT-Core/src/TimeKernelExecution.h:14-32) and checkCudaError/exit
+ * (BVHRT-Core/src/CudaErrorCheck.h:12-23).  stream may be NULL (a new stream
+ * is created) or a cudaStream_t the caller keeps ownership of. */
+int atr_ctx_create(int device, void* stream, atr_ctx** out);
+int atr_ctx_destroy(atr_ctx* ctx);
+int atr_ctx_synchronize(atr_ctx* ctx); /* also reports device-side errors */
+int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
+/* Per-phase CUDA-event timing of the next builds (milliseconds). */
+int atr_ctx_set_timing(atr_ctx* ctx, int enable);
+int atr_ctx_phase_times(atr_ctx* ctx, float* ms, int capacity, int* count);
+
+/* ---- scene -------------------------------------------------------------
+ * Replaces BVHRT::SceneWrapper(numberOfTriangles, float4* vertices, float3
+ * bbMin, float3 bbMax) (BVHRT-Core/src/SceneWrapper.h:25-26; H2D upload at
+ * SceneWrapper.cpp:24-29).  bbox_min/bbox_max (3 floats each) may be NULL: the
+ * scene box is then reduced on the device, seeding the maximum with the
+ * smallest positive normal float as gpu-ray-traversal/src/rt/SceneConverter.cpp:31-34
+ * does.  vertices_on_device != 0: vertices is a device pointer that is copied. */
+int atr_scene_create(atr_ctx* ctx, const float* vertices, uint32_t num_triangles,
+                     const float* bbox_min, const float* bbox_max, int vertices_on_device,
+                     atr_scene** out);
+int atr_scene_destroy(atr_scene* scene);
+int atr_scene_bounds(atr_ctx* ctx, const atr_scene* scene, float* bbox_min, float* bbox_max);
+int atr_scene_device_vertices(const atr_scene* scene, float** vertices, uint32_t* num_triangles);
+/* Replace the vertex positions (same triangle count) for a refit. */
+int atr_scene_set_vertices(atr_ctx* ctx, atr_scene* scene, const float* vertices,
+                           int vertices_on_device);
+
+/* ---- LBVH ----------------------------------------------------------------
+ * Replaces BVHRT::LBVHBuilder::BuildTree(const SceneWrapper*)
+ * (BVHRT-Core/src/LBVHBuilder.h:31, LBVHBuilder.cpp:21-130).  morton_bits is
+ * 30 (LBVHBuilder(false)) or 63 (LBVHBuilder(true)). */
+int atr_build_lbvh(atr_ctx* ctx, const atr_scene* scene, int morton_bits, atr_tree** out);
+int atr_tree_destroy(atr_tree* tree);
+/* BVHTreeInstanceManager::FreeDeviceTree (BVHTreeInstanceManager.h:67). */
+int atr_tree_view_get(const atr_tree* tree, atr_tree_view* view);
+/* BVHTreeInstanceManager::DeviceToHostTree (BVHTreeInstanceManager.h:57):
+ * copies the arrays to host buffers (2N-1 entries; float4 per node box);
+ * any pointer may be NULL. */
+int atr_tree_download(atr_ctx* ctx, const atr_tree* tree, int32_t* parent, int32_t* left,
+                      int32_t* right, int32_t* data, float* bbox_min, float* bbox_max,
+                      float* area);
+/* SoABVHTree::SAH (BVHRT-Core/src/SoABVHTree.cpp:50-74): the reference's
+ * sequential float sum over the areas, evaluated on the host after a copy. */
+int atr_tree_sah(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, float* sah);
+/* Sorted Morton keys (as uint64) and triangle order kept from the last build
+ * of this tree (the reference's sort output, CubWrapper.cu:37). */
+int atr_tree_sorted_keys(atr_ctx* ctx, const atr_tree* tree, uint64_t* keys, uint32_t* indices);
+
+/* ---- low-level device entry points (LBVH.h:20-155, CubWrapper.h:18-34) ----
+ * Device pointers; keys are uint32 (bits 30) or uint64 (bits 63). */
+int atr_device_morton(atr_ctx* ctx, const float* vertices, uint32_t num_triangles,
+                      const float* bbox_min, const float* bbox_max, int morton_bits,
+                      void* keys);
+int atr_device_sort_pairs(atr_ctx* ctx, void* keys, uint32_t* values, uint32_t count,
+                          int key_bits);
+
+/* ---- optimisers ------------------------------------------------------------
+ * AgglomerativeTreeletOptimizer(treeletSize, iterations)::Optimize
+ * (BVHRT-Core/src/AgglomerativeTreeletOptimizer.h:24, .cpp:24-110); treelet
+ * sizes 3..20 (the reference's shared-memory kernel range). */
+int atr_optimize_atrbvh(atr_ctx* ctx, atr_tree* tree, int treelet_size, int iterations,
+                        float ci, float ct);
+/* TRBVHOptimizer(treeletSize, iterations)::Optimize
+ * (BVHRT-Core/src/TRBVHOptimizer.h:27, .cpp:21-128); treelet size 7. */
+int atr_optimize_trbvh(atr_ctx* ctx, atr_tree* tree, int treelet_size, int iterations,
+                       float ci, float ct);
+/* Bottom-up box refit of an existing topology from the scene's current
+ * vertices (the refit pass of BVHRT-Core/src/LBVH.cu:465-570 on a resident tree). */
+int atr_refit(atr_ctx* ctx, atr_tree* tree, const atr_scene* scene);
+
+/* ---- collapse ----------------------------------------------------------------
+ * BVHTreeCollapser::Collapse(BVHTree*, float* sah, ci, ct)
+ * (BVHRT-Core/src/BVHTreeCollapser.h:39, .cpp:21-93).  max_leaf = 0 reproduces
+ * the reference (no leaf-size limit); max_leaf > 0 also forbids collapsing
+ * subtrees with more triangles.  sah receives cost[root] / area[root]. */
+int atr_collapse(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int max_leaf,
+                 atr_collapsed** out, float* sah);
+int atr_collapsed_destroy(atr_collapsed* collapsed);
+int atr_collapsed_view_get(const atr_collapsed* collapsed, atr_collapsed_view* view);
+/* BVHTreeInstanceManager::DeviceToHostCollapsedTree (BVHTreeInstanceManager.h:113). */
+int atr_collapsed_download(atr_ctx* ctx, const atr_collapsed* collapsed, int32_t* parent,
+                           int32_t* left, int32_t* right, int32_t* data,
+                           int32_t* triangle_count, float* bbox_min, float* bbox_max,
+                           int32_t* triangle_indices);
+
+/* ---- traversal layout + closest-hit traversal ------------------------------
+ * CudaBVH(const BVHCollapsedTree*, Scene*, BVHLayout_Compact2)
+ * (gpu-ray-traversal/src/rt/cuda/CudaBVH.cpp:60-79, createCompact :469-574,
+ * woopifyTri :579-600), built on the device. */
+int atr_flatten_compact2(atr_ctx* ctx, const atr_collapsed* collapsed, const atr_scene* scene,
+                         atr_compact** out);
+int atr_compact_destroy(atr_compact* compact);
+int atr_compact_view_get(const atr_compact* compact, atr_compact_view* view);
+/* The trace() kernel ABI (gpu-ray-traversal/src/rt/kernels/CudaTracerKernels.hpp:73-86,
+ * kepler_dynamic_fetch.cu:61-320): rays are float4 (origin, tmin), float4
+ * (direction, tmax) on the device; results are int4 (triangle id or -1,
+ * float bits of t, 0, 0) on the device. */
+int atr_trace(atr_ctx* ctx, const atr_compact* compact, const float* rays, int64_t num_rays,
+              int any_hit, int32_t* results);
+
+/* ---- synthetic workloads (host memory; deterministic in seed) ---------- */
+int atr_gen_scene(int kind, uint32_t num_triangles, uint64_t seed, float* vertices);
+int atr_gen_batch_sizes(uint32_t count, uint32_t min_tris, uint32_t max_tris, uint64_t seed,
+                        uint32_t* sizes);
+int atr_gen_batch_scene(uint32_t count, const uint32_t* sizes, uint64_t seed, float* vertices);
+int atr_gen_rays_pinhole(uint32_t width, uint32_t height, const float* eye, float fov_deg,
+                         float* rays);
+int atr_gen_rays_random(uint64_t count, uint64_t seed, const float* bbox_min,
+                        const float* bbox_max, float* rays);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ATRBVH_H */

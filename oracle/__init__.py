@@ -1,0 +1,294 @@
+"""ORACLE -- test infrastructure only.
+
+ctypes access to the CPU restatement (liboracle.so, from atr_oracle.cpp) and to
+the reference's own CUDA build (oracle/_ref/libbvhrt_ref*.so, from
+oracle/build.py).  Only tests/, __graft_entry__.smoke() and the CPU-baseline
+leg of bench.py use this package, and only as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libbvhrt_ref.so"
+REF_LIB_FMAD = HERE / "_ref" / "libbvhrt_ref_fmad.so"
+
+_p = C.c_void_p
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not ORACLE_LIB.exists():
+            from . import build
+            build.build_oracle()
+        _lib = C.CDLL(str(ORACLE_LIB))
+        L = _lib
+        L.orc_max_threads.restype = C.c_int
+        L.orc_scene_aabb.argtypes = [_p, C.c_uint32, _p, _p]
+        L.orc_morton.argtypes = [_p, C.c_uint32, _p, _p, _p, _p, C.c_int]
+        L.orc_sort_pairs32.argtypes = [_p, _p, C.c_uint32, C.c_int]
+        L.orc_sort_pairs64.argtypes = [_p, _p, C.c_uint32]
+        L.orc_karras.argtypes = [_p, _p, _p, C.c_uint32, _p, _p, _p, _p, C.c_int]
+        L.orc_refit.argtypes = [_p, C.c_uint32, _p, _p, _p, _p, _p, _p, _p, C.c_int]
+        L.orc_build_lbvh.argtypes = [_p, C.c_uint32, _p, _p, C.c_int, _p, _p, _p, _p, _p, _p, _p, _p, _p,
+                                     C.c_int]
+        L.orc_build_lbvh.restype = C.c_int
+        for f in (L.orc_atrbvh, L.orc_trbvh):
+            f.argtypes = [C.c_uint32, _p, _p, _p, _p, _p, _p, _p, C.c_int, C.c_int, C.c_float, C.c_float,
+                          C.c_int]
+            f.restype = C.c_int
+        L.orc_sah.argtypes = [C.c_uint32, _p, C.c_int, C.c_float, C.c_float]
+        L.orc_sah.restype = C.c_float
+        L.orc_collapse.argtypes = [C.c_uint32, _p, _p, _p, _p, _p, _p, _p, C.c_float, C.c_float, C.c_int,
+                                   _p, _p, _p, _p, _p, _p, _p, _p, _p]
+        L.orc_collapse.restype = C.c_float
+        L.orc_flatten_compact2.argtypes = [C.c_uint32, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p,
+                                           C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+        L.orc_flatten_compact2.restype = C.c_int
+        L.orc_trace.argtypes = [_p, _p, _p, _p, C.c_int64, C.c_int, _p, C.c_int]
+        L.orc_atrbvh_schedule.argtypes = [C.c_int, C.c_int, _p, C.c_int]
+        L.orc_atrbvh_schedule.restype = C.c_int
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def max_threads() -> int:
+    return lib().orc_max_threads()
+
+
+@dataclass
+class Tree:
+    parent: np.ndarray
+    left: np.ndarray
+    right: np.ndarray
+    data: np.ndarray
+    bbox_min: np.ndarray
+    bbox_max: np.ndarray
+    area: np.ndarray
+
+    @staticmethod
+    def empty(n: int) -> "Tree":
+        nn = 2 * n - 1
+        return Tree(*(np.zeros(nn, np.int32) for _ in range(4)), np.zeros((nn, 4), np.float32),
+                    np.zeros((nn, 4), np.float32), np.zeros(nn, np.float32))
+
+    def copy(self) -> "Tree":
+        return Tree(*(a.copy() for a in (self.parent, self.left, self.right, self.data, self.bbox_min,
+                                          self.bbox_max, self.area)))
+
+    @property
+    def n(self) -> int:
+        return (len(self.parent) + 1) // 2
+
+    def ptrs(self):
+        return [_ptr(a) for a in (self.parent, self.left, self.right, self.data, self.bbox_min, self.bbox_max,
+                                  self.area)]
+
+
+def scene_aabb(v: np.ndarray):
+    mn = np.zeros(3, np.float32)
+    mx = np.zeros(3, np.float32)
+    v = np.ascontiguousarray(v, np.float32)
+    lib().orc_scene_aabb(_ptr(v), v.shape[0], _ptr(mn), _ptr(mx))
+    return mn, mx
+
+
+def morton(v: np.ndarray, bbmin, bbmax, bits: int = 30, threads: int = 1) -> np.ndarray:
+    v = np.ascontiguousarray(v, np.float32)
+    mn = np.asarray(bbmin, np.float32)
+    mx = np.asarray(bbmax, np.float32)
+    n = v.shape[0]
+    if bits == 30:
+        k = np.empty(n, np.uint32)
+        lib().orc_morton(_ptr(v), n, _ptr(mn), _ptr(mx), _ptr(k), None, threads)
+    else:
+        k = np.empty(n, np.uint64)
+        lib().orc_morton(_ptr(v), n, _ptr(mn), _ptr(mx), None, _ptr(k), threads)
+    return k
+
+
+def sort_pairs(keys: np.ndarray, threads: int = 1):
+    k = np.ascontiguousarray(keys).copy()
+    idx = np.empty(len(k), np.uint32)
+    if k.dtype == np.uint32:
+        lib().orc_sort_pairs32(_ptr(k), _ptr(idx), len(k), threads)
+    else:
+        lib().orc_sort_pairs64(_ptr(k), _ptr(idx), len(k))
+    return k, idx
+
+
+def build_lbvh(v: np.ndarray, bbmin, bbmax, bits: int = 30, threads: int = 1):
+    """Returns (Tree, sorted_keys uint64, sorted_idx uint32)."""
+    v = np.ascontiguousarray(v, np.float32)
+    n = v.shape[0]
+    t = Tree.empty(n)
+    sk = np.empty(n, np.uint64)
+    si = np.empty(n, np.uint32)
+    mn = np.asarray(bbmin, np.float32)
+    mx = np.asarray(bbmax, np.float32)
+    rc = lib().orc_build_lbvh(_ptr(v), n, _ptr(mn), _ptr(mx), bits, *t.ptrs(), _ptr(sk), _ptr(si), threads)
+    if rc != 0:
+        raise ValueError(f"orc_build_lbvh rc={rc}")
+    return t, sk, si
+
+
+def atrbvh(t: Tree, treelet: int = 9, iterations: int = 2, ci: float = 1.2, ct: float = 1.0,
+           threads: int = 1) -> Tree:
+    out = t.copy()
+    rc = lib().orc_atrbvh(out.n, *out.ptrs(), treelet, iterations, ci, ct, threads)
+    if rc != 0:
+        raise ValueError(f"orc_atrbvh rc={rc}")
+    return out
+
+
+def trbvh(t: Tree, treelet: int = 7, iterations: int = 3, ci: float = 1.2, ct: float = 1.0,
+          threads: int = 1) -> Tree:
+    out = t.copy()
+    rc = lib().orc_trbvh(out.n, *out.ptrs(), treelet, iterations, ci, ct, threads)
+    if rc != 0:
+        raise ValueError(f"orc_trbvh rc={rc}")
+    return out
+
+
+def sah(t: Tree, ci: float = 1.2, ct: float = 1.0) -> float:
+    return float(lib().orc_sah(t.n, _ptr(t.area), 0, ci, ct))
+
+
+@dataclass
+class Collapsed:
+    parent: np.ndarray
+    left: np.ndarray
+    right: np.ndarray
+    data: np.ndarray
+    triangle_count: np.ndarray
+    bbox_min: np.ndarray
+    bbox_max: np.ndarray
+    triangle_indices: np.ndarray
+    cost: np.ndarray
+    sah: float
+
+
+def collapse(t: Tree, ci: float = 1.2, ct: float = 1.0, max_leaf: int = 0) -> Collapsed:
+    n = t.n
+    nn = 2 * n - 1
+    c = Collapsed(*(np.zeros(nn, np.int32) for _ in range(5)), np.zeros((nn, 4), np.float32),
+                  np.zeros((nn, 4), np.float32), np.full(n, -1, np.int32), np.zeros(nn, np.float32), 0.0)
+    s = lib().orc_collapse(n, _ptr(t.parent), _ptr(t.left), _ptr(t.right), _ptr(t.data), _ptr(t.bbox_min),
+                           _ptr(t.bbox_max), _ptr(t.area), ci, ct, max_leaf, _ptr(c.parent), _ptr(c.left),
+                           _ptr(c.right), _ptr(c.data), _ptr(c.triangle_count), _ptr(c.bbox_min),
+                           _ptr(c.bbox_max), _ptr(c.triangle_indices), _ptr(c.cost))
+    c.sah = float(s)
+    return c
+
+
+def leaf_lists(left, right, data, count, tri_indices, n: int) -> dict:
+    """Map each leaf reachable from the root of a collapsed tree to its triangle list."""
+    out = {}
+    stack = [0]
+    while stack:
+        x = stack.pop()
+        for ch in (int(left[x]), int(right[x])):
+            if data[ch] >= 0:
+                if count[ch] > 1:
+                    off = int(data[ch])
+                    out[ch] = tuple(int(i) for i in tri_indices[off:off + int(count[ch])])
+                else:
+                    out[ch] = (int(data[ch]),)
+            else:
+                stack.append(ch)
+    return out
+
+
+@dataclass
+class Compact:
+    nodes: np.ndarray  # (num_nodes, 16) int32
+    woop: np.ndarray   # (num_woop, 4) float32
+    tri_index: np.ndarray
+
+
+def flatten(c: Collapsed, v: np.ndarray) -> Compact:
+    n = len(c.triangle_indices)
+    v = np.ascontiguousarray(v, np.float32)
+    nodes = np.zeros((max(n - 1, 1), 16), np.int32)
+    woop = np.zeros((4 * n, 4), np.float32)
+    tri = np.zeros(4 * n, np.int32)
+    nn = C.c_int64()
+    nw = C.c_int64()
+    rc = lib().orc_flatten_compact2(n, _ptr(c.left), _ptr(c.right), _ptr(c.data), _ptr(c.triangle_count),
+                                    _ptr(c.bbox_min), _ptr(c.bbox_max), _ptr(c.triangle_indices), _ptr(v),
+                                    _ptr(nodes), _ptr(woop), _ptr(tri), C.byref(nn), C.byref(nw))
+    if rc != 0:
+        raise ValueError("orc_flatten_compact2 failed")
+    return Compact(nodes[:nn.value].copy(), woop[:nw.value].copy(), tri[:nw.value].copy())
+
+
+def trace(cp: Compact, rays: np.ndarray, any_hit: bool = False, threads: int = 0) -> np.ndarray:
+    rays = np.ascontiguousarray(rays, np.float32)
+    nr = rays.shape[0]
+    res = np.zeros((nr, 4), np.int32)
+    lib().orc_trace(_ptr(cp.nodes), _ptr(cp.woop), _ptr(cp.tri_index), _ptr(rays), nr, 1 if any_hit else 0,
+                    _ptr(res), threads)
+    return res
+
+
+def atrbvh_schedule(treelet: int, warp: int = 32) -> np.ndarray:
+    out = np.zeros(4096, np.int32)
+    k = lib().orc_atrbvh_schedule(treelet, warp, _ptr(out), len(out))
+    return out[:k]
+
+
+# ---- the reference's own CUDA build (GPU machine only) ------------------------
+
+_ref = {}
+
+
+def ref_available(fmad: bool = False) -> bool:
+    return (REF_LIB_FMAD if fmad else REF_LIB).exists()
+
+
+def ref_lib(fmad: bool = False) -> C.CDLL:
+    key = bool(fmad)
+    if key not in _ref:
+        L = C.CDLL(str(REF_LIB_FMAD if fmad else REF_LIB))
+        L.ref_run.restype = C.c_int
+        L.ref_run.argtypes = [_p, C.c_uint, _p, _p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int] + \
+            [_p] * 15 + [_p, _p]
+        _ref[key] = L
+    return _ref[key]
+
+
+def ref_run(v: np.ndarray, bbmin, bbmax, *, use64=False, optimizer=0, treelet=9, iterations=2,
+            collapse=False, fmad=False):
+    """Run the reference pipeline on the GPU; returns (Tree, Collapsed|None, times_ms)."""
+    v = np.ascontiguousarray(v, np.float32)
+    n = v.shape[0]
+    t = Tree.empty(n)
+    nn = 2 * n - 1
+    c = None
+    if collapse:
+        c = Collapsed(*(np.zeros(nn, np.int32) for _ in range(5)), np.zeros((nn, 4), np.float32),
+                      np.zeros((nn, 4), np.float32), np.zeros(n, np.int32), np.zeros(0, np.float32), 0.0)
+    sah_out = np.zeros(1, np.float32)
+    times = np.zeros(3, np.float64)
+    mn = np.asarray(bbmin, np.float32)
+    mx = np.asarray(bbmax, np.float32)
+    cp = [None] * 8 if c is None else [_ptr(c.parent), _ptr(c.left), _ptr(c.right), _ptr(c.data),
+                                      _ptr(c.triangle_count), _ptr(c.bbox_min), _ptr(c.bbox_max),
+                                      _ptr(c.triangle_indices)]
+    rc = ref_lib(fmad).ref_run(_ptr(v), n, _ptr(mn), _ptr(mx), 1 if use64 else 0, optimizer, treelet, iterations,
+                               1 if collapse else 0, 1, *t.ptrs(), *cp, _ptr(sah_out), _ptr(times))
+    if rc != 0:
+        raise RuntimeError(f"reference run failed: cuda error {rc}")
+    if c is not None:
+        c.sah = float(sah_out[0])
+    return t, c, times
