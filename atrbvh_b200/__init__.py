@@ -69,8 +69,10 @@ _SIGS = [
     ("atr_ctx_destroy", C.c_int, [_p]),
     ("atr_ctx_synchronize", C.c_int, [_p]),
     ("atr_ctx_get_stream", C.c_int, [_p, C.POINTER(_p)]),
+    ("atr_ctx_launch_count", C.c_int, [_p, C.POINTER(C.c_uint64)]),
     ("atr_ctx_set_timing", C.c_int, [_p, C.c_int]),
     ("atr_ctx_phase_times", C.c_int, [_p, _f32p, C.c_int, C.POINTER(C.c_int)]),
+    ("atr_ctx_phase_names", C.c_char_p, [_p]),
     ("atr_scene_create", C.c_int, [_p, _p, C.c_uint32, _f32p, _f32p, C.c_int, C.POINTER(_p)]),
     ("atr_scene_destroy", C.c_int, [_p]),
     ("atr_scene_bounds", C.c_int, [_p, _p, _f32p, _f32p]),
@@ -94,7 +96,9 @@ _SIGS = [
     ("atr_flatten_compact2", C.c_int, [_p, _p, _p, C.POINTER(_p)]),
     ("atr_compact_destroy", C.c_int, [_p]),
     ("atr_compact_view_get", C.c_int, [_p, C.POINTER(CompactView)]),
+    ("atr_compact_download", C.c_int, [_p, _p, _p, _p, _p]),
     ("atr_trace", C.c_int, [_p, _p, _p, C.c_int64, C.c_int, _p]),
+    ("atr_gen_bounce_rays", C.c_int, [_p, _p, _p, _p, C.c_int64, C.c_uint64, _p]),
     ("atr_gen_scene", C.c_int, [C.c_int, C.c_uint32, C.c_uint64, _p]),
     ("atr_gen_batch_sizes", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _p]),
     ("atr_gen_batch_scene", C.c_int, [C.c_uint32, _p, C.c_uint64, _p]),
@@ -189,14 +193,22 @@ class Context:
         check(lib().atr_ctx_get_stream(self.handle, C.byref(s)))
         return s.value or 0
 
+    def launch_count(self) -> int:
+        c = C.c_uint64()
+        check(lib().atr_ctx_launch_count(self.handle, C.byref(c)))
+        return c.value
+
     def set_timing(self, on: bool) -> None:
         check(lib().atr_ctx_set_timing(self.handle, 1 if on else 0))
 
-    def phase_times(self) -> list[float]:
-        buf = (C.c_float * 64)()
+    def phase_times(self) -> list[tuple[str, float]]:
+        """(name, ms) of every timed phase since timing was enabled or last read."""
+        cap = 4096
+        buf = (C.c_float * cap)()
         n = C.c_int()
-        check(lib().atr_ctx_phase_times(self.handle, buf, 64, C.byref(n)))
-        return [buf[i] for i in range(min(n.value, 64))]
+        check(lib().atr_ctx_phase_times(self.handle, buf, cap, C.byref(n)))
+        names = lib().atr_ctx_phase_names(self.handle).decode().split(",")
+        return [(names[i] if i < len(names) else "?", buf[i]) for i in range(min(n.value, cap))]
 
     def close(self) -> None:
         if getattr(self, "handle", None):
@@ -407,11 +419,14 @@ class BVHCollapsedTree:
 class BVHTreeCollapser:
     """BVHRT::BVHTreeCollapser::Collapse(tree, &sah, ci, ct); max_leaf=0 is the reference."""
 
-    def Collapse(self, tree: BVHTree, ci: float = 1.2, ct: float = 1.0, max_leaf: int = 0):
+    def Collapse(self, tree: BVHTree, ci: float = 1.2, ct: float = 1.0, max_leaf: int = 0, want_sah: bool = True):
+        """Returns (collapsed tree, SAH); with want_sah=False the SAH is None
+        and no host synchronisation happens."""
         h = C.c_void_p()
         s = C.c_float()
-        check(lib().atr_collapse(tree.ctx.handle, tree.handle, ci, ct, max_leaf, C.byref(h), C.byref(s)))
-        return BVHCollapsedTree(tree.ctx, h, tree.n), s.value
+        check(lib().atr_collapse(tree.ctx.handle, tree.handle, ci, ct, max_leaf, C.byref(h),
+                                 C.byref(s) if want_sah else None))
+        return BVHCollapsedTree(tree.ctx, h, tree.n), (s.value if want_sah else None)
 
 
 class BVHTreeInstanceManager:
@@ -455,6 +470,15 @@ class CudaBVH:
         v = CompactView()
         check(lib().atr_compact_view_get(self.handle, C.byref(v)))
         return v
+
+    def download(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Host copies (nodes (M,16) int32, woop (W,4) float32, tri_index (W,) int32)."""
+        v = self.view()
+        nodes = np.empty((v.num_nodes, 16), np.int32)
+        woop = np.empty((v.num_woop, 4), np.float32)
+        tri = np.empty(v.num_woop, np.int32)
+        check(lib().atr_compact_download(self.ctx.handle, self.handle, _ptr(nodes), _ptr(woop), _ptr(tri)))
+        return nodes, woop, tri
 
     def trace(self, rays_ptr: int, num_rays: int, results_ptr: int, any_hit: bool = False) -> None:
         """rays: device float4 pairs; results: device int4 per ray."""

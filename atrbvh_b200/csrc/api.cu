@@ -145,6 +145,12 @@ int atr_ctx_synchronize(atr_ctx* ctx) {
     return ATR_OK;
 }
 
+int atr_ctx_launch_count(atr_ctx* ctx, uint64_t* count) {
+    ATR_REQUIRE(ctx && count, ATR_ERR_INVALID_ARG, "atr_ctx_launch_count: NULL argument");
+    *count = ctx->launches;
+    return ATR_OK;
+}
+
 int atr_ctx_get_stream(atr_ctx* ctx, void** stream) {
     ATR_REQUIRE(ctx && stream, ATR_ERR_INVALID_ARG, "atr_ctx_get_stream: NULL argument");
     *stream = ctx->stream;
@@ -164,10 +170,13 @@ int atr_ctx_phase_times(atr_ctx* ctx, float* ms, int capacity, int* count) {
     ATR_REQUIRE(ctx && count, ATR_ERR_INVALID_ARG, "atr_ctx_phase_times: NULL argument");
     ATR_CUDA(cudaStreamSynchronize(ctx->stream));
     int k = 0;
+    ctx->phase_names.clear();
     for (auto& p : ctx->phases) {
         float t = 0.0f;
         ATR_CUDA(cudaEventElapsedTime(&t, p.a, p.b));
         if (ms && k < capacity) ms[k] = t;
+        if (!ctx->phase_names.empty()) ctx->phase_names += ",";
+        ctx->phase_names += p.name;
         ++k;
     }
     *count = k;
@@ -175,6 +184,8 @@ int atr_ctx_phase_times(atr_ctx* ctx, float* ms, int capacity, int* count) {
     ctx->phases.clear();
     return ATR_OK;
 }
+
+const char* atr_ctx_phase_names(atr_ctx* ctx) { return ctx ? ctx->phase_names.c_str() : ""; }
 
 int atr_scene_destroy(atr_scene* s) {
     if (!s) return ATR_OK;

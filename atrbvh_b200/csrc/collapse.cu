@@ -1,0 +1,246 @@
+// Leaf collapse (BVHRT-Core/src/TreeCollapser.cu:13-285, BVHTreeCollapser.cpp:21-93).
+//
+// Pass 1 (bottom-up, one thread per leaf, second arrival continues) copies the
+// tree into the collapsed layout and computes, per node: triangle count,
+// SAH cost (ci*A + cL + cR, or ct*A*count when that is cheaper -- :47-84), the
+// collapse flag, and whether a climbing thread of the reference's emission
+// kernel (:173-237) would pass the node upward.  The reference emits, at every
+// node reached by two such threads that is not collapsed, each child holding
+// more than one triangle as a multi-triangle leaf; pass 1 records those
+// children.  A scan gives their list offsets in node order (the reference
+// takes them from an atomicAdd, so its offsets vary between runs while the
+// lists themselves do not).  Pass 2 writes each triangle at its rank in the
+// right-first stack order of writeSubtreeLeavesNonrecursive (:95-137): the
+// number of leaves in right subtrees hanging off its path below the emitted
+// node.
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace atr {
+
+int exclusive_scan_u32(atr_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* d_total);
+
+namespace {
+
+struct CollapseRefs {
+    uint32_t n;
+    const int32_t* parent;
+    const int32_t* left;
+    const int32_t* right;
+    const int32_t* data;
+    const float4* bmin;
+    const float4* bmax;
+    int32_t* c_parent;
+    int32_t* c_left;
+    int32_t* c_right;
+    int32_t* c_data;
+    int32_t* c_count;
+    float4* c_bmin;
+    float4* c_bmax;
+    float* cost;
+    int32_t* pass;
+    uint32_t* emit_cnt;
+};
+
+__global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs t, uint32_t* __restrict__ counters, float ci,
+                                                        float ct, int max_leaf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= t.n) return;
+    const int leaf = (int)i + (int)t.n - 1;
+    {
+        const float4 mn = t.bmin[leaf], mx = t.bmax[leaf];
+        t.c_parent[leaf] = t.parent[leaf];
+        t.c_left[leaf] = t.left[leaf];
+        t.c_right[leaf] = t.right[leaf];
+        t.c_data[leaf] = t.data[leaf];
+        t.c_bmin[leaf] = mn;
+        t.c_bmax[leaf] = mx;
+        t.c_count[leaf] = 1;
+        t.cost[leaf] = __fmul_rn(ct, box_area(mn, mx));
+        t.pass[leaf] = 1;
+    }
+    int cur = t.parent[leaf];
+    while (cur >= 0) {
+        __threadfence();
+        if (atomicAdd(&counters[cur], 1u) == 0u) return;
+        __threadfence();
+        const int l = t.left[cur], r = t.right[cur];
+        const int cl = ld_cg(t.c_count + l), cr = ld_cg(t.c_count + r);
+        const float kl = ld_cg(t.cost + l), kr = ld_cg(t.cost + r);
+        const int pl = ld_cg(t.pass + l), pr = ld_cg(t.pass + r);
+        const float4 mn = t.bmin[cur], mx = t.bmax[cur];
+        const int cnt = cl + cr;
+        const float a = box_area(mn, mx);
+        float c = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), kl), kr);
+        const float leaf_cost = __fmul_rn(__fmul_rn(ct, a), (float)cnt);
+        const bool col = leaf_cost < c && (max_leaf <= 0 || cnt <= max_leaf);
+        if (col) c = leaf_cost;
+        const bool reached = pl && pr;
+        if (reached && !col) {
+            if (cl > 1) t.emit_cnt[l] = (uint32_t)cl;
+            if (cr > 1) t.emit_cnt[r] = (uint32_t)cr;
+        }
+        t.c_parent[cur] = t.parent[cur];
+        t.c_left[cur] = l;
+        t.c_right[cur] = r;
+        t.c_data[cur] = -1;
+        t.c_bmin[cur] = mn;
+        t.c_bmax[cur] = mx;
+        t.c_count[cur] = cnt;
+        t.cost[cur] = c;
+        t.pass[cur] = reached && col;
+        cur = t.parent[cur];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_collapse_emit(CollapseRefs t, const uint32_t* __restrict__ offsets,
+                                                        int32_t* __restrict__ tri_indices) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= t.n) return;
+    const int leaf = (int)i + (int)t.n - 1;
+    int ch = leaf, a = t.parent[leaf], top = -1;
+    uint32_t rank = 0;
+    while (a >= 0 && t.pass[a]) {
+        if (t.left[a] == ch) rank += (uint32_t)t.c_count[t.right[a]];
+        top = a;
+        ch = a;
+        a = t.parent[a];
+    }
+    if (top < 0 || t.emit_cnt[top] == 0) return;
+    const uint32_t off = offsets[top];
+    tri_indices[off + rank] = t.data[leaf];
+    if (rank == 0) t.c_data[top] = (int32_t)off;
+}
+
+}  // namespace
+
+int collapsed_alloc(atr_ctx* ctx, uint32_t n, atr_collapsed** out) {
+    const size_t nn = 2 * (size_t)n - 1;
+    const size_t b4 = align256(nn * 4), b16 = align256(nn * 16);
+    atr_collapsed* c = new atr_collapsed();
+    c->ctx = ctx;
+    c->n = n;
+    int s = ctx->alloc(&c->block, 5 * b4 + 2 * b16 + align256((size_t)n * 4));
+    if (s != ATR_OK) { delete c; return s; }
+    char* p = static_cast<char*>(c->block);
+    c->parent = reinterpret_cast<int32_t*>(p); p += b4;
+    c->left = reinterpret_cast<int32_t*>(p); p += b4;
+    c->right = reinterpret_cast<int32_t*>(p); p += b4;
+    c->data = reinterpret_cast<int32_t*>(p); p += b4;
+    c->count = reinterpret_cast<int32_t*>(p); p += b4;
+    c->bmin = reinterpret_cast<float4*>(p); p += b16;
+    c->bmax = reinterpret_cast<float4*>(p); p += b16;
+    c->tri_indices = reinterpret_cast<int32_t*>(p);
+    *out = c;
+    return ATR_OK;
+}
+
+int collapse_into(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int max_leaf, atr_collapsed* c,
+                  float* d_sah_parts) {
+    const uint32_t n = tree->n;
+    const size_t nn = 2 * (size_t)n - 1;
+    void* scratch = nullptr;
+    const size_t b4 = align256(nn * 4);
+    ATR_TRY(ctx->alloc(&scratch, 4 * b4 + align256((size_t)(n - 1) * 4)));
+    char* p = static_cast<char*>(scratch);
+    float* cost = reinterpret_cast<float*>(p); p += b4;
+    int32_t* pass = reinterpret_cast<int32_t*>(p); p += b4;
+    uint32_t* emit = reinterpret_cast<uint32_t*>(p); p += b4;
+    uint32_t* offs = reinterpret_cast<uint32_t*>(p); p += b4;
+    uint32_t* counters = reinterpret_cast<uint32_t*>(p);
+    cudaStream_t s = ctx->stream;
+    cudaMemsetAsync(emit, 0, nn * 4, s);
+    cudaMemsetAsync(counters, 0, (size_t)(n - 1) * 4, s);
+    cudaMemsetAsync(c->tri_indices, 0xff, (size_t)n * 4, s);
+    CollapseRefs r{n, tree->parent, tree->left, tree->right, tree->data, tree->bmin, tree->bmax, c->parent,
+                   c->left, c->right, c->data, c->count, c->bmin, c->bmax, cost, pass, emit};
+    const unsigned blocks = (n + 255) / 256;
+    k_collapse_cost<<<blocks, 256, 0, s>>>(r, counters, ci, ct, max_leaf);
+    ctx->launches += 1;
+    int st = exclusive_scan_u32(ctx, emit, offs, nn, nullptr);
+    if (st == ATR_OK) {
+        k_collapse_emit<<<blocks, 256, 0, s>>>(r, offs, c->tri_indices);
+        ctx->launches += 1;
+        if (d_sah_parts) {
+            cudaMemcpyAsync(d_sah_parts, cost, 4, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(d_sah_parts + 1, tree->area, 4, cudaMemcpyDeviceToDevice, s);
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "collapse kernels", __FILE__, __LINE__);
+    }
+    ctx->release(scratch);
+    return st;
+}
+
+}  // namespace atr
+
+using namespace atr;
+
+extern "C" {
+
+int atr_collapse(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int max_leaf, atr_collapsed** out,
+                 float* sah) {
+    ATR_REQUIRE(ctx && tree && out, ATR_ERR_INVALID_ARG, "atr_collapse: NULL argument");
+    ATR_REQUIRE(max_leaf >= 0, ATR_ERR_INVALID_ARG, "atr_collapse: max_leaf %d < 0", max_leaf);
+    *out = nullptr;
+    atr_collapsed* c = nullptr;
+    ATR_TRY(collapsed_alloc(ctx, tree->n, &c));
+    float* parts = nullptr;
+    int st = ATR_OK;
+    if (sah) st = ctx->alloc(reinterpret_cast<void**>(&parts), 8);
+    ctx->phase_begin("collapse");
+    if (st == ATR_OK) st = collapse_into(ctx, tree, ci, ct, max_leaf, c, parts);
+    ctx->phase_end();
+    if (st == ATR_OK && sah) {
+        float h[2];
+        cudaError_t e = cudaMemcpyAsync(h, parts, 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpyAsync(sah)", __FILE__, __LINE__);
+        if (st == ATR_OK) st = atr_ctx_synchronize(ctx);
+        if (st == ATR_OK) *sah = h[0] / h[1];
+    }
+    ctx->release(parts);
+    if (st != ATR_OK) { atr_collapsed_destroy(c); return st; }
+    *out = c;
+    return ATR_OK;
+}
+
+int atr_collapsed_destroy(atr_collapsed* c) {
+    if (!c) return ATR_OK;
+    c->ctx->release(c->block);
+    delete c;
+    return ATR_OK;
+}
+
+int atr_collapsed_view_get(const atr_collapsed* c, atr_collapsed_view* v) {
+    ATR_REQUIRE(c && v, ATR_ERR_INVALID_ARG, "atr_collapsed_view_get: NULL argument");
+    v->num_triangles = c->n;
+    v->root = 0;
+    v->parent = c->parent;
+    v->left = c->left;
+    v->right = c->right;
+    v->data = c->data;
+    v->triangle_count = c->count;
+    v->bbox_min = reinterpret_cast<float*>(c->bmin);
+    v->bbox_max = reinterpret_cast<float*>(c->bmax);
+    v->triangle_indices = c->tri_indices;
+    return ATR_OK;
+}
+
+int atr_collapsed_download(atr_ctx* ctx, const atr_collapsed* c, int32_t* parent, int32_t* left, int32_t* right,
+                           int32_t* data, int32_t* count, float* bmin, float* bmax, int32_t* tri) {
+    ATR_REQUIRE(ctx && c, ATR_ERR_INVALID_ARG, "atr_collapsed_download: NULL argument");
+    const size_t nn = 2 * (size_t)c->n - 1;
+    cudaStream_t s = ctx->stream;
+    if (parent) ATR_CUDA(cudaMemcpyAsync(parent, c->parent, nn * 4, cudaMemcpyDeviceToHost, s));
+    if (left) ATR_CUDA(cudaMemcpyAsync(left, c->left, nn * 4, cudaMemcpyDeviceToHost, s));
+    if (right) ATR_CUDA(cudaMemcpyAsync(right, c->right, nn * 4, cudaMemcpyDeviceToHost, s));
+    if (data) ATR_CUDA(cudaMemcpyAsync(data, c->data, nn * 4, cudaMemcpyDeviceToHost, s));
+    if (count) ATR_CUDA(cudaMemcpyAsync(count, c->count, nn * 4, cudaMemcpyDeviceToHost, s));
+    if (bmin) ATR_CUDA(cudaMemcpyAsync(bmin, c->bmin, nn * 16, cudaMemcpyDeviceToHost, s));
+    if (bmax) ATR_CUDA(cudaMemcpyAsync(bmax, c->bmax, nn * 16, cudaMemcpyDeviceToHost, s));
+    if (tri) ATR_CUDA(cudaMemcpyAsync(tri, c->tri_indices, (size_t)c->n * 4, cudaMemcpyDeviceToHost, s));
+    return atr_ctx_synchronize(ctx);
+}
+
+}  // extern "C"

@@ -57,6 +57,7 @@ struct atr_ctx {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     uint32_t* d_error = nullptr;  // device error bits
+    uint64_t launches = 0;        // kernels enqueued by this context
     bool timing = false;
     struct Phase {
         std::string name;
@@ -64,6 +65,7 @@ struct atr_ctx {
     };
     std::vector<Phase> phases;
     std::vector<float> phase_ms;
+    std::string phase_names;  // comma-separated names of the last atr_ctx_phase_times
 
     // Stream-ordered allocation from the device's default pool.
     int alloc(void** p, size_t bytes);

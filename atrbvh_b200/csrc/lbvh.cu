@@ -452,6 +452,7 @@ int sort_pairs(atr_ctx* ctx, K* keys, uint32_t* vals, uint32_t n, uint32_t* hist
         std::swap(ka, kb2);
         std::swap(va, vb2);
     }
+    ctx->launches += P + (hist_ready ? 0 : 1);
     e = cudaGetLastError();
     ctx->release(tmp);
     if (e != cudaSuccess) return cuda_fail(e, "k_onesweep launch", __FILE__, __LINE__);
@@ -477,6 +478,7 @@ int build_typed(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bo
     ctx->phase_begin("morton");
     k_morton<K><<<grid_for(ctx, n, 8, 256), 256, 0, s>>>(verts, n, d_bounds, static_cast<K*>(keys), hist);
     ctx->phase_end();
+    ctx->launches += 1;
     ctx->phase_begin("sort");
     st = sort_pairs<K>(ctx, static_cast<K*>(keys), static_cast<uint32_t*>(idx), n, hist, true, true);
     ctx->phase_end();
@@ -486,6 +488,7 @@ int build_typed(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bo
                                                   t->parent, t->left, t->right, t->data, t->bmin, t->bmax,
                                                   t->area, slot);
         ctx->phase_end();
+        ctx->launches += 1;
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) st = cuda_fail(e, "k_build launch", __FILE__, __LINE__);
     }
@@ -514,6 +517,7 @@ int refit_tree(atr_ctx* ctx, atr_tree* t, const float4* verts) {
     cudaMemsetAsync(ctr, 0, (size_t)(n - 1) * 4, ctx->stream);
     k_refit<<<(n + 255) / 256, 256, 0, ctx->stream>>>(verts, n, t->parent, t->left, t->right, t->data, t->bmin,
                                                       t->bmax, t->area, static_cast<uint32_t*>(ctr));
+    ctx->launches += 1;
     cudaError_t e = cudaGetLastError();
     ctx->release(ctr);
     if (e != cudaSuccess) return cuda_fail(e, "k_refit launch", __FILE__, __LINE__);
@@ -527,6 +531,7 @@ int scene_bounds_device(atr_ctx* ctx, const float4* verts, uint32_t n, float* d_
     ATR_TRY(ctx->alloc(&part, (size_t)blocks * 6 * 4));
     k_bounds_partial<<<blocks, 256, 0, ctx->stream>>>(verts, nv, static_cast<float*>(part));
     k_bounds_final<<<1, 32, 0, ctx->stream>>>(static_cast<float*>(part), blocks, d_out);
+    ctx->launches += 2;
     cudaError_t e = cudaGetLastError();
     ctx->release(part);
     if (e != cudaSuccess) return cuda_fail(e, "k_bounds launch", __FILE__, __LINE__);
@@ -612,6 +617,7 @@ int atr_device_morton(atr_ctx* ctx, const float* vertices, uint32_t n, const flo
     else
         k_morton<uint64_t><<<grid_for(ctx, n, 8, 256), 256, 0, ctx->stream>>>(v, n, static_cast<float*>(b),
                                                                                static_cast<uint64_t*>(keys), nullptr);
+    ctx->launches += 1;
     cudaError_t e = cudaStreamSynchronize(ctx->stream);  // h is a stack array
     ctx->release(b);
     if (e != cudaSuccess) return cuda_fail(e, "k_morton", __FILE__, __LINE__);

@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Benchmark of the ATRBVH build-and-traverse path on B200.
+
+Workload (the clustered-scene configuration): 4,194,304 fp32 triangles
+(75% from 64 anisotropic Gaussians, 25% ground-plane quad grid), seed 0.
+One step = LBVH (30-bit Morton, onesweep sort, fused Karras build + refit)
+-> ATRBVH (treelet 9, 2 iterations) -> collapse (Ci 1.2, Ct 1.0) -> Compact2
+flatten -> closest-hit traversal of 1920x1080 pinhole primary rays (eye
+(0.5, 0.5, -1.5), 60 degree vertical field of view) -> one cosine-weighted
+diffuse bounce per hit -> traversal of the bounces.
+
+value = build throughput in Mtri/s (Morton through collapse, device-resident
+input, CUDA events on the library's stream), summed over ranks; traversal
+Mrays/s is reported beside it.  e2e repeats the build through the public C ABI
+from pinned host vertices (H2D inside the timed region) to the SAH read back
+on the host.  With --gpus N > 1 every rank builds its own replica (the path
+has no data exchange for a single mesh).
+
+--impl reference times the CPU restatement of the same pipeline on the host
+cores (the reference has no CPU implementation of this path) and, where its
+compiled CUDA build is present, the reference's own CUDA builder.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_TRIS = 4194304
+WIDTH, HEIGHT = 1920, 1080
+METRIC = "ATRBVH build Mtri/s at equal SAH, batched vs plain; Mrays/s; p99 latency"
+WORKLOAD = ("clustered scene 4,194,304 tris (75% 64-Gaussian mixture, 25% 1024x512 ground-plane quads): "
+            "LBVH 30-bit + ATRBVH(9,2) + collapse + Compact2, closest-hit trace of 1920x1080 primary "
+            "rays + 1 diffuse bounce per hit")
+# Algorithmic bytes per triangle (reference data types) per HBM-bound phase.
+BYTES_PER_TRI = {"morton": 56.0, "sort": 4.0 + 16.0 * 4, "build": 40.0 + 180.0}
+
+
+def _read_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return {"hbm_gbs": float(d["hbm_gbs"]), "src": "measured"}
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_pipeline(v: np.ndarray, threads: int) -> float:
+    """Host-core LBVH + ATRBVH(9,2) + collapse on v; returns seconds."""
+    import oracle as O
+    t0 = time.perf_counter()
+    mn, mx = O.scene_aabb(v)
+    t, _, _ = O.build_lbvh(v, mn, mx, threads=threads)
+    a = O.atrbvh(t, 9, 2, threads=threads)
+    O.collapse(a)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(v_full: np.ndarray) -> dict:
+    import oracle as O
+    threads = O.max_threads()
+    m = min(len(v_full), 1 << 20)
+    v = np.ascontiguousarray(v_full[:m])
+    cpu_pipeline(v[: 1 << 14], threads)  # warm-up
+    secs = min(cpu_pipeline(v, threads) for _ in range(2))
+    return {"value": m / secs / 1e6, "unit": "Mtri/s", "cores": threads, "kind": "port",
+            "sample": f"first {m} triangles of the workload scene, LBVH+ATRBVH(9,2)+collapse, best of 2"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import atrbvh_b200 as ab
+    torch.cuda.set_device(local)
+    ctx = ab.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    v = ab.gen_scene(ab.SCENE_CLUSTERED, N_TRIS, 0)
+    scene = ab.SceneWrapper(ctx, v)  # scene box reduced on the device
+    prim = ab.gen_rays_pinhole(WIDTH, HEIGHT)
+    nr = len(prim)
+    with torch.cuda.stream(stream):
+        rays = torch.from_numpy(prim.reshape(-1)).to("cuda", non_blocking=False)
+        res = torch.zeros(nr * 4, dtype=torch.int32, device="cuda")
+        bounce = torch.zeros_like(rays)
+        res2 = torch.zeros_like(res)
+    torch.cuda.synchronize()
+
+    def step(timed: bool):
+        tree = ab.LBVHBuilder(False).BuildTree(scene)
+        ab.AgglomerativeTreeletOptimizer(9, 2).Optimize(tree)
+        col, _ = ab.BVHTreeCollapser().Collapse(tree, want_sah=False)
+        bvh = ab.CudaBVH(col, scene)
+        bvh.trace(rays.data_ptr(), nr, res.data_ptr())
+        ab.check(ab.lib().atr_gen_bounce_rays(ctx.handle, scene.handle, rays.data_ptr(), res.data_ptr(), nr, 1,
+                                              bounce.data_ptr()))
+        bvh.trace(bounce.data_ptr(), nr, res2.data_ptr())
+        bvh.close()
+        col.close()
+        tree.close()
+
+    for _ in range(args.warmup):
+        step(False)
+    ctx.synchronize()
+
+    # ---- device-resident timed region ----
+    ctx.set_timing(True)
+    clocks = ClockSampler(local)
+    launches0 = ctx.launch_count()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(True)
+    ev1.record(stream)
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    launches = ctx.launch_count() - launches0
+    total_ms = ev0.elapsed_time(ev1)
+    phases = ctx.phase_times()
+    ctx.set_timing(False)
+    per = {}
+    for name, ms in phases:
+        per.setdefault(name, []).append(ms)
+    ph_ms = {k: sum(x) / args.steps for k, x in per.items()}  # per step (trace: both launches)
+    build_ms = sum(ph_ms.get(k, 0.0) for k in ("morton", "sort", "build", "atrbvh", "collapse"))
+    trace_ms = ph_ms.get("trace", 0.0)
+    n_trace = len(per.get("trace", [])) / args.steps
+    rays_per_step = nr * n_trace
+    build_ms_max = max_over_ranks(build_ms, world)
+    trace_ms_max = max_over_ranks(trace_ms, world)
+    step_ms_max = max_over_ranks(total_ms / args.steps, world)
+
+    # ---- e2e through the public API from pinned host memory ----
+    pinned = torch.from_numpy(v.reshape(-1)).pin_memory().numpy().reshape(v.shape)
+    e2e_times = []
+    for it in range(args.warmup + args.steps):
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sc = ab.SceneWrapper(ctx, pinned)  # H2D of the triangles + device scene box
+        tree = ab.LBVHBuilder(False).BuildTree(sc)
+        ab.AgglomerativeTreeletOptimizer(9, 2).Optimize(tree)
+        col, sah = ab.BVHTreeCollapser().Collapse(tree)  # synchronises and reads the SAH back
+        dt = time.perf_counter() - t0
+        col.close()
+        tree.close()
+        sc.close()
+        if it >= args.warmup:
+            e2e_times.append(dt)
+    e2e_s = max_over_ranks(statistics.mean(e2e_times), world)
+
+    peaks = _read_peaks()
+    roof = {}
+    for k, bpt in BYTES_PER_TRI.items():
+        if ph_ms.get(k):
+            roof[k] = N_TRIS * bpt / (ph_ms[k] * 1e-3) / 1e9
+    # Dominant phase by time (trace counted per launch).
+    times = {k: (v2 / n_trace if k == "trace" and n_trace else v2) for k, v2 in ph_ms.items()}
+    dominant = max(times, key=times.get)
+    if dominant in roof:
+        achieved = roof[dominant]
+        rl = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+              "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_src": peaks["src"]}
+    else:
+        # Latency/issue-bound phase: bytes it must move (tree arrays read once, written once).
+        if dominant == "atrbvh":
+            bpt = 2 * 52.0  # 52 B of SoA per node, ~2 nodes per triangle, read + write once
+        elif dominant == "trace":
+            bpt = 0.0
+        else:
+            bpt = 0.0
+        achieved = (N_TRIS * bpt / (times[dominant] * 1e-3) / 1e9) if bpt else 0.0
+        rl = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+              "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_src": peaks["src"],
+              "note": "latency/issue-bound phase; HBM fraction shown for reference"}
+    out = {
+        "metric": METRIC,
+        "value": world * N_TRIS / (build_ms_max * 1e-3) / 1e6,
+        "unit": "Mtri/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step_ms_max,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded Philox: clustered scene + pinhole/diffuse rays)",
+        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "rays_per_step": int(rays_per_step),
+                   "treelet": 9, "iterations": 2, "morton_bits": 30, "collapse_max_leaf": 0,
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (201 MB of vertices)"},
+        "mrays_per_s": world * rays_per_step / (trace_ms_max * 1e-3) / 1e6 if trace_ms_max else None,
+        "phase_ms": {k: round(x, 4) for k, x in ph_ms.items()},
+        "build_ms": build_ms_max,
+        "phase_gbs": {k: round(x, 1) for k, x in roof.items()},
+        "roofline": rl,
+        "e2e": {"value": world * N_TRIS / e2e_s / 1e6, "unit": "Mtri/s",
+                "h2d_bytes_per_step": int(v.nbytes), "d2h_bytes_per_step": 8,
+                "path": "atr_scene_create(pinned host vertices) -> atr_build_lbvh -> atr_optimize_atrbvh -> "
+                        "atr_collapse (SAH read back)"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(v)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_reference(args, world, rank, local):
+    if rank != 0:
+        return
+    import oracle as O
+    import atrbvh_b200 as ab
+    v = ab.gen_scene(ab.SCENE_CLUSTERED, N_TRIS, 0)
+    threads = O.max_threads()
+    m = 1 << 20
+    sample = np.ascontiguousarray(v[:m])
+    for _ in range(args.warmup):
+        cpu_pipeline(sample[: 1 << 16], threads)
+    secs = [cpu_pipeline(sample, threads) for _ in range(args.steps)]
+    value = m / statistics.mean(secs) / 1e6
+    out = {
+        "metric": METRIC, "value": value, "unit": "Mtri/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": statistics.mean(secs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox)",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "sample_triangles": m},
+        "cpu_baseline": {"value": value, "unit": "Mtri/s", "cores": threads, "kind": "port",
+                         "sample": f"first {m} triangles of the workload scene per step: LBVH+ATRBVH(9,2)+collapse "
+                                   f"on {threads} host threads"},
+        "e2e": {"value": value, "unit": "Mtri/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    if O.ref_available():
+        try:
+            mn, mx = O.scene_aabb(v)
+            ts = []
+            for i in range(3):
+                _, _, t = O.ref_run(v, mn, mx, optimizer=1, treelet=9, iterations=2, collapse=True)
+                if i:
+                    ts.append(float(t.sum()))
+            out["reference_cuda"] = {"value": N_TRIS / (statistics.mean(ts) * 1e-3) / 1e6, "unit": "Mtri/s",
+                                     "ms": statistics.mean(ts),
+                                     "what": "the reference's own BVHRT-Core CUDA build (LBVH+ATRBVH(9,2)+collapse) "
+                                             "compiled for sm_100a, wall time of its API calls on this GPU"}
+        except Exception as e:  # the CPU baseline stands on its own
+            out["reference_cuda"] = {"unavailable": str(e)[:200]}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank, local)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

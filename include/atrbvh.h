@@ -100,9 +100,13 @@ int atr_ctx_create(int device, void* stream, atr_ctx** out);
 int atr_ctx_destroy(atr_ctx* ctx);
 int atr_ctx_synchronize(atr_ctx* ctx); /* also reports device-side errors */
 int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
+/* Number of kernels this context has enqueued since it was created. */
+int atr_ctx_launch_count(atr_ctx* ctx, uint64_t* count);
 /* Per-phase CUDA-event timing of the next builds (milliseconds). */
 int atr_ctx_set_timing(atr_ctx* ctx, int enable);
 int atr_ctx_phase_times(atr_ctx* ctx, float* ms, int capacity, int* count);
+/* Comma-separated phase names matching the last atr_ctx_phase_times call. */
+const char* atr_ctx_phase_names(atr_ctx* ctx);
 
 /* ---- scene -------------------------------------------------------------
  * Replaces BVHRT::SceneWrapper(numberOfTriangles, float4* vertices, float3
@@ -187,12 +191,22 @@ int atr_flatten_compact2(atr_ctx* ctx, const atr_collapsed* collapsed, const atr
                          atr_compact** out);
 int atr_compact_destroy(atr_compact* compact);
 int atr_compact_view_get(const atr_compact* compact, atr_compact_view* view);
+/* Host copies of CudaBVH's m_nodes / m_triWoop / m_triIndex buffers
+ * (gpu-ray-traversal/src/rt/cuda/CudaBVH.cpp:566-573); sizes from the view. */
+int atr_compact_download(atr_ctx* ctx, const atr_compact* compact, int32_t* nodes, float* woop,
+                         int32_t* tri_index);
 /* The trace() kernel ABI (gpu-ray-traversal/src/rt/kernels/CudaTracerKernels.hpp:73-86,
  * kepler_dynamic_fetch.cu:61-320): rays are float4 (origin, tmin), float4
  * (direction, tmax) on the device; results are int4 (triangle id or -1,
  * float bits of t, 0, 0) on the device. */
 int atr_trace(atr_ctx* ctx, const atr_compact* compact, const float* rays, int64_t num_rays,
               int any_hit, int32_t* results);
+
+/* One cosine-weighted diffuse bounce ray per primary result (the diffuse
+ * workload of gpu-ray-traversal/src/rt/ray/RayGenKernels.cu:114-223 with one
+ * sample): device arrays; misses produce rays with tmax = -1. */
+int atr_gen_bounce_rays(atr_ctx* ctx, const atr_scene* scene, const float* rays,
+                        const int32_t* results, int64_t num_rays, uint64_t seed, float* out_rays);
 
 /* ---- synthetic workloads (host memory; deterministic in seed) ---------- */
 int atr_gen_scene(int kind, uint32_t num_triangles, uint64_t seed, float* vertices);
