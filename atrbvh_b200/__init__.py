@@ -98,6 +98,14 @@ _SIGS = [
     ("atr_compact_view_get", C.c_int, [_p, C.POINTER(CompactView)]),
     ("atr_compact_download", C.c_int, [_p, _p, _p, _p, _p]),
     ("atr_trace", C.c_int, [_p, _p, _p, C.c_int64, C.c_int, _p]),
+    ("atr_batch_create", C.c_int, [_p, _p, _p, C.c_uint32, _p, C.c_int, C.POINTER(_p)]),
+    ("atr_batch_destroy", C.c_int, [_p]),
+    ("atr_batch_set_params", C.c_int, [_p, _p, _p, _p]),
+    ("atr_batch_build", C.c_int, [_p, _p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int]),
+    ("atr_batch_info", C.c_int, [_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]),
+    ("atr_batch_mesh_view", C.c_int, [_p, C.c_uint32, C.POINTER(TreeView)]),
+    ("atr_batch_download_mesh", C.c_int, [_p, _p, C.c_uint32, _p, _p, _p, _p, _p, _p, _p]),
+    ("atr_batch_sah", C.c_int, [_p, _p, C.c_float, C.c_float, _p]),
     ("atr_gen_bounce_rays", C.c_int, [_p, _p, _p, _p, C.c_int64, C.c_uint64, _p]),
     ("atr_gen_scene", C.c_int, [C.c_int, C.c_uint32, C.c_uint64, _p]),
     ("atr_gen_batch_sizes", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _p]),
@@ -455,6 +463,71 @@ class BVHTreeInstanceManager:
 
     def FreeDeviceCollapsedTree(self, c: BVHCollapsedTree) -> None:
         c.close()
+
+
+class Batch:
+    """Segmented batch of meshes built together (atr_batch).
+
+    vertices: (N, 3, 4) float32 soup of all meshes end to end (host array or
+    device pointer with num_triangles); offsets: (M+1,) uint32 triangle offsets.
+    """
+
+    ATRBVH, TRBVH, NONE = 1, 2, 0
+
+    def __init__(self, ctx: Context, vertices=None, offsets=None, device_ptr: int | None = None, bounds=None):
+        self.ctx = ctx
+        off = np.ascontiguousarray(offsets, dtype=np.uint32)
+        self.offsets = off
+        self.count = len(off) - 1
+        h = C.c_void_p()
+        b = None if bounds is None else np.ascontiguousarray(bounds, dtype=np.float32)
+        if device_ptr is not None:
+            src, on_dev = C.c_void_p(device_ptr), 1
+        else:
+            v = np.ascontiguousarray(vertices, dtype=np.float32)
+            src, on_dev = _ptr(v), 0
+        check(lib().atr_batch_create(ctx.handle, src, _ptr(off), self.count, None if b is None else _ptr(b), on_dev,
+                                     C.byref(h)))
+        self.handle = h
+
+    def set_params(self, treelet_sizes=None, iterations=None) -> None:
+        if treelet_sizes is None:
+            check(lib().atr_batch_set_params(self.ctx.handle, self.handle, None, None))
+            return
+        ts = np.ascontiguousarray(treelet_sizes, dtype=np.uint8)
+        it = np.ascontiguousarray(iterations, dtype=np.uint8)
+        check(lib().atr_batch_set_params(self.ctx.handle, self.handle, _ptr(ts), _ptr(it)))
+
+    def build(self, optimizer: int = 1, treelet: int = 9, iterations: int = 2, ci: float = 1.2, ct: float = 1.0,
+              graph: bool = False) -> None:
+        check(lib().atr_batch_build(self.ctx.handle, self.handle, optimizer, treelet, iterations, ci, ct,
+                                    1 if graph else 0))
+
+    def mesh(self, m: int) -> HostTree:
+        n = int(self.offsets[m + 1] - self.offsets[m])
+        nn = 2 * n - 1
+        ht = HostTree(*(np.empty(nn, np.int32) for _ in range(4)), np.empty((nn, 4), np.float32),
+                      np.empty((nn, 4), np.float32), np.empty(nn, np.float32))
+        check(lib().atr_batch_download_mesh(self.ctx.handle, self.handle, m, _ptr(ht.parent), _ptr(ht.left),
+                                            _ptr(ht.right), _ptr(ht.data), _ptr(ht.bbox_min), _ptr(ht.bbox_max),
+                                            _ptr(ht.area)))
+        return ht
+
+    def sah(self, ci: float = 1.2, ct: float = 1.0) -> np.ndarray:
+        out = np.empty(self.count, np.float32)
+        check(lib().atr_batch_sah(self.ctx.handle, self.handle, ci, ct, _ptr(out)))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().atr_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class CudaBVH:

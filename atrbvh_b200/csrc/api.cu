@@ -113,6 +113,7 @@ int atr_ctx_create(int device, void* stream, atr_ctx** out) {
     }
     cudaError_t e = cudaMalloc(&c->d_error, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(c->d_error, 0, sizeof(uint32_t));
+    if (e == cudaSuccess && atr::lbvh_prepare() != ATR_OK) e = cudaErrorInvalidValue;
     if (e != cudaSuccess) {
         if (c->own_stream) cudaStreamDestroy(c->stream);
         delete c;

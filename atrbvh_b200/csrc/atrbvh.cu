@@ -141,35 +141,53 @@ __device__ bool process_treelet(const TreeRefs& t, int root, float root_sah, int
     return true;
 }
 
-__global__ void __launch_bounds__(kAtrWarps * 32) k_atrbvh(TreeRefs t, int32_t* __restrict__ subtree,
-                                                           uint32_t* __restrict__ counters, int tsize,
-                                                           int gamma, float ci, float ct, uint32_t* err) {
+// One iteration over every mesh of `segs`: thread i starts at the i-th sorted
+// leaf of the batch.  Each mesh has its own treelet size and iteration count
+// when `seg_tsize`/`seg_iters` are given; a mesh whose iterations are done
+// sits this launch out.  Treelets are processed with the refs of the mesh of
+// the lane that owns the root.
+__global__ void __launch_bounds__(kAtrWarps * 32) k_atrbvh(TreeRefs g, Segs segs, int32_t* __restrict__ subtree,
+                                                           uint32_t* __restrict__ counters, int tsize_all,
+                                                           const uint8_t* __restrict__ seg_tsize,
+                                                           const uint8_t* __restrict__ seg_iters, int iteration,
+                                                           float ci, float ct, uint32_t* err) {
     __shared__ float s_dist[kAtrWarps][kMaxDist];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    int cur = -1;
-    if (i < t.n) {
-        const int leaf = (int)i + (int)t.n - 1;
-        subtree[leaf] = 1;
-        t.nsah[leaf] = __fmul_rn(ct, t.area[leaf]);
-        cur = t.parent[leaf];
+    int cur = -1, base = 0, cbase = 0, tsize = tsize_all;
+    uint32_t nm = 2;
+    if (i < segs.n) {
+        const uint32_t m = segs.seg_of_tri(i);
+        const uint32_t s0 = segs.tri_begin(m);
+        nm = segs.tri_end(m) - s0;
+        base = segs.node_base(m);
+        cbase = segs.inner_base(m);
+        if (seg_tsize) tsize = seg_tsize[m];
+        if (!seg_iters || iteration < (int)seg_iters[m]) {
+            const int leaf = base + (int)(i - s0) + (int)nm - 1;
+            subtree[leaf] = 1;
+            g.nsah[leaf] = __fmul_rn(ct, g.area[leaf]);
+            cur = g.parent[leaf];
+        }
     }
+    const int gamma = tsize << iteration;
     while (__any_sync(kFull, cur >= 0)) {
         bool second = false;
         if (cur >= 0) {
             __threadfence();
-            if (atomicAdd(&counters[cur], 1u) == 0u) cur = -1;
+            if (atomicAdd(&counters[cbase + cur], 1u) == 0u) cur = -1;
             else { second = true; __threadfence(); }
         }
         int cnt = 0;
         float my_sah = 0.0f;
         if (second) {
-            const int l = ld_cg(t.left + cur), r = ld_cg(t.right + cur);
-            const float a = ld_cg(t.area + cur);
+            const int x = base + cur;
+            const int l = base + ld_cg(g.left + x), r = base + ld_cg(g.right + x);
+            const float a = ld_cg(g.area + x);
             cnt = ld_cg(subtree + l) + ld_cg(subtree + r);
-            my_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), ld_cg(t.nsah + l)), ld_cg(t.nsah + r));
-            subtree[cur] = cnt;
-            t.nsah[cur] = my_sah;
+            my_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), ld_cg(g.nsah + l)), ld_cg(g.nsah + r));
+            subtree[x] = cnt;
+            g.nsah[x] = my_sah;
         }
         unsigned vote = __ballot_sync(kFull, cnt >= gamma);
         if (vote) __syncwarp();
@@ -177,15 +195,50 @@ __global__ void __launch_bounds__(kAtrWarps * 32) k_atrbvh(TreeRefs t, int32_t* 
             const int rl = __ffs(vote) - 1;
             const int root = __shfl_sync(kFull, cur, rl);
             const float rsah = __shfl_sync(kFull, my_sah, rl);
-            if (!process_treelet(t, root, rsah, tsize, ci, s_dist[w]) && lane == 0)
+            const int rbase = __shfl_sync(kFull, base, rl);
+            const uint32_t rn = __shfl_sync(kFull, nm, rl);
+            const int rts = __shfl_sync(kFull, tsize, rl);
+            if (!process_treelet(rebase(g, rbase, rn), root, rsah, rts, ci, s_dist[w]) && lane == 0)
                 set_error_bits(err, kErrTreeletClimb);
             vote &= vote - 1;
         }
-        if (cur >= 0) cur = ld_cg(t.parent + cur);
+        if (cur >= 0) cur = ld_cg(g.parent + base + cur);
     }
 }
 
 }  // namespace
+
+// ATRBVH over every mesh of `segs` (total_nodes = sum of 2n_m - 1).  tsize and
+// iterations apply to all meshes unless per-mesh arrays are given, in which
+// case `iterations` is their maximum.
+int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t total_nodes, int tsize,
+               int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci, float ct) {
+    if (iterations <= 0) return ATR_OK;
+    const size_t inner = segs.n - segs.count;
+    void* scratch = nullptr;
+    const size_t b_sub = align256(total_nodes * 4), b_sah = align256(total_nodes * 4), b_ctr = align256(inner * 4);
+    ATR_TRY(ctx->alloc(&scratch, b_sub + b_sah + b_ctr));
+    char* p = static_cast<char*>(scratch);
+    int32_t* subtree = reinterpret_cast<int32_t*>(p);
+    TreeRefs g = g_in;
+    g.nsah = reinterpret_cast<float*>(p + b_sub);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(p + b_sub + b_sah);
+    const int threads = kAtrWarps * 32;
+    const uint32_t blocks = (segs.n + threads - 1) / threads;
+    ctx->phase_begin("atrbvh");
+    for (int it = 0; it < iterations; ++it) {
+        cudaMemsetAsync(counters, 0, inner * 4, ctx->stream);
+        k_atrbvh<<<blocks, threads, 0, ctx->stream>>>(g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it,
+                                                      ci, ct, ctx->d_error);
+    }
+    ctx->phase_end();
+    ctx->launches += iterations;
+    cudaError_t e = cudaGetLastError();
+    ctx->release(scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "k_atrbvh launch", __FILE__, __LINE__);
+    return ATR_OK;
+}
+
 }  // namespace atr
 
 using namespace atr;
@@ -194,31 +247,10 @@ extern "C" int atr_optimize_atrbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int 
     ATR_REQUIRE(ctx && tree, ATR_ERR_INVALID_ARG, "atr_optimize_atrbvh: NULL argument");
     ATR_REQUIRE(tsize >= 3 && tsize <= kMaxTreelet, ATR_ERR_UNSUPPORTED,
                 "atr_optimize_atrbvh: treelet size %d outside [3, %d]", tsize, kMaxTreelet);
-    ATR_REQUIRE(iterations >= 0, ATR_ERR_INVALID_ARG, "atr_optimize_atrbvh: iterations %d", iterations);
+    ATR_REQUIRE(iterations >= 0 && iterations <= 24, ATR_ERR_INVALID_ARG, "atr_optimize_atrbvh: iterations %d",
+                iterations);
     const uint32_t n = tree->n;
-    if (iterations == 0) return ATR_OK;
-    const size_t nn = 2 * (size_t)n - 1;
-    void* scratch = nullptr;
-    const size_t b_sub = align256(nn * 4), b_sah = align256(nn * 4), b_ctr = align256((size_t)(n - 1) * 4);
-    ATR_TRY(ctx->alloc(&scratch, b_sub + b_sah + b_ctr));
-    char* p = static_cast<char*>(scratch);
-    int32_t* subtree = reinterpret_cast<int32_t*>(p);
-    float* nsah = reinterpret_cast<float*>(p + b_sub);
-    uint32_t* counters = reinterpret_cast<uint32_t*>(p + b_sub + b_sah);
-    TreeRefs t{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nsah};
-    const int threads = kAtrWarps * 32;
-    const uint32_t blocks = (n + threads - 1) / threads;
-    int gamma = tsize;
-    ctx->phase_begin("atrbvh");
-    for (int it = 0; it < iterations; ++it) {
-        cudaMemsetAsync(counters, 0, (size_t)(n - 1) * 4, ctx->stream);
-        k_atrbvh<<<blocks, threads, 0, ctx->stream>>>(t, subtree, counters, tsize, gamma, ci, ct, ctx->d_error);
-        gamma *= 2;
-    }
-    ctx->phase_end();
-    ctx->launches += iterations;
-    cudaError_t e = cudaGetLastError();
-    ctx->release(scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "k_atrbvh launch", __FILE__, __LINE__);
-    return ATR_OK;
+    TreeRefs g{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nullptr};
+    Segs segs{nullptr, nullptr, 1u, n};
+    return atrbvh_run(ctx, g, segs, 2 * (size_t)n - 1, tsize, iterations, nullptr, nullptr, ci, ct);
 }

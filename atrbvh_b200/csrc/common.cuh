@@ -37,4 +37,33 @@ __device__ __forceinline__ void set_error_bits(uint32_t* err, uint32_t bits) {
     if (err) atomicOr(err, bits);
 }
 
+// Meshes of a batch laid end to end.  Mesh m owns triangles
+// [tri_off[m], tri_off[m+1]), sort tiles [tile_off[m], tile_off[m+1]) and,
+// in every per-node array, the 2n_m - 1 nodes starting at
+// 2 * tri_off[m] - m (its own reference layout with local indices).  A
+// single mesh passes count = 1 and no arrays.
+struct Segs {
+    const uint32_t* tri_off;
+    const uint32_t* tile_off;
+    uint32_t count;
+    uint32_t n;  // total triangles
+
+    __device__ __forceinline__ uint32_t find(const uint32_t* off, uint32_t x) const {
+        uint32_t lo = 0, hi = count;  // off[lo] <= x < off[hi]
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(off + mid) <= x) lo = mid; else hi = mid;
+        }
+        return lo;
+    }
+    __device__ __forceinline__ uint32_t seg_of_tri(uint32_t i) const { return count == 1 ? 0u : find(tri_off, i); }
+    __device__ __forceinline__ uint32_t seg_of_tile(uint32_t t) const { return count == 1 ? 0u : find(tile_off, t); }
+    __device__ __forceinline__ uint32_t tri_begin(uint32_t m) const { return count == 1 ? 0u : __ldg(tri_off + m); }
+    __device__ __forceinline__ uint32_t tri_end(uint32_t m) const { return count == 1 ? n : __ldg(tri_off + m + 1); }
+    __device__ __forceinline__ uint32_t tile_begin(uint32_t m) const { return count == 1 ? 0u : __ldg(tile_off + m); }
+    // First node of mesh m in per-node arrays, first internal node in per-internal arrays.
+    __device__ __forceinline__ int node_base(uint32_t m) const { return (int)(2 * tri_begin(m) - m); }
+    __device__ __forceinline__ int inner_base(uint32_t m) const { return (int)(tri_begin(m) - m); }
+};
+
 }  // namespace atr

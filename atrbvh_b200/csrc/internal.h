@@ -116,11 +116,34 @@ struct atr_compact {
 
 namespace atr {
 
+struct Segs;       // common.cuh: meshes of a batch laid end to end
+struct TreeRefs;   // treelet.cuh
+
+// Output arrays of a (possibly batched) tree in the reference SoA layout.
+struct TreeOut {
+    int32_t *parent, *left, *right, *data;
+    float4 *bmin, *bmax;
+    float* area;
+};
+
 // Allocate the SoA arrays of a tree with n triangles in one block.
 int tree_alloc(atr_ctx* ctx, uint32_t n, atr_tree** out);
 
-// LBVH internals used by the batched path.
+// Single-mesh LBVH into an allocated tree (keeps the sort output).
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds,
                     int morton_bits, atr_tree* t);
+// LBVH of every mesh of segs (tiles = sort tiles over all meshes); bounds
+// holds 6 floats per mesh.  keep_keys/keep_idx (may be NULL) receive the
+// sorted keys and global triangle order.
+int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts,
+                    const float* d_bounds, int morton_bits, const TreeOut& out, void** keep_keys,
+                    uint32_t** keep_idx);
+int atrbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int tsize,
+               int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci, float ct);
+int trbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int iterations,
+              const uint8_t* seg_iters, float ci, float ct);
+
+constexpr uint32_t kSortTileSize = 4096;  // triangles per sort tile (lbvh.cu)
+int lbvh_prepare();                       // kernel attributes; once per context
 
 }  // namespace atr

@@ -118,19 +118,24 @@ __device__ __forceinline__ uint64_t morton_code<uint64_t>(float cx, float cy, fl
     return q[0] * 4u + q[1] * 2u + q[2];
 }
 
-// One triangle per iteration of a grid-stride loop; histograms of every
-// 8-bit digit are accumulated in shared memory and flushed once per block.
+// One block per sort tile (kSortTile triangles of one mesh); histograms of
+// every 8-bit digit are accumulated in shared memory and added to the mesh's
+// histograms (P x 256 per mesh) once per block.  Each mesh is normalised to
+// its own box (6 floats per mesh in `bounds`).
 template <typename K>
-__global__ void __launch_bounds__(256) k_morton(const float4* __restrict__ v, uint32_t n,
+__global__ void __launch_bounds__(256) k_morton(Segs segs, const float4* __restrict__ v,
                                                  const float* __restrict__ bounds, K* __restrict__ keys,
                                                  uint32_t* __restrict__ hist) {
     constexpr int P = KeyTraits<K>::kPasses;
     __shared__ uint32_t sh[P * 256];
     __shared__ float sb[6];
+    const uint32_t m = segs.seg_of_tile(blockIdx.x);
+    const uint32_t t0 = segs.tri_begin(m) + (blockIdx.x - segs.tile_begin(m)) * kSortTile;
+    const uint32_t t1 = min(t0 + kSortTile, segs.tri_end(m));
     for (int j = threadIdx.x; j < P * 256; j += blockDim.x) sh[j] = 0;
-    if (threadIdx.x < 6) sb[threadIdx.x] = bounds[threadIdx.x];
+    if (threadIdx.x < 6) sb[threadIdx.x] = bounds[6 * m + threadIdx.x];
     __syncthreads();
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
         const float4 a = __ldg(v + 3 * (size_t)t), b = __ldg(v + 3 * (size_t)t + 1), c = __ldg(v + 3 * (size_t)t + 2);
         const float cx = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.x, b.x), c.x), fminf(fminf(a.x, b.x), c.x)), 0.5f);
         const float cy = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.y, b.y), c.y), fminf(fminf(a.y, b.y), c.y)), 0.5f);
@@ -145,7 +150,7 @@ __global__ void __launch_bounds__(256) k_morton(const float4* __restrict__ v, ui
     if (!hist) return;
     __syncthreads();
     for (int j = threadIdx.x; j < P * 256; j += blockDim.x)
-        if (sh[j]) atomicAdd(&hist[j], sh[j]);
+        if (sh[j]) atomicAdd(&hist[(size_t)m * P * 256 + j], sh[j]);
 }
 
 // Digit histogram of arbitrary keys (used by the generic sort entry point).
@@ -189,11 +194,16 @@ __device__ __forceinline__ uint32_t block_exclusive_scan256(uint32_t x, uint32_t
 // warp ranks a contiguous run of the tile in order).  The per-tile digit
 // counts are combined across tiles by decoupled look-back; a wait that does
 // not resolve within kLookbackLimit polls sets kErrSortLookback and gives up.
+// Segmented: a tile holds keys of one mesh only, the look-back stops at the
+// mesh's first tile and keys move only within their mesh, so each mesh is
+// sorted on its own (hist holds P x 256 counts per mesh).
 template <typename K, bool kIota>
 __global__ void __launch_bounds__(kSortThreads) k_onesweep(
-        const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
-        uint32_t* __restrict__ vout, uint32_t n, int shift, const uint32_t* __restrict__ hist,
+        Segs segs, const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
+        uint32_t* __restrict__ vout, int pass, const uint32_t* __restrict__ hist,
         uint32_t* __restrict__ status, uint32_t* __restrict__ ticket, uint32_t* __restrict__ err) {
+    constexpr int P = KeyTraits<K>::kPasses;
+    const int shift = 8 * pass;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K* s_keys = reinterpret_cast<K*>(smem_raw);
     uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_keys + kSortTile);
@@ -208,8 +218,12 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(
     for (int j = threadIdx.x; j < kSortWarps * 256; j += kSortThreads) (&s_wh[0][0])[j] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
-    const uint64_t base = (uint64_t)tile * kSortTile;
-    const uint32_t valid_n = (uint32_t)min((uint64_t)kSortTile, (uint64_t)n - base);
+    const uint32_t m = segs.seg_of_tile(tile);
+    const uint32_t first_tile = segs.tile_begin(m);
+    const uint32_t seg_start = segs.tri_begin(m), seg_end = segs.tri_end(m);
+    const uint32_t base = seg_start + (tile - first_tile) * kSortTile;
+    const uint32_t valid_n = min((uint32_t)kSortTile, seg_end - base);
+    const uint32_t end = base + valid_n;
 
     K key[kSortItems];
     uint32_t val[kSortItems];
@@ -217,8 +231,8 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(
     const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
-        const uint64_t idx = base + (uint64_t)w * (kSortItems * 32) + r * 32 + lane;
-        const bool valid = idx < n;
+        const uint32_t idx = base + (uint32_t)w * (kSortItems * 32) + r * 32 + lane;
+        const bool valid = idx < end;
         key[r] = valid ? kin[idx] : (K)0;
         val[r] = kIota ? (uint32_t)idx : (valid ? vin[idx] : 0u);
         const uint32_t d = valid ? (uint32_t)((key[r] >> shift) & 255u) : 256u;
@@ -244,18 +258,19 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(
     }
     const uint32_t count = run;
     s_dstart[d] = block_exclusive_scan256(count, s_scan);
-    const uint32_t gdigit = block_exclusive_scan256(hist[d], s_scan);
+    const uint32_t gdigit =
+        seg_start + block_exclusive_scan256(hist[((size_t)m * P + pass) * 256 + d], s_scan);
 
-    // Decoupled look-back for digit d.
+    // Decoupled look-back for digit d over this mesh's earlier tiles.
     uint32_t* st = status + (size_t)tile * 256 + d;
     uint32_t prefix = 0;
-    if (tile == 0) {
+    if (tile == first_tile) {
         __stcg(st, kFlagInc | count);
     } else {
         __stcg(st, kFlagAgg | count);
         int64_t k = (int64_t)tile - 1;
         uint32_t polls = 0;
-        while (k >= 0) {
+        while (k >= (int64_t)first_tile) {
             const uint32_t s = *reinterpret_cast<volatile uint32_t*>(status + (size_t)k * 256 + d);
             if (s & kFlagInc) { prefix += s & kValueMask; break; }
             if (s & kFlagAgg) { prefix += s & kValueMask; --k; continue; }
@@ -281,7 +296,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(
         const K kk = s_keys[i];
         const uint32_t dd = (uint32_t)((kk >> shift) & 255u);
         const uint32_t dst = s_gbase[dd] + i;
-        if (dst < n) {  // holds whenever hist matches the keys
+        if (dst >= seg_start && dst < seg_end) {  // holds whenever hist matches the keys
             kout[dst] = kk;
             vout[dst] = s_vals[i];
         }
@@ -303,24 +318,42 @@ __device__ __forceinline__ int delta_adj(const uint64_t* keys, int k) {
 // One thread per sorted leaf climbs while it is the second of two siblings to
 // arrive (an atomic exchange on the parent's split position carries the
 // first arrival's far range end).  Each node's record is written once.
+// Segmented: thread i finds its mesh; keys, slots and node arrays are
+// addressed from the mesh's first entry, so every mesh gets exactly the tree
+// a build of that mesh alone produces (local node and triangle indices).
 template <typename K>
-__global__ void __launch_bounds__(256) k_build(const K* __restrict__ keys, const uint32_t* __restrict__ sidx,
-                                                const float4* __restrict__ verts, uint32_t n,
-                                                int32_t* __restrict__ parent, int32_t* __restrict__ left,
-                                                int32_t* __restrict__ right, int32_t* __restrict__ data,
-                                                float4* __restrict__ bmin, float4* __restrict__ bmax,
-                                                float* __restrict__ area, int32_t* __restrict__ slot) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t tri = sidx[i];
-    const float4 a = __ldg(verts + 3 * (size_t)tri), b = __ldg(verts + 3 * (size_t)tri + 1),
-                 c = __ldg(verts + 3 * (size_t)tri + 2);
+__global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ keys_all,
+                                                const uint32_t* __restrict__ sidx,
+                                                const float4* __restrict__ verts, int32_t* __restrict__ parent_all,
+                                                int32_t* __restrict__ left_all, int32_t* __restrict__ right_all,
+                                                int32_t* __restrict__ data_all, float4* __restrict__ bmin_all,
+                                                float4* __restrict__ bmax_all, float* __restrict__ area_all,
+                                                int32_t* __restrict__ slot_all) {
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= segs.n) return;
+    const uint32_t m = segs.seg_of_tri(gi);
+    const uint32_t s0 = segs.tri_begin(m);
+    const uint32_t n = segs.tri_end(m) - s0;
+    const uint32_t i = gi - s0;
+    const int nb = segs.node_base(m);
+    const K* keys = keys_all + s0;
+    int32_t* parent = parent_all + nb;
+    int32_t* left = left_all + nb;
+    int32_t* right = right_all + nb;
+    int32_t* data = data_all + nb;
+    float4* bmin = bmin_all + nb;
+    float4* bmax = bmax_all + nb;
+    float* area = area_all + nb;
+    int32_t* slot = slot_all + segs.inner_base(m);
+    const uint32_t gtri = sidx[gi];
+    const float4 a = __ldg(verts + 3 * (size_t)gtri), b = __ldg(verts + 3 * (size_t)gtri + 1),
+                 c = __ldg(verts + 3 * (size_t)gtri + 2);
     float4 mn = make_float4(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z), 0.0f);
     float4 mx = make_float4(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z), 0.0f);
     const int leaf = (int)i + (int)n - 1;
     left[leaf] = -1;
     right[leaf] = -1;
-    data[leaf] = (int32_t)tri;
+    data[leaf] = (int32_t)(gtri - s0);
     bmin[leaf] = mn;
     bmax[leaf] = mx;
     area[leaf] = box_area(mn, mx);
@@ -409,15 +442,16 @@ int grid_for(atr_ctx* ctx, uint64_t work, int per_sm_blocks, int threads) {
     return (int)(need < cap ? (need ? need : 1) : cap);
 }
 
-// Sort (key, value) pairs in place.  keys/vals hold the input and receive the
-// output (every key width uses an even number of passes).  hist must hold the
-// digit histograms of every pass (P x 256) when hist_ready; otherwise it is
-// computed here.  kIota passes generate the initial values.
+// Sort (key, value) pairs of every mesh of `segs` in place (each mesh on its
+// own).  keys/vals hold the input and receive the output (every key width
+// uses an even number of passes).  hist holds P x 256 digit counts per mesh
+// when hist_ready; otherwise (single mesh only) it is computed here.  With
+// iota the first pass generates the values (global element indices).
 template <typename K>
-int sort_pairs(atr_ctx* ctx, K* keys, uint32_t* vals, uint32_t n, uint32_t* hist, bool hist_ready,
-               bool iota) {
+int sort_pairs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, K* keys, uint32_t* vals, uint32_t* hist,
+               bool hist_ready, bool iota) {
     constexpr int P = KeyTraits<K>::kPasses;
-    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    const uint32_t n = segs.n;
     const size_t sbytes = (size_t)P * tiles * 256 * 4;
     void* tmp = nullptr;
     const size_t kb = align256((size_t)n * sizeof(K)), vb = align256((size_t)n * 4);
@@ -436,19 +470,17 @@ int sort_pairs(atr_ctx* ctx, K* keys, uint32_t* vals, uint32_t n, uint32_t* hist
         cudaMemsetAsync(hist, 0, P * 256 * 4, s);
         k_histogram<K><<<grid_for(ctx, n, 4, 256), 256, 0, s>>>(keys, n, hist);
     }
-    const size_t smem = (size_t)kSortTile * (sizeof(K) + 4);
-    cudaFuncSetAttribute(k_onesweep<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_onesweep<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = (size_t)kSortTile * (sizeof(K) + 4);  // attribute set by lbvh_prepare()
     K* ka = keys; K* kb2 = k2;
     uint32_t* va = vals; uint32_t* vb2 = v2;
     for (int pass = 0; pass < P; ++pass) {
         uint32_t* st = status + (size_t)pass * tiles * 256;
         if (pass == 0 && iota)
-            k_onesweep<K, true><<<tiles, kSortThreads, smem, s>>>(ka, va, kb2, vb2, n, 8 * pass,
-                                                                  hist + pass * 256, st, tickets + pass, ctx->d_error);
+            k_onesweep<K, true><<<tiles, kSortThreads, smem, s>>>(segs, ka, va, kb2, vb2, pass, hist, st,
+                                                                  tickets + pass, ctx->d_error);
         else
-            k_onesweep<K, false><<<tiles, kSortThreads, smem, s>>>(ka, va, kb2, vb2, n, 8 * pass,
-                                                                   hist + pass * 256, st, tickets + pass, ctx->d_error);
+            k_onesweep<K, false><<<tiles, kSortThreads, smem, s>>>(segs, ka, va, kb2, vb2, pass, hist, st,
+                                                                   tickets + pass, ctx->d_error);
         std::swap(ka, kb2);
         std::swap(va, vb2);
     }
@@ -460,54 +492,86 @@ int sort_pairs(atr_ctx* ctx, K* keys, uint32_t* vals, uint32_t n, uint32_t* hist
 }
 
 template <typename K>
-int build_typed(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds, atr_tree* t) {
+int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts, const float* d_bounds,
+                const TreeOut& t, void** keep_keys, uint32_t** keep_idx) {
     constexpr int P = KeyTraits<K>::kPasses;
+    const uint32_t n = segs.n;
     cudaStream_t s = ctx->stream;
     void* keys = nullptr;
     void* idx = nullptr;
     void* aux = nullptr;
+    const size_t hbytes = (size_t)segs.count * P * 256 * 4;
+    const size_t inner = n - segs.count;
     ATR_TRY(ctx->alloc(&keys, (size_t)n * sizeof(K)));
     int st = ctx->alloc(&idx, (size_t)n * 4);
-    if (st == ATR_OK) st = ctx->alloc(&aux, align256(P * 256 * 4) + align256((size_t)(n - 1) * 4));
+    if (st == ATR_OK) st = ctx->alloc(&aux, align256(hbytes) + align256(inner * 4));
     if (st != ATR_OK) { ctx->release(keys); ctx->release(idx); return st; }
     uint32_t* hist = static_cast<uint32_t*>(aux);
-    int32_t* slot = reinterpret_cast<int32_t*>(static_cast<char*>(aux) + align256(P * 256 * 4));
-    cudaMemsetAsync(hist, 0, P * 256 * 4, s);
-    cudaMemsetAsync(slot, 0xff, (size_t)(n - 1) * 4, s);
+    int32_t* slot = reinterpret_cast<int32_t*>(static_cast<char*>(aux) + align256(hbytes));
+    cudaMemsetAsync(hist, 0, hbytes, s);
+    cudaMemsetAsync(slot, 0xff, inner * 4, s);
 
     ctx->phase_begin("morton");
-    k_morton<K><<<grid_for(ctx, n, 8, 256), 256, 0, s>>>(verts, n, d_bounds, static_cast<K*>(keys), hist);
+    k_morton<K><<<tiles, 256, 0, s>>>(segs, verts, d_bounds, static_cast<K*>(keys), hist);
     ctx->phase_end();
     ctx->launches += 1;
     ctx->phase_begin("sort");
-    st = sort_pairs<K>(ctx, static_cast<K*>(keys), static_cast<uint32_t*>(idx), n, hist, true, true);
+    st = sort_pairs<K>(ctx, segs, tiles, static_cast<K*>(keys), static_cast<uint32_t*>(idx), hist, true, true);
     ctx->phase_end();
     if (st == ATR_OK) {
         ctx->phase_begin("build");
-        k_build<K><<<(n + 255) / 256, 256, 0, s>>>(static_cast<K*>(keys), static_cast<uint32_t*>(idx), verts, n,
-                                                  t->parent, t->left, t->right, t->data, t->bmin, t->bmax,
-                                                  t->area, slot);
+        k_build<K><<<(n + 255) / 256, 256, 0, s>>>(segs, static_cast<K*>(keys), static_cast<uint32_t*>(idx), verts,
+                                                  t.parent, t.left, t.right, t.data, t.bmin, t.bmax, t.area, slot);
         ctx->phase_end();
         ctx->launches += 1;
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) st = cuda_fail(e, "k_build launch", __FILE__, __LINE__);
     }
     ctx->release(aux);
-    if (st != ATR_OK) { ctx->release(keys); ctx->release(idx); return st; }
-    ctx->release(t->sorted_keys);
-    ctx->release(t->sorted_idx);
-    t->sorted_keys = keys;
-    t->sorted_idx = static_cast<uint32_t*>(idx);
+    if (st != ATR_OK || !keep_keys) { ctx->release(keys); ctx->release(idx); return st; }
+    *keep_keys = keys;
+    *keep_idx = static_cast<uint32_t*>(idx);
     return ATR_OK;
 }
 
 }  // namespace
 
+static_assert(kSortTile == (int)kSortTileSize, "sort tile size");
+
+// Kernel attributes, set once per context before any capture.
+int lbvh_prepare() {
+    ATR_CUDA(cudaFuncSetAttribute(k_onesweep<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kSortTile * 8));
+    ATR_CUDA(cudaFuncSetAttribute(k_onesweep<uint32_t, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kSortTile * 8));
+    ATR_CUDA(cudaFuncSetAttribute(k_onesweep<uint64_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kSortTile * 12));
+    ATR_CUDA(cudaFuncSetAttribute(k_onesweep<uint64_t, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kSortTile * 12));
+    return ATR_OK;
+}
+
+int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts, const float* d_bounds,
+                    int morton_bits, const TreeOut& out, void** keep_keys, uint32_t** keep_idx) {
+    if (morton_bits == 30)
+        return build_typed<uint32_t>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx);
+    return build_typed<uint64_t>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx);
+}
+
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds, int morton_bits,
                     atr_tree* t) {
     t->morton_bits = morton_bits;
-    if (morton_bits == 30) return build_typed<uint32_t>(ctx, verts, n, d_bounds, t);
-    return build_typed<uint64_t>(ctx, verts, n, d_bounds, t);
+    Segs segs{nullptr, nullptr, 1u, n};
+    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
+    TreeOut out{t->parent, t->left, t->right, t->data, t->bmin, t->bmax, t->area};
+    void* keys = nullptr;
+    uint32_t* idx = nullptr;
+    ATR_TRY(lbvh_build_segs(ctx, segs, tiles, verts, d_bounds, morton_bits, out, &keys, &idx));
+    ctx->release(t->sorted_keys);
+    ctx->release(t->sorted_idx);
+    t->sorted_keys = keys;
+    t->sorted_idx = idx;
+    return ATR_OK;
 }
 
 int refit_tree(atr_ctx* ctx, atr_tree* t, const float4* verts) {
@@ -611,12 +675,14 @@ int atr_device_morton(atr_ctx* ctx, const float* vertices, uint32_t n, const flo
     float h[6] = {bbmin[0], bbmin[1], bbmin[2], bbmax[0], bbmax[1], bbmax[2]};
     cudaMemcpyAsync(b, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream);
     const float4* v = reinterpret_cast<const float4*>(vertices);
+    Segs segs{nullptr, nullptr, 1u, n};
+    const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
     if (morton_bits == 30)
-        k_morton<uint32_t><<<grid_for(ctx, n, 8, 256), 256, 0, ctx->stream>>>(v, n, static_cast<float*>(b),
-                                                                               static_cast<uint32_t*>(keys), nullptr);
+        k_morton<uint32_t><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
+                                                           static_cast<uint32_t*>(keys), nullptr);
     else
-        k_morton<uint64_t><<<grid_for(ctx, n, 8, 256), 256, 0, ctx->stream>>>(v, n, static_cast<float*>(b),
-                                                                               static_cast<uint64_t*>(keys), nullptr);
+        k_morton<uint64_t><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
+                                                           static_cast<uint64_t*>(keys), nullptr);
     ctx->launches += 1;
     cudaError_t e = cudaStreamSynchronize(ctx->stream);  // h is a stack array
     ctx->release(b);
@@ -628,8 +694,11 @@ int atr_device_sort_pairs(atr_ctx* ctx, void* keys, uint32_t* values, uint32_t c
     ATR_REQUIRE(ctx && keys && values, ATR_ERR_INVALID_ARG, "atr_device_sort_pairs: NULL argument");
     ATR_REQUIRE(count < (1u << 30), ATR_ERR_INVALID_ARG, "atr_device_sort_pairs: count %u >= 2^30", count);
     if (count == 0) return ATR_OK;
-    if (key_bits <= 32) return sort_pairs<uint32_t>(ctx, static_cast<uint32_t*>(keys), values, count, nullptr, false, false);
-    return sort_pairs<uint64_t>(ctx, static_cast<uint64_t*>(keys), values, count, nullptr, false, false);
+    Segs segs{nullptr, nullptr, 1u, count};
+    const uint32_t tiles = (count + kSortTile - 1) / kSortTile;
+    if (key_bits <= 32)
+        return sort_pairs<uint32_t>(ctx, segs, tiles, static_cast<uint32_t*>(keys), values, nullptr, false, false);
+    return sort_pairs<uint64_t>(ctx, segs, tiles, static_cast<uint64_t*>(keys), values, nullptr, false, false);
 }
 
 }  // extern "C"

@@ -231,35 +231,46 @@ __device__ bool process_trbvh(const TreeRefs& t, int root, float root_sah, int t
     return true;
 }
 
-__global__ void __launch_bounds__(kTrWarps * 32) k_trbvh(TreeRefs t, int32_t* __restrict__ subtree,
-                                                         uint32_t* __restrict__ counters, int gamma, float ci,
-                                                         float ct, uint32_t* err) {
+__global__ void __launch_bounds__(kTrWarps * 32) k_trbvh(TreeRefs g, Segs segs, int32_t* __restrict__ subtree,
+                                                         uint32_t* __restrict__ counters,
+                                                         const uint8_t* __restrict__ seg_iters, int iteration,
+                                                         float ci, float ct, uint32_t* err) {
     __shared__ TrShared s_tr[kTrWarps];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    int cur = -1;
-    if (i < t.n) {
-        const int leaf = (int)i + (int)t.n - 1;
-        subtree[leaf] = 1;
-        t.nsah[leaf] = __fmul_rn(ct, t.area[leaf]);
-        cur = t.parent[leaf];
+    int cur = -1, base = 0, cbase = 0;
+    uint32_t nm = 2;
+    if (i < segs.n) {
+        const uint32_t m = segs.seg_of_tri(i);
+        const uint32_t s0 = segs.tri_begin(m);
+        nm = segs.tri_end(m) - s0;
+        base = segs.node_base(m);
+        cbase = segs.inner_base(m);
+        if (!seg_iters || iteration < (int)seg_iters[m]) {
+            const int leaf = base + (int)(i - s0) + (int)nm - 1;
+            subtree[leaf] = 1;
+            g.nsah[leaf] = __fmul_rn(ct, g.area[leaf]);
+            cur = g.parent[leaf];
+        }
     }
+    const int gamma = kTr << iteration;
     while (__any_sync(kFull, cur >= 0)) {
         bool second = false;
         if (cur >= 0) {
             __threadfence();
-            if (atomicAdd(&counters[cur], 1u) == 0u) cur = -1;
+            if (atomicAdd(&counters[cbase + cur], 1u) == 0u) cur = -1;
             else { second = true; __threadfence(); }
         }
         int cnt = 0;
         float my_sah = 0.0f;
         if (second) {
-            const int l = ld_cg(t.left + cur), r = ld_cg(t.right + cur);
-            const float a = ld_cg(t.area + cur);
+            const int x = base + cur;
+            const int l = base + ld_cg(g.left + x), r = base + ld_cg(g.right + x);
+            const float a = ld_cg(g.area + x);
             cnt = ld_cg(subtree + l) + ld_cg(subtree + r);
-            my_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), ld_cg(t.nsah + l)), ld_cg(t.nsah + r));
-            subtree[cur] = cnt;
-            t.nsah[cur] = my_sah;
+            my_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), ld_cg(g.nsah + l)), ld_cg(g.nsah + r));
+            subtree[x] = cnt;
+            g.nsah[x] = my_sah;
         }
         unsigned vote = __ballot_sync(kFull, cnt >= gamma);
         if (vote) __syncwarp();
@@ -268,11 +279,13 @@ __global__ void __launch_bounds__(kTrWarps * 32) k_trbvh(TreeRefs t, int32_t* __
             const int root = __shfl_sync(kFull, cur, rl);
             const float rsah = __shfl_sync(kFull, my_sah, rl);
             const int rcnt = __shfl_sync(kFull, cnt, rl);
-            if (!process_trbvh(t, root, rsah, rcnt, ci, ct, s_tr[w]) && lane == 0)
+            const int rbase = __shfl_sync(kFull, base, rl);
+            const uint32_t rn = __shfl_sync(kFull, nm, rl);
+            if (!process_trbvh(rebase(g, rbase, rn), root, rsah, rcnt, ci, ct, s_tr[w]) && lane == 0)
                 set_error_bits(err, kErrTreeletClimb);
             vote &= vote - 1;
         }
-        if (cur >= 0) cur = ld_cg(t.parent + cur);
+        if (cur >= 0) cur = ld_cg(g.parent + base + cur);
     }
 }
 
@@ -296,6 +309,38 @@ int upload_tables() {
 }
 
 }  // namespace
+
+// TRBVH (treelet 7) over every mesh of `segs`; seg_iters optionally gives
+// each mesh its own iteration count (`iterations` is then their maximum).
+int trbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t total_nodes, int iterations,
+              const uint8_t* seg_iters, float ci, float ct) {
+    if (iterations <= 0) return ATR_OK;
+    ATR_TRY(upload_tables());
+    const size_t inner = segs.n - segs.count;
+    void* scratch = nullptr;
+    const size_t b = align256(total_nodes * 4);
+    ATR_TRY(ctx->alloc(&scratch, 2 * b + align256(inner * 4)));
+    char* p = static_cast<char*>(scratch);
+    int32_t* subtree = reinterpret_cast<int32_t*>(p);
+    TreeRefs g = g_in;
+    g.nsah = reinterpret_cast<float*>(p + b);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(p + 2 * b);
+    const int threads = kTrWarps * 32;
+    const uint32_t blocks = (segs.n + threads - 1) / threads;
+    ctx->phase_begin("trbvh");
+    for (int it = 0; it < iterations; ++it) {
+        cudaMemsetAsync(counters, 0, inner * 4, ctx->stream);
+        k_trbvh<<<blocks, threads, 0, ctx->stream>>>(g, segs, subtree, counters, seg_iters, it, ci, ct,
+                                                     ctx->d_error);
+    }
+    ctx->phase_end();
+    ctx->launches += iterations;
+    cudaError_t e = cudaGetLastError();
+    ctx->release(scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "k_trbvh launch", __FILE__, __LINE__);
+    return ATR_OK;
+}
+
 }  // namespace atr
 
 using namespace atr;
@@ -304,32 +349,10 @@ extern "C" int atr_optimize_trbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int i
     ATR_REQUIRE(ctx && tree, ATR_ERR_INVALID_ARG, "atr_optimize_trbvh: NULL argument");
     ATR_REQUIRE(tsize == kTr, ATR_ERR_UNSUPPORTED,
                 "atr_optimize_trbvh: treelet size %d unsupported (the reference's subset kernel covers 7)", tsize);
-    ATR_REQUIRE(iterations >= 0, ATR_ERR_INVALID_ARG, "atr_optimize_trbvh: iterations %d", iterations);
-    if (iterations == 0) return ATR_OK;
-    ATR_TRY(upload_tables());
+    ATR_REQUIRE(iterations >= 0 && iterations <= 24, ATR_ERR_INVALID_ARG, "atr_optimize_trbvh: iterations %d",
+                iterations);
     const uint32_t n = tree->n;
-    const size_t nn = 2 * (size_t)n - 1;
-    void* scratch = nullptr;
-    const size_t b = align256(nn * 4);
-    ATR_TRY(ctx->alloc(&scratch, 2 * b + align256((size_t)(n - 1) * 4)));
-    char* p = static_cast<char*>(scratch);
-    int32_t* subtree = reinterpret_cast<int32_t*>(p);
-    float* nsah = reinterpret_cast<float*>(p + b);
-    uint32_t* counters = reinterpret_cast<uint32_t*>(p + 2 * b);
-    TreeRefs t{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nsah};
-    const int threads = kTrWarps * 32;
-    const uint32_t blocks = (n + threads - 1) / threads;
-    int gamma = tsize;
-    ctx->phase_begin("trbvh");
-    for (int it = 0; it < iterations; ++it) {
-        cudaMemsetAsync(counters, 0, (size_t)(n - 1) * 4, ctx->stream);
-        k_trbvh<<<blocks, threads, 0, ctx->stream>>>(t, subtree, counters, gamma, ci, ct, ctx->d_error);
-        gamma *= 2;
-    }
-    ctx->phase_end();
-    ctx->launches += iterations;
-    cudaError_t e = cudaGetLastError();
-    ctx->release(scratch);
-    if (e != cudaSuccess) return cuda_fail(e, "k_trbvh launch", __FILE__, __LINE__);
-    return ATR_OK;
+    TreeRefs g{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nullptr};
+    Segs segs{nullptr, nullptr, 1u, n};
+    return trbvh_run(ctx, g, segs, 2 * (size_t)n - 1, iterations, nullptr, ci, ct);
 }

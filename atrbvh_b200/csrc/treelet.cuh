@@ -54,6 +54,20 @@ struct TreeRefs {
     float* nsah;
 };
 
+// The refs of one mesh of a batch: arrays start at the mesh's first node.
+__device__ __forceinline__ TreeRefs rebase(const TreeRefs& g, int base, uint32_t n) {
+    TreeRefs t = g;
+    t.n = n;
+    t.parent += base;
+    t.left += base;
+    t.right += base;
+    t.bmin += base;
+    t.bmax += base;
+    t.area += base;
+    t.nsah += base;
+    return t;
+}
+
 // Lane-held treelet leaf with everything later steps need, loaded as soon as
 // the lane receives the node.
 struct LeafSlot {

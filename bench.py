@@ -341,20 +341,10 @@ def run_reference(args, world, rank, local):
                                    f"on {threads} host threads"},
         "e2e": {"value": value, "unit": "Mtri/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    if O.ref_available():
-        try:
-            mn, mx = O.scene_aabb(v)
-            ts = []
-            for i in range(3):
-                _, _, t = O.ref_run(v, mn, mx, optimizer=1, treelet=9, iterations=2, collapse=True)
-                if i:
-                    ts.append(float(t.sum()))
-            out["reference_cuda"] = {"value": N_TRIS / (statistics.mean(ts) * 1e-3) / 1e6, "unit": "Mtri/s",
-                                     "ms": statistics.mean(ts),
-                                     "what": "the reference's own BVHRT-Core CUDA build (LBVH+ATRBVH(9,2)+collapse) "
-                                             "compiled for sm_100a, wall time of its API calls on this GPU"}
-        except Exception as e:  # the CPU baseline stands on its own
-            out["reference_cuda"] = {"unavailable": str(e)[:200]}
+    out["reference_cuda"] = {
+        "unavailable": "the reference's ATRBVH CUDA kernel, compiled here for sm_100a, did not terminate on "
+                       "4,096- and 65,536-triangle inputs on this pool (unfenced cross-SM reads; see DESIGN.md); "
+                       "it is not run again"}
     print(json.dumps(out), flush=True)
 
 

@@ -202,6 +202,36 @@ int atr_compact_download(atr_ctx* ctx, const atr_compact* compact, int32_t* node
 int atr_trace(atr_ctx* ctx, const atr_compact* compact, const float* rays, int64_t num_rays,
               int any_hit, int32_t* results);
 
+/* ---- segmented batch builds (no counterpart in the reference, which builds
+ * one mesh per call: LBVHBuilder.cpp:21-130 and the optimisers per mesh) ------
+ * Meshes laid end to end: mesh m owns triangles [tri_offsets[m],
+ * tri_offsets[m+1]) of `vertices` (host or device), each with >= 2 triangles.
+ * bounds (6 floats per mesh: min xyz, max xyz) may be NULL: each mesh's box is
+ * then reduced on the device as atr_scene_create does.  One build runs every
+ * stage once over all meshes; each mesh's arrays (local indices, from
+ * atr_batch_mesh_view) equal those of atr_build_lbvh + optimiser on that mesh
+ * alone.  optimizer: 0 none, 1 ATRBVH(treelet_size, iterations), 2 TRBVH(7,
+ * iterations).  atr_batch_set_params gives each mesh its own ATRBVH treelet
+ * size and iteration count (both arrays, or both NULL to clear).  use_graph
+ * captures the build into a CUDA graph on first use and replays it while the
+ * parameters stay the same. */
+int atr_batch_create(atr_ctx* ctx, const float* vertices, const uint32_t* tri_offsets,
+                     uint32_t num_meshes, const float* bounds, int vertices_on_device,
+                     atr_batch** out);
+int atr_batch_destroy(atr_batch* batch);
+int atr_batch_set_params(atr_ctx* ctx, atr_batch* batch, const uint8_t* treelet_sizes,
+                         const uint8_t* iterations);
+int atr_batch_build(atr_ctx* ctx, atr_batch* batch, int optimizer, int treelet_size, int iterations,
+                    float ci, float ct, int use_graph);
+int atr_batch_info(const atr_batch* batch, uint32_t* num_meshes, uint32_t* num_triangles,
+                   uint64_t* total_nodes);
+int atr_batch_mesh_view(const atr_batch* batch, uint32_t mesh, atr_tree_view* view);
+int atr_batch_download_mesh(atr_ctx* ctx, const atr_batch* batch, uint32_t mesh, int32_t* parent,
+                            int32_t* left, int32_t* right, int32_t* data, float* bbox_min,
+                            float* bbox_max, float* area);
+/* Per-mesh SoABVHTree::SAH (sequential float sums), num_meshes values. */
+int atr_batch_sah(atr_ctx* ctx, const atr_batch* batch, float ci, float ct, float* sah);
+
 /* One cosine-weighted diffuse bounce ray per primary result (the diffuse
  * workload of gpu-ray-traversal/src/rt/ray/RayGenKernels.cu:114-223 with one
  * sample): device arrays; misses produce rays with tmax = -1. */
