@@ -106,6 +106,12 @@ _SIGS = [
     ("atr_batch_mesh_view", C.c_int, [_p, C.c_uint32, C.POINTER(TreeView)]),
     ("atr_batch_download_mesh", C.c_int, [_p, _p, C.c_uint32, _p, _p, _p, _p, _p, _p, _p]),
     ("atr_batch_sah", C.c_int, [_p, _p, C.c_float, C.c_float, _p]),
+    ("atr_batch_collapse", C.c_int, [_p, _p, C.c_float, C.c_float, C.c_int, _p]),
+    ("atr_batch_flatten", C.c_int, [_p, _p]),
+    ("atr_batch_compact_view", C.c_int, [_p, C.c_uint32, C.POINTER(CompactView)]),
+    ("atr_batch_compact_download", C.c_int, [_p, _p, C.c_uint32, _p, _p, _p]),
+    ("atr_batch_trace", C.c_int, [_p, _p, _p, C.c_int64, _p, _p, C.c_uint32, C.c_int, _p]),
+    ("atr_batch_refit_mesh", C.c_int, [_p, _p, C.c_uint32, _p, C.c_int]),
     ("atr_gen_bounce_rays", C.c_int, [_p, _p, _p, _p, C.c_int64, C.c_uint64, _p]),
     ("atr_gen_scene", C.c_int, [C.c_int, C.c_uint32, C.c_uint64, _p]),
     ("atr_gen_batch_sizes", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _p]),
@@ -517,6 +523,44 @@ class Batch:
         out = np.empty(self.count, np.float32)
         check(lib().atr_batch_sah(self.ctx.handle, self.handle, ci, ct, _ptr(out)))
         return out
+
+    def collapse(self, ci: float = 1.2, ct: float = 1.0, max_leaf: int = 0, want_sah: bool = True):
+        out = np.empty(self.count, np.float32) if want_sah else None
+        check(lib().atr_batch_collapse(self.ctx.handle, self.handle, ci, ct, max_leaf,
+                                       _ptr(out) if want_sah else None))
+        return out
+
+    def flatten(self) -> None:
+        check(lib().atr_batch_flatten(self.ctx.handle, self.handle))
+
+    def compact_view(self, m: int) -> CompactView:
+        v = CompactView()
+        check(lib().atr_batch_compact_view(self.handle, m, C.byref(v)))
+        return v
+
+    def compact(self, m: int) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Host copies of mesh m's Compact2 arrays (nodes, woop, tri_index)."""
+        v = self.compact_view(m)
+        nodes = np.empty((v.num_nodes, 16), np.int32)
+        woop = np.empty((v.num_woop, 4), np.float32)
+        tri = np.empty(v.num_woop, np.int32)
+        check(lib().atr_batch_compact_download(self.ctx.handle, self.handle, m, _ptr(nodes), _ptr(woop), _ptr(tri)))
+        return nodes, woop, tri
+
+    def trace(self, rays_ptr: int, num_rays: int, ray_offsets, group_mesh, results_ptr: int,
+              any_hit: bool = False) -> None:
+        off = np.ascontiguousarray(ray_offsets, dtype=np.uint32)
+        gm = np.ascontiguousarray(group_mesh, dtype=np.uint32)
+        check(lib().atr_batch_trace(self.ctx.handle, self.handle, C.c_void_p(rays_ptr), num_rays, _ptr(off),
+                                    _ptr(gm), len(gm), 1 if any_hit else 0, C.c_void_p(results_ptr)))
+
+    def refit_mesh(self, m: int, vertices=None, device_ptr: int | None = None) -> None:
+        if device_ptr is not None:
+            check(lib().atr_batch_refit_mesh(self.ctx.handle, self.handle, m, C.c_void_p(device_ptr), 1))
+        else:
+            v = np.ascontiguousarray(vertices, dtype=np.float32)
+            check(lib().atr_batch_refit_mesh(self.ctx.handle, self.handle, m, _ptr(v), 0))
+            self.ctx.synchronize()
 
     def close(self) -> None:
         if getattr(self, "handle", None):

@@ -40,6 +40,17 @@ struct atr_batch {
     int graph_key[4] = {0, 0, 0, 0};
     float graph_cf[2] = {0, 0};
     uint64_t graph_launches = 0;
+    // Collapsed trees and Compact2 layouts (allocated on first use).
+    void* col_block = nullptr;
+    atr::CollapsedOut col{};
+    void* cp_block = nullptr;
+    int4* cp_nodes = nullptr;
+    float4* cp_woop = nullptr;
+    int32_t* cp_tri = nullptr;
+    int64_t* d_sizes = nullptr;  // per mesh: nodes then woop entries
+    std::vector<int64_t> h_sizes;
+    int32_t max_depth = 0;
+    bool flattened = false;
 };
 
 namespace atr {
@@ -179,6 +190,8 @@ int atr_batch_create(atr_ctx* ctx, const float* vertices, const uint32_t* tri_of
 int atr_batch_destroy(atr_batch* b) {
     if (!b) return ATR_OK;
     if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->ctx->release(b->col_block);
+    b->ctx->release(b->cp_block);
     b->ctx->release(b->block);
     b->ctx->release(b->verts);
     b->ctx->release(b->meta);
@@ -290,6 +303,156 @@ int atr_batch_download_mesh(atr_ctx* ctx, const atr_batch* b, uint32_t mesh, int
     if (bmax) ATR_CUDA(cudaMemcpyAsync(bmax, v.bbox_max, nn * 16, cudaMemcpyDeviceToHost, s));
     if (area) ATR_CUDA(cudaMemcpyAsync(area, v.area, nn * 4, cudaMemcpyDeviceToHost, s));
     return atr_ctx_synchronize(ctx);
+}
+
+static int batch_alloc_outputs(atr_ctx* ctx, atr_batch* b) {
+    const size_t nn = b->total_nodes, n = b->n;
+    if (!b->col_block) {
+        const size_t b4 = align256(nn * 4), b16 = align256(nn * 16);
+        ATR_TRY(ctx->alloc(&b->col_block, 5 * b4 + 2 * b16 + align256(n * 4)));
+        char* p = static_cast<char*>(b->col_block);
+        b->col.parent = reinterpret_cast<int32_t*>(p); p += b4;
+        b->col.left = reinterpret_cast<int32_t*>(p); p += b4;
+        b->col.right = reinterpret_cast<int32_t*>(p); p += b4;
+        b->col.data = reinterpret_cast<int32_t*>(p); p += b4;
+        b->col.count = reinterpret_cast<int32_t*>(p); p += b4;
+        b->col.bmin = reinterpret_cast<float4*>(p); p += b16;
+        b->col.bmax = reinterpret_cast<float4*>(p); p += b16;
+        b->col.tri_indices = reinterpret_cast<int32_t*>(p);
+    }
+    if (!b->cp_block) {
+        const size_t bn = align256((n - b->count) * 64), bw = align256(n * 64), bt = align256(n * 16);
+        const size_t bs = align256(b->count * 16ull);
+        ATR_TRY(ctx->alloc(&b->cp_block, bn + bw + bt + bs));
+        char* p = static_cast<char*>(b->cp_block);
+        b->cp_nodes = reinterpret_cast<int4*>(p); p += bn;
+        b->cp_woop = reinterpret_cast<float4*>(p); p += bw;
+        b->cp_tri = reinterpret_cast<int32_t*>(p); p += bt;
+        b->d_sizes = reinterpret_cast<int64_t*>(p);
+    }
+    return ATR_OK;
+}
+
+int atr_batch_collapse(atr_ctx* ctx, atr_batch* b, float ci, float ct, int max_leaf, float* sah) {
+    ATR_REQUIRE(ctx && b, ATR_ERR_INVALID_ARG, "atr_batch_collapse: NULL argument");
+    ATR_REQUIRE(max_leaf >= 0, ATR_ERR_INVALID_ARG, "atr_batch_collapse: max_leaf %d", max_leaf);
+    ATR_TRY(batch_alloc_outputs(ctx, b));
+    const Segs segs{b->d_tri_off, b->d_tile_off, b->count, b->n};
+    float* parts = nullptr;
+    if (sah) ATR_TRY(ctx->alloc(reinterpret_cast<void**>(&parts), 8ull * b->count));
+    ctx->phase_begin("collapse");
+    int st = collapse_segs(ctx, segs, b->total_nodes, b->tree, b->col, ci, ct, max_leaf, parts);
+    ctx->phase_end();
+    if (st == ATR_OK && sah) {
+        std::vector<float> h(2ull * b->count);
+        cudaError_t e = cudaMemcpyAsync(h.data(), parts, h.size() * 4, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) st = atr_ctx_synchronize(ctx);
+        else st = cuda_fail(e, "cudaMemcpyAsync(sah)", __FILE__, __LINE__);
+        if (st == ATR_OK)
+            for (uint32_t m = 0; m < b->count; ++m) sah[m] = h[2 * m] / h[2 * m + 1];
+    }
+    ctx->release(parts);
+    b->flattened = false;
+    return st;
+}
+
+int atr_batch_flatten(atr_ctx* ctx, atr_batch* b) {
+    ATR_REQUIRE(ctx && b, ATR_ERR_INVALID_ARG, "atr_batch_flatten: NULL argument");
+    ATR_REQUIRE(b->col_block, ATR_ERR_INVALID_ARG, "atr_batch_flatten: collapse the batch first");
+    const Segs segs{b->d_tri_off, b->d_tile_off, b->count, b->n};
+    ctx->phase_begin("flatten");
+    int st = flatten_segs(ctx, segs, b->col, b->verts, b->cp_nodes, b->cp_woop, b->cp_tri, b->d_sizes, &b->max_depth);
+    ctx->phase_end();
+    ATR_TRY(st);
+    b->h_sizes.resize(2ull * b->count);
+    ATR_CUDA(cudaMemcpy(b->h_sizes.data(), b->d_sizes, b->h_sizes.size() * 8, cudaMemcpyDeviceToHost));
+    b->flattened = true;
+    return ATR_OK;
+}
+
+int atr_batch_compact_view(const atr_batch* b, uint32_t mesh, atr_compact_view* v) {
+    ATR_REQUIRE(b && v, ATR_ERR_INVALID_ARG, "atr_batch_compact_view: NULL argument");
+    ATR_REQUIRE(b->flattened, ATR_ERR_INVALID_ARG, "atr_batch_compact_view: flatten the batch first");
+    ATR_REQUIRE(mesh < b->count, ATR_ERR_INVALID_ARG, "atr_batch_compact_view: mesh %u of %u", mesh, b->count);
+    const size_t s0 = b->h_tri_off[mesh];
+    v->num_nodes = b->h_sizes[mesh];
+    v->num_woop = b->h_sizes[b->count + mesh];
+    v->nodes = reinterpret_cast<int32_t*>(b->cp_nodes + 4 * (s0 - mesh));
+    v->woop = reinterpret_cast<float*>(b->cp_woop + 4 * s0);
+    v->tri_index = b->cp_tri + 4 * s0;
+    v->max_depth = b->max_depth;
+    return ATR_OK;
+}
+
+int atr_batch_compact_download(atr_ctx* ctx, const atr_batch* b, uint32_t mesh, int32_t* nodes, float* woop,
+                               int32_t* tri) {
+    ATR_REQUIRE(ctx, ATR_ERR_INVALID_ARG, "atr_batch_compact_download: NULL argument");
+    atr_compact_view v;
+    ATR_TRY(atr_batch_compact_view(b, mesh, &v));
+    cudaStream_t s = ctx->stream;
+    if (nodes) ATR_CUDA(cudaMemcpyAsync(nodes, v.nodes, (size_t)v.num_nodes * 64, cudaMemcpyDeviceToHost, s));
+    if (woop) ATR_CUDA(cudaMemcpyAsync(woop, v.woop, (size_t)v.num_woop * 16, cudaMemcpyDeviceToHost, s));
+    if (tri) ATR_CUDA(cudaMemcpyAsync(tri, v.tri_index, (size_t)v.num_woop * 4, cudaMemcpyDeviceToHost, s));
+    return atr_ctx_synchronize(ctx);
+}
+
+int atr_batch_trace(atr_ctx* ctx, const atr_batch* b, const float* rays, int64_t num_rays,
+                    const uint32_t* ray_offsets, const uint32_t* group_mesh, uint32_t groups, int any_hit,
+                    int32_t* results) {
+    ATR_REQUIRE(ctx && b && rays && results && ray_offsets && group_mesh, ATR_ERR_INVALID_ARG,
+                "atr_batch_trace: NULL argument");
+    ATR_REQUIRE(b->flattened, ATR_ERR_INVALID_ARG, "atr_batch_trace: flatten the batch first");
+    ATR_REQUIRE(groups >= 1 && ray_offsets[0] == 0 && (int64_t)ray_offsets[groups] == num_rays,
+                ATR_ERR_INVALID_ARG, "atr_batch_trace: ray_offsets must run from 0 to num_rays");
+    for (uint32_t g = 0; g < groups; ++g) {
+        ATR_REQUIRE(group_mesh[g] < b->count, ATR_ERR_INVALID_ARG, "atr_batch_trace: group %u mesh %u", g,
+                    group_mesh[g]);
+        ATR_REQUIRE(ray_offsets[g + 1] >= ray_offsets[g], ATR_ERR_INVALID_ARG, "atr_batch_trace: offsets decrease");
+    }
+    uint32_t* map = nullptr;
+    ATR_TRY(ctx->alloc(reinterpret_cast<void**>(&map), (2ull * groups + 1) * 4));
+    cudaMemcpyAsync(map, ray_offsets, (groups + 1) * 4ull, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(map + groups + 1, group_mesh, groups * 4ull, cudaMemcpyHostToDevice, ctx->stream);
+    const int st = trace_batch(ctx, b->cp_nodes, b->cp_woop, b->cp_tri, map, map + groups + 1, b->d_tri_off, groups,
+                               b->max_depth, reinterpret_cast<const float4*>(rays), num_rays, any_hit,
+                               reinterpret_cast<int4*>(results));
+    ctx->release(map);
+    return st;
+}
+
+int atr_batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* vertices, int on_device) {
+    ATR_REQUIRE(ctx && b && vertices, ATR_ERR_INVALID_ARG, "atr_batch_refit_mesh: NULL argument");
+    ATR_REQUIRE(mesh < b->count, ATR_ERR_INVALID_ARG, "atr_batch_refit_mesh: mesh %u of %u", mesh, b->count);
+    const size_t s0 = b->h_tri_off[mesh];
+    const uint32_t n = b->h_tri_off[mesh + 1] - b->h_tri_off[mesh];
+    ATR_CUDA(cudaMemcpyAsync(b->verts + 3 * s0, vertices, n * 48ull,
+                             on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream));
+    const size_t nb = 2 * s0 - mesh;
+    const TreeOut t{b->tree.parent + nb, b->tree.left + nb, b->tree.right + nb, b->tree.data + nb,
+                    b->tree.bmin + nb, b->tree.bmax + nb, b->tree.area + nb};
+    ATR_TRY(refit_arrays(ctx, n, t, b->verts + 3 * s0));
+    if (!b->flattened) return ATR_OK;
+    // Re-collapse and re-flatten this mesh only, in place in its slices.
+    const Segs one{nullptr, nullptr, 1u, n};
+    const CollapsedOut c{b->col.parent + nb, b->col.left + nb, b->col.right + nb, b->col.data + nb,
+                         b->col.count + nb, b->col.bmin + nb, b->col.bmax + nb, b->col.tri_indices + s0};
+    ATR_TRY(collapse_segs(ctx, one, 2 * (size_t)n - 1, t, c, 1.2f, 1.0f, 0, nullptr));
+    int32_t depth = 0;
+    int64_t* sizes = nullptr;
+    ATR_TRY(ctx->alloc(reinterpret_cast<void**>(&sizes), 16));
+    int st = flatten_segs(ctx, one, c, b->verts + 3 * s0, b->cp_nodes + 4 * (s0 - mesh), b->cp_woop + 4 * s0,
+                          b->cp_tri + 4 * s0, sizes, &depth);
+    int64_t h[2] = {0, 0};
+    if (st == ATR_OK) {
+        cudaError_t e = cudaMemcpy(h, sizes, 16, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpy(sizes)", __FILE__, __LINE__);
+    }
+    ctx->release(sizes);
+    ATR_TRY(st);
+    b->h_sizes[mesh] = h[0];
+    b->h_sizes[b->count + mesh] = h[1];
+    b->max_depth = std::max(b->max_depth, depth);
+    return ATR_OK;
 }
 
 int atr_batch_sah(atr_ctx* ctx, const atr_batch* b, float ci, float ct, float* sah) {

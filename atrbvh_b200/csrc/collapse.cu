@@ -43,33 +43,43 @@ struct CollapseRefs {
     uint32_t* emit_cnt;
 };
 
-__global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs t, uint32_t* __restrict__ counters, float ci,
-                                                        float ct, int max_leaf) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= t.n) return;
-    const int leaf = (int)i + (int)t.n - 1;
+// Segmented: thread i starts at the i-th leaf of the batch; node arrays are
+// addressed from the mesh's first node (local indices); each mesh's lists
+// live in its own slice [tri_begin, tri_end) of tri_indices.
+__global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs, uint32_t* __restrict__ counters,
+                                                        float ci, float ct, int max_leaf) {
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= segs.n) return;
+    const uint32_t m = segs.seg_of_tri(gi);
+    const uint32_t s0 = segs.tri_begin(m);
+    const uint32_t n = segs.tri_end(m) - s0;
+    const int nb = segs.node_base(m);
+    uint32_t* ctr = counters + segs.inner_base(m);
+    const int leaf = (int)(gi - s0) + (int)n - 1;
     {
-        const float4 mn = t.bmin[leaf], mx = t.bmax[leaf];
-        t.c_parent[leaf] = t.parent[leaf];
-        t.c_left[leaf] = t.left[leaf];
-        t.c_right[leaf] = t.right[leaf];
-        t.c_data[leaf] = t.data[leaf];
-        t.c_bmin[leaf] = mn;
-        t.c_bmax[leaf] = mx;
-        t.c_count[leaf] = 1;
-        t.cost[leaf] = __fmul_rn(ct, box_area(mn, mx));
-        t.pass[leaf] = 1;
+        const int x = nb + leaf;
+        const float4 mn = g.bmin[x], mx = g.bmax[x];
+        g.c_parent[x] = g.parent[x];
+        g.c_left[x] = g.left[x];
+        g.c_right[x] = g.right[x];
+        g.c_data[x] = g.data[x];
+        g.c_bmin[x] = mn;
+        g.c_bmax[x] = mx;
+        g.c_count[x] = 1;
+        g.cost[x] = __fmul_rn(ct, box_area(mn, mx));
+        g.pass[x] = 1;
     }
-    int cur = t.parent[leaf];
+    int cur = g.parent[nb + leaf];
     while (cur >= 0) {
         __threadfence();
-        if (atomicAdd(&counters[cur], 1u) == 0u) return;
+        if (atomicAdd(&ctr[cur], 1u) == 0u) return;
         __threadfence();
-        const int l = t.left[cur], r = t.right[cur];
-        const int cl = ld_cg(t.c_count + l), cr = ld_cg(t.c_count + r);
-        const float kl = ld_cg(t.cost + l), kr = ld_cg(t.cost + r);
-        const int pl = ld_cg(t.pass + l), pr = ld_cg(t.pass + r);
-        const float4 mn = t.bmin[cur], mx = t.bmax[cur];
+        const int x = nb + cur;
+        const int l = g.left[x], r = g.right[x];
+        const int cl = ld_cg(g.c_count + nb + l), cr = ld_cg(g.c_count + nb + r);
+        const float kl = ld_cg(g.cost + nb + l), kr = ld_cg(g.cost + nb + r);
+        const int pl = ld_cg(g.pass + nb + l), pr = ld_cg(g.pass + nb + r);
+        const float4 mn = g.bmin[x], mx = g.bmax[x];
         const int cnt = cl + cr;
         const float a = box_area(mn, mx);
         float c = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), kl), kr);
@@ -78,39 +88,52 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs t, uint32_t*
         if (col) c = leaf_cost;
         const bool reached = pl && pr;
         if (reached && !col) {
-            if (cl > 1) t.emit_cnt[l] = (uint32_t)cl;
-            if (cr > 1) t.emit_cnt[r] = (uint32_t)cr;
+            if (cl > 1) g.emit_cnt[nb + l] = (uint32_t)cl;
+            if (cr > 1) g.emit_cnt[nb + r] = (uint32_t)cr;
         }
-        t.c_parent[cur] = t.parent[cur];
-        t.c_left[cur] = l;
-        t.c_right[cur] = r;
-        t.c_data[cur] = -1;
-        t.c_bmin[cur] = mn;
-        t.c_bmax[cur] = mx;
-        t.c_count[cur] = cnt;
-        t.cost[cur] = c;
-        t.pass[cur] = reached && col;
-        cur = t.parent[cur];
+        g.c_parent[x] = g.parent[x];
+        g.c_left[x] = l;
+        g.c_right[x] = r;
+        g.c_data[x] = -1;
+        g.c_bmin[x] = mn;
+        g.c_bmax[x] = mx;
+        g.c_count[x] = cnt;
+        g.cost[x] = c;
+        g.pass[x] = reached && col;
+        cur = g.parent[x];
     }
 }
 
-__global__ void __launch_bounds__(256) k_collapse_emit(CollapseRefs t, const uint32_t* __restrict__ offsets,
+__global__ void __launch_bounds__(256) k_collapse_emit(CollapseRefs g, Segs segs, const uint32_t* __restrict__ offsets,
                                                         int32_t* __restrict__ tri_indices) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= t.n) return;
-    const int leaf = (int)i + (int)t.n - 1;
-    int ch = leaf, a = t.parent[leaf], top = -1;
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= segs.n) return;
+    const uint32_t m = segs.seg_of_tri(gi);
+    const uint32_t s0 = segs.tri_begin(m);
+    const uint32_t n = segs.tri_end(m) - s0;
+    const int nb = segs.node_base(m);
+    const int leaf = (int)(gi - s0) + (int)n - 1;
+    int ch = leaf, a = g.parent[nb + leaf], top = -1;
     uint32_t rank = 0;
-    while (a >= 0 && t.pass[a]) {
-        if (t.left[a] == ch) rank += (uint32_t)t.c_count[t.right[a]];
+    while (a >= 0 && g.pass[nb + a]) {
+        if (g.left[nb + a] == ch) rank += (uint32_t)g.c_count[nb + g.right[nb + a]];
         top = a;
         ch = a;
-        a = t.parent[a];
+        a = g.parent[nb + a];
     }
-    if (top < 0 || t.emit_cnt[top] == 0) return;
-    const uint32_t off = offsets[top];
-    tri_indices[off + rank] = t.data[leaf];
-    if (rank == 0) t.c_data[top] = (int32_t)off;
+    if (top < 0 || g.emit_cnt[nb + top] == 0) return;
+    const uint32_t off = offsets[nb + top] - offsets[nb];  // local to the mesh's list slice
+    tri_indices[s0 + off + rank] = g.data[nb + leaf];
+    if (rank == 0) g.c_data[nb + top] = (int32_t)off;
+}
+
+__global__ void k_sah_parts(Segs segs, const float* __restrict__ cost, const float* __restrict__ area,
+                            float* __restrict__ out) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= segs.count) return;
+    const int nb = segs.node_base(m);
+    out[2 * m] = cost[nb];
+    out[2 * m + 1] = area[nb];
 }
 
 }  // namespace
@@ -136,13 +159,17 @@ int collapsed_alloc(atr_ctx* ctx, uint32_t n, atr_collapsed** out) {
     return ATR_OK;
 }
 
-int collapse_into(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int max_leaf, atr_collapsed* c,
-                  float* d_sah_parts) {
-    const uint32_t n = tree->n;
-    const size_t nn = 2 * (size_t)n - 1;
+// Collapse every mesh of segs (total_nodes = sum of 2n_m - 1).  src holds the
+// optimised trees, dst the collapsed arrays; d_sah_parts (optional) receives
+// cost[root] and area[root] of every mesh (2 floats per mesh).
+int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const TreeOut& src, const CollapsedOut& dst,
+                  float ci, float ct, int max_leaf, float* d_sah_parts) {
+    const uint32_t n = segs.n;
+    const size_t nn = total_nodes;
     void* scratch = nullptr;
     const size_t b4 = align256(nn * 4);
-    ATR_TRY(ctx->alloc(&scratch, 4 * b4 + align256((size_t)(n - 1) * 4)));
+    const size_t inner = n - segs.count;
+    ATR_TRY(ctx->alloc(&scratch, 4 * b4 + align256(inner * 4)));
     char* p = static_cast<char*>(scratch);
     float* cost = reinterpret_cast<float*>(p); p += b4;
     int32_t* pass = reinterpret_cast<int32_t*>(p); p += b4;
@@ -151,26 +178,34 @@ int collapse_into(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int ma
     uint32_t* counters = reinterpret_cast<uint32_t*>(p);
     cudaStream_t s = ctx->stream;
     cudaMemsetAsync(emit, 0, nn * 4, s);
-    cudaMemsetAsync(counters, 0, (size_t)(n - 1) * 4, s);
-    cudaMemsetAsync(c->tri_indices, 0xff, (size_t)n * 4, s);
-    CollapseRefs r{n, tree->parent, tree->left, tree->right, tree->data, tree->bmin, tree->bmax, c->parent,
-                   c->left, c->right, c->data, c->count, c->bmin, c->bmax, cost, pass, emit};
+    cudaMemsetAsync(counters, 0, inner * 4, s);
+    cudaMemsetAsync(dst.tri_indices, 0xff, (size_t)n * 4, s);
+    CollapseRefs r{n, src.parent, src.left, src.right, src.data, src.bmin, src.bmax, dst.parent, dst.left, dst.right,
+                   dst.data, dst.count, dst.bmin, dst.bmax, cost, pass, emit};
     const unsigned blocks = (n + 255) / 256;
-    k_collapse_cost<<<blocks, 256, 0, s>>>(r, counters, ci, ct, max_leaf);
+    k_collapse_cost<<<blocks, 256, 0, s>>>(r, segs, counters, ci, ct, max_leaf);
     ctx->launches += 1;
     int st = exclusive_scan_u32(ctx, emit, offs, nn, nullptr);
     if (st == ATR_OK) {
-        k_collapse_emit<<<blocks, 256, 0, s>>>(r, offs, c->tri_indices);
+        k_collapse_emit<<<blocks, 256, 0, s>>>(r, segs, offs, dst.tri_indices);
         ctx->launches += 1;
         if (d_sah_parts) {
-            cudaMemcpyAsync(d_sah_parts, cost, 4, cudaMemcpyDeviceToDevice, s);
-            cudaMemcpyAsync(d_sah_parts + 1, tree->area, 4, cudaMemcpyDeviceToDevice, s);
+            k_sah_parts<<<(segs.count + 255) / 256, 256, 0, s>>>(segs, cost, src.area, d_sah_parts);
+            ctx->launches += 1;
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) st = cuda_fail(e, "collapse kernels", __FILE__, __LINE__);
     }
     ctx->release(scratch);
     return st;
+}
+
+int collapse_into(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int max_leaf, atr_collapsed* c,
+                  float* d_sah_parts) {
+    const Segs segs{nullptr, nullptr, 1u, tree->n};
+    const TreeOut src{tree->parent, tree->left, tree->right, tree->data, tree->bmin, tree->bmax, tree->area};
+    const CollapsedOut dst{c->parent, c->left, c->right, c->data, c->count, c->bmin, c->bmax, c->tri_indices};
+    return collapse_segs(ctx, segs, 2 * (size_t)tree->n - 1, src, dst, ci, ct, max_leaf, d_sah_parts);
 }
 
 }  // namespace atr

@@ -28,10 +28,9 @@ int exclusive_scan_u32(atr_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t
 
 namespace {
 
-constexpr int kJumpRounds = 8;  // enough for depth < 256; more rounds run if needed
+constexpr int kJumpRounds = 8;  // 2^8 ancestors per block of rounds; depth >= 256 runs more
 
 struct FlatRefs {
-    uint32_t n;
     const int32_t* parent;
     const int32_t* left;
     const int32_t* right;
@@ -42,54 +41,78 @@ struct FlatRefs {
     const int32_t* tri;
 };
 
-__device__ __forceinline__ bool c_leaf(const FlatRefs& t, int x) { return t.data[x] >= 0; }
-__device__ __forceinline__ uint32_t woop_entries(const FlatRefs& t, int x) {
-    const int c = t.count[x];
+// Segment view of thread gi: the mesh, its first node (nb), its first inner
+// node (cb), its first triangle (s0), its triangle count (n) and the local
+// index li of the leaf (and of the inner node) this thread owns.
+struct SegPos {
+    uint32_t m, s0, n, li;
+    int nb, cb;
+};
+__device__ __forceinline__ SegPos seg_pos(const Segs& segs, uint32_t gi) {
+    SegPos p;
+    p.m = segs.seg_of_tri(gi);
+    p.s0 = segs.tri_begin(p.m);
+    p.n = segs.tri_end(p.m) - p.s0;
+    p.li = gi - p.s0;
+    p.nb = segs.node_base(p.m);
+    p.cb = segs.inner_base(p.m);
+    return p;
+}
+
+__device__ __forceinline__ bool c_leaf(const FlatRefs& t, int nb, int x) { return t.data[nb + x] >= 0; }
+__device__ __forceinline__ uint32_t woop_entries(const FlatRefs& t, int nb, int x) {
+    const int c = t.count[nb + x];
     return 3u * (uint32_t)(c > 1 ? c : 1) + 1u;
 }
 
-// Pass 1: inner-node counts, inner-children counts, Woop entries of leaf children.
-__global__ void __launch_bounds__(256) k_flat_counts(FlatRefs t, uint32_t* __restrict__ icnt,
+// Pass 1: per inner node, inner nodes in its subtree, inner children, Woop
+// entries of its leaf children (inner arrays are indexed cb + local index).
+__global__ void __launch_bounds__(256) k_flat_counts(FlatRefs t, Segs segs, uint32_t* __restrict__ icnt,
                                                       uint32_t* __restrict__ ic, uint32_t* __restrict__ tw,
                                                       uint32_t* __restrict__ counters) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= t.n) return;
-    int cur = t.parent[(int)i + (int)t.n - 1];
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= segs.n) return;
+    const SegPos q = seg_pos(segs, gi);
+    int cur = t.parent[q.nb + (int)q.li + (int)q.n - 1];
     while (cur >= 0) {
         __threadfence();
-        if (atomicAdd(&counters[cur], 1u) == 0u) return;
+        if (atomicAdd(&counters[q.cb + cur], 1u) == 0u) return;
         __threadfence();
-        const int l = t.left[cur], r = t.right[cur];
-        const bool ll = c_leaf(t, l), rl = c_leaf(t, r);
-        const uint32_t il = ll ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + l);
-        const uint32_t ir = rl ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + r);
-        icnt[cur] = c_leaf(t, cur) ? 0u : 1u + il + ir;
-        ic[cur] = (ll ? 0u : 1u) + (rl ? 0u : 1u);
-        tw[cur] = (ll ? woop_entries(t, l) : 0u) + (rl ? woop_entries(t, r) : 0u);
-        cur = t.parent[cur];
+        const int l = t.left[q.nb + cur], r = t.right[q.nb + cur];
+        const bool ll = c_leaf(t, q.nb, l), rl = c_leaf(t, q.nb, r);
+        const uint32_t il = ll ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + q.cb + l);
+        const uint32_t ir = rl ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + q.cb + r);
+        icnt[q.cb + cur] = c_leaf(t, q.nb, cur) ? 0u : 1u + il + ir;
+        ic[q.cb + cur] = (ll ? 0u : 1u) + (rl ? 0u : 1u);
+        tw[q.cb + cur] = (ll ? woop_entries(t, q.nb, l) : 0u) + (rl ? woop_entries(t, q.nb, r) : 0u);
+        cur = t.parent[q.nb + cur];
     }
 }
 
-// Pointer-jumping initialisation over inner nodes.
-__global__ void __launch_bounds__(256) k_flat_jump_init(FlatRefs t, const uint32_t* __restrict__ icnt,
+// Pointer-jumping initialisation; thread gi owns inner node li of its mesh.
+// .x: pop-rank contribution; .y: depth in the low 16 bits, bit 30 set when a
+// leaf of the collapsed tree lies on the path (the node itself included).
+__global__ void __launch_bounds__(256) k_flat_jump_init(FlatRefs t, Segs segs, const uint32_t* __restrict__ icnt,
                                                          int2* __restrict__ acc, int* __restrict__ jmp) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= t.n - 1) return;
-    const int p = t.parent[x];
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= segs.n) return;
+    const SegPos q = seg_pos(segs, gi);
+    if (q.li >= q.n - 1) return;
+    const int x = (int)q.li;
+    const int gx = q.cb + x;
+    const int p = t.parent[q.nb + x];
     if (p < 0) {
-        acc[x] = make_int2(0, 0);
-        jmp[x] = -1;
+        acc[gx] = make_int2(0, 0);
+        jmp[gx] = -1;
         return;
     }
-    const bool is_left = t.left[p] == (int)x;
-    const int sib = is_left ? t.right[p] : t.left[p];
-    const int sib_inner = c_leaf(t, sib) ? 0 : (int)icnt[sib];
+    const bool is_left = t.left[q.nb + p] == x;
+    const int sib = is_left ? t.right[q.nb + p] : t.left[q.nb + p];
+    const int sib_inner = c_leaf(t, q.nb, sib) ? 0 : (int)icnt[q.cb + sib];
     const int val = 1 + (is_left ? sib_inner : 0);
-    // .x: rank contribution, .y: depth in the low 16 bits and an
-    // above-is-a-leaf flag in bit 30.
-    const int blocked = c_leaf(t, (int)x) ? (1 << 30) : 0;
-    acc[x] = make_int2(val, 1 | blocked);
-    jmp[x] = p;
+    const int blocked = c_leaf(t, q.nb, x) ? (1 << 30) : 0;
+    acc[gx] = make_int2(val, 1 | blocked);
+    jmp[gx] = q.cb + p;
 }
 
 __global__ void __launch_bounds__(256) k_flat_jump(uint32_t m, const int2* __restrict__ acc_in,
@@ -111,22 +134,23 @@ __global__ void __launch_bounds__(256) k_flat_jump(uint32_t m, const int2* __res
     jmp_out[x] = nj;
 }
 
-// A node is reachable from the root through inner nodes when no node on its
-// path (itself included) is a leaf of the collapsed tree.  The flag folded in
-// above includes the node itself; inner nodes of the layout are exactly the
-// reachable ones that are not leaves.
-__global__ void __launch_bounds__(256) k_flat_scatter(FlatRefs t, const int2* __restrict__ acc,
+// Inner nodes of the layout are the reachable ones (no collapsed-tree leaf on
+// their path); scatter their inner-child counts and Woop sizes by pop rank.
+__global__ void __launch_bounds__(256) k_flat_scatter(Segs segs, const int2* __restrict__ acc,
                                                        const uint32_t* __restrict__ ic,
                                                        const uint32_t* __restrict__ tw,
                                                        uint32_t* __restrict__ ic_by_rank,
                                                        uint32_t* __restrict__ tw_by_rank,
                                                        int* __restrict__ max_depth) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= t.n - 1) return;
-    const int2 a = acc[x];
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= segs.n) return;
+    const SegPos q = seg_pos(segs, gi);
+    if (q.li >= q.n - 1) return;
+    const int gx = q.cb + (int)q.li;
+    const int2 a = acc[gx];
     if (a.y & (1 << 30)) return;
-    ic_by_rank[a.x] = ic[x];
-    tw_by_rank[a.x] = tw[x];
+    ic_by_rank[q.cb + a.x] = ic[gx];
+    tw_by_rank[q.cb + a.x] = tw[gx];
     atomicMax(max_depth, (a.y & 0xffff) + 1);
 }
 
@@ -181,94 +205,106 @@ __device__ void woopify(const float4* __restrict__ v, int tri, float4* __restric
     out[2] = make_float4(R[1][0], R[1][1], R[1][2], R[1][3]);
 }
 
-__global__ void __launch_bounds__(256) k_flat_slots(FlatRefs t, const int2* __restrict__ acc,
-                                                     const uint32_t* __restrict__ ic,
+__global__ void __launch_bounds__(256) k_flat_slots(FlatRefs t, Segs segs, const int2* __restrict__ acc,
                                                      const uint32_t* __restrict__ s_by_rank,
                                                      int* __restrict__ slot_of) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= t.n - 1) return;
-    const int2 a = acc[x];
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= segs.n) return;
+    const SegPos q = seg_pos(segs, gi);
+    if (q.li >= q.n - 1) return;
+    const int x = (int)q.li;
+    const int2 a = acc[q.cb + x];
     if (a.y & (1 << 30)) return;
-    if (t.parent[x] < 0) slot_of[x] = 0;
-    const int l = t.left[x], r = t.right[x];
-    const uint32_t base = 1u + s_by_rank[a.x];
-    const bool li = !c_leaf(t, l), ri = !c_leaf(t, r);
-    if (li) slot_of[l] = (int)base;
-    if (ri) slot_of[r] = (int)(base + (li ? 1u : 0u));
+    if (t.parent[q.nb + x] < 0) slot_of[q.cb + x] = 0;
+    const int l = t.left[q.nb + x], r = t.right[q.nb + x];
+    const uint32_t base = 1u + s_by_rank[q.cb + a.x] - s_by_rank[q.cb];
+    const bool li = !c_leaf(t, q.nb, l), ri = !c_leaf(t, q.nb, r);
+    if (li) slot_of[q.cb + l] = (int)base;
+    if (ri) slot_of[q.cb + r] = (int)(base + (li ? 1u : 0u));
 }
 
-__global__ void __launch_bounds__(128) k_flat_write(FlatRefs t, const float4* __restrict__ verts,
+// One thread per reachable inner node: its 64-byte record in the mesh's node
+// slice (first node 4 * cb in float4 units) and its leaf children's Woop
+// triangles in the mesh's Woop slice (first entry 4 * s0).
+__global__ void __launch_bounds__(128) k_flat_write(FlatRefs t, Segs segs, const float4* __restrict__ verts,
                                                      const int2* __restrict__ acc,
                                                      const uint32_t* __restrict__ w_by_rank,
                                                      const int* __restrict__ slot_of, int4* __restrict__ nodes,
                                                      float4* __restrict__ woop, int32_t* __restrict__ tri_index) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= t.n - 1) return;
-    const int2 a = acc[x];
+    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gi >= segs.n) return;
+    const SegPos q = seg_pos(segs, gi);
+    if (q.li >= q.n - 1) return;
+    const int x = (int)q.li;
+    const int2 a = acc[q.cb + x];
     if (a.y & (1 << 30)) return;
-    const int ch[2] = {t.left[x], t.right[x]};
+    const float4* mv = verts + 3 * (size_t)q.s0;
+    float4* mw = woop + 4 * (size_t)q.s0;
+    int32_t* mt = tri_index + 4 * (size_t)q.s0;
+    const int ch[2] = {t.left[q.nb + x], t.right[q.nb + x]};
     int cref[2];
-    uint32_t w = w_by_rank[a.x];
+    uint32_t w = w_by_rank[q.cb + a.x] - w_by_rank[q.cb];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const int c = ch[k];
-        if (!c_leaf(t, c)) {
-            cref[k] = 4 * slot_of[c];
+        if (!c_leaf(t, q.nb, c)) {
+            cref[k] = 4 * slot_of[q.cb + c];
             continue;
         }
         cref[k] = ~(int)w;
-        const int cnt = t.count[c];
-        const int d = t.data[c];
-        const int m = cnt > 1 ? cnt : 1;
-        for (int j = 0; j < m; ++j) {
-            const int tri = cnt > 1 ? t.tri[d + j] : d;
-            woopify(verts, tri, woop + w);
-            tri_index[w] = tri;
-            tri_index[w + 1] = 0;
-            tri_index[w + 2] = 0;
+        const int cnt = t.count[q.nb + c];
+        const int d = t.data[q.nb + c];
+        const int mcount = cnt > 1 ? cnt : 1;
+        for (int j = 0; j < mcount; ++j) {
+            const int tri = cnt > 1 ? t.tri[q.s0 + d + j] : d;
+            woopify(mv, tri, mw + w);
+            mt[w] = tri;
+            mt[w + 1] = 0;
+            mt[w + 2] = 0;
             w += 3;
         }
         const float term = __int_as_float((int)0x80000000u);
-        woop[w] = make_float4(term, term, term, term);
-        tri_index[w] = 0;
+        mw[w] = make_float4(term, term, term, term);
+        mt[w] = 0;
         w += 1;
     }
-    const float4 lm = t.bmin[ch[0]], lx = t.bmax[ch[0]], rm = t.bmin[ch[1]], rx = t.bmax[ch[1]];
-    int4* dst = nodes + 4 * (size_t)slot_of[x];
+    const float4 lm = t.bmin[q.nb + ch[0]], lx = t.bmax[q.nb + ch[0]];
+    const float4 rm = t.bmin[q.nb + ch[1]], rx = t.bmax[q.nb + ch[1]];
+    int4* dst = nodes + 4 * ((size_t)q.cb + (size_t)slot_of[q.cb + x]);
     dst[0] = make_int4(__float_as_int(lm.x), __float_as_int(lx.x), __float_as_int(lm.y), __float_as_int(lx.y));
     dst[1] = make_int4(__float_as_int(rm.x), __float_as_int(rx.x), __float_as_int(rm.y), __float_as_int(rx.y));
     dst[2] = make_int4(__float_as_int(lm.z), __float_as_int(lx.z), __float_as_int(rm.z), __float_as_int(rx.z));
     dst[3] = make_int4(cref[0], cref[1], 0, 0);
 }
 
+// Per-mesh sizes: inner nodes = 1 + inner children, Woop entries.
+__global__ void k_flat_sizes(Segs segs, const uint32_t* __restrict__ ic_scan, const uint32_t* __restrict__ tw_scan,
+                             const uint32_t* __restrict__ totals, int64_t* __restrict__ nodes_out,
+                             int64_t* __restrict__ woop_out) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= segs.count) return;
+    const int cb = segs.inner_base(m);
+    const bool last = m + 1 == segs.count;
+    const uint32_t ic_end = last ? totals[0] : ic_scan[segs.inner_base(m + 1)];
+    const uint32_t tw_end = last ? totals[1] : tw_scan[segs.inner_base(m + 1)];
+    nodes_out[m] = 1 + (int64_t)(ic_end - ic_scan[cb]);
+    woop_out[m] = (int64_t)(tw_end - tw_scan[cb]);
+}
+
 }  // namespace
-}  // namespace atr
 
-using namespace atr;
-
-extern "C" {
-
-int atr_flatten_compact2(atr_ctx* ctx, const atr_collapsed* c, const atr_scene* scene, atr_compact** out) {
-    ATR_REQUIRE(ctx && c && scene && out, ATR_ERR_INVALID_ARG, "atr_flatten_compact2: NULL argument");
-    ATR_REQUIRE(c->n == scene->n, ATR_ERR_INVALID_ARG, "atr_flatten_compact2: tree/scene size mismatch");
-    *out = nullptr;
-    const uint32_t n = c->n;
-    const uint32_t m = n - 1;  // inner nodes of the binary tree
+// Compact2 layout of every mesh of segs into per-mesh slices of nodes (mesh m
+// from node inner_base(m)), woop and tri_index (mesh m from entry 4 *
+// tri_begin(m)).  d_sizes receives 2 * count int64 (nodes, woop per mesh);
+// h_max_depth the deepest inner level over all meshes (host, synchronises).
+int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const float4* verts, int4* nodes,
+                 float4* woop, int32_t* tri_index, int64_t* d_sizes, int32_t* h_max_depth) {
+    const uint32_t n = segs.n;
+    const uint32_t m = n - segs.count;  // inner nodes over all meshes
     cudaStream_t s = ctx->stream;
-    atr_compact* cp = new atr_compact();
-    cp->ctx = ctx;
-    // Upper bounds: every inner node, and 3 entries per triangle + 1 terminator per triangle.
-    int st = ctx->alloc(reinterpret_cast<void**>(&cp->nodes), (size_t)m * 64);
-    if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&cp->woop), (size_t)n * 4 * 16);
-    if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&cp->tri_index), (size_t)n * 4 * 4);
     void* scratch = nullptr;
     const size_t bm = align256((size_t)m * 4), b2 = align256((size_t)m * 8);
-    if (st == ATR_OK) st = ctx->alloc(&scratch, 7 * bm + 2 * b2 + 2 * bm + 256);
-    if (st != ATR_OK) {
-        ctx->release(scratch);
-        atr_compact_destroy(cp);
-        return st;
-    }
+    ATR_TRY(ctx->alloc(&scratch, 9 * bm + 2 * b2 + 256));
     char* p = static_cast<char*>(scratch);
     uint32_t* icnt = reinterpret_cast<uint32_t*>(p); p += bm;
     uint32_t* ic = reinterpret_cast<uint32_t*>(p); p += bm;
@@ -281,20 +317,17 @@ int atr_flatten_compact2(atr_ctx* ctx, const atr_collapsed* c, const atr_scene* 
     int2* acc1 = reinterpret_cast<int2*>(p); p += b2;
     uint32_t* ic_r = reinterpret_cast<uint32_t*>(p); p += bm;
     uint32_t* tw_r = reinterpret_cast<uint32_t*>(p); p += bm;
-    uint32_t* flags = reinterpret_cast<uint32_t*>(p);  // [0] pending, [1] max depth, [2] totals
-    FlatRefs t{n, c->parent, c->left, c->right, c->data, c->count, c->bmin, c->bmax, c->tri_indices};
+    uint32_t* flags = reinterpret_cast<uint32_t*>(p);  // [0] pending, [1] max depth, [2..3] totals
+    FlatRefs t{c.parent, c.left, c.right, c.data, c.count, c.bmin, c.bmax, c.tri_indices};
     const unsigned gb = (n + 255) / 256, gm = (m + 255) / 256;
     cudaMemsetAsync(counters, 0, (size_t)m * 4, s);
     cudaMemsetAsync(ic_r, 0, 2 * bm, s);
     cudaMemsetAsync(flags, 0, 256, s);
-    ctx->phase_begin("flatten");
-    k_flat_counts<<<gb, 256, 0, s>>>(t, icnt, ic, tw, counters);
-    k_flat_jump_init<<<gm, 256, 0, s>>>(t, icnt, acc0, jmp0);
+    k_flat_counts<<<gb, 256, 0, s>>>(t, segs, icnt, ic, tw, counters);
+    k_flat_jump_init<<<gb, 256, 0, s>>>(t, segs, icnt, acc0, jmp0);
     ctx->launches += 2;
     int2* ai = acc0; int2* ao = acc1;
     int* ji = jmp0; int* jo = jmp1;
-    // 2^8 ancestors per 8 rounds; the flag of the last round of a block tells
-    // whether any jump pointer is still live (depth >= 256 needs more rounds).
     for (int round = 0; round < 8 * kJumpRounds; ++round) {
         const bool check = round % kJumpRounds == kJumpRounds - 1;
         if (check) cudaMemsetAsync(flags, 0, 4, s);
@@ -309,25 +342,63 @@ int atr_flatten_compact2(atr_ctx* ctx, const atr_collapsed* c, const atr_scene* 
             if (!pending) break;
         }
     }
-    k_flat_scatter<<<gm, 256, 0, s>>>(t, ai, ic, tw, ic_r, tw_r, reinterpret_cast<int*>(flags + 1));
+    k_flat_scatter<<<gb, 256, 0, s>>>(segs, ai, ic, tw, ic_r, tw_r, reinterpret_cast<int*>(flags + 1));
     ctx->launches += 1;
-    st = exclusive_scan_u32(ctx, ic_r, ic_r, m, flags + 2);
+    int st = exclusive_scan_u32(ctx, ic_r, ic_r, m, flags + 2);
     if (st == ATR_OK) st = exclusive_scan_u32(ctx, tw_r, tw_r, m, flags + 3);
     if (st == ATR_OK) {
-        k_flat_slots<<<gm, 256, 0, s>>>(t, ai, ic, ic_r, slot_of);
-        k_flat_write<<<(m + 127) / 128, 128, 0, s>>>(t, scene->verts, ai, tw_r, slot_of, cp->nodes, cp->woop,
-                                                      cp->tri_index);
-        ctx->launches += 2;
+        k_flat_slots<<<gb, 256, 0, s>>>(t, segs, ai, ic_r, slot_of);
+        k_flat_write<<<(n + 127) / 128, 128, 0, s>>>(t, segs, verts, ai, tw_r, slot_of, nodes, woop, tri_index);
+        k_flat_sizes<<<(segs.count + 255) / 256, 256, 0, s>>>(segs, ic_r, tw_r, flags + 2, d_sizes,
+                                                             d_sizes + segs.count);
+        ctx->launches += 3;
         uint32_t h[4];
         cudaMemcpyAsync(h, flags, 16, cudaMemcpyDeviceToHost, s);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) st = cuda_fail(e, "flatten kernels", __FILE__, __LINE__);
-        cp->num_nodes = (int64_t)h[2] + 1;
-        cp->num_woop = (int64_t)h[3];
-        cp->max_depth = (int32_t)h[1];
+        if (h_max_depth) *h_max_depth = (int32_t)h[1];
     }
-    ctx->phase_end();
     ctx->release(scratch);
+    return st;
+}
+
+}  // namespace atr
+
+using namespace atr;
+
+extern "C" {
+
+int atr_flatten_compact2(atr_ctx* ctx, const atr_collapsed* c, const atr_scene* scene, atr_compact** out) {
+    ATR_REQUIRE(ctx && c && scene && out, ATR_ERR_INVALID_ARG, "atr_flatten_compact2: NULL argument");
+    ATR_REQUIRE(c->n == scene->n, ATR_ERR_INVALID_ARG, "atr_flatten_compact2: tree/scene size mismatch");
+    *out = nullptr;
+    const uint32_t n = c->n;
+    atr_compact* cp = new atr_compact();
+    cp->ctx = ctx;
+    // Upper bounds: every inner node, and 3 entries per triangle + 1 terminator per triangle.
+    int st = ctx->alloc(reinterpret_cast<void**>(&cp->nodes), (size_t)(n - 1) * 64);
+    if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&cp->woop), (size_t)n * 4 * 16);
+    if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&cp->tri_index), (size_t)n * 4 * 4);
+    int64_t* sizes = nullptr;
+    if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&sizes), 16);
+    if (st != ATR_OK) {
+        ctx->release(sizes);
+        atr_compact_destroy(cp);
+        return st;
+    }
+    const Segs segs{nullptr, nullptr, 1u, n};
+    const CollapsedOut co{c->parent, c->left, c->right, c->data, c->count, c->bmin, c->bmax, c->tri_indices};
+    ctx->phase_begin("flatten");
+    st = flatten_segs(ctx, segs, co, scene->verts, cp->nodes, cp->woop, cp->tri_index, sizes, &cp->max_depth);
+    ctx->phase_end();
+    if (st == ATR_OK) {
+        int64_t h[2];
+        cudaError_t e = cudaMemcpy(h, sizes, 16, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpy(sizes)", __FILE__, __LINE__);
+        cp->num_nodes = h[0];
+        cp->num_woop = h[1];
+    }
+    ctx->release(sizes);
     if (st != ATR_OK) { atr_compact_destroy(cp); return st; }
     *out = cp;
     return ATR_OK;

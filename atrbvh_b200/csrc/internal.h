@@ -126,8 +126,28 @@ struct TreeOut {
     float* area;
 };
 
+// Collapsed-tree arrays (possibly batched: per-mesh node slices, per-mesh
+// triangle-list slices).
+struct CollapsedOut {
+    int32_t *parent, *left, *right, *data, *count;
+    float4 *bmin, *bmax;
+    int32_t* tri_indices;
+};
+
 // Allocate the SoA arrays of a tree with n triangles in one block.
 int tree_alloc(atr_ctx* ctx, uint32_t n, atr_tree** out);
+int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const TreeOut& src,
+                  const CollapsedOut& dst, float ci, float ct, int max_leaf, float* d_sah_parts);
+int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const float4* verts, int4* nodes,
+                 float4* woop, int32_t* tri_index, int64_t* d_sizes, int32_t* h_max_depth);
+struct RayMeshMap;  // trace.cu
+int trace_run(atr_ctx* ctx, const int4* nodes, const float4* woop, const int32_t* tri, const RayMeshMap& map,
+              int max_depth, const float4* rays, int64_t n, int any_hit, int4* res);
+int trace_batch(atr_ctx* ctx, const int4* nodes, const float4* woop, const int32_t* tri, const uint32_t* ray_off,
+                const uint32_t* group_mesh, const uint32_t* tri_off, uint32_t groups, int max_depth,
+                const float4* rays, int64_t n, int any_hit, int4* res);
+// Bottom-up box refit of one tree (local indices) from vertices of its mesh.
+int refit_arrays(atr_ctx* ctx, uint32_t n, const TreeOut& t, const float4* verts);
 
 // Single-mesh LBVH into an allocated tree (keeps the sort output).
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds,

@@ -574,13 +574,12 @@ int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* 
     return ATR_OK;
 }
 
-int refit_tree(atr_ctx* ctx, atr_tree* t, const float4* verts) {
-    const uint32_t n = t->n;
+int refit_arrays(atr_ctx* ctx, uint32_t n, const TreeOut& t, const float4* verts) {
     void* ctr = nullptr;
     ATR_TRY(ctx->alloc(&ctr, (size_t)(n - 1) * 4));
     cudaMemsetAsync(ctr, 0, (size_t)(n - 1) * 4, ctx->stream);
-    k_refit<<<(n + 255) / 256, 256, 0, ctx->stream>>>(verts, n, t->parent, t->left, t->right, t->data, t->bmin,
-                                                      t->bmax, t->area, static_cast<uint32_t*>(ctr));
+    k_refit<<<(n + 255) / 256, 256, 0, ctx->stream>>>(verts, n, t.parent, t.left, t.right, t.data, t.bmin, t.bmax,
+                                                      t.area, static_cast<uint32_t*>(ctr));
     ctx->launches += 1;
     cudaError_t e = cudaGetLastError();
     ctx->release(ctr);
@@ -662,7 +661,8 @@ int atr_refit(atr_ctx* ctx, atr_tree* tree, const atr_scene* scene) {
     ATR_REQUIRE(ctx && tree && scene, ATR_ERR_INVALID_ARG, "atr_refit: NULL argument");
     ATR_REQUIRE(tree->n == scene->n, ATR_ERR_INVALID_ARG, "atr_refit: tree has %u triangles, scene %u",
                 tree->n, scene->n);
-    return refit_tree(ctx, tree, scene->verts);
+    const TreeOut t{tree->parent, tree->left, tree->right, tree->data, tree->bmin, tree->bmax, tree->area};
+    return refit_arrays(ctx, tree->n, t, scene->verts);
 }
 
 int atr_device_morton(atr_ctx* ctx, const float* vertices, uint32_t n, const float* bbmin, const float* bbmax,

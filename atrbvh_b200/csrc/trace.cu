@@ -20,6 +20,18 @@
 #include "internal.h"
 
 namespace atr {
+
+// Which layout each ray traverses: with groups == 0 every ray uses the arrays
+// as given; otherwise rays [ray_off[g], ray_off[g+1]) trace mesh
+// group_mesh[g] of a batch whose mesh m starts at node 4 * (tri_off[m] - m)
+// (float4 units) and Woop entry 4 * tri_off[m].
+struct RayMeshMap {
+    const uint32_t* ray_off;
+    const uint32_t* group_mesh;
+    const uint32_t* tri_off;
+    uint32_t groups;
+};
+
 namespace {
 
 constexpr int kSentinel = 0x76543210;
@@ -38,10 +50,12 @@ __device__ __forceinline__ float span_end(float a0, float a1, float b0, float b1
 }
 
 template <int kStack>
-__global__ void __launch_bounds__(128) k_trace(const float4* __restrict__ nodes, const float4* __restrict__ woop,
-                                               const int* __restrict__ tri_index, const float4* __restrict__ rays,
-                                               int64_t nrays, int any_hit, int4* __restrict__ results,
-                                               unsigned long long* __restrict__ counter, uint32_t* __restrict__ err) {
+__global__ void __launch_bounds__(128) k_trace(const float4* __restrict__ nodes_all,
+                                               const float4* __restrict__ woop_all,
+                                               const int* __restrict__ tri_all, RayMeshMap map,
+                                               const float4* __restrict__ rays, int64_t nrays, int any_hit,
+                                               int4* __restrict__ results, unsigned long long* __restrict__ counter,
+                                               uint32_t* __restrict__ err) {
     int stack[kStack];
     const int lane = threadIdx.x & 31;
     float ox = 0, oy = 0, oz = 0, tmin = 0, dx = 0, dy = 0, dz = 0, hitT = 0;
@@ -49,6 +63,9 @@ __global__ void __launch_bounds__(128) k_trace(const float4* __restrict__ nodes,
     int nodeAddr = kSentinel, leafAddr = 0, hitIndex = -1, sp = 0;
     long long rayidx = 0;
     bool overflow = false;
+    const float4* nodes = nodes_all;
+    const float4* woop = woop_all;
+    const int* tri_index = tri_all;
 
     while (true) {
         const bool terminated = nodeAddr == kSentinel;
@@ -61,6 +78,18 @@ __global__ void __launch_bounds__(128) k_trace(const float4* __restrict__ nodes,
             base = __shfl_sync(mt, base, leader);
             rayidx = (long long)base + __popc(mt & lanemask_lt());
             if (rayidx >= nrays) break;
+            if (map.groups) {
+                uint32_t lo = 0, hi = map.groups;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if ((long long)__ldg(map.ray_off + mid) <= rayidx) lo = mid; else hi = mid;
+                }
+                const uint32_t mesh = __ldg(map.group_mesh + lo);
+                const uint32_t s0 = __ldg(map.tri_off + mesh);
+                nodes = nodes_all + 4 * ((size_t)s0 - mesh);
+                woop = woop_all + 4 * (size_t)s0;
+                tri_index = tri_all + 4 * (size_t)s0;
+            }
             const float4 o = __ldg(rays + 2 * rayidx), d = __ldg(rays + 2 * rayidx + 1);
             ox = o.x; oy = o.y; oz = o.z; tmin = o.w;
             dx = d.x; dy = d.y; dz = d.z; hitT = d.w;
@@ -155,8 +184,8 @@ __global__ void __launch_bounds__(128) k_trace(const float4* __restrict__ nodes,
 }
 
 template <int kStack>
-int launch_trace(atr_ctx* ctx, const atr_compact* cp, const float4* rays, int64_t n, int any_hit, int4* res,
-                 unsigned long long* counter) {
+void launch_trace(atr_ctx* ctx, const int4* nodes, const float4* woop, const int32_t* tri, const RayMeshMap& map,
+                  const float4* rays, int64_t n, int any_hit, int4* res, unsigned long long* counter) {
     static int blocks_per_sm = 0;
     if (!blocks_per_sm) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_trace<kStack>, 128, 0);
@@ -165,11 +194,9 @@ int launch_trace(atr_ctx* ctx, const atr_compact* cp, const float4* rays, int64_
     const int64_t need = (n + 127) / 128;
     int64_t grid = (int64_t)ctx->num_sms * blocks_per_sm;
     if (need < grid) grid = need;
-    k_trace<kStack><<<(unsigned)grid, 128, 0, ctx->stream>>>(reinterpret_cast<const float4*>(cp->nodes), cp->woop,
-                                                             cp->tri_index, rays, n, any_hit, res, counter,
-                                                             ctx->d_error);
+    k_trace<kStack><<<(unsigned)grid, 128, 0, ctx->stream>>>(reinterpret_cast<const float4*>(nodes), woop, tri, map,
+                                                             rays, n, any_hit, res, counter, ctx->d_error);
     ctx->launches += 1;
-    return ATR_OK;
 }
 
 // Cosine-weighted diffuse bounce per primary hit (the workload of
@@ -219,6 +246,35 @@ __global__ void __launch_bounds__(256) k_bounce(const float4* __restrict__ verts
 }
 
 }  // namespace
+
+int trace_run(atr_ctx* ctx, const int4* nodes, const float4* woop, const int32_t* tri, const RayMeshMap& map,
+              int max_depth, const float4* rays, int64_t n, int any_hit, int4* res) {
+    if (n == 0) return ATR_OK;
+    unsigned long long* counter = nullptr;
+    ATR_TRY(ctx->alloc(reinterpret_cast<void**>(&counter), 8));
+    cudaMemsetAsync(counter, 0, 8, ctx->stream);
+    int st = ATR_OK;
+    ctx->phase_begin("trace");
+    if (max_depth + 1 < 64) launch_trace<64>(ctx, nodes, woop, tri, map, rays, n, any_hit, res, counter);
+    else if (max_depth + 1 < 256) launch_trace<256>(ctx, nodes, woop, tri, map, rays, n, any_hit, res, counter);
+    else st = ATR_ERR_UNSUPPORTED;
+    ctx->phase_end();
+    ctx->release(counter);
+    if (st == ATR_ERR_UNSUPPORTED) {
+        set_error("trace: layout depth %d exceeds the traversal stack", max_depth);
+        return st;
+    }
+    ATR_CUDA(cudaGetLastError());
+    return ATR_OK;
+}
+
+int trace_batch(atr_ctx* ctx, const int4* nodes, const float4* woop, const int32_t* tri, const uint32_t* ray_off,
+                const uint32_t* group_mesh, const uint32_t* tri_off, uint32_t groups, int max_depth,
+                const float4* rays, int64_t n, int any_hit, int4* res) {
+    const RayMeshMap map{ray_off, group_mesh, tri_off, groups};
+    return trace_run(ctx, nodes, woop, tri, map, max_depth, rays, n, any_hit, res);
+}
+
 }  // namespace atr
 
 using namespace atr;
@@ -228,25 +284,9 @@ extern "C" {
 int atr_trace(atr_ctx* ctx, const atr_compact* cp, const float* rays, int64_t n, int any_hit, int32_t* results) {
     ATR_REQUIRE(ctx && cp && rays && results, ATR_ERR_INVALID_ARG, "atr_trace: NULL argument");
     ATR_REQUIRE(n >= 0, ATR_ERR_INVALID_ARG, "atr_trace: negative ray count");
-    if (n == 0) return ATR_OK;
-    unsigned long long* counter = nullptr;
-    ATR_TRY(ctx->alloc(reinterpret_cast<void**>(&counter), 8));
-    cudaMemsetAsync(counter, 0, 8, ctx->stream);
-    const float4* r = reinterpret_cast<const float4*>(rays);
-    int4* res = reinterpret_cast<int4*>(results);
-    int st;
-    ctx->phase_begin("trace");
-    if (cp->max_depth + 1 < 64) st = launch_trace<64>(ctx, cp, r, n, any_hit, res, counter);
-    else if (cp->max_depth + 1 < 256) st = launch_trace<256>(ctx, cp, r, n, any_hit, res, counter);
-    else st = ATR_ERR_UNSUPPORTED;
-    ctx->phase_end();
-    ctx->release(counter);
-    if (st == ATR_ERR_UNSUPPORTED) {
-        set_error("atr_trace: layout depth %d exceeds the traversal stack", cp->max_depth);
-        return st;
-    }
-    ATR_CUDA(cudaGetLastError());
-    return st;
+    const RayMeshMap map{nullptr, nullptr, nullptr, 0u};
+    return trace_run(ctx, cp->nodes, cp->woop, cp->tri_index, map, cp->max_depth, reinterpret_cast<const float4*>(rays),
+                     n, any_hit, reinterpret_cast<int4*>(results));
 }
 
 int atr_gen_bounce_rays(atr_ctx* ctx, const atr_scene* scene, const float* rays, const int32_t* results, int64_t n,

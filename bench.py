@@ -179,7 +179,8 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     ctx = ab.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream)
-    v = ab.gen_scene(ab.SCENE_CLUSTERED, N_TRIS, 0)
+    n_tris = args.triangles
+    v = ab.gen_scene(ab.SCENE_CLUSTERED, n_tris, 0)
     scene = ab.SceneWrapper(ctx, v)  # scene box reduced on the device
     prim = ab.gen_rays_pinhole(WIDTH, HEIGHT)
     nr = len(prim)
@@ -243,7 +244,7 @@ def run_ours(args, world, rank, local):
     # ---- e2e through the public API from pinned host memory ----
     pinned = torch.from_numpy(v.reshape(-1)).pin_memory().numpy().reshape(v.shape)
     e2e_times = []
-    for it in range(args.warmup + args.steps):
+    for it in range(0 if args.no_e2e else args.warmup + args.steps):
         barrier(world)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -257,13 +258,13 @@ def run_ours(args, world, rank, local):
         sc.close()
         if it >= args.warmup:
             e2e_times.append(dt)
-    e2e_s = max_over_ranks(statistics.mean(e2e_times), world)
+    e2e_s = max_over_ranks(statistics.mean(e2e_times), world) if e2e_times else float("nan")
 
     peaks = _read_peaks()
     roof = {}
     for k, bpt in BYTES_PER_TRI.items():
         if ph_ms.get(k):
-            roof[k] = N_TRIS * bpt / (ph_ms[k] * 1e-3) / 1e9
+            roof[k] = n_tris * bpt / (ph_ms[k] * 1e-3) / 1e9
     # Dominant phase by time (trace counted per launch).
     times = {k: (v2 / n_trace if k == "trace" and n_trace else v2) for k, v2 in ph_ms.items()}
     dominant = max(times, key=times.get)
@@ -279,13 +280,13 @@ def run_ours(args, world, rank, local):
             bpt = 0.0
         else:
             bpt = 0.0
-        achieved = (N_TRIS * bpt / (times[dominant] * 1e-3) / 1e9) if bpt else 0.0
+        achieved = (n_tris * bpt / (times[dominant] * 1e-3) / 1e9) if bpt else 0.0
         rl = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
               "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_src": peaks["src"],
               "note": "latency/issue-bound phase; HBM fraction shown for reference"}
     out = {
         "metric": METRIC,
-        "value": world * N_TRIS / (build_ms_max * 1e-3) / 1e6,
+        "value": world * n_tris / (build_ms_max * 1e-3) / 1e6,
         "unit": "Mtri/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -296,7 +297,8 @@ def run_ours(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded Philox: clustered scene + pinhole/diffuse rays)",
-        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "rays_per_step": int(rays_per_step),
+        "config": {"workload": WORKLOAD if n_tris == N_TRIS else f"{n_tris}-triangle instance of: {WORKLOAD}",
+                   "triangles": n_tris, "rays_per_step": int(rays_per_step),
                    "treelet": 9, "iterations": 2, "morton_bits": 30, "collapse_max_leaf": 0,
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (201 MB of vertices)"},
         "mrays_per_s": world * rays_per_step / (trace_ms_max * 1e-3) / 1e6 if trace_ms_max else None,
@@ -304,7 +306,7 @@ def run_ours(args, world, rank, local):
         "build_ms": build_ms_max,
         "phase_gbs": {k: round(x, 1) for k, x in roof.items()},
         "roofline": rl,
-        "e2e": {"value": world * N_TRIS / e2e_s / 1e6, "unit": "Mtri/s",
+        "e2e": {"value": world * n_tris / e2e_s / 1e6, "unit": "Mtri/s",
                 "h2d_bytes_per_step": int(v.nbytes), "d2h_bytes_per_step": 8,
                 "path": "atr_scene_create(pinned host vertices) -> atr_build_lbvh -> atr_optimize_atrbvh -> "
                         "atr_collapse (SAH read back)"},
@@ -355,6 +357,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--triangles", type=int, default=N_TRIS,
+                    help="scene size (default: the workload's 4,194,304); smaller values are for profiling")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

@@ -231,6 +231,24 @@ int atr_batch_download_mesh(atr_ctx* ctx, const atr_batch* batch, uint32_t mesh,
                             float* bbox_max, float* area);
 /* Per-mesh SoABVHTree::SAH (sequential float sums), num_meshes values. */
 int atr_batch_sah(atr_ctx* ctx, const atr_batch* batch, float ci, float ct, float* sah);
+/* Collapse every mesh (as atr_collapse per mesh; sah may be NULL, else one
+ * value per mesh), then lay every mesh out in Compact2 (as
+ * atr_flatten_compact2 per mesh). */
+int atr_batch_collapse(atr_ctx* ctx, atr_batch* batch, float ci, float ct, int max_leaf, float* sah);
+int atr_batch_flatten(atr_ctx* ctx, atr_batch* batch);
+int atr_batch_compact_view(const atr_batch* batch, uint32_t mesh, atr_compact_view* view);
+int atr_batch_compact_download(atr_ctx* ctx, const atr_batch* batch, uint32_t mesh, int32_t* nodes,
+                               float* woop, int32_t* tri_index);
+/* Merged ray queue: rays [ray_offsets[g], ray_offsets[g+1]) trace mesh
+ * group_mesh[g] (host arrays, groups entries / groups+1 offsets); rays and
+ * results are device arrays as in atr_trace; triangle ids are mesh-local. */
+int atr_batch_trace(atr_ctx* ctx, const atr_batch* batch, const float* rays, int64_t num_rays,
+                    const uint32_t* ray_offsets, const uint32_t* group_mesh, uint32_t groups,
+                    int any_hit, int32_t* results);
+/* Replace one mesh's vertices (same count), refit its tree, and (when the
+ * batch was flattened) re-collapse and re-flatten that mesh in place. */
+int atr_batch_refit_mesh(atr_ctx* ctx, atr_batch* batch, uint32_t mesh, const float* vertices,
+                         int vertices_on_device);
 
 /* One cosine-weighted diffuse bounce ray per primary result (the diffuse
  * workload of gpu-ray-traversal/src/rt/ray/RayGenKernels.cu:114-223 with one
