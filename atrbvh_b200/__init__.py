@@ -19,6 +19,7 @@ CPU fallback: without the library or a B200 every call raises.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass
 from pathlib import Path
 
@@ -197,6 +198,12 @@ class Context:
         h = C.c_void_p()
         check(lib().atr_ctx_create(device, C.c_void_p(stream) if stream else None, C.byref(h)))
         self.handle = h
+        # Objects whose device memory came from this context's pool: they are
+        # freed before the context (a destroy after it would touch freed state).
+        self._deps = weakref.WeakSet()
+
+    def _adopt(self, obj) -> None:
+        self._deps.add(obj)
 
     def synchronize(self) -> None:
         check(lib().atr_ctx_synchronize(self.handle))
@@ -226,6 +233,8 @@ class Context:
 
     def close(self) -> None:
         if getattr(self, "handle", None):
+            for obj in list(getattr(self, "_deps", ())):
+                obj.close()
             lib().atr_ctx_destroy(self.handle)
             self.handle = None
 
@@ -256,6 +265,7 @@ class SceneWrapper:
         check(lib().atr_scene_create(ctx.handle, src, n, bmin, bmax, on_dev, C.byref(h)))
         self.handle = h
         self.n = n
+        ctx._adopt(self)
 
     def bounds(self) -> tuple[np.ndarray, np.ndarray]:
         a = (C.c_float * 3)()
@@ -326,6 +336,7 @@ class BVHTree:
         self.ctx = ctx
         self.handle = handle
         self.n = n
+        ctx._adopt(self)
 
     def view(self) -> TreeView:
         v = TreeView()
@@ -412,6 +423,7 @@ class HostCollapsedTree:
 class BVHCollapsedTree:
     def __init__(self, ctx: Context, handle: C.c_void_p, n: int):
         self.ctx, self.handle, self.n = ctx, handle, n
+        ctx._adopt(self)
 
     def view(self) -> CollapsedView:
         v = CollapsedView()
@@ -495,6 +507,7 @@ class Batch:
         check(lib().atr_batch_create(ctx.handle, src, _ptr(off), self.count, None if b is None else _ptr(b), on_dev,
                                      C.byref(h)))
         self.handle = h
+        ctx._adopt(self)
 
     def set_params(self, treelet_sizes=None, iterations=None) -> None:
         if treelet_sizes is None:
@@ -582,6 +595,7 @@ class CudaBVH:
         check(lib().atr_flatten_compact2(scene.ctx.handle, collapsed.handle, scene.handle, C.byref(h)))
         self.ctx = scene.ctx
         self.handle = h
+        self.ctx._adopt(self)
 
     def view(self) -> CompactView:
         v = CompactView()
@@ -612,3 +626,4 @@ class CudaBVH:
             self.close()
         except Exception:
             pass
+

@@ -51,6 +51,9 @@ struct atr_batch {
     std::vector<int64_t> h_sizes;
     int32_t max_depth = 0;
     bool flattened = false;
+    // Parameters of the last atr_batch_collapse (reused when one mesh is refit).
+    float col_ci = 1.2f, col_ct = 1.0f;
+    int col_max_leaf = 0;
 };
 
 namespace atr {
@@ -352,6 +355,9 @@ int atr_batch_collapse(atr_ctx* ctx, atr_batch* b, float ci, float ct, int max_l
             for (uint32_t m = 0; m < b->count; ++m) sah[m] = h[2 * m] / h[2 * m + 1];
     }
     ctx->release(parts);
+    b->col_ci = ci;
+    b->col_ct = ct;
+    b->col_max_leaf = max_leaf;
     b->flattened = false;
     return st;
 }
@@ -411,8 +417,13 @@ int atr_batch_trace(atr_ctx* ctx, const atr_batch* b, const float* rays, int64_t
     }
     uint32_t* map = nullptr;
     ATR_TRY(ctx->alloc(reinterpret_cast<void**>(&map), (2ull * groups + 1) * 4));
-    cudaMemcpyAsync(map, ray_offsets, (groups + 1) * 4ull, cudaMemcpyHostToDevice, ctx->stream);
-    cudaMemcpyAsync(map + groups + 1, group_mesh, groups * 4ull, cudaMemcpyHostToDevice, ctx->stream);
+    cudaError_t e = cudaMemcpyAsync(map, ray_offsets, (groups + 1) * 4ull, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(map + groups + 1, group_mesh, groups * 4ull, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+        ctx->release(map);
+        return cuda_fail(e, "cudaMemcpyAsync(ray groups)", __FILE__, __LINE__);
+    }
     const int st = trace_batch(ctx, b->cp_nodes, b->cp_woop, b->cp_tri, map, map + groups + 1, b->d_tri_off, groups,
                                b->max_depth, reinterpret_cast<const float4*>(rays), num_rays, any_hit,
                                reinterpret_cast<int4*>(results));
@@ -421,6 +432,15 @@ int atr_batch_trace(atr_ctx* ctx, const atr_batch* b, const float* rays, int64_t
 }
 
 int atr_batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* vertices, int on_device) {
+    return atr::batch_refit_mesh(ctx, b, mesh, vertices, on_device, nullptr);
+}
+
+}  // extern "C"
+
+namespace atr {
+
+int batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* vertices, int on_device,
+                     float* h_sah) {
     ATR_REQUIRE(ctx && b && vertices, ATR_ERR_INVALID_ARG, "atr_batch_refit_mesh: NULL argument");
     ATR_REQUIRE(mesh < b->count, ATR_ERR_INVALID_ARG, "atr_batch_refit_mesh: mesh %u of %u", mesh, b->count);
     const size_t s0 = b->h_tri_off[mesh];
@@ -436,24 +456,37 @@ int atr_batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float*
     const Segs one{nullptr, nullptr, 1u, n};
     const CollapsedOut c{b->col.parent + nb, b->col.left + nb, b->col.right + nb, b->col.data + nb,
                          b->col.count + nb, b->col.bmin + nb, b->col.bmax + nb, b->col.tri_indices + s0};
-    ATR_TRY(collapse_segs(ctx, one, 2 * (size_t)n - 1, t, c, 1.2f, 1.0f, 0, nullptr));
-    int32_t depth = 0;
+    // sizes: Compact2 node and Woop counts, then (when asked) the SAH parts.
     int64_t* sizes = nullptr;
-    ATR_TRY(ctx->alloc(reinterpret_cast<void**>(&sizes), 16));
-    int st = flatten_segs(ctx, one, c, b->verts + 3 * s0, b->cp_nodes + 4 * (s0 - mesh), b->cp_woop + 4 * s0,
+    ATR_TRY(ctx->alloc(reinterpret_cast<void**>(&sizes), 32));
+    float* parts = h_sah ? reinterpret_cast<float*>(sizes + 2) : nullptr;
+    int st = collapse_segs(ctx, one, 2 * (size_t)n - 1, t, c, b->col_ci, b->col_ct, b->col_max_leaf, parts);
+    int32_t depth = 0;
+    if (st == ATR_OK)
+        st = flatten_segs(ctx, one, c, b->verts + 3 * s0, b->cp_nodes + 4 * (s0 - mesh), b->cp_woop + 4 * s0,
                           b->cp_tri + 4 * s0, sizes, &depth);
-    int64_t h[2] = {0, 0};
+    int64_t h[4] = {0, 0, 0, 0};
     if (st == ATR_OK) {
-        cudaError_t e = cudaMemcpy(h, sizes, 16, cudaMemcpyDeviceToHost);
+        cudaError_t e = cudaMemcpyAsync(h, sizes, 32, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpy(sizes)", __FILE__, __LINE__);
     }
     ctx->release(sizes);
     ATR_TRY(st);
+    if (h_sah) {
+        float p[2];
+        std::memcpy(p, h + 2, 8);
+        *h_sah = p[0] / p[1];
+    }
     b->h_sizes[mesh] = h[0];
     b->h_sizes[b->count + mesh] = h[1];
     b->max_depth = std::max(b->max_depth, depth);
     return ATR_OK;
 }
+
+}  // namespace atr
+
+extern "C" {
 
 int atr_batch_sah(atr_ctx* ctx, const atr_batch* b, float ci, float ct, float* sah) {
     ATR_REQUIRE(ctx && b && sah, ATR_ERR_INVALID_ARG, "atr_batch_sah: NULL argument");

@@ -148,6 +148,10 @@ int trace_batch(atr_ctx* ctx, const int4* nodes, const float4* woop, const int32
                 const float4* rays, int64_t n, int any_hit, int4* res);
 // Bottom-up box refit of one tree (local indices) from vertices of its mesh.
 int refit_arrays(atr_ctx* ctx, uint32_t n, const TreeOut& t, const float4* verts);
+// atr_batch_refit_mesh that also returns the mesh's collapsed-tree SAH
+// (h_sah may be NULL).
+int batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* vertices, int on_device,
+                     float* h_sah);
 
 // Single-mesh LBVH into an allocated tree (keeps the sort output).
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds,
