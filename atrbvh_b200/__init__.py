@@ -90,6 +90,7 @@ _SIGS = [
     ("atr_optimize_atrbvh", C.c_int, [_p, _p, C.c_int, C.c_int, C.c_float, C.c_float]),
     ("atr_optimize_trbvh", C.c_int, [_p, _p, C.c_int, C.c_int, C.c_float, C.c_float]),
     ("atr_refit", C.c_int, [_p, _p, _p]),
+    ("atr_refit_noalloc", C.c_int, [_p, C.c_uint32, _p, _p, _p, _p, _p, _p, _p, _p]),
     ("atr_collapse", C.c_int, [_p, _p, C.c_float, C.c_float, C.c_int, C.POINTER(_p), _f32p]),
     ("atr_collapsed_destroy", C.c_int, [_p]),
     ("atr_collapsed_view_get", C.c_int, [_p, C.POINTER(CollapsedView)]),

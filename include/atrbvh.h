@@ -168,6 +168,21 @@ int atr_optimize_trbvh(atr_ctx* ctx, atr_tree* tree, int treelet_size, int itera
  * vertices (the refit pass of BVHRT-Core/src/LBVH.cu:465-570 on a resident tree). */
 int atr_refit(atr_ctx* ctx, atr_tree* tree, const atr_scene* scene);
 
+/* Refit that allocates no device memory.  No counterpart in the reference.
+ * For callers that cannot allocate when they refit -- a frame or serving
+ * loop running under a fixed, pre-reserved memory budget, or code that may
+ * only enqueue work on a stream it was given.  The caller passes the tree's
+ * device arrays (atr_tree_view_get, or its own copies) and the mesh's device
+ * vertices; the per-node counters live in a fixed __device__ array inside the
+ * library: at most 1,048,576 triangles (larger meshes are rejected; use
+ * atr_refit), one array per device for the life of the process, shared by all
+ * calls -- calls that overlap on the GPU race, so order them on one stream.
+ * The first call on a device looks up the array's address; make it before
+ * any stream capture.  stream may be NULL (legacy default stream). */
+int atr_refit_noalloc(void* stream, uint32_t num_triangles, const float* vertices,
+                      const int32_t* parent, const int32_t* left, const int32_t* right,
+                      const int32_t* data, float* bbox_min, float* bbox_max, float* area);
+
 /* ---- collapse ----------------------------------------------------------------
  * BVHTreeCollapser::Collapse(BVHTree*, float* sah, ci, ct)
  * (BVHRT-Core/src/BVHTreeCollapser.h:39, .cpp:21-93).  max_leaf = 0 reproduces
