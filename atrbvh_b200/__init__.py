@@ -62,6 +62,31 @@ class CompactView(C.Structure):
                 ("tri_index", _p), ("max_depth", C.c_int32)]
 
 
+class ServerRequest(C.Structure):
+    _fields_ = [("kind", C.c_int), ("mesh_id", C.c_uint64), ("vertices", _p), ("num_triangles", C.c_uint32),
+                ("rays", _p), ("num_rays", C.c_uint32), ("results", _p), ("keep_resident", C.c_int)]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("sah", C.c_float), ("queue_ms", C.c_double), ("latency_ms", C.c_double),
+                ("batch_requests", C.c_uint32), ("lane", C.c_uint32), ("error", C.c_char * 160)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("lanes", C.c_uint32), ("max_batch_requests", C.c_uint32),
+                ("max_batch_triangles", C.c_uint64), ("treelet_size", C.c_int), ("iterations", C.c_int),
+                ("max_leaf", C.c_int), ("class_treelet", _p), ("class_iters", _p)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("failed", C.c_uint64), ("builds", C.c_uint64), ("refits", C.c_uint64),
+                ("evictions", C.c_uint64), ("triangles_built", C.c_uint64), ("triangles_refit", C.c_uint64),
+                ("rays_traced", C.c_uint64), ("lane_batches", C.c_uint64), ("max_batch_requests_seen", C.c_uint32),
+                ("max_lanes_busy", C.c_uint32), ("resident_meshes", C.c_uint32), ("resident_bytes", C.c_uint64),
+                ("peak_bytes", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("max_ms", C.c_double), ("overlap_fraction", C.c_double), ("busy_ms", C.c_double)]
+
+
 # (name, restype, argtypes) for every exported entry point of include/atrbvh.h.
 _SIGS = [
     ("atr_last_error", C.c_char_p, []),
@@ -120,6 +145,12 @@ _SIGS = [
     ("atr_gen_batch_scene", C.c_int, [C.c_uint32, _p, C.c_uint64, _p]),
     ("atr_gen_rays_pinhole", C.c_int, [C.c_uint32, C.c_uint32, _f32p, C.c_float, _p]),
     ("atr_gen_rays_random", C.c_int, [C.c_uint64, C.c_uint64, _f32p, _f32p, _p]),
+    ("atr_server_create", C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(_p)]),
+    ("atr_server_submit", C.c_int, [_p, C.POINTER(ServerRequest), C.POINTER(C.c_uint64)]),
+    ("atr_server_wait", C.c_int, [_p, C.c_uint64, C.POINTER(ServerResult)]),
+    ("atr_server_release", C.c_int, [_p, C.c_uint64]),
+    ("atr_server_stats_get", C.c_int, [_p, C.POINTER(ServerStats)]),
+    ("atr_server_destroy", C.c_int, [_p]),
 ]
 
 EXPORTED = [name for name, _, _ in _SIGS]
@@ -628,3 +659,73 @@ class CudaBVH:
         except Exception:
             pass
 
+
+# ---- serving loop ----------------------------------------------------------------
+
+REQ_BUILD, REQ_REFIT = 0, 1
+ERR_NOT_RESIDENT = 7
+
+
+class Server:
+    """Build/refit + trace request server (atr_server): admission by device
+    memory, resident BVHs for refits, continuous batching over `lanes` streams.
+
+    submit() returns a ticket; the arrays passed stay referenced until wait()
+    returns that ticket's result (a dict).  results (N, 4) int32 is filled in
+    place."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 120 << 30, lanes: int = 2, max_batch_requests: int = 64,
+                 max_batch_triangles: int = 1 << 26, treelet: int = 9, iterations: int = 2, max_leaf: int = 0,
+                 class_treelet=None, class_iters=None):
+        cfg = ServerConfig(hbm_budget, lanes, max_batch_requests, max_batch_triangles, treelet, iterations, max_leaf,
+                           None, None)
+        if class_treelet is not None:
+            self._ct = np.ascontiguousarray(class_treelet, dtype=np.uint8)
+            self._ci = np.ascontiguousarray(class_iters, dtype=np.uint8)
+            assert self._ct.shape == (32,) and self._ci.shape == (32,)
+            cfg.class_treelet, cfg.class_iters = self._ct.ctypes.data, self._ci.ctypes.data
+        h = C.c_void_p()
+        check(lib().atr_server_create(device, C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self._keep: dict[int, tuple] = {}
+
+    def submit(self, kind: int, mesh_id: int, vertices, rays=None, results=None, keep_resident: bool = True) -> int:
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3, 4)
+        r = None if rays is None else np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        nr = 0 if r is None else r.shape[0]
+        if nr:
+            assert results is not None and results.dtype == np.int32 and results.flags.c_contiguous
+            assert results.size >= 4 * nr
+        req = ServerRequest(kind, mesh_id, v.ctypes.data, v.shape[0], None if r is None else r.ctypes.data, nr,
+                            None if not nr else results.ctypes.data, 1 if keep_resident else 0)
+        t = C.c_uint64()
+        check(lib().atr_server_submit(self.handle, C.byref(req), C.byref(t)))
+        self._keep[t.value] = (v, r, results)
+        return t.value
+
+    def wait(self, ticket: int) -> dict:
+        res = ServerResult()
+        check(lib().atr_server_wait(self.handle, ticket, C.byref(res)))
+        self._keep.pop(ticket, None)
+        return {"status": res.status, "sah": res.sah, "queue_ms": res.queue_ms, "latency_ms": res.latency_ms,
+                "batch_requests": res.batch_requests, "lane": res.lane, "error": res.error.decode()}
+
+    def release(self, mesh_id: int) -> None:
+        check(lib().atr_server_release(self.handle, mesh_id))
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib().atr_server_stats_get(self.handle, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().atr_server_destroy(self.handle)
+            self.handle = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -27,7 +27,8 @@ enum atr_status {
     ATR_ERR_OOM = 3,          /* device allocation failed */
     ATR_ERR_UNSUPPORTED = 4,  /* parameter outside the supported range */
     ATR_ERR_DEVICE_WAIT = 5,  /* a bounded device-side wait gave up */
-    ATR_ERR_NO_DEVICE = 6     /* no CUDA device / wrong architecture */
+    ATR_ERR_NO_DEVICE = 6,    /* no CUDA device / wrong architecture */
+    ATR_ERR_NOT_RESIDENT = 7  /* server refit of a mesh id it does not hold */
 };
 
 enum atr_scene_kind { ATR_SCENE_UNIFORM = 0, ATR_SCENE_CLUSTERED = 1 };
@@ -264,6 +265,79 @@ int atr_batch_trace(atr_ctx* ctx, const atr_batch* batch, const float* rays, int
  * batch was flattened) re-collapse and re-flatten that mesh in place. */
 int atr_batch_refit_mesh(atr_ctx* ctx, atr_batch* batch, uint32_t mesh, const float* vertices,
                          int vertices_on_device);
+
+/* ---- serving loop (no counterpart in the reference, whose Renderer builds
+ * and traces one scene at a time: gpu-ray-traversal/src/rt/cuda/Renderer.cpp:85-105,
+ * 115-265) ---------------------------------------------------------------------
+ * A request builds a mesh (or refits a mesh kept resident by an earlier
+ * build) and traces rays against it.  Requests are admitted while their
+ * estimated device memory fits the budget beside the resident meshes (idle
+ * resident meshes are evicted oldest-use first to make room); each free lane
+ * (own stream and thread) takes every admissible waiting request at once,
+ * builds the new meshes in one segmented batch, refits the resident ones,
+ * traces all their rays in one merged queue and copies the results back, so
+ * requests that arrive while other lanes are busy run beside them on the
+ * device.  Each result equals that of the same request run alone.  Host
+ * buffers of a request must stay valid until atr_server_wait returns it. */
+typedef struct atr_server atr_server;
+
+enum { ATR_REQ_BUILD = 0, ATR_REQ_REFIT = 1 };
+
+typedef struct atr_request {
+    int kind;               /* ATR_REQ_BUILD or ATR_REQ_REFIT */
+    uint64_t mesh_id;       /* build: id to keep the mesh under; refit: resident mesh */
+    const float* vertices;  /* host, 3 float4 per triangle; refit: same count as built */
+    uint32_t num_triangles; /* build: >= 2; refit: ignored (the resident count is used) */
+    const float* rays;      /* host, 2 float4 per ray (origin+tmin, direction+tmax) */
+    uint32_t num_rays;
+    int32_t* results;       /* host, 4 int32 per ray as atr_trace (mesh-local ids) */
+    int keep_resident;      /* build: keep the BVH on the device for refits */
+} atr_request;
+
+typedef struct atr_request_result {
+    int status;             /* ATR_OK or an error code (message in `error`) */
+    float sah;              /* SAH of the collapsed tree (Ci 1.2, Ct 1) */
+    double queue_ms;        /* submit -> taken by a lane */
+    double latency_ms;      /* submit -> results in host memory */
+    uint32_t batch_requests;/* requests in the lane batch that carried it */
+    uint32_t lane;
+    char error[160];
+} atr_request_result;
+
+typedef struct atr_server_config {
+    uint64_t hbm_budget_bytes;     /* device memory the server may hold */
+    uint32_t lanes;                /* concurrent lane threads/streams (1..8) */
+    uint32_t max_batch_requests;   /* requests per lane batch */
+    uint64_t max_batch_triangles;  /* triangles per segmented build */
+    int treelet_size;              /* ATRBVH treelet size when no size-class table */
+    int iterations;                /* ATRBVH iterations when no size-class table */
+    int max_leaf;                  /* collapse leaf cap (0: none) */
+    const uint8_t* class_treelet;  /* 32 entries by floor(log2(triangles)), or NULL */
+    const uint8_t* class_iters;    /* 32 entries, or NULL */
+} atr_server_config;
+
+typedef struct atr_server_stats {
+    uint64_t completed, failed, builds, refits, evictions;
+    uint64_t triangles_built, triangles_refit, rays_traced;
+    uint64_t lane_batches;
+    uint32_t max_batch_requests_seen;
+    uint32_t max_lanes_busy;       /* most lanes that held a batch at once */
+    uint32_t resident_meshes;
+    uint64_t resident_bytes, peak_bytes;
+    double p50_ms, p99_ms, mean_ms, max_ms;
+    double overlap_fraction;       /* share of busy time with >= 2 lanes busy */
+    double busy_ms;                /* time with >= 1 lane busy */
+} atr_server_stats;
+
+int atr_server_create(int device, const atr_server_config* config, atr_server** out);
+int atr_server_submit(atr_server* server, const atr_request* request, uint64_t* ticket);
+/* Blocks until the request is done; each ticket can be waited on once. */
+int atr_server_wait(atr_server* server, uint64_t ticket, atr_request_result* result);
+/* Drop a resident mesh (its memory is freed once no lane uses it). */
+int atr_server_release(atr_server* server, uint64_t mesh_id);
+int atr_server_stats_get(atr_server* server, atr_server_stats* stats);
+/* Finishes queued work, then frees everything. */
+int atr_server_destroy(atr_server* server);
 
 /* One cosine-weighted diffuse bounce ray per primary result (the diffuse
  * workload of gpu-ray-traversal/src/rt/ray/RayGenKernels.cu:114-223 with one
