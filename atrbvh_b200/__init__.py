@@ -31,6 +31,8 @@ LIB_PATH = _HERE / "libatrbvh.so"
 ATR_OK = 0
 SCENE_UNIFORM = 0
 SCENE_CLUSTERED = 1
+TUNE_ATR_WARPS = 0
+TUNE_ATR_GROUP_MIN = 1
 
 
 class AtrError(RuntimeError):
@@ -97,6 +99,8 @@ _SIGS = [
     ("atr_ctx_get_stream", C.c_int, [_p, C.POINTER(_p)]),
     ("atr_ctx_launch_count", C.c_int, [_p, C.POINTER(C.c_uint64)]),
     ("atr_ctx_set_timing", C.c_int, [_p, C.c_int]),
+    ("atr_ctx_set_tuning", C.c_int, [_p, C.c_int, C.c_int]),
+    ("atr_ctx_get_tuning", C.c_int, [_p, C.c_int, C.POINTER(C.c_int)]),
     ("atr_ctx_phase_times", C.c_int, [_p, _f32p, C.c_int, C.POINTER(C.c_int)]),
     ("atr_ctx_phase_names", C.c_char_p, [_p]),
     ("atr_scene_create", C.c_int, [_p, _p, C.c_uint32, _f32p, _f32p, C.c_int, C.POINTER(_p)]),
@@ -250,6 +254,14 @@ class Context:
         c = C.c_uint64()
         check(lib().atr_ctx_launch_count(self.handle, C.byref(c)))
         return c.value
+
+    def set_tuning(self, knob: int, value: int) -> None:
+        check(lib().atr_ctx_set_tuning(self.handle, knob, value))
+
+    def get_tuning(self, knob: int) -> int:
+        v = C.c_int()
+        check(lib().atr_ctx_get_tuning(self.handle, knob, C.byref(v)))
+        return v.value
 
     def set_timing(self, on: bool) -> None:
         check(lib().atr_ctx_set_timing(self.handle, 1 if on else 0))

@@ -158,6 +158,35 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream) {
     return ATR_OK;
 }
 
+int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value) {
+    ATR_REQUIRE(ctx, ATR_ERR_INVALID_ARG, "atr_ctx_set_tuning: ctx is NULL");
+    switch (knob) {
+        case ATR_TUNE_ATR_WARPS:
+            ATR_REQUIRE(value == 2 || value == 4 || value == 8, ATR_ERR_INVALID_ARG,
+                        "atr_ctx_set_tuning: ATRBVH warps per block %d (2, 4 or 8)", value);
+            ctx->atr_warps = value;
+            return ATR_OK;
+        case ATR_TUNE_ATR_GROUP_MIN:
+            ATR_REQUIRE(value >= 2 && value <= 33, ATR_ERR_INVALID_ARG,
+                        "atr_ctx_set_tuning: group threshold %d outside [2, 33]", value);
+            ctx->atr_group_min = value;
+            return ATR_OK;
+        default:
+            break;
+    }
+    ATR_REQUIRE(false, ATR_ERR_INVALID_ARG, "atr_ctx_set_tuning: unknown knob %d", knob);
+}
+
+int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value) {
+    ATR_REQUIRE(ctx && value, ATR_ERR_INVALID_ARG, "atr_ctx_get_tuning: NULL argument");
+    switch (knob) {
+        case ATR_TUNE_ATR_WARPS: *value = ctx->atr_warps; return ATR_OK;
+        case ATR_TUNE_ATR_GROUP_MIN: *value = ctx->atr_group_min; return ATR_OK;
+        default: break;
+    }
+    ATR_REQUIRE(false, ATR_ERR_INVALID_ARG, "atr_ctx_get_tuning: unknown knob %d", knob);
+}
+
 int atr_ctx_set_timing(atr_ctx* ctx, int enable) {
     ATR_REQUIRE(ctx, ATR_ERR_INVALID_ARG, "atr_ctx_set_timing: ctx is NULL");
     ATR_CUDA(cudaStreamSynchronize(ctx->stream));

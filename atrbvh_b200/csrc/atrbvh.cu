@@ -4,10 +4,34 @@
 // pass, one thread per leaf; the second child to arrive processes a node; a
 // warp restructures the treelets of its lanes' nodes whose subtree holds at
 // least gamma triangles) and AgglomerativeTreeletOptimizer.cpp:73-92 (gamma
-// starts at the treelet size and doubles per iteration).  The treelet state
-// lives in registers, one treelet leaf per lane; only the distance matrix is
-// in shared memory.  Every reduction keeps the reference's shuffle-down tree
-// and strict comparisons, so ties resolve as in the reference.
+// starts at the treelet size and doubles per iteration).
+//
+// Lane groups: the reference gives every treelet a whole warp although a
+// treelet of n leaves keeps only n lanes busy.  Here a warp splits into
+// 32/G groups of G >= n lanes (G = 8, 10, 16 or 32) and, when several of its
+// lanes vote at once, restructures up to 32/G of their treelets together, one
+// per group.  Treelets processed together root disjoint subtrees (a node is
+// reached only after both of its subtrees are finished), so they touch
+// disjoint nodes and the result does not depend on the order.  A single voter
+// takes the whole warp.
+//
+// Per group, treelet formation keeps one treelet leaf per lane in registers;
+// the merge phase keeps each treelet leaf's box, nodesSah and node id in
+// shared memory (two float4 per leaf) beside the distance matrix, so a merge
+// step reads the boxes it needs directly instead of broadcasting them.
+//
+// Ties resolve as in the reference.  formTreelet's argmax (Treelet.cuh:23-39)
+// is a shuffle-down tree over the current leaves whose result on ties depends
+// on its shape, so each group replays that exact tree on its own lanes.
+// findMinimumDistance (AgglomerativeTreelet.cu:65-99) scans with lane stride 32
+// (lane l keeps the first of its minima, j = l, l+32, ...) and then reduces
+// with shuffle-down offsets 16, 8, 4, 2, 1 where the lower lane keeps ties.
+// That tournament settles ties on lane bit 0 first (even lanes win), then
+// bit 1, ..., bit 4, so it returns the minimum of the lexicographic key
+// (distance, bit-reversed lane j mod 32, j); it is evaluated here as the
+// minimum of a 64-bit key with those three fields.  Distances are surface
+// areas, never negative, so their bit patterns order like the values; entries
+// not below FLT_MAX are never chosen, as in the reference's strict comparison.
 //
 // Memory ordering: a node's data is published by the thread that finished it
 // (plain stores, fence, atomic); the second arrival fences after its atomic
@@ -21,137 +45,345 @@
 namespace atr {
 namespace {
 
-constexpr int kAtrWarps = 4;
+// Shared-memory layout of one lane group: distance matrix, then two float4
+// per treelet leaf: (min.xyz, nodesSah) and (max.xyz, node id bits).
+template <int G>
+struct GroupLayout {
+    static constexpr int kGroups = 32 / G;
+    static constexpr int kLeaves = G == 32 ? kMaxTreelet : G;
+    static constexpr int kDist = kLeaves * (kLeaves - 1) / 2;
+    static constexpr int kDistPad = (kDist + 3) & ~3;
+    static constexpr int kFloats = kDistPad + 8 * kLeaves;
+};
 
-// One treelet rooted at `root`, processed by the whole warp.
-__device__ bool process_treelet(const TreeRefs& t, int root, float root_sah, int tsize, float ci,
-                                float* dist) {
+template <int G>
+constexpr int warp_floats() {
+    return GroupLayout<G>::kFloats * GroupLayout<G>::kGroups > GroupLayout<32>::kFloats
+               ? GroupLayout<G>::kFloats * GroupLayout<G>::kGroups
+               : GroupLayout<32>::kFloats;
+}
+
+// formTreelet's argmax tree (Treelet.cuh:23-39) over m lanes -- lane i takes
+// lane i + floor(c/2) when that value is strictly larger, c halving upward --
+// returns the largest value and, among equal largest values, the lane that
+// comes first in a fixed order that depends only on m.  tree_winner replays
+// the tree on a tie pattern; argmax_priority ranks the lanes by removing
+// winners one at a time.  The full-warp path then needs two warp reductions:
+// the maximum value, then the lowest rank among the lanes holding it.
+struct ArgmaxPriority {
+    uint8_t rank[kMaxTreelet + 1][32];
+};
+
+constexpr int tree_winner(int m, uint32_t tied) {
+    int val[32] = {};
+    int idx[32] = {};
+    for (int i = 0; i < 32; ++i) {
+        val[i] = (i < m && ((tied >> i) & 1u)) ? 1 : 0;
+        idx[i] = i;
+    }
+    int c = m, sh = m / 2;
+    while (c > 1) {
+        for (int i = 0; i < c - sh; ++i)  // ascending: lane i + sh is read before it is updated
+            if (val[i + sh] > val[i]) {
+                val[i] = val[i + sh];
+                idx[i] = idx[i + sh];
+            }
+        c = (c + 1) / 2;
+        sh = c / 2;
+    }
+    return idx[0];
+}
+
+constexpr ArgmaxPriority argmax_priority() {
+    ArgmaxPriority t{};
+    for (int m = 0; m <= kMaxTreelet; ++m)
+        for (int i = 0; i < 32; ++i) t.rank[m][i] = 255;
+    for (int m = 1; m <= kMaxTreelet; ++m) {
+        uint32_t rem = m == 32 ? 0xffffffffu : ((1u << m) - 1u);
+        int k = 0;
+        while (rem) {
+            const int w = tree_winner(m, rem);
+            t.rank[m][w] = (uint8_t)k++;
+            rem &= ~(1u << w);
+        }
+    }
+    return t;
+}
+
+__device__ const ArgmaxPriority g_argmax_priority = argmax_priority();
+
+__device__ __forceinline__ float union_area3(float ax0, float ay0, float az0, float ax1, float ay1, float az1,
+                                             float bx0, float by0, float bz0, float bx1, float by1, float bz1) {
+    return sa3(__fsub_rn(fmaxf(ax1, bx1), fminf(ax0, bx0)), __fsub_rn(fmaxf(ay1, by1), fminf(ay0, by0)),
+               __fsub_rn(fmaxf(az1, bz1), fminf(az0, bz0)));
+}
+
+// One treelet per lane group.  Lanes of a group hold the same root/mesh
+// arguments; `active` is false for groups without a treelet (and for lanes
+// outside every group).  maxts is the largest treelet size of the active
+// groups of the warp: every lane runs the same number of loop trips so that
+// the shuffles stay warp-wide.  sm is this group's shared memory.
+template <int G>
+__device__ __forceinline__ void process_group(const TreeRefs& g, bool active, int nb, uint32_t n, int root,
+                                              float root_sah, int tsize, int maxts, float ci, float* sm,
+                                              const uint16_t* __restrict__ s_rc, const uint8_t* __restrict__ s_prio,
+                                              uint32_t* err) {
+    using Lay = GroupLayout<G>;
     const int lane = threadIdx.x & 31;
+    const int gb = G == 32 ? 0 : (lane / G) * G;
+    const int gl = lane - gb;
+    int32_t* const P = g.parent + nb;
+    int32_t* const Lf = g.left + nb;
+    int32_t* const Rt = g.right + nb;
+    float4* const BMN = g.bmin + nb;
+    float4* const BMX = g.bmax + nb;
+    float* const AR = g.area + nb;
+    float* const NS = g.nsah + nb;
 
-    // ---- formTreelet ----
-    int internal_node;
-    LeafSlot slot;
-    if (!form_treelet(t, root, tsize, slot, internal_node)) return false;
+    // ---- formTreelet (Treelet.cuh:57-114) ----
+    int internal_node = gl == 0 ? root : -1;
+    int s_node = -1, s_cl = -1, s_cr = -1;
+    float s_area = 0.0f, s_cal = 0.0f, s_car = 0.0f, s_sah = 0.0f;
+    float4 s_mn = make_float4(0.f, 0.f, 0.f, 0.f), s_mx = s_mn;
+    auto load = [&](int node, float area) {
+        s_node = node;
+        s_area = area;
+        s_mn = ld_cg(BMN + node);
+        s_mx = ld_cg(BMX + node);
+        s_sah = ld_cg(NS + node);
+        s_cl = s_cr = -1;
+        if (is_internal(node, n)) {
+            s_cl = ld_cg(Lf + node);
+            s_cr = ld_cg(Rt + node);
+            s_cal = ld_cg(AR + s_cl);
+            s_car = ld_cg(AR + s_cr);
+        }
+    };
+    if (active && gl < 2) {
+        const int c = gl == 0 ? ld_cg(Lf + root) : ld_cg(Rt + root);
+        load(c, ld_cg(AR + c));
+    }
+    bool ok = true;
+    for (int it = 0; it < maxts - 2; ++it) {
+        const bool act = active && ok && it < tsize - 2;
+        const int m = 2 + it;
+        int largest;
+        if constexpr (G == 32) {
+            // Largest value (internal nodes' areas as bits + 1, which order like
+            // the areas; other leaves 0, the reference's -FLT_MAX), then the
+            // first lane in the tree's tie order.
+            const uint32_t ev = (gl < m && is_internal(s_node, n)) ? __float_as_uint(s_area) + 1u : 0u;
+            const uint32_t vmax = __reduce_max_sync(kFull, ev);
+            const uint32_t pk = (gl < m && ev == vmax) ? (uint32_t)s_prio[m * 32 + gl] : 255u;
+            const uint32_t pmin = __reduce_min_sync(kFull, pk);
+            largest = __ffs(__ballot_sync(kFull, pk == pmin)) - 1;
+        } else {
+            float v = (gl < m && is_internal(s_node, n)) ? s_area : -FLT_MAX;
+            int ix = gl;
+            int c = m, sh = m >> 1;
+            while (c > 1) {
+                const float ov = __shfl_sync(kFull, v, lane + sh);
+                const int oi = __shfl_sync(kFull, ix, lane + sh);
+                if (gl < c - sh && ov > v) { v = ov; ix = oi; }
+                c = (c + 1) >> 1;
+                sh = c >> 1;
+            }
+            largest = __shfl_sync(kFull, ix, gb);
+        }
+        const int src = gb + largest;
+        const int rep = __shfl_sync(kFull, s_node, src);
+        const int cl = __shfl_sync(kFull, s_cl, src);
+        const int cr = __shfl_sync(kFull, s_cr, src);
+        const float al = __shfl_sync(kFull, s_cal, src);
+        const float ar = __shfl_sync(kFull, s_car, src);
+        if (act) {
+            if (!is_internal(rep, n)) {
+                ok = false;
+            } else {
+                if (gl == it + 1) internal_node = rep;
+                if (gl == largest || gl == it + 2) {
+                    const bool isl = gl == largest;
+                    load(isl ? cl : cr, isl ? al : ar);
+                }
+            }
+        }
+    }
+    const bool run = active && ok;
+    if (active && !ok && gl == 0) set_error_bits(err, kErrTreeletClimb);
 
-    // ---- agglomerative merge (AgglomerativeTreelet.cu:476-532) ----
-    Box box;
-    box.mnx = slot.mn.x; box.mny = slot.mn.y; box.mnz = slot.mn.z;
-    box.mxx = slot.mx.x; box.mxy = slot.mx.y; box.mxz = slot.mx.z;
-    int node = slot.node;
-    float sah = slot.sah;
-    int right_node = -1;  // treeletLeaves[lane] after the merge that fills this lane
-    float la = 0.0f;      // treeletLeavesAreas[lane]
-
-    const int npairs = tsize * (tsize - 1) / 2;
-    for (int base = 0; base < npairs; base += 32) {
-        const int j = base + lane;
-        int r = 0, c = 0;
-        if (j < npairs) trm_rc(j, r, c);
-        const Box a = shfl_box(box, r);
-        const Box b = shfl_box(box, c);
-        if (j < npairs) dist[j] = union_area(a, b);
+    // ---- distance matrix (AgglomerativeTreelet.cu:18-63) ----
+    float* const dist = sm;
+    float4* const lmn = reinterpret_cast<float4*>(sm + Lay::kDistPad);
+    float4* const lmx = lmn + Lay::kLeaves;
+    if (run && gl < tsize) {
+        lmn[gl] = make_float4(s_mn.x, s_mn.y, s_mn.z, s_sah);
+        lmx[gl] = make_float4(s_mx.x, s_mx.y, s_mx.z, __int_as_float(s_node));
+    }
+    __syncwarp();
+    if (run) {
+        const int np = tsize * (tsize - 1) / 2;
+        for (int j = gl; j < np; j += G) {
+            const uint32_t rc = s_rc[j];
+            const float4 a0 = lmn[rc >> 8], a1 = lmx[rc >> 8], b0 = lmn[rc & 255u], b1 = lmx[rc & 255u];
+            dist[j] = union_area3(a0.x, a0.y, a0.z, a1.x, a1.y, a1.z, b0.x, b0.y, b0.z, b1.x, b1.y, b1.z);
+        }
     }
     __syncwarp();
 
-    for (int last = tsize - 1; last > 0; --last) {
-        // findMinimumDistance (:83-99): strided scan, strict <, shuffle-down reduce.
-        const int msize = last * (last + 1) / 2;
-        float best = FLT_MAX;
-        int bi = 0;
-        for (int j = lane; j < msize; j += 32) {
-            const float d = dist[j];
-            if (d < best) { best = d; bi = j; }
-        }
+    // ---- agglomerative merge (AgglomerativeTreelet.cu:476-532) ----
+    float my0x = s_mn.x, my0y = s_mn.y, my0z = s_mn.z, my1x = s_mx.x, my1y = s_mx.y, my1z = s_mx.z;
+    int fin_l = -1, fin_r = -1;
+    float fin_la = 0.0f;
+    float f0x = 0.f, f0y = 0.f, f0z = 0.f, f1x = 0.f, f1y = 0.f, f1z = 0.f;
+    for (int step = 0; step < maxts - 1; ++step) {
+        const int last = tsize - 1 - step;
+        const bool act = run && last >= 1;
+        // findMinimumDistance (:83-99) as the minimum of (distance, brev5(j mod 32), j).
+        int mi;
+        if constexpr (G == 32) {
+            // Lane l scans j = l, l + 32, ...; then the minimum distance, then
+            // the lowest (brev5(l), j) among the lanes holding it.
+            float bd = FLT_MAX;
+            int bj = -1;
+            if (act) {
+                const int msize = last * (last + 1) / 2;
+                for (int j = lane; j < msize; j += 32) {
+                    const float d = dist[j];
+                    if (d < bd) { bd = d; bj = j; }
+                }
+            }
+            const uint32_t db = bj >= 0 ? __float_as_uint(bd) : 0xffffffffu;
+            const uint32_t dmin = __reduce_min_sync(kFull, db);
+            const uint32_t tk = (bj >= 0 && db == dmin) ? (((__brev((uint32_t)lane) >> 27) << 8) | (uint32_t)bj)
+                                                        : 0xffffffffu;
+            const uint32_t kmin = __reduce_min_sync(kFull, tk);
+            mi = dmin == 0xffffffffu ? 0 : (int)(kmin & 255u);
+        } else {
+            unsigned long long best = ~0ull;
+            if (act) {
+                const int msize = last * (last + 1) / 2;
+                for (int j = gl; j < msize; j += G) {
+                    const float d = dist[j];
+                    if (d < FLT_MAX) {
+                        const unsigned long long k = ((unsigned long long)__float_as_uint(d) << 32) |
+                                                     (uint32_t)(((__brev((uint32_t)j) >> 27) << 8) | (uint32_t)j);
+                        best = k < best ? k : best;
+                    }
+                }
+            }
+            if ((G & (G - 1)) == 0) {
 #pragma unroll
-        for (int sh = 16; sh > 0; sh >>= 1) {
-            const float ob = __shfl_down_sync(kFull, best, sh);
-            const int oi = __shfl_down_sync(kFull, bi, sh);
-            if (ob < best) { best = ob; bi = oi; }
+                for (int o = G >> 1; o > 0; o >>= 1) {
+                    const unsigned long long ob = __shfl_xor_sync(kFull, best, o);
+                    best = ob < best ? ob : best;
+                }
+            } else {
+                int c = G, sh = G >> 1;
+                while (c > 1) {
+                    const unsigned long long ob = __shfl_sync(kFull, best, lane + sh);
+                    if (gl < c - sh && ob < best) best = ob;
+                    c = (c + 1) >> 1;
+                    sh = c >> 1;
+                }
+                best = __shfl_sync(kFull, best, gb);
+            }
+            mi = best == ~0ull ? 0 : (int)(best & 255u);
         }
-        const int mi = __shfl_sync(kFull, bi, 0);
-        int jr, jc;
-        trm_rc(mi, jr, jc);
-
-        // updateState (:101-150).
-        const float sah_new = __fadd_rn(__shfl_sync(kFull, sah, jr), __shfl_sync(kFull, sah, jc));
-        const int left_index = __shfl_sync(kFull, node, jr);
-        const int right_index = __shfl_sync(kFull, node, jc);
-        const Box bjr = shfl_box(box, jr);
-        const Box bjc = shfl_box(box, jc);
-        Box A;
-        A.mnx = fminf(bjc.mnx, bjr.mnx); A.mny = fminf(bjc.mny, bjr.mny); A.mnz = fminf(bjc.mnz, bjr.mnz);
-        A.mxx = fmaxf(bjc.mxx, bjr.mxx); A.mxy = fmaxf(bjc.mxy, bjr.mxy); A.mxz = fmaxf(bjc.mxz, bjr.mxz);
-        const int new_internal = __shfl_sync(kFull, internal_node, last - 1);
-        const float la_new = __fadd_rn(sah_new, __fmul_rn(ci, box_area(A.mnx, A.mny, A.mnz, A.mxx, A.mxy, A.mxz)));
-        if (lane == jc) {
-            node = new_internal;
-            box = A;
-            sah = la_new;
+        const int new_internal = __shfl_sync(kFull, internal_node, gb + (last >= 1 ? last - 1 : 0));
+        // updateState (:101-150): the new node (union of rows jr and jc) takes
+        // slot jc, the last leaf moves to slot jr, and lane `last` records the
+        // new node for the final rewrite.
+        int jr = 0, jc = 0;
+        float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f, la_new = 0.f;
+        float4 z0 = make_float4(0.f, 0.f, 0.f, 0.f), z1 = z0;
+        int li = -1, ri = -1;
+        if (act) {
+            const uint32_t rc = s_rc[mi];
+            jr = (int)(rc >> 8);
+            jc = (int)(rc & 255u);
+            const float4 r0 = lmn[jr], r1 = lmx[jr], c0 = lmn[jc], c1 = lmx[jc];
+            z0 = lmn[last];
+            z1 = lmx[last];
+            a0x = fminf(c0.x, r0.x); a0y = fminf(c0.y, r0.y); a0z = fminf(c0.z, r0.z);
+            a1x = fmaxf(c1.x, r1.x); a1y = fmaxf(c1.y, r1.y); a1z = fmaxf(c1.z, r1.z);
+            la_new = __fadd_rn(__fadd_rn(r0.w, c0.w), __fmul_rn(ci, box_area(a0x, a0y, a0z, a1x, a1y, a1z)));
+            li = __float_as_int(r1.w);
+            ri = __float_as_int(c1.w);
         }
-        if (lane == last) la = la_new;
-        const int last_index = __shfl_sync(kFull, node, last);
-        const float sah_last = __shfl_sync(kFull, sah, last);
-        const Box blast = shfl_box(box, last);
-        if (lane == jr) {
-            node = last_index;
-            sah = sah_last;
-            box = blast;
+        __syncwarp();
+        if (act) {
+            if (gl == jc) {
+                lmn[jc] = make_float4(a0x, a0y, a0z, la_new);
+                lmx[jc] = make_float4(a1x, a1y, a1z, __int_as_float(new_internal));
+                my0x = a0x; my0y = a0y; my0z = a0z; my1x = a1x; my1y = a1y; my1z = a1z;
+            }
+            if (gl == jr) {
+                lmn[jr] = z0;
+                lmx[jr] = z1;
+                my0x = z0.x; my0y = z0.y; my0z = z0.z; my1x = z1.x; my1y = z1.y; my1z = z1.z;
+            }
+            if (gl == last) {
+                fin_l = li;
+                fin_r = ri;
+                fin_la = la_new;
+                f0x = a0x; f0y = a0y; f0z = a0z; f1x = a1x; f1y = a1y; f1z = a1z;
+            }
         }
-        if (lane == last) {
-            node = left_index;
-            right_node = right_index;
-            box = A;
-        }
-
-        // updateDistancesMatrix (:152-188).
-        if (last > 1) {
-            float moved = 0.0f;
-            const bool mv = lane < last && lane != jr;
-            if (mv) moved = dist[trm_idx(last, lane)];
-            __syncwarp();
-            if (mv) dist[trm_idx(max(jr, lane), min(jr, lane))] = moved;
-            __syncwarp();
-            int r = lane, c = lane;
-            const bool up = lane < last && lane != jc;
-            if (up) { r = max(jc, lane); c = min(jc, lane); }
-            const Box br = shfl_box(box, r);
-            const Box bc = shfl_box(box, c);
-            const float d = union_area(br, bc);
-            if (up) dist[trm_idx(r, c)] = d;
-            __syncwarp();
-        }
+        // updateDistancesMatrix (:152-188): row `last` moves to row jr, then the
+        // distances to the new node at jc are recomputed.
+        const bool du = act && last > 1;
+        const bool mv = du && gl < last && gl != jr;
+        float moved = 0.0f;
+        if (mv) moved = dist[trm_idx(last, gl)];
+        __syncwarp();
+        if (mv) dist[trm_idx(max(jr, gl), min(jr, gl))] = moved;
+        __syncwarp();
+        if (du && gl < last && gl != jc)
+            dist[trm_idx(max(jc, gl), min(jc, gl))] =
+                union_area3(a0x, a0y, a0z, a1x, a1y, a1z, my0x, my0y, my0z, my1x, my1y, my1z);
+        __syncwarp();
     }
 
     // ---- updateTreelet (:190-212) ----
-    const float la1 = __shfl_sync(kFull, la, 1);
-    const int ni = __shfl_sync(kFull, internal_node, lane > 0 ? lane - 1 : 0);
-    if (la1 < root_sah && lane >= 1 && lane < tsize) {
-        t.left[ni] = node;
-        t.right[ni] = right_node;
-        t.parent[node] = ni;
-        t.parent[right_node] = ni;
-        t.nsah[ni] = la;
-        const float4 mn = make_float4(box.mnx, box.mny, box.mnz, 0.0f);
-        const float4 mx = make_float4(box.mxx, box.mxy, box.mxz, 0.0f);
-        t.bmin[ni] = mn;
-        t.bmax[ni] = mx;
-        t.area[ni] = box_area(mn, mx);
+    const float la1 = __shfl_sync(kFull, fin_la, gb + 1);
+    const int ni = __shfl_sync(kFull, internal_node, gb + (gl > 0 ? gl - 1 : 0));
+    if (run && la1 < root_sah && gl >= 1 && gl < tsize) {
+        Lf[ni] = fin_l;
+        Rt[ni] = fin_r;
+        P[fin_l] = ni;
+        P[fin_r] = ni;
+        NS[ni] = fin_la;
+        const float4 mn = make_float4(f0x, f0y, f0z, 0.0f);
+        const float4 mx = make_float4(f1x, f1y, f1z, 0.0f);
+        BMN[ni] = mn;
+        BMX[ni] = mx;
+        AR[ni] = box_area(mn, mx);
     }
     __syncwarp();
-    return true;
 }
 
 // One iteration over every mesh of `segs`: thread i starts at the i-th sorted
 // leaf of the batch.  Each mesh has its own treelet size and iteration count
 // when `seg_tsize`/`seg_iters` are given; a mesh whose iterations are done
-// sits this launch out.  Treelets are processed with the refs of the mesh of
-// the lane that owns the root.
-__global__ void __launch_bounds__(kAtrWarps * 32) k_atrbvh(TreeRefs g, Segs segs, int32_t* __restrict__ subtree,
-                                                           uint32_t* __restrict__ counters, int tsize_all,
-                                                           const uint8_t* __restrict__ seg_tsize,
-                                                           const uint8_t* __restrict__ seg_iters, int iteration,
-                                                           float ci, float ct, uint32_t* err) {
-    __shared__ float s_dist[kAtrWarps][kMaxDist];
+// sits this launch out.
+template <int G, int W>
+__global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs, int32_t* __restrict__ subtree,
+                                                   uint32_t* __restrict__ counters, int tsize_all,
+                                                   const uint8_t* __restrict__ seg_tsize,
+                                                   const uint8_t* __restrict__ seg_iters, int iteration, float ci,
+                                                   float ct, int group_min, uint32_t* err) {
+    constexpr int kWarpFloats = warp_floats<G>();
+    __shared__ __align__(16) float s_mem[W][kWarpFloats];
+    __shared__ uint16_t s_rc[kMaxDist];
+    __shared__ __align__(4) uint8_t s_prio[(kMaxTreelet + 1) * 32];
+    for (int k = threadIdx.x; k < kMaxDist; k += blockDim.x) {
+        int r, c;
+        trm_rc(k, r, c);
+        s_rc[k] = (uint16_t)((r << 8) | c);
+    }
+    for (int k = threadIdx.x; k < (kMaxTreelet + 1) * 8; k += blockDim.x)
+        reinterpret_cast<uint32_t*>(s_prio)[k] = reinterpret_cast<const uint32_t*>(&g_argmax_priority.rank[0][0])[k];
+    __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int cur = -1, base = 0, cbase = 0, tsize = tsize_all;
@@ -192,27 +424,63 @@ __global__ void __launch_bounds__(kAtrWarps * 32) k_atrbvh(TreeRefs g, Segs segs
         unsigned vote = __ballot_sync(kFull, cnt >= gamma);
         if (vote) __syncwarp();
         while (vote) {
-            const int rl = __ffs(vote) - 1;
-            const int root = __shfl_sync(kFull, cur, rl);
-            const float rsah = __shfl_sync(kFull, my_sah, rl);
-            const int rbase = __shfl_sync(kFull, base, rl);
-            const uint32_t rn = __shfl_sync(kFull, nm, rl);
-            const int rts = __shfl_sync(kFull, tsize, rl);
-            if (!process_treelet(rebase(g, rbase, rn), root, rsah, rts, ci, s_dist[w]) && lane == 0)
-                set_error_bits(err, kErrTreeletClimb);
-            vote &= vote - 1;
+            if (G < 32 && __popc(vote) >= group_min) {
+                constexpr int NG = GroupLayout<G>::kGroups;
+                const int grp = lane / G;
+                unsigned v = vote;
+                for (int k = 0; k < grp && v; ++k) v &= v - 1;
+                const bool has = grp < NG && v != 0;
+                const int rl = has ? __ffs(v) - 1 : 0;
+                const int root = __shfl_sync(kFull, cur, rl);
+                const float rsah = __shfl_sync(kFull, my_sah, rl);
+                const int rbase = __shfl_sync(kFull, base, rl);
+                const uint32_t rn = __shfl_sync(kFull, nm, rl);
+                const int rts = __shfl_sync(kFull, tsize, rl);
+                const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)rts : 0u);
+                process_group<G>(g, has, rbase, rn, root, rsah, rts, maxts, ci,
+                                 &s_mem[w][0] + (grp < NG ? grp : NG - 1) * GroupLayout<G>::kFloats, s_rc, s_prio, err);
+#pragma unroll
+                for (int k = 0; k < NG; ++k) vote &= vote - 1;
+            } else {
+                const int rl = __ffs(vote) - 1;
+                const int root = __shfl_sync(kFull, cur, rl);
+                const float rsah = __shfl_sync(kFull, my_sah, rl);
+                const int rbase = __shfl_sync(kFull, base, rl);
+                const uint32_t rn = __shfl_sync(kFull, nm, rl);
+                const int rts = __shfl_sync(kFull, tsize, rl);
+                process_group<32>(g, true, rbase, rn, root, rsah, rts, rts, ci, &s_mem[w][0], s_rc, s_prio, err);
+                vote &= vote - 1;
+            }
         }
         if (cur >= 0) cur = ld_cg(g.parent + base + cur);
     }
 }
 
+template <int G>
+cudaError_t launch_atrbvh_g(int warps, uint32_t blocks, cudaStream_t s, const TreeRefs& g, const Segs& segs,
+                            int32_t* subtree, uint32_t* counters, int tsize, const uint8_t* seg_tsize,
+                            const uint8_t* seg_iters, int it, float ci, float ct, int gmin, uint32_t* err) {
+    switch (warps) {
+        case 2: k_atrbvh<G, 2><<<blocks, 64, 0, s>>>(g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
+        case 8: k_atrbvh<G, 8><<<blocks, 256, 0, s>>>(g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
+        default: k_atrbvh<G, 4><<<blocks, 128, 0, s>>>(g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+// Lane-group width for treelets of at most max_tsize leaves.
+int atrbvh_group_width(int max_tsize) {
+    return max_tsize <= 8 ? 8 : max_tsize <= 10 ? 10 : max_tsize <= 16 ? 16 : 32;
+}
 
 // ATRBVH over every mesh of `segs` (total_nodes = sum of 2n_m - 1).  tsize and
 // iterations apply to all meshes unless per-mesh arrays are given, in which
-// case `iterations` is their maximum.
+// case `iterations` is their maximum and max_tsize the largest per-mesh size.
 int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t total_nodes, int tsize,
-               int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci, float ct) {
+               int max_tsize, int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci,
+               float ct) {
     if (iterations <= 0) return ATR_OK;
     const size_t inner = segs.n - segs.count;
     void* scratch = nullptr;
@@ -223,17 +491,25 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     TreeRefs g = g_in;
     g.nsah = reinterpret_cast<float*>(p + b_sub);
     uint32_t* counters = reinterpret_cast<uint32_t*>(p + b_sub + b_sah);
-    const int threads = kAtrWarps * 32;
+    const int warps = ctx->atr_warps == 2 || ctx->atr_warps == 8 ? ctx->atr_warps : 4;
+    const int threads = warps * 32;
     const uint32_t blocks = (segs.n + threads - 1) / threads;
+    const int gw = atrbvh_group_width(seg_tsize ? max_tsize : tsize);
+    const int gmin = ctx->atr_group_min < 2 ? 2 : ctx->atr_group_min;
+    cudaError_t e = cudaSuccess;
     ctx->phase_begin("atrbvh");
-    for (int it = 0; it < iterations; ++it) {
-        cudaMemsetAsync(counters, 0, inner * 4, ctx->stream);
-        k_atrbvh<<<blocks, threads, 0, ctx->stream>>>(g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it,
-                                                      ci, ct, ctx->d_error);
+    for (int it = 0; it < iterations && e == cudaSuccess; ++it) {
+        e = cudaMemsetAsync(counters, 0, inner * 4, ctx->stream);
+        if (e != cudaSuccess) break;
+        switch (gw) {
+            case 8: e = launch_atrbvh_g<8>(warps, blocks, ctx->stream, g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
+            case 10: e = launch_atrbvh_g<10>(warps, blocks, ctx->stream, g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
+            case 16: e = launch_atrbvh_g<16>(warps, blocks, ctx->stream, g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
+            default: e = launch_atrbvh_g<32>(warps, blocks, ctx->stream, g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
+        }
+        ++ctx->launches;
     }
     ctx->phase_end();
-    ctx->launches += iterations;
-    cudaError_t e = cudaGetLastError();
     ctx->release(scratch);
     if (e != cudaSuccess) return cuda_fail(e, "k_atrbvh launch", __FILE__, __LINE__);
     return ATR_OK;
@@ -252,5 +528,5 @@ extern "C" int atr_optimize_atrbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int 
     const uint32_t n = tree->n;
     TreeRefs g{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nullptr};
     Segs segs{nullptr, nullptr, 1u, n};
-    return atrbvh_run(ctx, g, segs, 2 * (size_t)n - 1, tsize, iterations, nullptr, nullptr, ci, ct);
+    return atrbvh_run(ctx, g, segs, 2 * (size_t)n - 1, tsize, tsize, iterations, nullptr, nullptr, ci, ct);
 }

@@ -32,6 +32,7 @@ struct atr_batch {
     uint8_t* d_iters = nullptr;
     bool per_mesh_params = false;
     int max_iters = 0;
+    int max_tsize = 0;
     float* d_bounds = nullptr;
     float4* verts = nullptr;
     void* block = nullptr;
@@ -115,7 +116,9 @@ int batch_run(atr_ctx* ctx, atr_batch* b, int optimizer, int tsize, int iteratio
     const uint8_t* ts = b->per_mesh_params ? b->d_tsize : nullptr;
     const uint8_t* it = b->per_mesh_params ? b->d_iters : nullptr;
     const int iters = b->per_mesh_params ? b->max_iters : iterations;
-    if (optimizer == 1) return atrbvh_run(ctx, g, segs, b->total_nodes, tsize, iters, ts, it, ci, ct);
+    if (optimizer == 1)
+        return atrbvh_run(ctx, g, segs, b->total_nodes, tsize, b->per_mesh_params ? b->max_tsize : tsize, iters, ts, it,
+                          ci, ct);
     if (optimizer == 2) return trbvh_run(ctx, g, segs, b->total_nodes, iters, it, ci, ct);
     return ATR_OK;
 }
@@ -209,18 +212,20 @@ int atr_batch_set_params(atr_ctx* ctx, atr_batch* b, const uint8_t* treelet_size
         return ATR_OK;
     }
     ATR_REQUIRE(treelet_sizes && iterations, ATR_ERR_INVALID_ARG, "atr_batch_set_params: give both arrays");
-    int mx = 0;
+    int mx = 0, mts = 0;
     for (uint32_t m = 0; m < b->count; ++m) {
         ATR_REQUIRE(treelet_sizes[m] >= 3 && treelet_sizes[m] <= 20, ATR_ERR_UNSUPPORTED,
                     "atr_batch_set_params: treelet size %d of mesh %u", treelet_sizes[m], m);
         ATR_REQUIRE(iterations[m] <= 24, ATR_ERR_INVALID_ARG, "atr_batch_set_params: iterations %d", iterations[m]);
         mx = std::max(mx, (int)iterations[m]);
+        mts = std::max(mts, (int)treelet_sizes[m]);
     }
     ATR_CUDA(cudaMemcpyAsync(b->d_tsize, treelet_sizes, b->count, cudaMemcpyHostToDevice, ctx->stream));
     ATR_CUDA(cudaMemcpyAsync(b->d_iters, iterations, b->count, cudaMemcpyHostToDevice, ctx->stream));
     ATR_CUDA(cudaStreamSynchronize(ctx->stream));
     b->per_mesh_params = true;
     b->max_iters = mx;
+    b->max_tsize = mts;
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
     return ATR_OK;
 }

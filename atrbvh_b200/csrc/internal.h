@@ -59,6 +59,11 @@ struct atr_ctx {
     uint32_t* d_error = nullptr;  // device error bits
     uint64_t launches = 0;        // kernels enqueued by this context
     bool timing = false;
+    // Launch tuning (atr_ctx_set_tuning): ATRBVH warps per block (2, 4, 8);
+    // fewest simultaneous treelet roots in a warp that are restructured in
+    // lane groups (33: never; a single root always takes the whole warp).
+    int atr_warps = 4;
+    int atr_group_min = 2;
     struct Phase {
         std::string name;
         cudaEvent_t a, b;
@@ -163,7 +168,9 @@ int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4
                     const float* d_bounds, int morton_bits, const TreeOut& out, void** keep_keys,
                     uint32_t** keep_idx);
 int atrbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int tsize,
-               int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci, float ct);
+               int max_tsize, int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci,
+               float ct);
+int atrbvh_group_width(int max_tsize);
 int trbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int iterations,
               const uint8_t* seg_iters, float ci, float ct);
 

@@ -101,6 +101,16 @@ int atr_ctx_create(int device, void* stream, atr_ctx** out);
 int atr_ctx_destroy(atr_ctx* ctx);
 int atr_ctx_synchronize(atr_ctx* ctx); /* also reports device-side errors */
 int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
+/* Launch tuning of this context's kernels (no counterpart in the reference,
+ * whose launch shapes are fixed: AgglomerativeTreelet.cu:556-595).  Results
+ * do not depend on the tuning; only speed does.
+ *   ATR_TUNE_ATR_WARPS      ATRBVH warps per block: 2, 4 (default) or 8.
+ *   ATR_TUNE_ATR_GROUP_MIN  fewest treelet roots reached by one warp at once
+ *                           that are restructured side by side in lane groups
+ *                           (2..32; 33 = never; default 2). */
+enum atr_tune_knob { ATR_TUNE_ATR_WARPS = 0, ATR_TUNE_ATR_GROUP_MIN = 1 };
+int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value);
+int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value);
 /* Number of kernels this context has enqueued since it was created. */
 int atr_ctx_launch_count(atr_ctx* ctx, uint64_t* count);
 /* Per-phase CUDA-event timing of the next builds (milliseconds). */
