@@ -125,7 +125,7 @@ __device__ __forceinline__ float union_area3(float ax0, float ay0, float az0, fl
 // the shuffles stay warp-wide.  sm is this group's shared memory.
 template <int G>
 __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, int nb, uint32_t n, int root,
-                                              float root_sah, int tsize, int maxts, float ci, float* sm,
+                                              int4* KD, float root_sah, int tsize, int maxts, float ci, float* sm,
                                               const uint16_t* __restrict__ s_rc, const uint8_t* __restrict__ s_prio,
                                               uint32_t* err) {
     using Lay = GroupLayout<G>;
@@ -153,15 +153,16 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
         s_sah = ld_cg(NS + node);
         s_cl = s_cr = -1;
         if (is_internal(node, n)) {
-            s_cl = ld_cg(Lf + node);
-            s_cr = ld_cg(Rt + node);
-            s_cal = ld_cg(AR + s_cl);
-            s_car = ld_cg(AR + s_cr);
+            const int4 k = __ldcg(KD + node);
+            s_cl = k.x;
+            s_cr = k.y;
+            s_cal = __int_as_float(k.z);
+            s_car = __int_as_float(k.w);
         }
     };
     if (active && gl < 2) {
-        const int c = gl == 0 ? ld_cg(Lf + root) : ld_cg(Rt + root);
-        load(c, ld_cg(AR + c));
+        const int4 k = __ldcg(KD + root);
+        load(gl == 0 ? k.x : k.y, __int_as_float(gl == 0 ? k.z : k.w));
     }
     bool ok = true;
     for (int it = 0; it < maxts - 2; ++it) {
@@ -347,7 +348,8 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     // ---- updateTreelet (:190-212) ----
     const float la1 = __shfl_sync(kFull, fin_la, gb + 1);
     const int ni = __shfl_sync(kFull, internal_node, gb + (gl > 0 ? gl - 1 : 0));
-    if (run && la1 < root_sah && gl >= 1 && gl < tsize) {
+    const bool wr = run && la1 < root_sah && gl >= 1 && gl < tsize;
+    if (wr) {
         Lf[ni] = fin_l;
         Rt[ni] = fin_r;
         P[fin_l] = ni;
@@ -360,6 +362,9 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
         AR[ni] = box_area(mn, mx);
     }
     __syncwarp();
+    // The rewritten nodes' child records, once every new area is stored.
+    if (wr) KD[ni] = make_int4(fin_l, fin_r, __float_as_int(__ldcg(AR + fin_l)), __float_as_int(__ldcg(AR + fin_r)));
+    __syncwarp();
 }
 
 // One iteration over every mesh of `segs`: thread i starts at the i-th sorted
@@ -368,7 +373,8 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
 // sits this launch out.
 template <int G, int W>
 __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs, int32_t* __restrict__ subtree,
-                                                   uint32_t* __restrict__ counters, int tsize_all,
+                                                   uint32_t* __restrict__ counters, int4* __restrict__ kids,
+                                                   int tsize_all,
                                                    const uint8_t* __restrict__ seg_tsize,
                                                    const uint8_t* __restrict__ seg_iters, int iteration, float ci,
                                                    float ct, int group_min, uint32_t* err) {
@@ -406,20 +412,24 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
     while (__any_sync(kFull, cur >= 0)) {
         bool second = false;
         if (cur >= 0) {
-            __threadfence();
+            fence_acq_rel_gpu();
             if (atomicAdd(&counters[cbase + cur], 1u) == 0u) cur = -1;
-            else { second = true; __threadfence(); }
+            else { second = true; fence_acq_rel_gpu(); }
         }
         int cnt = 0;
         float my_sah = 0.0f;
         if (second) {
             const int x = base + cur;
-            const int l = base + ld_cg(g.left + x), r = base + ld_cg(g.right + x);
+            const int lc = ld_cg(g.left + x), rc = ld_cg(g.right + x);
+            const int l = base + lc, r = base + rc;
             const float a = ld_cg(g.area + x);
             cnt = ld_cg(subtree + l) + ld_cg(subtree + r);
             my_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), ld_cg(g.nsah + l)), ld_cg(g.nsah + r));
             subtree[x] = cnt;
             g.nsah[x] = my_sah;
+            // Child record for treelet formation: one load yields both
+            // children and their areas.
+            kids[cbase + cur] = make_int4(lc, rc, __float_as_int(ld_cg(g.area + l)), __float_as_int(ld_cg(g.area + r)));
         }
         unsigned vote = __ballot_sync(kFull, cnt >= gamma);
         if (vote) __syncwarp();
@@ -434,10 +444,11 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                 const int root = __shfl_sync(kFull, cur, rl);
                 const float rsah = __shfl_sync(kFull, my_sah, rl);
                 const int rbase = __shfl_sync(kFull, base, rl);
+                const int rcb = __shfl_sync(kFull, cbase, rl);
                 const uint32_t rn = __shfl_sync(kFull, nm, rl);
                 const int rts = __shfl_sync(kFull, tsize, rl);
                 const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)rts : 0u);
-                process_group<G>(g, has, rbase, rn, root, rsah, rts, maxts, ci,
+                process_group<G>(g, has, rbase, rn, root, kids + rcb, rsah, rts, maxts, ci,
                                  &s_mem[w][0] + (grp < NG ? grp : NG - 1) * GroupLayout<G>::kFloats, s_rc, s_prio, err);
 #pragma unroll
                 for (int k = 0; k < NG; ++k) vote &= vote - 1;
@@ -446,9 +457,11 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                 const int root = __shfl_sync(kFull, cur, rl);
                 const float rsah = __shfl_sync(kFull, my_sah, rl);
                 const int rbase = __shfl_sync(kFull, base, rl);
+                const int rcb = __shfl_sync(kFull, cbase, rl);
                 const uint32_t rn = __shfl_sync(kFull, nm, rl);
                 const int rts = __shfl_sync(kFull, tsize, rl);
-                process_group<32>(g, true, rbase, rn, root, rsah, rts, rts, ci, &s_mem[w][0], s_rc, s_prio, err);
+                process_group<32>(g, true, rbase, rn, root, kids + rcb, rsah, rts, rts, ci, &s_mem[w][0], s_rc, s_prio,
+                                  err);
                 vote &= vote - 1;
             }
         }
@@ -458,12 +471,12 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
 
 template <int G>
 cudaError_t launch_atrbvh_g(int warps, uint32_t blocks, cudaStream_t s, const TreeRefs& g, const Segs& segs,
-                            int32_t* subtree, uint32_t* counters, int tsize, const uint8_t* seg_tsize,
+                            int32_t* subtree, uint32_t* counters, int4* kids, int tsize, const uint8_t* seg_tsize,
                             const uint8_t* seg_iters, int it, float ci, float ct, int gmin, uint32_t* err) {
     switch (warps) {
-        case 2: k_atrbvh<G, 2><<<blocks, 64, 0, s>>>(g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
-        case 8: k_atrbvh<G, 8><<<blocks, 256, 0, s>>>(g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
-        default: k_atrbvh<G, 4><<<blocks, 128, 0, s>>>(g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
+        case 2: k_atrbvh<G, 2><<<blocks, 64, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
+        case 8: k_atrbvh<G, 8><<<blocks, 256, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
+        default: k_atrbvh<G, 4><<<blocks, 128, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
     }
     return cudaGetLastError();
 }
@@ -485,12 +498,14 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     const size_t inner = segs.n - segs.count;
     void* scratch = nullptr;
     const size_t b_sub = align256(total_nodes * 4), b_sah = align256(total_nodes * 4), b_ctr = align256(inner * 4);
-    ATR_TRY(ctx->alloc(&scratch, b_sub + b_sah + b_ctr));
+    const size_t b_kid = align256(inner * 16);
+    ATR_TRY(ctx->alloc(&scratch, b_sub + b_sah + b_ctr + b_kid));
     char* p = static_cast<char*>(scratch);
     int32_t* subtree = reinterpret_cast<int32_t*>(p);
     TreeRefs g = g_in;
     g.nsah = reinterpret_cast<float*>(p + b_sub);
     uint32_t* counters = reinterpret_cast<uint32_t*>(p + b_sub + b_sah);
+    int4* kids = reinterpret_cast<int4*>(p + b_sub + b_sah + b_ctr);
     const int warps = ctx->atr_warps == 2 || ctx->atr_warps == 8 ? ctx->atr_warps : 4;
     const int threads = warps * 32;
     const uint32_t blocks = (segs.n + threads - 1) / threads;
@@ -502,10 +517,10 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         e = cudaMemsetAsync(counters, 0, inner * 4, ctx->stream);
         if (e != cudaSuccess) break;
         switch (gw) {
-            case 8: e = launch_atrbvh_g<8>(warps, blocks, ctx->stream, g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
-            case 10: e = launch_atrbvh_g<10>(warps, blocks, ctx->stream, g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
-            case 16: e = launch_atrbvh_g<16>(warps, blocks, ctx->stream, g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
-            default: e = launch_atrbvh_g<32>(warps, blocks, ctx->stream, g, segs, subtree, counters, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
+            case 8: e = launch_atrbvh_g<8>(warps, blocks, ctx->stream, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
+            case 10: e = launch_atrbvh_g<10>(warps, blocks, ctx->stream, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
+            case 16: e = launch_atrbvh_g<16>(warps, blocks, ctx->stream, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
+            default: e = launch_atrbvh_g<32>(warps, blocks, ctx->stream, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
         }
         ++ctx->launches;
     }

@@ -71,9 +71,9 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
     }
     int cur = g.parent[nb + leaf];
     while (cur >= 0) {
-        __threadfence();
+        fence_acq_rel_gpu();
         if (atomicAdd(&ctr[cur], 1u) == 0u) return;
-        __threadfence();
+        fence_acq_rel_gpu();
         const int x = nb + cur;
         const int l = g.left[x], r = g.right[x];
         const int cl = ld_cg(g.c_count + nb + l), cr = ld_cg(g.c_count + nb + r);

@@ -27,6 +27,13 @@ __device__ __forceinline__ float4 ld_cg(const float4* p) { return __ldcg(p); }
 __device__ __forceinline__ int ld_cg(const int* p) { return __ldcg(p); }
 __device__ __forceinline__ float ld_cg(const float* p) { return __ldcg(p); }
 
+// Release/acquire fence at GPU scope (fence.acq_rel.gpu).  Placed before a
+// relaxed atomic it makes the thread's earlier writes (and writes it has
+// observed, e.g. its warp's behind a __syncwarp) visible to a thread whose
+// atomic reads the result and which then runs the same fence before its
+// loads; lighter than the sequentially consistent __threadfence().
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

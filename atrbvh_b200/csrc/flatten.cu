@@ -75,9 +75,9 @@ __global__ void __launch_bounds__(256) k_flat_counts(FlatRefs t, Segs segs, uint
     const SegPos q = seg_pos(segs, gi);
     int cur = t.parent[q.nb + (int)q.li + (int)q.n - 1];
     while (cur >= 0) {
-        __threadfence();
+        fence_acq_rel_gpu();
         if (atomicAdd(&counters[q.cb + cur], 1u) == 0u) return;
-        __threadfence();
+        fence_acq_rel_gpu();
         const int l = t.left[q.nb + cur], r = t.right[q.nb + cur];
         const bool ll = c_leaf(t, q.nb, l), rl = c_leaf(t, q.nb, r);
         const uint32_t il = ll ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + q.cb + l);

@@ -365,10 +365,10 @@ __global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ 
     while (true) {
         const bool is_left = dr > dl;
         const int split = is_left ? r : l - 1;
-        __threadfence();
+        fence_acq_rel_gpu();
         const int other = atomicExch(&slot[split], is_left ? l : r);
         if (other < 0) return;  // first of the two children: the sibling finishes the parent
-        __threadfence();
+        fence_acq_rel_gpu();
         const int pl = is_left ? l : other;
         const int pr = is_left ? other : r;
         const int lc = split == pl ? split + last : split;
@@ -422,9 +422,9 @@ __global__ void __launch_bounds__(256) k_refit(const float4* __restrict__ verts,
     area[leaf] = box_area(mn, mx);
     int cur = parent[leaf];
     while (cur >= 0) {
-        __threadfence();
+        fence_acq_rel_gpu();
         if (atomicAdd(&counters[cur], 1u) == 0u) return;
-        __threadfence();
+        fence_acq_rel_gpu();
         const int l = left[cur], r = right[cur];
         const float4 lm = ld_cg(bmin + l), lx = ld_cg(bmax + l), rm = ld_cg(bmin + r), rx = ld_cg(bmax + r);
         mn = make_float4(fminf(lm.x, rm.x), fminf(lm.y, rm.y), fminf(lm.z, rm.z), 0.0f);

@@ -257,9 +257,9 @@ __global__ void __launch_bounds__(kTrWarps * 32) k_trbvh(TreeRefs g, Segs segs, 
     while (__any_sync(kFull, cur >= 0)) {
         bool second = false;
         if (cur >= 0) {
-            __threadfence();
+            fence_acq_rel_gpu();
             if (atomicAdd(&counters[cbase + cur], 1u) == 0u) cur = -1;
-            else { second = true; __threadfence(); }
+            else { second = true; fence_acq_rel_gpu(); }
         }
         int cnt = 0;
         float my_sah = 0.0f;
