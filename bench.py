@@ -319,6 +319,253 @@ def run_ours(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
+BATCH_MESHES = 4096
+BATCH_MIN, BATCH_MAX = 256, 262144
+BATCH_WORKLOAD = ("4096 meshes, triangle counts log-uniform in [256, 262144] (seed 0), each a uniform-centroid "
+                  "scene (vertex offsets N(0, 0.005^2)) rescaled into its own random unit box: LBVH 30-bit + "
+                  "ATRBVH(9,2) per mesh, segmented batch build replayed from a CUDA graph vs per-mesh plain launches")
+
+
+def _cuda_ms(stream, fn, reps: int) -> list[float]:
+    """Device time of fn() per repetition (CUDA events on the library's stream)."""
+    import torch
+    out = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out
+
+
+def run_batch(args, world, rank, local):
+    """Segmented batched builds of the 4096-mesh workload against per-mesh
+    plain launches of the same library on the same GPU (equal trees, so equal
+    SAH: every 64th mesh's SAH is compared bit for bit)."""
+    import torch
+    import atrbvh_b200 as ab
+    torch.cuda.set_device(local)
+    ctx = ab.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    sizes = ab.gen_batch_sizes(args.meshes, BATCH_MIN, BATCH_MAX, 0)
+    v = ab.gen_batch_scene(sizes, 0)
+    off = np.concatenate([[0], np.cumsum(sizes, dtype=np.uint64)]).astype(np.uint32)
+    n_tris = int(off[-1])
+    batch = ab.Batch(ctx, v, off)
+    launches0 = ctx.launch_count()
+
+    def build_batched():
+        batch.build(1, 9, 2, graph=True)
+
+    for _ in range(args.warmup):
+        build_batched()
+    ctx.synchronize()
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = ctx.launch_count()
+    bt = _cuda_ms(stream, build_batched, args.steps)
+    launches = (ctx.launch_count() - l0) // max(1, args.steps)
+    clk = clocks.stop()
+    sah_b = batch.sah()
+
+    # Per-mesh plain launches: one scene per mesh made up front (like the
+    # batch's own upload), then LBVH + ATRBVH per mesh in the timed loop.
+    scenes = [ab.SceneWrapper(ctx, np.ascontiguousarray(v[off[m]:off[m + 1]])) for m in range(len(sizes))]
+    ctx.synchronize()
+
+    def build_plain():
+        for sc in scenes:
+            t = ab.LBVHBuilder(False).BuildTree(sc)
+            ab.AgglomerativeTreeletOptimizer(9, 2).Optimize(t)
+            t.close()
+
+    build_plain()
+    ctx.synchronize()
+    pt = _cuda_ms(stream, build_plain, max(1, min(args.steps, 3)))
+    sah_equal = True
+    checked = 0
+    for m in range(0, len(sizes), 64):
+        t = ab.LBVHBuilder(False).BuildTree(scenes[m])
+        ab.AgglomerativeTreeletOptimizer(9, 2).Optimize(t)
+        sah_equal &= bool(np.float32(t.sah()) == np.float32(sah_b[m]))
+        checked += 1
+        t.close()
+    for sc in scenes:
+        sc.close()
+    # e2e: pinned host vertices -> atr_batch_create -> build -> per-mesh SAH on the host.
+    pinned = torch.from_numpy(v.reshape(-1)).pin_memory().numpy().reshape(v.shape)
+    e2e = []
+    for it in range(0 if args.no_e2e else 2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b2 = ab.Batch(ctx, pinned, off)
+        b2.build(1, 9, 2)
+        b2.sah()
+        e2e.append(time.perf_counter() - t0)
+        b2.close()
+    batch.close()
+    b_ms = max_over_ranks(statistics.median(bt), world)
+    p_ms = max_over_ranks(statistics.median(pt), world)
+    out = {
+        "metric": METRIC, "value": world * n_tris / (b_ms * 1e-3) / 1e6, "unit": "Mtri/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox)",
+        "config": {"workload": BATCH_WORKLOAD, "meshes": len(sizes), "triangles": n_tris, "treelet": 9,
+                   "iterations": 2, "morton_bits": 30, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2 ({n_tris * 48 / 1e9:.1f} GB of vertices)"},
+        "plain_mtri_per_s": world * n_tris / (p_ms * 1e-3) / 1e6,
+        "plain_ms": p_ms,
+        "batched_vs_plain": p_ms / b_ms,
+        "sah_equal_checked_meshes": checked, "sah_equal": sah_equal,
+        "gpu_launches": int(launches),
+        "e2e": {"value": (world * n_tris / statistics.median(e2e) / 1e6) if e2e else None, "unit": "Mtri/s",
+                "h2d_bytes_per_step": int(v.nbytes), "d2h_bytes_per_step": 4 * len(sizes),
+                "path": "atr_batch_create(pinned host vertices) -> atr_batch_build -> atr_batch_sah"},
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+SERVE_WORKLOAD = ("serving loop: Poisson arrivals; each request builds a mesh (log-uniform 1k-2M triangles, "
+                  "uniform-centroid scene) or refits a resident one after N(0, 0.001^2) vertex jitter, then traces "
+                  "64k-1M random rays; 120 GB device-memory budget")
+
+
+def run_serve(args, world, rank, local):
+    """The serving loop under Poisson arrivals: p50/p99 request latency beside
+    build and trace throughput, one JSON line per arrival rate."""
+    import atrbvh_b200 as ab
+    rng = np.random.default_rng(0)
+    pool = []
+    for k in range(args.pool):
+        n = int(np.exp(rng.uniform(np.log(1000), np.log(2_000_000))))
+        v = ab.gen_scene(ab.SCENE_UNIFORM, n, 1000 + k)
+        j = (v + rng.normal(0.0, 0.001, v.shape).astype(np.float32)).astype(np.float32)
+        j[:, :, 3] = 0.0
+        p = v[:, :, :3].reshape(-1, 3)
+        nr = int(np.exp(rng.uniform(np.log(65536), np.log(1 << 20))))
+        rays = ab.gen_rays_random(nr, p.min(0), p.max(0), seed=2000 + k)
+        pool.append((v, j, rays))
+    max_rays = max(len(r) for _, _, r in pool)
+    for rate in [float(x) for x in args.rates.split(",")]:
+        srv = ab.Server(device=local, hbm_budget=120 << 30, lanes=args.lanes, max_batch_requests=32,
+                        max_batch_triangles=1 << 25)
+        outs = [np.empty((max_rays, 4), np.int32) for _ in range(2 * args.lanes * 32 + 8)]
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, args.requests))
+        resident: list[int] = []
+        tickets = []
+        t0 = time.perf_counter()
+        for i in range(args.requests):
+            delay = arrivals[i] - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            k = int(rng.integers(len(pool)))
+            v, j, rays = pool[k]
+            out = outs[i % len(outs)]
+            keep = False
+            if resident and rng.random() < 0.3:
+                mid = resident[int(rng.integers(len(resident)))]
+                kind, verts = ab.REQ_REFIT, pool[mid % len(pool)][1]
+                rays = pool[mid % len(pool)][2]
+            else:
+                mid = i * len(pool) + k  # mesh id encodes its pool entry
+                kind, verts = ab.REQ_BUILD, v
+                if len(resident) < 64:  # the first 64 builds stay resident for refits
+                    resident.append(mid)
+                    keep = True
+            tickets.append(srv.submit(kind, mid, verts, rays, out, keep_resident=keep))
+            # Keep the output buffers' reuse distance: wait for old requests.
+            if len(tickets) >= len(outs) - 4:
+                srv.wait(tickets.pop(0))
+        while tickets:
+            srv.wait(tickets.pop(0))
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        out = {
+            "metric": METRIC, "value": st["p99_ms"], "unit": "ms (p99 request latency)", "n_gpus": 1,
+            "steps": args.requests, "warmup": 0, "ms_per_step": wall * 1e3 / args.requests,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": SERVE_WORKLOAD, "requests": args.requests, "rate_per_s": rate,
+                       "pool_meshes": args.pool, "lanes": args.lanes},
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
+            "completed": st["completed"], "failed": st["failed"], "builds": st["builds"], "refits": st["refits"],
+            "build_mtri_per_s": st["triangles_built"] / wall / 1e6,
+            "trace_mrays_per_s": st["rays_traced"] / wall / 1e6,
+            "lane_batches": st["lane_batches"], "max_batch_requests_seen": st["max_batch_requests_seen"],
+            "overlap_fraction": st["overlap_fraction"], "peak_gb": st["peak_bytes"] / 1e9,
+        }
+        print(json.dumps(out), flush=True)
+
+
+SWEEP_WORKLOAD = ("16,777,216 uniform-centroid triangles (vertex offsets N(0, 0.005^2)), seed 0: LBVH, "
+                  "TRBVH(7,3), ATRBVH(5/7/9 x 1-3); 8,388,608 random rays (origins in the scene box, "
+                  "directions uniform on the sphere)")
+
+
+def run_sweep(args, world, rank, local):
+    """Quality/speed sweep: SAH, per-phase Mtri/s and Mrays/s per optimiser."""
+    import torch
+    import atrbvh_b200 as ab
+    torch.cuda.set_device(local)
+    ctx = ab.Context(local)
+    n = args.sweep_triangles
+    v = ab.gen_scene(ab.SCENE_UNIFORM, n, 0)
+    scene = ab.SceneWrapper(ctx, v)
+    mn, mx = scene.bounds()
+    rays_h = ab.gen_rays_random(1 << 23, mn, mx, seed=0)
+    nr = len(rays_h)
+    with torch.cuda.stream(torch.cuda.ExternalStream(ctx.stream)):
+        rays = torch.from_numpy(rays_h.reshape(-1)).cuda()
+        res = torch.empty(nr * 4, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    variants = [("lbvh", 0, 0, 0)] + [("trbvh", 2, 7, 3)] + [("atrbvh", 1, t, i) for t in (5, 7, 9) for i in (1, 2, 3)]
+    rows = []
+    for name, opt, ts, it in variants:
+        ph_all = []
+        for rep in range(args.warmup + args.steps):
+            ctx.set_timing(True)
+            tree = ab.LBVHBuilder(False).BuildTree(scene)
+            if opt == 1:
+                ab.AgglomerativeTreeletOptimizer(ts, it).Optimize(tree)
+            elif opt == 2:
+                ab.TRBVHOptimizer(ts, it).Optimize(tree)
+            col, csah = ab.BVHTreeCollapser().Collapse(tree)
+            bvh = ab.CudaBVH(col, scene)
+            bvh.trace(rays.data_ptr(), nr, res.data_ptr())
+            ctx.synchronize()
+            ph = ctx.phase_times()
+            ctx.set_timing(False)
+            sah = tree.sah()
+            bvh.close(); col.close(); tree.close()
+            if rep >= args.warmup:
+                d = {}
+                for k2, ms in ph:
+                    d[k2] = d.get(k2, 0.0) + ms
+                ph_all.append(d)
+        med = {k2: statistics.median(x[k2] for x in ph_all) for k2 in ph_all[0]}
+        build_ms = sum(med.get(k2, 0.0) for k2 in ("morton", "sort", "build", "atrbvh", "trbvh"))
+        rows.append({"optimizer": name, "treelet": ts, "iterations": it, "sah": sah, "collapsed_sah": csah,
+                     "build_ms": build_ms, "build_mtri_per_s": n / (build_ms * 1e-3) / 1e6,
+                     "phase_ms": {k2: round(x, 4) for k2, x in med.items()},
+                     "phase_mtri_per_s": {k2: round(n / (x * 1e-3) / 1e6, 1) for k2, x in med.items() if k2 != "trace"},
+                     "mrays_per_s": nr / (med["trace"] * 1e-3) / 1e6})
+    best = max(rows, key=lambda r: r["build_mtri_per_s"] if r["optimizer"] == "atrbvh" and r["treelet"] == 9
+               and r["iterations"] == 2 else -1)
+    out = {"metric": METRIC, "value": best["build_mtri_per_s"], "unit": "Mtri/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": best["build_ms"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox)",
+           "config": {"workload": SWEEP_WORKLOAD, "triangles": n, "rays": nr, "value_of": "ATRBVH(9,2) build"},
+           "sweep": rows}
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args, world, rank, local):
     if rank != 0:
         return
@@ -360,11 +607,28 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--triangles", type=int, default=N_TRIS,
                     help="scene size (default: the workload's 4,194,304); smaller values are for profiling")
+    ap.add_argument("--workload", default="clustered", choices=["clustered", "batch", "serve", "sweep"],
+                    help="clustered: 4.2M-triangle build+trace (the default line); batch: 4096-mesh segmented "
+                         "build vs per-mesh launches; serve: the request loop; sweep: 16.8M-triangle optimiser sweep")
+    ap.add_argument("--meshes", type=int, default=BATCH_MESHES, help="batch: number of meshes")
+    ap.add_argument("--requests", type=int, default=20000, help="serve: requests per arrival rate")
+    ap.add_argument("--rates", default="1000,5000", help="serve: comma-separated arrival rates per second")
+    ap.add_argument("--lanes", type=int, default=2, help="serve: concurrent lanes")
+    ap.add_argument("--pool", type=int, default=48, help="serve: distinct meshes drawn by the requests")
+    ap.add_argument("--sweep-triangles", type=int, default=1 << 24, help="sweep: scene size")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:
         if args.impl == "reference":
             run_reference(args, world, rank, local)
+        elif args.workload == "batch":
+            run_batch(args, world, rank, local)
+        elif args.workload == "serve":
+            if rank == 0:
+                run_serve(args, world, rank, local)
+        elif args.workload == "sweep":
+            if rank == 0:
+                run_sweep(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
