@@ -33,6 +33,7 @@ SCENE_UNIFORM = 0
 SCENE_CLUSTERED = 1
 TUNE_ATR_WARPS = 0
 TUNE_ATR_GROUP_MIN = 1
+TUNE_SORT_BITS = 2
 
 
 class AtrError(RuntimeError):
@@ -87,6 +88,41 @@ class ServerStats(C.Structure):
                 ("max_lanes_busy", C.c_uint32), ("resident_meshes", C.c_uint32), ("resident_bytes", C.c_uint64),
                 ("peak_bytes", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
                 ("max_ms", C.c_double), ("overlap_fraction", C.c_double), ("busy_ms", C.c_double)]
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("treelet", C.c_uint8), ("iterations", C.c_uint8), ("atr_warps", C.c_uint8),
+                ("sort_bits", C.c_uint8), ("build_ms", C.c_float), ("reference_ms", C.c_float),
+                ("sah_ratio", C.c_float), ("sample_triangles", C.c_uint32), ("sample_meshes", C.c_uint32)]
+
+
+class TuneTable(C.Structure):
+    _fields_ = [("cls", TuneEntry * 32), ("tuned_mask", C.c_uint32)]
+
+    def classes(self) -> dict:
+        """{class: entry dict} of the tuned classes."""
+        out = {}
+        for c in range(32):
+            if self.tuned_mask >> c & 1:
+                e = self.cls[c]
+                out[c] = {name: getattr(e, name) for name, _ in TuneEntry._fields_}
+        return out
+
+    def class_arrays(self) -> tuple[np.ndarray, np.ndarray]:
+        """32-entry treelet / iteration arrays by class (nearest tuned class
+        for the others), as the serving loop's configuration takes them."""
+        ts = np.zeros(32, np.uint8)
+        it = np.zeros(32, np.uint8)
+        for c in range(32):
+            e = TuneEntry()
+            check(lib().atr_tune_lookup(C.byref(self), max(2, 1 << c), C.byref(e)))
+            ts[c], it[c] = e.treelet, e.iterations
+        return ts, it
+
+
+class AutotuneConfig(C.Structure):
+    _fields_ = [("min_class", C.c_uint32), ("max_class", C.c_uint32), ("sample_triangles", C.c_uint64),
+                ("sah_tolerance", C.c_float), ("reps", C.c_uint32), ("seed", C.c_uint64)]
 
 
 # (name, restype, argtypes) for every exported entry point of include/atrbvh.h.
@@ -149,6 +185,9 @@ _SIGS = [
     ("atr_gen_batch_scene", C.c_int, [C.c_uint32, _p, C.c_uint64, _p]),
     ("atr_gen_rays_pinhole", C.c_int, [C.c_uint32, C.c_uint32, _f32p, C.c_float, _p]),
     ("atr_gen_rays_random", C.c_int, [C.c_uint64, C.c_uint64, _f32p, _f32p, _p]),
+    ("atr_autotune", C.c_int, [_p, C.POINTER(AutotuneConfig), C.POINTER(TuneTable)]),
+    ("atr_tune_lookup", C.c_int, [C.POINTER(TuneTable), C.c_uint32, C.POINTER(TuneEntry)]),
+    ("atr_batch_apply_tuning", C.c_int, [_p, _p, C.POINTER(TuneTable)]),
     ("atr_server_create", C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(_p)]),
     ("atr_server_submit", C.c_int, [_p, C.POINTER(ServerRequest), C.POINTER(C.c_uint64)]),
     ("atr_server_wait", C.c_int, [_p, C.c_uint64, C.POINTER(ServerResult)]),
@@ -561,6 +600,11 @@ class Batch:
         it = np.ascontiguousarray(iterations, dtype=np.uint8)
         check(lib().atr_batch_set_params(self.ctx.handle, self.handle, _ptr(ts), _ptr(it)))
 
+    def apply_tuning(self, table: "TuneTable") -> None:
+        """Per-mesh treelet/iterations from an autotuner table, and the
+        context's launch tuning from the class holding most triangles."""
+        check(lib().atr_batch_apply_tuning(self.ctx.handle, self.handle, C.byref(table)))
+
     def build(self, optimizer: int = 1, treelet: int = 9, iterations: int = 2, ci: float = 1.2, ct: float = 1.0,
               graph: bool = False) -> None:
         check(lib().atr_batch_build(self.ctx.handle, self.handle, optimizer, treelet, iterations, ci, ct,
@@ -670,6 +714,17 @@ class CudaBVH:
             self.close()
         except Exception:
             pass
+
+
+def autotune(ctx: Context, min_class: int = 8, max_class: int = 21, sample_triangles: int = 1 << 21,
+             sah_tolerance: float = 0.0, reps: int = 3, seed: int = 0) -> TuneTable:
+    """Per size class, the fastest ATRBVH treelet size / iterations at an SAH no
+    worse than ATRBVH(9,2) (within sah_tolerance), then the fastest ATRBVH
+    block size and sort digit width (atr_autotune)."""
+    cfg = AutotuneConfig(min_class, max_class, sample_triangles, sah_tolerance, reps, seed)
+    t = TuneTable()
+    check(lib().atr_autotune(ctx.handle, C.byref(cfg), C.byref(t)))
+    return t
 
 
 # ---- serving loop ----------------------------------------------------------------

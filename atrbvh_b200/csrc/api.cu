@@ -171,6 +171,11 @@ int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value) {
                         "atr_ctx_set_tuning: group threshold %d outside [2, 33]", value);
             ctx->atr_group_min = value;
             return ATR_OK;
+        case ATR_TUNE_SORT_BITS:
+            ATR_REQUIRE(value == 8 || value == 10, ATR_ERR_INVALID_ARG,
+                        "atr_ctx_set_tuning: sort digit width %d (8 or 10)", value);
+            ctx->sort_bits = value;
+            return ATR_OK;
         default:
             break;
     }
@@ -182,6 +187,7 @@ int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value) {
     switch (knob) {
         case ATR_TUNE_ATR_WARPS: *value = ctx->atr_warps; return ATR_OK;
         case ATR_TUNE_ATR_GROUP_MIN: *value = ctx->atr_group_min; return ATR_OK;
+        case ATR_TUNE_SORT_BITS: *value = ctx->sort_bits; return ATR_OK;
         default: break;
     }
     ATR_REQUIRE(false, ATR_ERR_INVALID_ARG, "atr_ctx_get_tuning: unknown knob %d", knob);

@@ -64,6 +64,9 @@ struct atr_ctx {
     // lane groups (33: never; a single root always takes the whole warp).
     int atr_warps = 4;
     int atr_group_min = 2;
+    // Radix sort digit width of LBVH builds: 8 (4 passes for 30-bit codes)
+    // or 10 (3 passes).
+    int sort_bits = 8;
     struct Phase {
         std::string name;
         cudaEvent_t a, b;

@@ -28,9 +28,20 @@ constexpr uint32_t kFlagInc = 0x80000000u;
 constexpr uint32_t kValueMask = 0x3fffffffu;
 constexpr uint32_t kLookbackLimit = 1u << 26;
 
-template <typename K> struct KeyTraits;
-template <> struct KeyTraits<uint32_t> { static constexpr int kPasses = 4; };
-template <> struct KeyTraits<uint64_t> { static constexpr int kPasses = 8; };
+// Digit plan of an LSD sort of K keys with BITS-bit digits.  8-bit digits
+// cover every key bit (4 passes for uint32, 8 for uint64).  10-bit digits are
+// used for Morton codes only, whose top bits are always zero: 30-bit codes in
+// uint32 take 3 passes and 63-bit codes in uint64 take 7.
+template <typename K, int BITS>
+struct SortPlan {
+    static_assert(BITS == 8 || BITS == 10, "digit width");
+    static constexpr int kDigits = 1 << BITS;
+    static constexpr int kPasses = BITS == 8 ? (int)sizeof(K) : (sizeof(K) == 4 ? 3 : 7);
+    static constexpr int kPerThread = kDigits / kSortThreads;  // digits per thread in tile-wide steps
+    // Dynamic shared memory of one onesweep block: the tile's keys and
+    // values, per-warp digit counters, digit starts and global bases.
+    static constexpr size_t kSmem = (size_t)kSortTile * (sizeof(K) + 4) + (size_t)(kSortWarps + 2) * kDigits * 4;
+};
 
 // ---- scene bounds (SceneConverter.cpp:28-60 on the device) -----------------
 __global__ void __launch_bounds__(256) k_bounds_partial(const float4* __restrict__ v, uint64_t nv,
@@ -119,20 +130,20 @@ __device__ __forceinline__ uint64_t morton_code<uint64_t>(float cx, float cy, fl
 }
 
 // One block per sort tile (kSortTile triangles of one mesh); histograms of
-// every 8-bit digit are accumulated in shared memory and added to the mesh's
-// histograms (P x 256 per mesh) once per block.  Each mesh is normalised to
-// its own box (6 floats per mesh in `bounds`).
-template <typename K>
+// every digit of every pass are accumulated in shared memory and added to the
+// mesh's histograms (P x D per mesh) once per block.  Each mesh is normalised
+// to its own box (6 floats per mesh in `bounds`).
+template <typename K, int BITS>
 __global__ void __launch_bounds__(256) k_morton(Segs segs, const float4* __restrict__ v,
                                                  const float* __restrict__ bounds, K* __restrict__ keys,
                                                  uint32_t* __restrict__ hist) {
-    constexpr int P = KeyTraits<K>::kPasses;
-    __shared__ uint32_t sh[P * 256];
+    constexpr int P = SortPlan<K, BITS>::kPasses, D = SortPlan<K, BITS>::kDigits;
+    __shared__ uint32_t sh[P * D];
     __shared__ float sb[6];
     const uint32_t m = segs.seg_of_tile(blockIdx.x);
     const uint32_t t0 = segs.tri_begin(m) + (blockIdx.x - segs.tile_begin(m)) * kSortTile;
     const uint32_t t1 = min(t0 + kSortTile, segs.tri_end(m));
-    for (int j = threadIdx.x; j < P * 256; j += blockDim.x) sh[j] = 0;
+    for (int j = threadIdx.x; j < P * D; j += blockDim.x) sh[j] = 0;
     if (threadIdx.x < 6) sb[threadIdx.x] = bounds[6 * m + threadIdx.x];
     __syncthreads();
     for (uint32_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
@@ -144,20 +155,20 @@ __global__ void __launch_bounds__(256) k_morton(Segs segs, const float4* __restr
         keys[t] = code;
         if (hist) {
 #pragma unroll
-            for (int p = 0; p < P; ++p) atomicAdd(&sh[p * 256 + (uint32_t)((code >> (8 * p)) & 255u)], 1u);
+            for (int p = 0; p < P; ++p) atomicAdd(&sh[p * D + (uint32_t)((code >> (BITS * p)) & (D - 1))], 1u);
         }
     }
     if (!hist) return;
     __syncthreads();
-    for (int j = threadIdx.x; j < P * 256; j += blockDim.x)
-        if (sh[j]) atomicAdd(&hist[(size_t)m * P * 256 + j], sh[j]);
+    for (int j = threadIdx.x; j < P * D; j += blockDim.x)
+        if (sh[j]) atomicAdd(&hist[(size_t)m * P * D + j], sh[j]);
 }
 
-// Digit histogram of arbitrary keys (used by the generic sort entry point).
+// 8-bit digit histograms of arbitrary keys (the generic sort entry point).
 template <typename K>
 __global__ void __launch_bounds__(256) k_histogram(const K* __restrict__ keys, uint32_t n,
                                                     uint32_t* __restrict__ hist) {
-    constexpr int P = KeyTraits<K>::kPasses;
+    constexpr int P = SortPlan<K, 8>::kPasses;
     __shared__ uint32_t sh[P * 256];
     for (int j = threadIdx.x; j < P * 256; j += blockDim.x) sh[j] = 0;
     __syncthreads();
@@ -188,34 +199,53 @@ __device__ __forceinline__ uint32_t block_exclusive_scan256(uint32_t x, uint32_t
     return wbase + inc - x;
 }
 
+// Exclusive scan over the block of R consecutive values per thread (thread t
+// holds values t*R .. t*R+R-1).
+template <int R>
+__device__ __forceinline__ void block_exclusive_scan(const uint32_t (&x)[R], uint32_t (&out)[R], uint32_t* s_warp) {
+    uint32_t tot = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) tot += x[r];
+    uint32_t run = block_exclusive_scan256(tot, s_warp);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        out[r] = run;
+        run += x[r];
+    }
+}
+
 // ---- onesweep radix sort pass ------------------------------------------------
 // Stable: keys of one digit keep their input order (tiles are numbered by an
 // atomic ticket so that every tile's predecessors are already running; each
 // warp ranks a contiguous run of the tile in order).  The per-tile digit
-// counts are combined across tiles by decoupled look-back; a wait that does
-// not resolve within kLookbackLimit polls sets kErrSortLookback and gives up.
-// Segmented: a tile holds keys of one mesh only, the look-back stops at the
-// mesh's first tile and keys move only within their mesh, so each mesh is
-// sorted on its own (hist holds P x 256 counts per mesh).
-template <typename K, bool kIota>
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(
+// counts are combined across tiles by decoupled look-back: a tile publishes
+// the counts of all its digits before it waits on any earlier tile, and a
+// wait that does not resolve within kLookbackLimit polls sets
+// kErrSortLookback and gives up.  Segmented: a tile holds keys of one mesh
+// only, the look-back stops at the mesh's first tile and keys move only
+// within their mesh, so each mesh is sorted on its own (hist holds P x D
+// counts per mesh).  Each thread owns R = D / 256 consecutive digits in the
+// tile-wide steps.
+template <typename K, bool kIota, int BITS>
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(
         Segs segs, const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
         uint32_t* __restrict__ vout, int pass, const uint32_t* __restrict__ hist,
         uint32_t* __restrict__ status, uint32_t* __restrict__ ticket, uint32_t* __restrict__ err) {
-    constexpr int P = KeyTraits<K>::kPasses;
-    const int shift = 8 * pass;
+    using Plan = SortPlan<K, BITS>;
+    constexpr int P = Plan::kPasses, D = Plan::kDigits, R = Plan::kPerThread;
+    const int shift = BITS * pass;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K* s_keys = reinterpret_cast<K*>(smem_raw);
     uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_keys + kSortTile);
-    __shared__ uint32_t s_wh[kSortWarps][256];
-    __shared__ uint32_t s_dstart[256];
-    __shared__ uint32_t s_gbase[256];
+    uint32_t* s_wh = s_vals + kSortTile;         // [kSortWarps][D] per-warp digit counters
+    uint32_t* s_dstart = s_wh + kSortWarps * D;  // [D] digit start within the tile
+    uint32_t* s_gbase = s_dstart + D;            // [D] output base minus digit start
     __shared__ uint32_t s_scan[kSortWarps];
     __shared__ uint32_t s_tile;
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
-    for (int j = threadIdx.x; j < kSortWarps * 256; j += kSortThreads) (&s_wh[0][0])[j] = 0;
+    for (int j = threadIdx.x; j < kSortWarps * D; j += kSortThreads) s_wh[j] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
     const uint32_t m = segs.seg_of_tile(tile);
@@ -229,72 +259,82 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(
     uint32_t val[kSortItems];
     uint32_t rank[kSortItems];
     const uint32_t lt = lanemask_lt();
+    uint32_t* const wh = s_wh + w * D;
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const uint32_t idx = base + (uint32_t)w * (kSortItems * 32) + r * 32 + lane;
         const bool valid = idx < end;
         key[r] = valid ? kin[idx] : (K)0;
         val[r] = kIota ? (uint32_t)idx : (valid ? vin[idx] : 0u);
-        const uint32_t d = valid ? (uint32_t)((key[r] >> shift) & 255u) : 256u;
+        const uint32_t d = valid ? (uint32_t)((key[r] >> shift) & (D - 1)) : (uint32_t)D;
         const uint32_t peers = __match_any_sync(kFull, d);
         const uint32_t before = __popc(peers & lt);
         uint32_t cnt = 0;
-        if (valid) cnt = s_wh[w][d];
+        if (valid) cnt = wh[d];
         __syncwarp();
-        if (valid && before == 0) s_wh[w][d] = cnt + __popc(peers);
+        if (valid && before == 0) wh[d] = cnt + __popc(peers);
         __syncwarp();
         rank[r] = valid ? cnt + before : 0xffffffffu;
     }
     __syncthreads();
 
     // Per-digit exclusive offsets across warps, tile totals, digit starts.
-    const uint32_t d = threadIdx.x;
-    uint32_t run = 0;
+    uint32_t count[R], hv[R], dstart[R], gdig[R];
 #pragma unroll
-    for (int j = 0; j < kSortWarps; ++j) {
-        const uint32_t c = s_wh[j][d];
-        s_wh[j][d] = run;
-        run += c;
-    }
-    const uint32_t count = run;
-    s_dstart[d] = block_exclusive_scan256(count, s_scan);
-    const uint32_t gdigit =
-        seg_start + block_exclusive_scan256(hist[((size_t)m * P + pass) * 256 + d], s_scan);
-
-    // Decoupled look-back for digit d over this mesh's earlier tiles.
-    uint32_t* st = status + (size_t)tile * 256 + d;
-    uint32_t prefix = 0;
-    if (tile == first_tile) {
-        __stcg(st, kFlagInc | count);
-    } else {
-        __stcg(st, kFlagAgg | count);
-        int64_t k = (int64_t)tile - 1;
-        uint32_t polls = 0;
-        while (k >= (int64_t)first_tile) {
-            const uint32_t s = *reinterpret_cast<volatile uint32_t*>(status + (size_t)k * 256 + d);
-            if (s & kFlagInc) { prefix += s & kValueMask; break; }
-            if (s & kFlagAgg) { prefix += s & kValueMask; --k; continue; }
-            if (++polls > kLookbackLimit) { set_error_bits(err, kErrSortLookback); break; }
+    for (int r = 0; r < R; ++r) {
+        const int d = threadIdx.x * R + r;
+        uint32_t run = 0;
+#pragma unroll
+        for (int j = 0; j < kSortWarps; ++j) {
+            const uint32_t c = s_wh[j * D + d];
+            s_wh[j * D + d] = run;
+            run += c;
         }
-        __threadfence();
-        __stcg(st, kFlagInc | (prefix + count));
+        count[r] = run;
+        hv[r] = hist[((size_t)m * P + pass) * D + d];
     }
-    s_gbase[d] = gdigit + prefix - s_dstart[d];
+    block_exclusive_scan<R>(count, dstart, s_scan);
+    block_exclusive_scan<R>(hv, gdig, s_scan);
+
+    // Decoupled look-back for each owned digit over this mesh's earlier tiles:
+    // publish every aggregate first, then resolve the prefixes.
+    uint32_t* const st = status + (size_t)tile * D + threadIdx.x * R;
+#pragma unroll
+    for (int r = 0; r < R; ++r) __stcg(st + r, (tile == first_tile ? kFlagInc : kFlagAgg) | count[r]);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int d = threadIdx.x * R + r;
+        uint32_t prefix = 0;
+        if (tile != first_tile) {
+            int64_t k = (int64_t)tile - 1;
+            uint32_t polls = 0;
+            while (k >= (int64_t)first_tile) {
+                const uint32_t sv = *reinterpret_cast<volatile uint32_t*>(status + (size_t)k * D + d);
+                if (sv & kFlagInc) { prefix += sv & kValueMask; break; }
+                if (sv & kFlagAgg) { prefix += sv & kValueMask; --k; continue; }
+                if (++polls > kLookbackLimit) { set_error_bits(err, kErrSortLookback); break; }
+            }
+            __threadfence();
+            __stcg(st + r, kFlagInc | (prefix + count[r]));
+        }
+        s_dstart[d] = dstart[r];
+        s_gbase[d] = seg_start + gdig[r] + prefix - dstart[r];
+    }
     __syncthreads();
 
     // Scatter into shared memory in digit order, then write out coalesced.
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         if (rank[r] == 0xffffffffu) continue;
-        const uint32_t dd = (uint32_t)((key[r] >> shift) & 255u);
-        const uint32_t p = s_dstart[dd] + s_wh[w][dd] + rank[r];
+        const uint32_t dd = (uint32_t)((key[r] >> shift) & (D - 1));
+        const uint32_t p = s_dstart[dd] + wh[dd] + rank[r];
         s_keys[p] = key[r];
         s_vals[p] = val[r];
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < valid_n; i += kSortThreads) {
         const K kk = s_keys[i];
-        const uint32_t dd = (uint32_t)((kk >> shift) & 255u);
+        const uint32_t dd = (uint32_t)((kk >> shift) & (D - 1));
         const uint32_t dst = s_gbase[dd] + i;
         if (dst >= seg_start && dst < seg_end) {  // holds whenever hist matches the keys
             kout[dst] = kk;
@@ -442,86 +482,114 @@ int grid_for(atr_ctx* ctx, uint64_t work, int per_sm_blocks, int threads) {
     return (int)(need < cap ? (need ? need : 1) : cap);
 }
 
-// Sort (key, value) pairs of every mesh of `segs` in place (each mesh on its
-// own).  keys/vals hold the input and receive the output (every key width
-// uses an even number of passes).  hist holds P x 256 digit counts per mesh
-// when hist_ready; otherwise (single mesh only) it is computed here.  With
-// iota the first pass generates the values (global element indices).
-template <typename K>
-int sort_pairs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, K* keys, uint32_t* vals, uint32_t* hist,
-               bool hist_ready, bool iota) {
-    constexpr int P = KeyTraits<K>::kPasses;
+// Sort (key, value) pairs of every mesh of `segs` (each mesh on its own) with
+// BITS-bit digits.  *keys / *vals hold the input; with an odd number of
+// passes the output lands in a second pair of buffers, which then replaces
+// them (*keys and *vals are then separate ctx->alloc allocations that are
+// released: owned = true); with an even number it lands back in place
+// (required when !owned).  hist holds P x D
+// digit counts per mesh when hist_ready; otherwise (single mesh, 8-bit digits
+// only) it is computed here.  With iota the first pass generates the values
+// (global element indices).
+template <typename K, int BITS>
+int sort_pairs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, K** keys, uint32_t** vals, uint32_t* hist,
+               bool hist_ready, bool iota, bool owned) {
+    using Plan = SortPlan<K, BITS>;
+    constexpr int P = Plan::kPasses, D = Plan::kDigits;
+    static_assert(BITS == 8 || P % 2 == 1, "10-bit plans have an odd pass count");
+    ATR_REQUIRE(owned || P % 2 == 0, ATR_ERR_INVALID_ARG, "sort: odd pass count needs owned buffers");
+    ATR_REQUIRE(hist_ready || BITS == 8, ATR_ERR_INVALID_ARG, "sort: 10-bit digits need Morton histograms");
     const uint32_t n = segs.n;
-    const size_t sbytes = (size_t)P * tiles * 256 * 4;
+    const size_t sbytes = (size_t)P * tiles * D * 4;
     void* tmp = nullptr;
-    const size_t kb = align256((size_t)n * sizeof(K)), vb = align256((size_t)n * 4);
-    const size_t hb = hist ? 0 : align256(P * 256 * 4);
-    ATR_TRY(ctx->alloc(&tmp, kb + vb + align256(sbytes) + 256 + hb));
+    void* k2v = nullptr;
+    void* v2v = nullptr;
+    const size_t hb = hist ? 0 : align256(P * D * 4);
+    ATR_TRY(ctx->alloc(&k2v, (size_t)n * sizeof(K)));
+    int st = ctx->alloc(&v2v, (size_t)n * 4);
+    if (st == ATR_OK) st = ctx->alloc(&tmp, align256(sbytes) + 256 + hb);
+    if (st != ATR_OK) { ctx->release(k2v); ctx->release(v2v); return st; }
+    K* k2 = static_cast<K*>(k2v);
+    uint32_t* v2 = static_cast<uint32_t*>(v2v);
     char* p = static_cast<char*>(tmp);
-    K* k2 = reinterpret_cast<K*>(p); p += kb;
-    uint32_t* v2 = reinterpret_cast<uint32_t*>(p); p += vb;
     uint32_t* status = reinterpret_cast<uint32_t*>(p); p += align256(sbytes);
     uint32_t* tickets = reinterpret_cast<uint32_t*>(p); p += 256;
     if (!hist) hist = reinterpret_cast<uint32_t*>(p);
     cudaStream_t s = ctx->stream;
     cudaError_t e = cudaMemsetAsync(status, 0, align256(sbytes) + 256, s);
-    if (e != cudaSuccess) { ctx->release(tmp); return cuda_fail(e, "cudaMemsetAsync", __FILE__, __LINE__); }
-    if (!hist_ready) {
-        cudaMemsetAsync(hist, 0, P * 256 * 4, s);
-        k_histogram<K><<<grid_for(ctx, n, 4, 256), 256, 0, s>>>(keys, n, hist);
+    if (e != cudaSuccess) {
+        ctx->release(tmp);
+        ctx->release(k2v);
+        ctx->release(v2v);
+        return cuda_fail(e, "cudaMemsetAsync", __FILE__, __LINE__);
     }
-    const size_t smem = (size_t)kSortTile * (sizeof(K) + 4);  // attribute set by lbvh_prepare()
-    K* ka = keys; K* kb2 = k2;
-    uint32_t* va = vals; uint32_t* vb2 = v2;
+    if (!hist_ready) {
+        cudaMemsetAsync(hist, 0, P * D * 4, s);
+        k_histogram<K><<<grid_for(ctx, n, 4, 256), 256, 0, s>>>(*keys, n, hist);
+    }
+    K* ka = *keys; K* kb2 = k2;
+    uint32_t* va = *vals; uint32_t* vb2 = v2;
     for (int pass = 0; pass < P; ++pass) {
-        uint32_t* st = status + (size_t)pass * tiles * 256;
+        uint32_t* stp = status + (size_t)pass * tiles * D;
         if (pass == 0 && iota)
-            k_onesweep<K, true><<<tiles, kSortThreads, smem, s>>>(segs, ka, va, kb2, vb2, pass, hist, st,
-                                                                  tickets + pass, ctx->d_error);
+            k_onesweep<K, true, BITS><<<tiles, kSortThreads, Plan::kSmem, s>>>(segs, ka, va, kb2, vb2, pass, hist,
+                                                                               stp, tickets + pass, ctx->d_error);
         else
-            k_onesweep<K, false><<<tiles, kSortThreads, smem, s>>>(segs, ka, va, kb2, vb2, pass, hist, st,
-                                                                   tickets + pass, ctx->d_error);
+            k_onesweep<K, false, BITS><<<tiles, kSortThreads, Plan::kSmem, s>>>(segs, ka, va, kb2, vb2, pass, hist,
+                                                                                stp, tickets + pass, ctx->d_error);
         std::swap(ka, kb2);
         std::swap(va, vb2);
     }
     ctx->launches += P + (hist_ready ? 0 : 1);
     e = cudaGetLastError();
     ctx->release(tmp);
+    if (P % 2 == 1) {
+        // Output in the second pair: hand it to the caller, release the first.
+        ctx->release(*keys);
+        ctx->release(*vals);
+        *keys = k2;
+        *vals = v2;
+    } else {
+        ctx->release(k2v);
+        ctx->release(v2v);
+    }
     if (e != cudaSuccess) return cuda_fail(e, "k_onesweep launch", __FILE__, __LINE__);
     return ATR_OK;
 }
 
-template <typename K>
+template <typename K, int BITS>
 int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts, const float* d_bounds,
                 const TreeOut& t, void** keep_keys, uint32_t** keep_idx) {
-    constexpr int P = KeyTraits<K>::kPasses;
+    constexpr int P = SortPlan<K, BITS>::kPasses, D = SortPlan<K, BITS>::kDigits;
     const uint32_t n = segs.n;
     cudaStream_t s = ctx->stream;
-    void* keys = nullptr;
-    void* idx = nullptr;
+    void* kv = nullptr;
+    void* iv = nullptr;
     void* aux = nullptr;
-    const size_t hbytes = (size_t)segs.count * P * 256 * 4;
+    const size_t hbytes = (size_t)segs.count * P * D * 4;
     const size_t inner = n - segs.count;
-    ATR_TRY(ctx->alloc(&keys, (size_t)n * sizeof(K)));
-    int st = ctx->alloc(&idx, (size_t)n * 4);
+    ATR_TRY(ctx->alloc(&kv, (size_t)n * sizeof(K)));
+    int st = ctx->alloc(&iv, (size_t)n * 4);
     if (st == ATR_OK) st = ctx->alloc(&aux, align256(hbytes) + align256(inner * 4));
-    if (st != ATR_OK) { ctx->release(keys); ctx->release(idx); return st; }
+    if (st != ATR_OK) { ctx->release(kv); ctx->release(iv); return st; }
+    K* keys = static_cast<K*>(kv);
+    uint32_t* idx = static_cast<uint32_t*>(iv);
     uint32_t* hist = static_cast<uint32_t*>(aux);
     int32_t* slot = reinterpret_cast<int32_t*>(static_cast<char*>(aux) + align256(hbytes));
     cudaMemsetAsync(hist, 0, hbytes, s);
     cudaMemsetAsync(slot, 0xff, inner * 4, s);
 
     ctx->phase_begin("morton");
-    k_morton<K><<<tiles, 256, 0, s>>>(segs, verts, d_bounds, static_cast<K*>(keys), hist);
+    k_morton<K, BITS><<<tiles, 256, 0, s>>>(segs, verts, d_bounds, keys, hist);
     ctx->phase_end();
     ctx->launches += 1;
     ctx->phase_begin("sort");
-    st = sort_pairs<K>(ctx, segs, tiles, static_cast<K*>(keys), static_cast<uint32_t*>(idx), hist, true, true);
+    st = sort_pairs<K, BITS>(ctx, segs, tiles, &keys, &idx, hist, true, true, true);
     ctx->phase_end();
     if (st == ATR_OK) {
         ctx->phase_begin("build");
-        k_build<K><<<(n + 255) / 256, 256, 0, s>>>(segs, static_cast<K*>(keys), static_cast<uint32_t*>(idx), verts,
-                                                  t.parent, t.left, t.right, t.data, t.bmin, t.bmax, t.area, slot);
+        k_build<K><<<(n + 255) / 256, 256, 0, s>>>(segs, keys, idx, verts, t.parent, t.left, t.right, t.data, t.bmin,
+                                                  t.bmax, t.area, slot);
         ctx->phase_end();
         ctx->launches += 1;
         cudaError_t e = cudaGetLastError();
@@ -530,7 +598,7 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
     ctx->release(aux);
     if (st != ATR_OK || !keep_keys) { ctx->release(keys); ctx->release(idx); return st; }
     *keep_keys = keys;
-    *keep_idx = static_cast<uint32_t*>(idx);
+    *keep_idx = idx;
     return ATR_OK;
 }
 
@@ -538,24 +606,32 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
 
 static_assert(kSortTile == (int)kSortTileSize, "sort tile size");
 
+template <typename K, int BITS>
+cudaError_t onesweep_attrs() {
+    const int smem = (int)SortPlan<K, BITS>::kSmem;
+    cudaError_t e = cudaFuncSetAttribute(k_onesweep<K, true, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_onesweep<K, false, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return e;
+}
+
 // Kernel attributes, set once per context before any capture.
 int lbvh_prepare() {
-    ATR_CUDA(cudaFuncSetAttribute(k_onesweep<uint32_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kSortTile * 8));
-    ATR_CUDA(cudaFuncSetAttribute(k_onesweep<uint32_t, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kSortTile * 8));
-    ATR_CUDA(cudaFuncSetAttribute(k_onesweep<uint64_t, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kSortTile * 12));
-    ATR_CUDA(cudaFuncSetAttribute(k_onesweep<uint64_t, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  kSortTile * 12));
+    ATR_CUDA((onesweep_attrs<uint32_t, 8>()));
+    ATR_CUDA((onesweep_attrs<uint32_t, 10>()));
+    ATR_CUDA((onesweep_attrs<uint64_t, 8>()));
+    ATR_CUDA((onesweep_attrs<uint64_t, 10>()));
     return ATR_OK;
 }
 
 int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts, const float* d_bounds,
                     int morton_bits, const TreeOut& out, void** keep_keys, uint32_t** keep_idx) {
+    const bool ten = ctx->sort_bits == 10;
     if (morton_bits == 30)
-        return build_typed<uint32_t>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx);
-    return build_typed<uint64_t>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx);
+        return ten ? build_typed<uint32_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx)
+                   : build_typed<uint32_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx);
+    return ten ? build_typed<uint64_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx)
+               : build_typed<uint64_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx);
 }
 
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds, int morton_bits,
@@ -678,11 +754,11 @@ int atr_device_morton(atr_ctx* ctx, const float* vertices, uint32_t n, const flo
     Segs segs{nullptr, nullptr, 1u, n};
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
     if (morton_bits == 30)
-        k_morton<uint32_t><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
-                                                           static_cast<uint32_t*>(keys), nullptr);
+        k_morton<uint32_t, 8><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
+                                                              static_cast<uint32_t*>(keys), nullptr);
     else
-        k_morton<uint64_t><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
-                                                           static_cast<uint64_t*>(keys), nullptr);
+        k_morton<uint64_t, 8><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
+                                                              static_cast<uint64_t*>(keys), nullptr);
     ctx->launches += 1;
     cudaError_t e = cudaStreamSynchronize(ctx->stream);  // h is a stack array
     ctx->release(b);
@@ -696,9 +772,12 @@ int atr_device_sort_pairs(atr_ctx* ctx, void* keys, uint32_t* values, uint32_t c
     if (count == 0) return ATR_OK;
     Segs segs{nullptr, nullptr, 1u, count};
     const uint32_t tiles = (count + kSortTile - 1) / kSortTile;
-    if (key_bits <= 32)
-        return sort_pairs<uint32_t>(ctx, segs, tiles, static_cast<uint32_t*>(keys), values, nullptr, false, false);
-    return sort_pairs<uint64_t>(ctx, segs, tiles, static_cast<uint64_t*>(keys), values, nullptr, false, false);
+    if (key_bits <= 32) {
+        uint32_t* k = static_cast<uint32_t*>(keys);
+        return sort_pairs<uint32_t, 8>(ctx, segs, tiles, &k, &values, nullptr, false, false, false);
+    }
+    uint64_t* k = static_cast<uint64_t*>(keys);
+    return sort_pairs<uint64_t, 8>(ctx, segs, tiles, &k, &values, nullptr, false, false, false);
 }
 
 }  // extern "C"

@@ -84,7 +84,30 @@ struct Lane {
     size_t h_rays_cap = 0;
     void* h_res = nullptr;
     size_t h_res_cap = 0;
+    void* h_rverts = nullptr;  // refit vertices
+    size_t h_rverts_cap = 0;
 };
+
+struct CopyJob {
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+
+// Host copies between request buffers and pinned staging, cut into 4 MiB
+// chunks spread over OpenMP threads: a lane batch moves hundreds of MB of
+// vertices, rays and results, which one thread copies at a fraction of the
+// host's memory bandwidth.
+void par_copy(const std::vector<CopyJob>& jobs) {
+    constexpr size_t kChunk = (size_t)4 << 20;
+    std::vector<CopyJob> chunks;
+    for (const CopyJob& j : jobs)
+        for (size_t o = 0; o < j.bytes; o += kChunk)
+            chunks.push_back({static_cast<char*>(j.dst) + o, static_cast<const char*>(j.src) + o,
+                              std::min(kChunk, j.bytes - o)});
+#pragma omp parallel for schedule(dynamic, 1) if (chunks.size() > 1)
+    for (long i = 0; i < (long)chunks.size(); ++i) std::memcpy(chunks[i].dst, chunks[i].src, chunks[i].bytes);
+}
 
 int grow_pinned(void** p, size_t* cap, size_t need) {
     if (need <= *cap) return ATR_OK;
@@ -285,12 +308,38 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
     ATR_TRY(grow_pinned(&L.h_rays, &L.h_rays_cap, std::max<uint64_t>(total_rays, 1) * 32));
     ATR_TRY(grow_pinned(&L.h_res, &L.h_res_cap, std::max<uint64_t>(total_rays, 1) * 16));
     std::vector<uint64_t> ray_at(work.size() + 1, 0);
+    std::vector<CopyJob> jobs;
     for (size_t i = 0; i < work.size(); ++i) {
         ray_at[i + 1] = ray_at[i] + work[i]->req.num_rays;
         if (work[i]->req.num_rays)
-            std::memcpy(static_cast<char*>(L.h_rays) + ray_at[i] * 32, work[i]->req.rays,
-                        (size_t)work[i]->req.num_rays * 32);
+            jobs.push_back({static_cast<char*>(L.h_rays) + ray_at[i] * 32, work[i]->req.rays,
+                            (size_t)work[i]->req.num_rays * 32});
     }
+    // Refit vertices go to their own staging buffer (copied before any launch).
+    uint64_t refit_tris = 0;
+    std::vector<size_t> refit_at(work.size(), 0);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (size_t i = 0; i < work.size(); ++i) {
+            if (work[i]->req.kind != ATR_REQ_REFIT) continue;
+            auto f = resident.find(work[i]->req.mesh_id);
+            if (f == resident.end()) continue;
+            refit_at[i] = refit_tris;
+            refit_tris += f->second.n;
+        }
+    }
+    ATR_TRY(grow_pinned(&L.h_rverts, &L.h_rverts_cap, std::max<uint64_t>(refit_tris, 1) * 48));
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (size_t i = 0; i < work.size(); ++i) {
+            if (work[i]->req.kind != ATR_REQ_REFIT) continue;
+            auto f = resident.find(work[i]->req.mesh_id);
+            if (f == resident.end()) continue;
+            jobs.push_back({static_cast<char*>(L.h_rverts) + refit_at[i] * 48, work[i]->req.vertices,
+                            (size_t)f->second.n * 48});
+        }
+    }
+    par_copy(jobs);
     void* d_rays = nullptr;
     void* d_res = nullptr;
     if (total_rays) {
@@ -325,12 +374,14 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
         if (s != ATR_OK) { release_rays(); return s; }
         std::vector<uint32_t> off(builds.size() + 1, 0);
         std::vector<uint8_t> ts(builds.size()), it(builds.size());
+        std::vector<CopyJob> vjobs;
         for (size_t m = 0; m < builds.size(); ++m) {
             const uint32_t n = builds[m]->req.num_triangles;
-            std::memcpy(static_cast<char*>(L.h_verts) + (size_t)off[m] * 48, builds[m]->req.vertices, (size_t)n * 48);
+            vjobs.push_back({static_cast<char*>(L.h_verts) + (size_t)off[m] * 48, builds[m]->req.vertices, (size_t)n * 48});
             off[m + 1] = off[m] + n;
             params_for(n, &ts[m], &it[m]);
         }
+        par_copy(vjobs);
         atr_batch* b = nullptr;
         s = atr_batch_create(ctx, static_cast<const float*>(L.h_verts), off.data(), (uint32_t)builds.size(), nullptr,
                              0, &b);
@@ -378,8 +429,10 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
             res = f->second;
         }
         float sah = 0.0f;
-        int s = atr::batch_refit_mesh(ctx, res.rec->batch, res.index, r->req.vertices, 0, &sah);
         const size_t p = work_pos(r);
+        int s = atr::batch_refit_mesh(ctx, res.rec->batch, res.index,
+                                      reinterpret_cast<const float*>(static_cast<char*>(L.h_rverts) + refit_at[p] * 48),
+                                      0, &sah);
         if (s == ATR_OK && r->req.num_rays) {
             const uint32_t roff[2] = {0, r->req.num_rays};
             const uint32_t gm[1] = {res.index};
@@ -398,10 +451,12 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
     const int s = atr_ctx_synchronize(ctx);
     release_rays();
     ATR_TRY(s);
+    std::vector<CopyJob> out;
     for (size_t i = 0; i < work.size(); ++i)
         if (work[i]->req.num_rays && work[i]->status == ATR_OK)
-            std::memcpy(work[i]->req.results, static_cast<char*>(L.h_res) + ray_at[i] * 16,
-                        (size_t)work[i]->req.num_rays * 16);
+            out.push_back({work[i]->req.results, static_cast<char*>(L.h_res) + ray_at[i] * 16,
+                           (size_t)work[i]->req.num_rays * 16});
+    par_copy(out);
     return ATR_OK;
 }
 
@@ -650,6 +705,7 @@ int atr_server_destroy(atr_server* s) {
         if (L->h_verts) cudaFreeHost(L->h_verts);
         if (L->h_rays) cudaFreeHost(L->h_rays);
         if (L->h_res) cudaFreeHost(L->h_res);
+        if (L->h_rverts) cudaFreeHost(L->h_rverts);
         atr_ctx_destroy(L->ctx);
     }
     delete s;

@@ -372,6 +372,28 @@ def run_batch(args, world, rank, local):
     clk = clocks.stop()
     sah_b = batch.sah()
 
+    # Autotuned arm: per-class treelet/iterations at SAH no worse than
+    # ATRBVH(9,2), ATRBVH block size and sort digit width of the dominant class.
+    tuned = None
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        table = ab.autotune(ctx, min_class=8, max_class=18, sample_triangles=1 << 21, reps=2)
+        tune_s = time.perf_counter() - t0
+        batch.apply_tuning(table)
+        for _ in range(args.warmup):
+            build_batched()
+        tt = _cuda_ms(stream, build_batched, args.steps)
+        sah_t = batch.sah()
+        t_ms = max_over_ranks(statistics.median(tt), world)
+        tuned = {"mtri_per_s": world * n_tris / (t_ms * 1e-3) / 1e6, "ms": t_ms,
+                 "sah_ratio_vs_atrbvh_9_2": float(np.sum(sah_t, dtype=np.float64) / np.sum(sah_b, dtype=np.float64)),
+                 "tuning_seconds": tune_s,
+                 "table": {str(c): {k: e[k] for k in ("treelet", "iterations", "atr_warps", "sort_bits", "sah_ratio")}
+                           for c, e in table.classes().items()}}
+        batch.set_params(None)
+        ctx.set_tuning(ab.TUNE_ATR_WARPS, 4)
+        ctx.set_tuning(ab.TUNE_SORT_BITS, 8)
+
     # Per-mesh plain launches: one scene per mesh made up front (like the
     # batch's own upload), then LBVH + ATRBVH per mesh in the timed loop.
     scenes = [ab.SceneWrapper(ctx, np.ascontiguousarray(v[off[m]:off[m + 1]])) for m in range(len(sizes))]
@@ -421,6 +443,7 @@ def run_batch(args, world, rank, local):
         "plain_ms": p_ms,
         "batched_vs_plain": p_ms / b_ms,
         "sah_equal_checked_meshes": checked, "sah_equal": sah_equal,
+        "autotuned": tuned,
         "gpu_launches": int(launches),
         "e2e": {"value": (world * n_tris / statistics.median(e2e) / 1e6) if e2e else None, "unit": "Mtri/s",
                 "h2d_bytes_per_step": int(v.nbytes), "d2h_bytes_per_step": 4 * len(sizes),
@@ -611,6 +634,7 @@ def main():
                     help="clustered: 4.2M-triangle build+trace (the default line); batch: 4096-mesh segmented "
                          "build vs per-mesh launches; serve: the request loop; sweep: 16.8M-triangle optimiser sweep")
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES, help="batch: number of meshes")
+    ap.add_argument("--no-autotune", action="store_true", help="batch: skip the autotuned arm")
     ap.add_argument("--requests", type=int, default=20000, help="serve: requests per arrival rate")
     ap.add_argument("--rates", default="1000,5000", help="serve: comma-separated arrival rates per second")
     ap.add_argument("--lanes", type=int, default=2, help="serve: concurrent lanes")

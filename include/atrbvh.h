@@ -107,8 +107,11 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
  *   ATR_TUNE_ATR_WARPS      ATRBVH warps per block: 2, 4 (default) or 8.
  *   ATR_TUNE_ATR_GROUP_MIN  fewest treelet roots reached by one warp at once
  *                           that are restructured side by side in lane groups
- *                           (2..32; 33 = never; default 2). */
-enum atr_tune_knob { ATR_TUNE_ATR_WARPS = 0, ATR_TUNE_ATR_GROUP_MIN = 1 };
+ *                           (2..32; 33 = never; default 2).
+ *   ATR_TUNE_SORT_BITS      radix-sort digit width of LBVH builds: 8 (default;
+ *                           4 passes over 30-bit codes, 8 over 63-bit) or 10
+ *                           (3 and 7 passes). */
+enum atr_tune_knob { ATR_TUNE_ATR_WARPS = 0, ATR_TUNE_ATR_GROUP_MIN = 1, ATR_TUNE_SORT_BITS = 2 };
 int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value);
 int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value);
 /* Number of kernels this context has enqueued since it was created. */
@@ -275,6 +278,50 @@ int atr_batch_trace(atr_ctx* ctx, const atr_batch* batch, const float* rays, int
  * batch was flattened) re-collapse and re-flatten that mesh in place. */
 int atr_batch_refit_mesh(atr_ctx* ctx, atr_batch* batch, uint32_t mesh, const float* vertices,
                          int vertices_on_device);
+
+/* ---- autotuner (no counterpart in the reference, whose treelet size and
+ * iteration count are fixed per run by gpu-ray-traversal/src/rt/BVHRTSettings.cpp:7-84
+ * and whose launch shapes are constants, AgglomerativeTreelet.cu:556-595) ------
+ * Size class c holds meshes of [2^c, 2^(c+1)) triangles.  For each class in
+ * [min_class, max_class] a sample batch of about sample_triangles triangles
+ * (the uniform-centroid distribution, each mesh in its own box) is built with
+ * ATRBVH(9,2); every ATRBVH(treelet 5..9, iterations 1..3) is then timed and
+ * the fastest whose summed per-mesh SAH is at most (1 + sah_tolerance) times
+ * that of ATRBVH(9,2) is kept; then the ATRBVH warps per block (2, 4, 8) and
+ * sort digit width (8, 10) that build it fastest.  Takes seconds; results are
+ * timings of this GPU. */
+typedef struct atr_tune_entry {
+    uint8_t treelet;
+    uint8_t iterations;
+    uint8_t atr_warps;
+    uint8_t sort_bits;
+    float build_ms;          /* median LBVH+ATRBVH time of the class sample, tuned */
+    float reference_ms;      /* same with ATRBVH(9,2), 4 warps, 8-bit digits */
+    float sah_ratio;         /* summed SAH of the tuned build / that of ATRBVH(9,2) */
+    uint32_t sample_triangles;
+    uint32_t sample_meshes;
+} atr_tune_entry;
+
+typedef struct atr_tune_table {
+    atr_tune_entry cls[32];
+    uint32_t tuned_mask;     /* bit c set: class c was tuned */
+} atr_tune_table;
+
+typedef struct atr_autotune_config {
+    uint32_t min_class, max_class;  /* within [1, 29] */
+    uint64_t sample_triangles;      /* per class (at least two meshes are used) */
+    float sah_tolerance;            /* 0: SAH no worse than ATRBVH(9,2) */
+    uint32_t reps;                  /* timed builds per candidate (median) */
+    uint64_t seed;
+} atr_autotune_config;
+
+int atr_autotune(atr_ctx* ctx, const atr_autotune_config* config, atr_tune_table* table);
+/* The entry for a mesh of num_triangles: its class, or the nearest tuned one. */
+int atr_tune_lookup(const atr_tune_table* table, uint32_t num_triangles, atr_tune_entry* entry);
+/* Per-mesh treelet size and iterations of a batch from the table
+ * (atr_batch_set_params), and the context's ATRBVH warps and sort digit width
+ * from the class holding most of the batch's triangles. */
+int atr_batch_apply_tuning(atr_ctx* ctx, atr_batch* batch, const atr_tune_table* table);
 
 /* ---- serving loop (no counterpart in the reference, whose Renderer builds
  * and traces one scene at a time: gpu-ray-traversal/src/rt/cuda/Renderer.cpp:85-105,

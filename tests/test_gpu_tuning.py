@@ -1,0 +1,89 @@
+"""Launch tuning and the autotuner: every tuning knob leaves the results
+bit-exact (10-bit sort digits, ATRBVH block sizes, lane-group threshold), and
+an autotuned batch equals the oracle built with each mesh's tuned parameters."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import atrbvh_b200 as ab
+import oracle as O
+from tests._util import assert_trees_equal, scene_case
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture()
+def tuned_ctx():
+    c = ab.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.mark.parametrize("bits", [30, 63])
+@pytest.mark.parametrize("case", ["u2", "u17", "u4097", "c1", "clu65536", "dupes3000", "same64"])
+def test_ten_bit_sort_digits_bit_exact(tuned_ctx, case, bits):
+    tuned_ctx.set_tuning(ab.TUNE_SORT_BITS, 10)
+    v = scene_case(case)
+    mn, mx = O.scene_aabb(v)
+    want, sk, si = O.build_lbvh(v, mn, mx, bits=bits, threads=8)
+    scene = ab.SceneWrapper(tuned_ctx, v, mn, mx)
+    tree = ab.LBVHBuilder(bits == 63).BuildTree(scene)
+    keys, idx = tree.sorted_keys()
+    assert np.array_equal(keys, sk) and np.array_equal(idx, si)
+    assert_trees_equal(ab.BVHTreeInstanceManager().DeviceToHostTree(tree), want, f"{case}/{bits} 10-bit digits")
+
+
+@pytest.mark.parametrize("warps,gmin", [(2, 2), (8, 2), (4, 3), (4, 33)])
+@pytest.mark.parametrize("treelet,iters", [(5, 2), (9, 2), (12, 1), (20, 1)])
+def test_atrbvh_launch_tuning_bit_exact(tuned_ctx, warps, gmin, treelet, iters):
+    tuned_ctx.set_tuning(ab.TUNE_ATR_WARPS, warps)
+    tuned_ctx.set_tuning(ab.TUNE_ATR_GROUP_MIN, gmin)
+    v = scene_case("clu65536")
+    mn, mx = O.scene_aabb(v)
+    base, _, _ = O.build_lbvh(v, mn, mx, threads=8)
+    want = O.atrbvh(base, treelet, iters, threads=8)
+    scene = ab.SceneWrapper(tuned_ctx, v, mn, mx)
+    tree = ab.LBVHBuilder().BuildTree(scene)
+    ab.AgglomerativeTreeletOptimizer(treelet, iters).Optimize(tree)
+    assert_trees_equal(ab.BVHTreeInstanceManager().DeviceToHostTree(tree), want,
+                       f"ATRBVH({treelet},{iters}) warps {warps} group_min {gmin}")
+
+
+def test_tuning_rejects_bad_values(tuned_ctx):
+    for knob, bad in [(ab.TUNE_ATR_WARPS, 3), (ab.TUNE_ATR_GROUP_MIN, 1), (ab.TUNE_SORT_BITS, 9), (7, 1)]:
+        with pytest.raises(ab.AtrError):
+            tuned_ctx.set_tuning(knob, bad)
+
+
+def test_autotune_table_and_tuned_batch(tuned_ctx):
+    table = ab.autotune(tuned_ctx, min_class=8, max_class=11, sample_triangles=1 << 15, reps=1)
+    cls = table.classes()
+    assert sorted(cls) == [8, 9, 10, 11]
+    for c, e in cls.items():
+        assert 5 <= e["treelet"] <= 9 and 1 <= e["iterations"] <= 3, e
+        assert e["atr_warps"] in (2, 4, 8) and e["sort_bits"] in (8, 10), e
+        assert e["sah_ratio"] <= 1.0 + 1e-6, e
+        assert 0.0 < e["build_ms"] <= e["reference_ms"], e
+        assert e["sample_meshes"] >= 2
+    # The tuning context's own knobs are restored.
+    assert tuned_ctx.get_tuning(ab.TUNE_ATR_WARPS) == 4 and tuned_ctx.get_tuning(ab.TUNE_SORT_BITS) == 8
+    ts, it = table.class_arrays()
+    assert ts[8] == cls[8]["treelet"] and ts[20] == cls[11]["treelet"] and ts[3] == cls[8]["treelet"]
+
+    sizes = ab.gen_batch_sizes(24, 200, 5000, 4)
+    v = ab.gen_batch_scene(sizes, 4)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint32)
+    b = ab.Batch(tuned_ctx, v, off)
+    b.apply_tuning(table)
+    b.build(1, 9, 2, graph=True)
+    b.build(1, 9, 2, graph=True)
+    for m in range(len(sizes)):
+        n = int(sizes[m])
+        c = min(max(n.bit_length() - 1, 8), 11)
+        vm = np.ascontiguousarray(v[off[m]:off[m + 1]])
+        mn, mx = O.scene_aabb(vm)
+        base, _, _ = O.build_lbvh(vm, mn, mx, threads=8)
+        want = O.atrbvh(base, cls[c]["treelet"], cls[c]["iterations"], threads=8)
+        assert_trees_equal(b.mesh(m), want, f"mesh {m} ({n} tris, class {c})")
+    b.close()
