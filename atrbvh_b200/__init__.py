@@ -34,6 +34,7 @@ SCENE_CLUSTERED = 1
 TUNE_ATR_WARPS = 0
 TUNE_ATR_GROUP_MIN = 1
 TUNE_SORT_BITS = 2
+TUNE_ATR_LEVELS = 3
 
 
 class AtrError(RuntimeError):

@@ -114,6 +114,7 @@ int atr_ctx_create(int device, void* stream, atr_ctx** out) {
     cudaError_t e = cudaMalloc(&c->d_error, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(c->d_error, 0, sizeof(uint32_t));
     if (e == cudaSuccess && atr::lbvh_prepare() != ATR_OK) e = cudaErrorInvalidValue;
+    if (e == cudaSuccess && atr::atrbvh_prepare() != ATR_OK) e = cudaErrorInvalidValue;
     if (e != cudaSuccess) {
         if (c->own_stream) cudaStreamDestroy(c->stream);
         delete c;
@@ -176,6 +177,11 @@ int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value) {
                         "atr_ctx_set_tuning: sort digit width %d (8 or 10)", value);
             ctx->sort_bits = value;
             return ATR_OK;
+        case ATR_TUNE_ATR_LEVELS:
+            ATR_REQUIRE(value >= 0 && value <= 64, ATR_ERR_INVALID_ARG,
+                        "atr_ctx_set_tuning: level passes %d outside [0, 64]", value);
+            ctx->atr_levels = value;
+            return ATR_OK;
         default:
             break;
     }
@@ -188,6 +194,7 @@ int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value) {
         case ATR_TUNE_ATR_WARPS: *value = ctx->atr_warps; return ATR_OK;
         case ATR_TUNE_ATR_GROUP_MIN: *value = ctx->atr_group_min; return ATR_OK;
         case ATR_TUNE_SORT_BITS: *value = ctx->sort_bits; return ATR_OK;
+        case ATR_TUNE_ATR_LEVELS: *value = ctx->atr_levels; return ATR_OK;
         default: break;
     }
     ATR_REQUIRE(false, ATR_ERR_INVALID_ARG, "atr_ctx_get_tuning: unknown knob %d", knob);

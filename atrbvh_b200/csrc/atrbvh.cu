@@ -45,15 +45,31 @@
 namespace atr {
 namespace {
 
-// Shared-memory layout of one lane group: distance matrix, then two float4
-// per treelet leaf: (min.xyz, nodesSah) and (max.xyz, node id bits).
+// Shared-memory layout of one lane group: distance matrix, then three float4
+// per treelet leaf: (min.xyz, nodesSah), (max.xyz, node id bits) and
+// (subtree count, next-iteration level, next-iteration nodesSah, unused).
 template <int G>
 struct GroupLayout {
     static constexpr int kGroups = 32 / G;
     static constexpr int kLeaves = G == 32 ? kMaxTreelet : G;
     static constexpr int kDist = kLeaves * (kLeaves - 1) / 2;
     static constexpr int kDistPad = (kDist + 3) & ~3;
-    static constexpr int kFloats = kDistPad + 8 * kLeaves;
+    static constexpr int kFloats = kDistPad + 12 * kLeaves;
+};
+
+// What the treelet code keeps up to date for the next iteration, per mesh, for
+// every node it finishes or rewrites: subtree counts (node-indexed),
+// next-iteration levels (indexed by internal node) under the next
+// iteration's gamma, and next-iteration nodesSah (node-indexed).  The
+// reference recomputes nodesSah bottom-up every iteration as
+// (ci*A + left) + right, while a rewritten node stores the merge cost
+// (left + right) + ci*A; the two can differ in the last bit, so the next
+// iteration's values are kept in the recomputation's order.
+struct NextRefs {
+    int32_t* sub;
+    int32_t* nlv;
+    float* nsn;
+    int gamma;
 };
 
 template <int G>
@@ -125,9 +141,9 @@ __device__ __forceinline__ float union_area3(float ax0, float ay0, float az0, fl
 // the shuffles stay warp-wide.  sm is this group's shared memory.
 template <int G>
 __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, int nb, uint32_t n, int root,
-                                              int4* KD, float root_sah, int tsize, int maxts, float ci, float* sm,
-                                              const uint16_t* __restrict__ s_rc, const uint8_t* __restrict__ s_prio,
-                                              uint32_t* err) {
+                                              int4* KD, const NextRefs& nx, float root_sah, int tsize, int maxts,
+                                              float ci, float* sm, const uint16_t* __restrict__ s_rc,
+                                              const uint8_t* __restrict__ s_prio, uint32_t* err) {
     using Lay = GroupLayout<G>;
     const int lane = threadIdx.x & 31;
     const int gb = G == 32 ? 0 : (lane / G) * G;
@@ -141,6 +157,8 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     float* const NS = g.nsah + nb;
 
     // ---- formTreelet (Treelet.cuh:57-114) ----
+    // Lane k holds treelet leaf k: its node, area and box, and (for an
+    // internal node) its children and their areas from the child record.
     int internal_node = gl == 0 ? root : -1;
     int s_node = -1, s_cl = -1, s_cr = -1;
     float s_area = 0.0f, s_cal = 0.0f, s_car = 0.0f, s_sah = 0.0f;
@@ -213,12 +231,21 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     if (active && !ok && gl == 0) set_error_bits(err, kErrTreeletClimb);
 
     // ---- distance matrix (AgglomerativeTreelet.cu:18-63) ----
+    // Slot k: (min.xyz, nodesSah), (max.xyz, node), (count, next level,
+    // next nodesSah, -).  When the merge retires slot k (step last = k) it
+    // takes the new node instead: (min.xyz, cost), (max.xyz, left child),
+    // (count, next level, next nodesSah, right child).
     float* const dist = sm;
     float4* const lmn = reinterpret_cast<float4*>(sm + Lay::kDistPad);
     float4* const lmx = lmn + Lay::kLeaves;
+    int4* const lcn = reinterpret_cast<int4*>(lmx + Lay::kLeaves);
     if (run && gl < tsize) {
+        const int cnt = ld_cg(nx.sub + s_node);
+        const float nsn = ld_cg(nx.nsn + s_node);
+        const int nlv = is_internal(s_node, n) ? ld_cg(nx.nlv + s_node) : 0;
         lmn[gl] = make_float4(s_mn.x, s_mn.y, s_mn.z, s_sah);
         lmx[gl] = make_float4(s_mx.x, s_mx.y, s_mx.z, __int_as_float(s_node));
+        lcn[gl] = make_int4(cnt, nlv, __float_as_int(nsn), 0);
     }
     __syncwarp();
     if (run) {
@@ -233,13 +260,9 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
 
     // ---- agglomerative merge (AgglomerativeTreelet.cu:476-532) ----
     float my0x = s_mn.x, my0y = s_mn.y, my0z = s_mn.z, my1x = s_mx.x, my1y = s_mx.y, my1z = s_mx.z;
-    int fin_l = -1, fin_r = -1;
-    float fin_la = 0.0f;
-    float f0x = 0.f, f0y = 0.f, f0z = 0.f, f1x = 0.f, f1y = 0.f, f1z = 0.f;
     for (int step = 0; step < maxts - 1; ++step) {
         const int last = tsize - 1 - step;
         const bool act = run && last >= 1;
-        // findMinimumDistance (:83-99) as the minimum of (distance, brev5(j mod 32), j).
         int mi;
         if constexpr (G == 32) {
             // Lane l scans j = l, l + 32, ...; then the minimum distance, then
@@ -292,42 +315,51 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
         }
         const int new_internal = __shfl_sync(kFull, internal_node, gb + (last >= 1 ? last - 1 : 0));
         // updateState (:101-150): the new node (union of rows jr and jc) takes
-        // slot jc, the last leaf moves to slot jr, and lane `last` records the
-        // new node for the final rewrite.
+        // slot jc, the last leaf moves to slot jr, slot `last` retires with
+        // the new node for the final rewrite.
         int jr = 0, jc = 0;
-        float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f, la_new = 0.f;
-        float4 z0 = make_float4(0.f, 0.f, 0.f, 0.f), z1 = z0;
-        int li = -1, ri = -1;
+        float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f;
+        float4 z0 = make_float4(0.f, 0.f, 0.f, 0.f), z1 = z0, nw0 = z0, nw1 = z0;
+        int4 z2 = make_int4(0, 0, 0, 0), nw2 = z2;
         if (act) {
             const uint32_t rc = s_rc[mi];
             jr = (int)(rc >> 8);
             jc = (int)(rc & 255u);
             const float4 r0 = lmn[jr], r1 = lmx[jr], c0 = lmn[jc], c1 = lmx[jc];
+            const int4 r2 = lcn[jr], c2 = lcn[jc];
             z0 = lmn[last];
             z1 = lmx[last];
+            z2 = lcn[last];
             a0x = fminf(c0.x, r0.x); a0y = fminf(c0.y, r0.y); a0z = fminf(c0.z, r0.z);
             a1x = fmaxf(c1.x, r1.x); a1y = fmaxf(c1.y, r1.y); a1z = fmaxf(c1.z, r1.z);
-            la_new = __fadd_rn(__fadd_rn(r0.w, c0.w), __fmul_rn(ci, box_area(a0x, a0y, a0z, a1x, a1y, a1z)));
-            li = __float_as_int(r1.w);
-            ri = __float_as_int(c1.w);
+            const float area_new = box_area(a0x, a0y, a0z, a1x, a1y, a1z);
+            const float la = __fadd_rn(__fadd_rn(r0.w, c0.w), __fmul_rn(ci, area_new));
+            const int cnt = r2.x + c2.x;
+            // Next iteration's nodesSah of the new node (left = row jr).
+            const float nsn = __fadd_rn(__fadd_rn(__fmul_rn(ci, area_new), __int_as_float(r2.z)), __int_as_float(c2.z));
+            nw0 = make_float4(a0x, a0y, a0z, la);
+            nw1 = make_float4(a1x, a1y, a1z, r1.w);  // left child: row jr's node
+            nw2 = make_int4(cnt, cnt >= nx.gamma ? 1 + max(r2.y, c2.y) : 0, __float_as_int(nsn),
+                            __float_as_int(c1.w));  // right child: row jc's node
         }
         __syncwarp();
         if (act) {
             if (gl == jc) {
-                lmn[jc] = make_float4(a0x, a0y, a0z, la_new);
+                lmn[jc] = nw0;
                 lmx[jc] = make_float4(a1x, a1y, a1z, __int_as_float(new_internal));
+                lcn[jc] = make_int4(nw2.x, nw2.y, nw2.z, 0);
                 my0x = a0x; my0y = a0y; my0z = a0z; my1x = a1x; my1y = a1y; my1z = a1z;
             }
             if (gl == jr) {
                 lmn[jr] = z0;
                 lmx[jr] = z1;
+                lcn[jr] = z2;
                 my0x = z0.x; my0y = z0.y; my0z = z0.z; my1x = z1.x; my1y = z1.y; my1z = z1.z;
             }
             if (gl == last) {
-                fin_l = li;
-                fin_r = ri;
-                fin_la = la_new;
-                f0x = a0x; f0y = a0y; f0z = a0z; f1x = a1x; f1y = a1y; f1z = a1z;
+                lmn[last] = nw0;
+                lmx[last] = nw1;
+                lcn[last] = nw2;
             }
         }
         // updateDistancesMatrix (:152-188): row `last` moves to row jr, then the
@@ -346,24 +378,41 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     }
 
     // ---- updateTreelet (:190-212) ----
-    const float la1 = __shfl_sync(kFull, fin_la, gb + 1);
     const int ni = __shfl_sync(kFull, internal_node, gb + (gl > 0 ? gl - 1 : 0));
-    const bool wr = run && la1 < root_sah && gl >= 1 && gl < tsize;
+    const bool accept = run && lmn[1].w < root_sah;
+    const bool wr = accept && gl >= 1 && gl < tsize;
+    int fl = 0, fr = 0;
     if (wr) {
-        Lf[ni] = fin_l;
-        Rt[ni] = fin_r;
-        P[fin_l] = ni;
-        P[fin_r] = ni;
-        NS[ni] = fin_la;
-        const float4 mn = make_float4(f0x, f0y, f0z, 0.0f);
-        const float4 mx = make_float4(f1x, f1y, f1z, 0.0f);
+        const float4 f0 = lmn[gl], f1 = lmx[gl];
+        const int4 f2 = lcn[gl];
+        fl = __float_as_int(f1.w);
+        fr = f2.w;
+        Lf[ni] = fl;
+        Rt[ni] = fr;
+        P[fl] = ni;
+        P[fr] = ni;
+        NS[ni] = f0.w;
+        const float4 mn = make_float4(f0.x, f0.y, f0.z, 0.0f);
+        const float4 mx = make_float4(f1.x, f1.y, f1.z, 0.0f);
         BMN[ni] = mn;
         BMX[ni] = mx;
         AR[ni] = box_area(mn, mx);
+        nx.sub[ni] = f2.x;
+        nx.nlv[ni] = f2.y;
+        nx.nsn[ni] = __int_as_float(f2.z);
     }
     __syncwarp();
     // The rewritten nodes' child records, once every new area is stored.
-    if (wr) KD[ni] = make_int4(fin_l, fin_r, __float_as_int(__ldcg(AR + fin_l)), __float_as_int(__ldcg(AR + fin_r)));
+    if (wr) KD[ni] = make_int4(fl, fr, __float_as_int(__ldcg(AR + fl)), __float_as_int(__ldcg(AR + fr)));
+    // A treelet left as it was: its root's next level and next nodesSah from
+    // its children.
+    if (run && !accept && gl == 0) {
+        const int lc = ld_cg(Lf + root), rc = ld_cg(Rt + root);
+        const int a = is_internal(lc, n) ? ld_cg(nx.nlv + lc) : 0;
+        const int b = is_internal(rc, n) ? ld_cg(nx.nlv + rc) : 0;
+        nx.nlv[root] = ld_cg(nx.sub + root) >= nx.gamma ? 1 + max(a, b) : 0;
+        nx.nsn[root] = __fadd_rn(__fadd_rn(__fmul_rn(ci, ld_cg(AR + root)), ld_cg(nx.nsn + lc)), ld_cg(nx.nsn + rc));
+    }
     __syncwarp();
 }
 
@@ -377,7 +426,10 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                                                    int tsize_all,
                                                    const uint8_t* __restrict__ seg_tsize,
                                                    const uint8_t* __restrict__ seg_iters, int iteration, float ci,
-                                                   float ct, int group_min, uint32_t* err) {
+                                                   float ct, int group_min, const uint2* __restrict__ start,
+                                                   const uint32_t* __restrict__ start_count,
+                                                   int32_t* __restrict__ next_lv, float* __restrict__ nsah_next,
+                                                   uint32_t* err) {
     constexpr int kWarpFloats = warp_floats<G>();
     __shared__ __align__(16) float s_mem[W][kWarpFloats];
     __shared__ uint16_t s_rc[kMaxDist];
@@ -394,7 +446,24 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int cur = -1, base = 0, cbase = 0, tsize = tsize_all;
     uint32_t nm = 2;
-    if (i < segs.n) {
+    // Frontier mode: climb from the frontier below the nodes the level passes
+    // left over (everything under a start node is final); a thread takes the
+    // next start whenever its climb ends, so any frontier size fits the grid.
+    const uint32_t n_start = start ? *start_count : 0u;
+    uint32_t next = i;
+    auto take_start = [&]() {
+        const uint2 e = start[next];
+        next += gridDim.x * blockDim.x;
+        const uint32_t s0 = segs.tri_begin(e.x);
+        nm = segs.tri_end(e.x) - s0;
+        base = segs.node_base(e.x);
+        cbase = segs.inner_base(e.x);
+        tsize = seg_tsize ? (int)seg_tsize[e.x] : tsize_all;
+        cur = g.parent[base + (int)e.y];
+    };
+    if (start) {
+        if (next < n_start) take_start();
+    } else if (i < segs.n) {
         const uint32_t m = segs.seg_of_tri(i);
         const uint32_t s0 = segs.tri_begin(m);
         nm = segs.tri_end(m) - s0;
@@ -405,11 +474,13 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
             const int leaf = base + (int)(i - s0) + (int)nm - 1;
             subtree[leaf] = 1;
             g.nsah[leaf] = __fmul_rn(ct, g.area[leaf]);
+            nsah_next[leaf] = g.nsah[leaf];
             cur = g.parent[leaf];
         }
     }
-    const int gamma = tsize << iteration;
-    while (__any_sync(kFull, cur >= 0)) {
+    while (__any_sync(kFull, cur >= 0 || next < n_start)) {
+        if (cur < 0 && next < n_start) take_start();
+        const int gamma = tsize << iteration;
         bool second = false;
         if (cur >= 0) {
             fence_acq_rel_gpu();
@@ -430,6 +501,10 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
             // Child record for treelet formation: one load yields both
             // children and their areas.
             kids[cbase + cur] = make_int4(lc, rc, __float_as_int(ld_cg(g.area + l)), __float_as_int(ld_cg(g.area + r)));
+            if (cnt < gamma) {  // not a treelet root now, nor next iteration
+                next_lv[cbase + cur] = 0;
+                nsah_next[x] = my_sah;
+            }
         }
         unsigned vote = __ballot_sync(kFull, cnt >= gamma);
         if (vote) __syncwarp();
@@ -448,7 +523,8 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                 const uint32_t rn = __shfl_sync(kFull, nm, rl);
                 const int rts = __shfl_sync(kFull, tsize, rl);
                 const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)rts : 0u);
-                process_group<G>(g, has, rbase, rn, root, kids + rcb, rsah, rts, maxts, ci,
+                const NextRefs nx{subtree + rbase, next_lv + rcb, nsah_next + rbase, rts << (iteration + 1)};
+                process_group<G>(g, has, rbase, rn, root, kids + rcb, nx, rsah, rts, maxts, ci,
                                  &s_mem[w][0] + (grp < NG ? grp : NG - 1) * GroupLayout<G>::kFloats, s_rc, s_prio, err);
 #pragma unroll
                 for (int k = 0; k < NG; ++k) vote &= vote - 1;
@@ -460,8 +536,9 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                 const int rcb = __shfl_sync(kFull, cbase, rl);
                 const uint32_t rn = __shfl_sync(kFull, nm, rl);
                 const int rts = __shfl_sync(kFull, tsize, rl);
-                process_group<32>(g, true, rbase, rn, root, kids + rcb, rsah, rts, rts, ci, &s_mem[w][0], s_rc, s_prio,
-                                  err);
+                const NextRefs nx{subtree + rbase, next_lv + rcb, nsah_next + rbase, rts << (iteration + 1)};
+                process_group<32>(g, true, rbase, rn, root, kids + rcb, nx, rsah, rts, rts, ci, &s_mem[w][0], s_rc,
+                                  s_prio, err);
                 vote &= vote - 1;
             }
         }
@@ -472,13 +549,235 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
 template <int G>
 cudaError_t launch_atrbvh_g(int warps, uint32_t blocks, cudaStream_t s, const TreeRefs& g, const Segs& segs,
                             int32_t* subtree, uint32_t* counters, int4* kids, int tsize, const uint8_t* seg_tsize,
-                            const uint8_t* seg_iters, int it, float ci, float ct, int gmin, uint32_t* err) {
+                            const uint8_t* seg_iters, int it, float ci, float ct, int gmin, const uint2* start,
+                            const uint32_t* start_count, int32_t* next_lv, float* nsah_next, uint32_t* err) {
     switch (warps) {
-        case 2: k_atrbvh<G, 2><<<blocks, 64, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
-        case 8: k_atrbvh<G, 8><<<blocks, 256, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
-        default: k_atrbvh<G, 4><<<blocks, 128, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, err); break;
+        case 2: k_atrbvh<G, 2><<<blocks, 64, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, nsah_next, err); break;
+        case 8: k_atrbvh<G, 8><<<blocks, 256, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, nsah_next, err); break;
+        default: k_atrbvh<G, 4><<<blocks, 128, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, nsah_next, err); break;
     }
     return cudaGetLastError();
+}
+
+// ---- level passes ---------------------------------------------------------------
+// A node whose subtree holds at least gamma triangles ("big") is a treelet
+// root; its results depend only on its subtree, so any order that finishes a
+// node's big descendants first gives the reference's result.  The level of a
+// big node is 1 + the largest level of its big children (0 for the others).
+// Phase A (k_levels) climbs once from every leaf and finishes every node that
+// is not big (subtree count, nodesSah, child record) and levels the big ones;
+// phase B sorts big nodes of levels 1..L into per-level lists; phase C
+// restructures each level's treelets at once, one thread per treelet; the
+// dataflow kernel then climbs from the frontier below the levels above L.
+
+struct LevelRefs {
+    int32_t* subtree;
+    uint32_t* counters;
+    int4* kids;
+    int32_t* level;        // per internal node (inner-indexed): this iteration's levels
+    int32_t* next;         // the next iteration's levels, filled as nodes are finished
+    float* nsah;           // this iteration's nodesSah (node-indexed)
+    float* nsah_next;      // the next iteration's nodesSah
+    uint32_t* hist;        // [L + 2]: level histogram, then per-level offsets
+    uint32_t* cursor;      // [L + 2]
+    uint2* order;          // (mesh, local node) of big nodes by level
+    uint2* frontier;       // climb starts of the dataflow pass
+    uint32_t* n_frontier;
+};
+
+__global__ void __launch_bounds__(256) k_levels(TreeRefs g, Segs segs, LevelRefs lv, int tsize_all,
+                                                const uint8_t* __restrict__ seg_tsize,
+                                                const uint8_t* __restrict__ seg_iters, int iteration, float ci,
+                                                float ct, int L) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= segs.n) return;
+    const uint32_t m = segs.seg_of_tri(i);
+    if (seg_iters && iteration >= (int)seg_iters[m]) return;
+    const uint32_t s0 = segs.tri_begin(m);
+    const uint32_t n = segs.tri_end(m) - s0;
+    const int base = segs.node_base(m), cb = segs.inner_base(m);
+    const int gamma = (seg_tsize ? (int)seg_tsize[m] : tsize_all) << iteration;
+    const int leaf = base + (int)(i - s0) + (int)n - 1;
+    lv.subtree[leaf] = 1;
+    g.nsah[leaf] = __fmul_rn(ct, g.area[leaf]);
+    lv.nsah_next[leaf] = g.nsah[leaf];
+    int cur = g.parent[leaf];
+    while (cur >= 0) {
+        if (atomic_add_acq_rel_gpu(&lv.counters[cb + cur], 1u) == 0u) return;
+        const int x = base + cur;
+        const int lc = ld_cg(g.left + x), rc = ld_cg(g.right + x);
+        const int l = base + lc, r = base + rc;
+        const int cnt = ld_cg(lv.subtree + l) + ld_cg(lv.subtree + r);
+        lv.subtree[x] = cnt;
+        lv.kids[cb + cur] = make_int4(lc, rc, __float_as_int(ld_cg(g.area + l)), __float_as_int(ld_cg(g.area + r)));
+        if (cnt < gamma) {
+            const float v = __fadd_rn(__fadd_rn(__fmul_rn(ci, ld_cg(g.area + x)), ld_cg(g.nsah + l)), ld_cg(g.nsah + r));
+            g.nsah[x] = v;
+            lv.nsah_next[x] = v;
+            lv.level[cb + cur] = 0;
+            lv.next[cb + cur] = 0;
+        } else {
+            const int ll = is_internal(lc, n) ? ld_cg(lv.level + cb + lc) : 0;
+            const int lr = is_internal(rc, n) ? ld_cg(lv.level + cb + rc) : 0;
+            const int me = 1 + max(ll, lr);
+            lv.level[cb + cur] = me;
+            if (me <= L) {
+                atomicAdd(&lv.hist[me], 1u);
+            } else {
+                // A node left to the dataflow pass: its children that the
+                // level passes finish become climb starts.
+                if (ll <= L) lv.frontier[atomicAdd(lv.n_frontier, 1u)] = make_uint2(m, (uint32_t)lc);
+                if (lr <= L) lv.frontier[atomicAdd(lv.n_frontier, 1u)] = make_uint2(m, (uint32_t)rc);
+            }
+        }
+        cur = g.parent[x];
+    }
+}
+
+// Phase A of iterations after the first: the previous iteration left every
+// internal node's level for this one (next levels of the nodes it finished,
+// kept current by treelet rewrites), and subtree counts, nodesSah and child
+// records that are already final for nodes that are not treelet roots now.
+// Count the levels, mark this iteration's non-roots as non-roots for the next
+// one too, and list the frontier below the levels above L.
+__global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, const uint8_t* __restrict__ seg_iters,
+                                                    int iteration, int L) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int me = 0, push = 0;
+    uint32_t m = 0;
+    uint2 ent[2];
+    if (i < segs.n) {
+        m = segs.seg_of_tri(i);
+        const uint32_t s0 = segs.tri_begin(m);
+        const uint32_t n = segs.tri_end(m) - s0;
+        const uint32_t li = i - s0;
+        if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
+            const int cb = segs.inner_base(m), nb = segs.node_base(m);
+            me = lv.level[cb + (int)li];
+            if (me == 0) {
+                lv.next[cb + (int)li] = 0;
+                lv.nsah_next[nb + (int)li] = lv.nsah[nb + (int)li];
+            } else if (me > L) {
+                const int lc = lv.kids[cb + (int)li].x, rc = lv.kids[cb + (int)li].y;
+                if ((is_internal(lc, n) ? lv.level[cb + lc] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)lc);
+                if ((is_internal(rc, n) ? lv.level[cb + rc] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)rc);
+                me = 0;
+            }
+        }
+    }
+    // One atomic per level present in the warp, one for the frontier.
+    const uint32_t peers = __match_any_sync(kFull, me);
+    const int leader = __ffs(peers) - 1;
+    if (me > 0 && (threadIdx.x & 31) == leader) atomicAdd(&lv.hist[me], (uint32_t)__popc(peers));
+    uint32_t incl = push;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, incl, o);
+        if ((threadIdx.x & 31) >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    uint32_t at = 0;
+    if ((threadIdx.x & 31) == 31 && total) at = atomicAdd(lv.n_frontier, total);
+    at = __shfl_sync(kFull, at, 31) + incl - push;
+    for (int k = 0; k < push; ++k) lv.frontier[at + k] = ent[k];
+}
+
+// Exclusive scan of the level histogram into offsets (one small block).
+__global__ void k_level_offsets(LevelRefs lv, int L) {
+    if (threadIdx.x != 0) return;
+    uint32_t run = 0;
+    for (int l = 0; l <= L + 1; ++l) {
+        const uint32_t c = lv.hist[l];
+        lv.hist[l] = run;
+        lv.cursor[l] = 0;
+        run += c;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, const uint8_t* __restrict__ seg_iters,
+                                                       int iteration, int L) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int me = 0;
+    uint32_t m = 0, li = 0;
+    if (i < segs.n) {
+        m = segs.seg_of_tri(i);
+        const uint32_t s0 = segs.tri_begin(m);
+        const uint32_t n = segs.tri_end(m) - s0;
+        li = i - s0;
+        if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
+            me = lv.level[segs.inner_base(m) + (int)li];
+            if (me > L) me = 0;
+        }
+    }
+    // One atomic per level present in the warp.
+    const uint32_t peers = __match_any_sync(kFull, me);
+    const int leader = __ffs(peers) - 1;
+    uint32_t at = 0;
+    if (me > 0 && (threadIdx.x & 31) == leader) at = atomicAdd(&lv.cursor[me], (uint32_t)__popc(peers));
+    at = __shfl_sync(kFull, at, leader);
+    if (me > 0) lv.order[lv.hist[me] + at + __popc(peers & lanemask_lt())] = make_uint2(m, li);
+}
+
+// Phase C: every treelet root of level `lev`; each warp takes 32/G roots at a
+// time, one per lane group (the list is dense, so the groups stay full).
+template <int G, int W>
+__global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Segs segs, LevelRefs lv, int lev,
+                                                                 int tsize_all, const uint8_t* __restrict__ seg_tsize,
+                                                                 int iteration, float ci, uint32_t* err) {
+    constexpr int NG = GroupLayout<G>::kGroups;
+    __shared__ __align__(16) float s_mem[W][GroupLayout<G>::kFloats * NG];
+    __shared__ uint16_t s_rc[kMaxDist];
+    __shared__ __align__(4) uint8_t s_prio[(kMaxTreelet + 1) * 32];
+    for (int k = threadIdx.x; k < kMaxDist; k += blockDim.x) {
+        int r, c;
+        trm_rc(k, r, c);
+        s_rc[k] = (uint16_t)((r << 8) | c);
+    }
+    for (int k = threadIdx.x; k < (kMaxTreelet + 1) * 8; k += blockDim.x)
+        reinterpret_cast<uint32_t*>(s_prio)[k] = reinterpret_cast<const uint32_t*>(&g_argmax_priority.rank[0][0])[k];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int grp = lane / G;
+    const uint32_t beg = lv.hist[lev], end = lv.hist[lev + 1];
+    const uint32_t warp = blockIdx.x * W + w, nwarps = gridDim.x * W;
+    for (uint32_t e0 = beg + warp * NG; e0 < end; e0 += nwarps * NG) {
+        const uint32_t e = e0 + (uint32_t)grp;
+        const bool has = grp < NG && e < end;
+        int nb = 0, x = 0, tsize = 0;
+        uint32_t n = 2;
+        int4* kd = lv.kids;
+        int32_t* nl = lv.next;
+        float root_sah = 0.0f;
+        if (has) {
+            const uint2 q = lv.order[e];
+            const uint32_t s0 = segs.tri_begin(q.x);
+            n = segs.tri_end(q.x) - s0;
+            nb = segs.node_base(q.x);
+            kd = lv.kids + segs.inner_base(q.x);
+            nl = lv.next + segs.inner_base(q.x);
+            x = (int)q.y;
+            tsize = seg_tsize ? (int)seg_tsize[q.x] : tsize_all;
+            const int4 k = __ldcg(kd + x);
+            root_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, __ldcg(g.area + nb + x)), __ldcg(g.nsah + nb + k.x)),
+                                 __ldcg(g.nsah + nb + k.y));
+            if (lane == grp * G) g.nsah[nb + x] = root_sah;
+        }
+        const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)tsize : 0u);
+        __syncwarp();
+        const NextRefs nx{lv.subtree + nb, nl, lv.nsah_next + nb, tsize << (iteration + 1)};
+        process_group<G>(g, has, nb, n, x, kd, nx, root_sah, tsize, maxts, ci,
+                         &s_mem[w][0] + (grp < NG ? grp : NG - 1) * GroupLayout<G>::kFloats, s_rc, s_prio, err);
+    }
+}
+
+template <int G>
+void launch_level_g(int warps, unsigned blocks, cudaStream_t s, const TreeRefs& g, const Segs& segs,
+                    const LevelRefs& lv, int lev, int tsize, const uint8_t* seg_tsize, int it, float ci,
+                    uint32_t* err) {
+    switch (warps) {
+        case 2: k_level_groups<G, 2><<<blocks, 64, 0, s>>>(g, segs, lv, lev, tsize, seg_tsize, it, ci, err); break;
+        case 8: k_level_groups<G, 8><<<blocks, 256, 0, s>>>(g, segs, lv, lev, tsize, seg_tsize, it, ci, err); break;
+        default: k_level_groups<G, 4><<<blocks, 128, 0, s>>>(g, segs, lv, lev, tsize, seg_tsize, it, ci, err); break;
+    }
 }
 
 }  // namespace
@@ -496,31 +795,90 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
                float ct) {
     if (iterations <= 0) return ATR_OK;
     const size_t inner = segs.n - segs.count;
+    const int max_ts = seg_tsize ? max_tsize : tsize;
+    const int L = ctx->atr_levels;
     void* scratch = nullptr;
     const size_t b_sub = align256(total_nodes * 4), b_sah = align256(total_nodes * 4), b_ctr = align256(inner * 4);
     const size_t b_kid = align256(inner * 16);
-    ATR_TRY(ctx->alloc(&scratch, b_sub + b_sah + b_ctr + b_kid));
+    // Big nodes of levels 1..L number at most the internal nodes; frontier
+    // nodes root disjoint subtrees, so they number at most the triangles.
+    // Two level arrays: this iteration's and the next one's.
+    const size_t b_lvl = align256(inner * 4), b_ord = L ? align256(inner * 8) : 0;
+    const size_t b_front = L ? align256((size_t)segs.n * 8) : 0;
+    const size_t b_small = L ? align256((size_t)(2 * (L + 2) + 1) * 4) : 0;
+    ATR_TRY(ctx->alloc(&scratch, b_sub + 2 * b_sah + b_ctr + b_kid + 2 * b_lvl + b_ord + b_front + b_small));
     char* p = static_cast<char*>(scratch);
-    int32_t* subtree = reinterpret_cast<int32_t*>(p);
+    int32_t* subtree = reinterpret_cast<int32_t*>(p); p += b_sub;
     TreeRefs g = g_in;
-    g.nsah = reinterpret_cast<float*>(p + b_sub);
-    uint32_t* counters = reinterpret_cast<uint32_t*>(p + b_sub + b_sah);
-    int4* kids = reinterpret_cast<int4*>(p + b_sub + b_sah + b_ctr);
+    float* ns[2];  // nodesSah: this iteration's and the next one's
+    ns[0] = reinterpret_cast<float*>(p); p += b_sah;
+    ns[1] = reinterpret_cast<float*>(p); p += b_sah;
+    uint32_t* counters = reinterpret_cast<uint32_t*>(p); p += b_ctr;
+    int4* kids = reinterpret_cast<int4*>(p); p += b_kid;
+    int32_t* lvl[2];
+    lvl[0] = reinterpret_cast<int32_t*>(p); p += b_lvl;
+    lvl[1] = reinterpret_cast<int32_t*>(p); p += b_lvl;
+    LevelRefs lv{};
+    lv.subtree = subtree;
+    lv.counters = counters;
+    lv.kids = kids;
+    if (L) {
+        lv.order = reinterpret_cast<uint2*>(p); p += b_ord;
+        lv.frontier = reinterpret_cast<uint2*>(p); p += b_front;
+        lv.hist = reinterpret_cast<uint32_t*>(p);
+        lv.cursor = lv.hist + (L + 2);
+        lv.n_frontier = lv.cursor + (L + 2);
+    }
     const int warps = ctx->atr_warps == 2 || ctx->atr_warps == 8 ? ctx->atr_warps : 4;
     const int threads = warps * 32;
-    const uint32_t blocks = (segs.n + threads - 1) / threads;
-    const int gw = atrbvh_group_width(seg_tsize ? max_tsize : tsize);
+    const uint32_t leaf_blocks = (segs.n + threads - 1) / threads;
+    const uint32_t front_blocks = (uint32_t)ctx->num_sms * (256 / threads) * 4;  // grid-stride over the frontier
+    const int gw = atrbvh_group_width(max_ts);
     const int gmin = ctx->atr_group_min < 2 ? 2 : ctx->atr_group_min;
+    cudaStream_t st = ctx->stream;
     cudaError_t e = cudaSuccess;
     ctx->phase_begin("atrbvh");
     for (int it = 0; it < iterations && e == cudaSuccess; ++it) {
-        e = cudaMemsetAsync(counters, 0, inner * 4, ctx->stream);
+        lv.level = lvl[it & 1];
+        lv.next = lvl[(it + 1) & 1];
+        g.nsah = lv.nsah = ns[it & 1];
+        lv.nsah_next = ns[(it + 1) & 1];
+        int32_t* const next_lv = lv.next;
+        e = cudaMemsetAsync(counters, 0, inner * 4, st);
+        const uint2* start = nullptr;
+        const uint32_t* start_count = nullptr;
+        uint32_t blocks = leaf_blocks;
+        if (L && e == cudaSuccess) {
+            e = cudaMemsetAsync(lv.hist, 0, b_small, st);
+            const unsigned gb = (segs.n + 255) / 256;
+            if (it == 0)
+                k_levels<<<gb, 256, 0, st>>>(g, segs, lv, tsize, seg_tsize, seg_iters, it, ci, ct, L);
+            else
+                k_level_hist<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
+            k_level_offsets<<<1, 32, 0, st>>>(lv, L);
+            k_level_scatter<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
+            ctx->launches += 3;
+            const unsigned lg = (unsigned)ctx->num_sms * (256 / threads) * 4;
+            for (int lev = 1; lev <= L; ++lev) {
+                switch (gw) {
+                    case 8: launch_level_g<8>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
+                    case 10: launch_level_g<10>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
+                    case 16: launch_level_g<16>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
+                    default: launch_level_g<32>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
+                }
+                ++ctx->launches;
+            }
+            if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, inner * 4, st);
+            start = lv.frontier;
+            start_count = lv.n_frontier;
+            blocks = front_blocks;
+        }
         if (e != cudaSuccess) break;
         switch (gw) {
-            case 8: e = launch_atrbvh_g<8>(warps, blocks, ctx->stream, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
-            case 10: e = launch_atrbvh_g<10>(warps, blocks, ctx->stream, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
-            case 16: e = launch_atrbvh_g<16>(warps, blocks, ctx->stream, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
-            default: e = launch_atrbvh_g<32>(warps, blocks, ctx->stream, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, ctx->d_error); break;
+            case 8: e = launch_atrbvh_g<8>(warps, blocks, st, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, lv.nsah_next, ctx->d_error); break;
+            case 10: e = launch_atrbvh_g<10>(warps, blocks, st, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, lv.nsah_next, ctx->d_error); break;
+            case 16: e = launch_atrbvh_g<16>(warps, blocks, st, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, lv.nsah_next, ctx->d_error); break;
+            default: e = launch_atrbvh_g<32>(warps, blocks, st, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, lv.nsah_next, ctx->d_error); break;
         }
         ++ctx->launches;
     }
@@ -529,6 +887,9 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     if (e != cudaSuccess) return cuda_fail(e, "k_atrbvh launch", __FILE__, __LINE__);
     return ATR_OK;
 }
+
+// Kernel attributes (once per context); none are needed at present.
+int atrbvh_prepare() { return ATR_OK; }
 
 }  // namespace atr
 

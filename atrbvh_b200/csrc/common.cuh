@@ -34,6 +34,14 @@ __device__ __forceinline__ float ld_cg(const float* p) { return __ldcg(p); }
 // loads; lighter than the sequentially consistent __threadfence().
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
+// Atomic add with acquire-release semantics at GPU scope: one instruction in
+// place of fence, relaxed atomic, fence on the bottom-up arrival counters.
+__device__ __forceinline__ uint32_t atomic_add_acq_rel_gpu(uint32_t* p, uint32_t v) {
+    uint32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

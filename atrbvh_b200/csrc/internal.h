@@ -67,6 +67,9 @@ struct atr_ctx {
     // Radix sort digit width of LBVH builds: 8 (4 passes for 30-bit codes)
     // or 10 (3 passes).
     int sort_bits = 8;
+    // ATRBVH levels restructured by the level passes (one thread per
+    // treelet) before the dataflow pass takes the rest; 0 = dataflow only.
+    int atr_levels = 16;
     struct Phase {
         std::string name;
         cudaEvent_t a, b;
@@ -174,6 +177,7 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_n
                int max_tsize, int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci,
                float ct);
 int atrbvh_group_width(int max_tsize);
+int atrbvh_prepare();  // kernel attributes; once per context
 int trbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int iterations,
               const uint8_t* seg_iters, float ci, float ct);
 

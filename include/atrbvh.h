@@ -110,8 +110,17 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
  *                           (2..32; 33 = never; default 2).
  *   ATR_TUNE_SORT_BITS      radix-sort digit width of LBVH builds: 8 (default;
  *                           4 passes over 30-bit codes, 8 over 63-bit) or 10
- *                           (3 and 7 passes). */
-enum atr_tune_knob { ATR_TUNE_ATR_WARPS = 0, ATR_TUNE_ATR_GROUP_MIN = 1, ATR_TUNE_SORT_BITS = 2 };
+ *                           (3 and 7 passes).
+ *   ATR_TUNE_ATR_LEVELS     ATRBVH levels of treelet roots restructured level
+ *                           by level, one thread per treelet (0..64; default
+ *                           16; 0 = all by the bottom-up warp pass); used when
+ *                           every treelet size is at most 10. */
+enum atr_tune_knob {
+    ATR_TUNE_ATR_WARPS = 0,
+    ATR_TUNE_ATR_GROUP_MIN = 1,
+    ATR_TUNE_SORT_BITS = 2,
+    ATR_TUNE_ATR_LEVELS = 3
+};
 int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value);
 int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value);
 /* Number of kernels this context has enqueued since it was created. */
