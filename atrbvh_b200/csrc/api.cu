@@ -28,11 +28,11 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
 
 int tree_alloc(atr_ctx* ctx, uint32_t n, atr_tree** out) {
     const size_t nn = 2 * (size_t)n - 1;
-    const size_t b4 = align256(nn * 4), b16 = align256(nn * 16);
+    const size_t b4 = align256(nn * 4), b16 = align256(nn * 16), b8 = align256((size_t)(n - 1) * 8);
     atr_tree* t = new atr_tree();
     t->ctx = ctx;
     t->n = n;
-    int s = ctx->alloc(&t->block, 5 * b4 + 2 * b16);
+    int s = ctx->alloc(&t->block, 5 * b4 + 2 * b16 + b8);
     if (s != ATR_OK) { delete t; return s; }
     char* p = static_cast<char*>(t->block);
     t->parent = reinterpret_cast<int32_t*>(p); p += b4;
@@ -41,7 +41,8 @@ int tree_alloc(atr_ctx* ctx, uint32_t n, atr_tree** out) {
     t->data = reinterpret_cast<int32_t*>(p); p += b4;
     t->area = reinterpret_cast<float*>(p); p += b4;
     t->bmin = reinterpret_cast<float4*>(p); p += b16;
-    t->bmax = reinterpret_cast<float4*>(p);
+    t->bmax = reinterpret_cast<float4*>(p); p += b16;
+    t->range = reinterpret_cast<int2*>(p);
     *out = t;
     return ATR_OK;
 }

@@ -585,10 +585,24 @@ struct LevelRefs {
     uint32_t* n_frontier;
 };
 
-__global__ void __launch_bounds__(256) k_levels(TreeRefs g, Segs segs, LevelRefs lv, int tsize_all,
-                                                const uint8_t* __restrict__ seg_tsize,
-                                                const uint8_t* __restrict__ seg_iters, int iteration, float ci,
-                                                float ct, int L) {
+constexpr int kLvBlock = 512;  // threads (leaves) per block of the phase-A climb
+
+// Phase A of the first iteration: one climb from every leaf (sorted order)
+// that finishes the nodes that are not treelet roots and levels the roots.
+// With the radix tree's leaf ranges (a tree straight from the LBVH build), a
+// node whose range lies inside the block's leaves is reached only by threads
+// of the block, so its arrival counter and the first child's summary live in
+// shared memory under block-scope ordering; only nodes whose range crosses a
+// block boundary use a device-scope acquire-release atomic in global memory.
+// Without ranges every node takes the global path.
+__global__ void __launch_bounds__(kLvBlock) k_levels(TreeRefs g, Segs segs, LevelRefs lv, int tsize_all,
+                                                     const uint8_t* __restrict__ seg_tsize,
+                                                     const uint8_t* __restrict__ seg_iters, int iteration, float ci,
+                                                     float ct, int L, const int2* __restrict__ ranges) {
+    __shared__ uint32_t s_ctr[kLvBlock];
+    __shared__ int4 s_rec[kLvBlock][2];  // per local node and side: (count, level, nodesSah, area)
+    for (int k = threadIdx.x; k < kLvBlock; k += blockDim.x) s_ctr[k] = 0;
+    __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= segs.n) return;
     const uint32_t m = segs.seg_of_tri(i);
@@ -597,32 +611,72 @@ __global__ void __launch_bounds__(256) k_levels(TreeRefs g, Segs segs, LevelRefs
     const uint32_t n = segs.tri_end(m) - s0;
     const int base = segs.node_base(m), cb = segs.inner_base(m);
     const int gamma = (seg_tsize ? (int)seg_tsize[m] : tsize_all) << iteration;
-    const int leaf = base + (int)(i - s0) + (int)n - 1;
+    const int64_t blo = (int64_t)blockIdx.x * blockDim.x, bhi = blo + blockDim.x - 1;
+    const int li = (int)(i - s0);
+    const int leaf = base + li + (int)n - 1;
+    // Summary of the subtree this thread has just finished (the leaf first).
+    const float la = g.area[leaf];
+    int my_cnt = 1, my_lvl = 0, my_first = li, child = li + (int)n - 1;
+    float my_nsah = __fmul_rn(ct, la), my_area = la;
     lv.subtree[leaf] = 1;
-    g.nsah[leaf] = __fmul_rn(ct, g.area[leaf]);
-    lv.nsah_next[leaf] = g.nsah[leaf];
+    g.nsah[leaf] = my_nsah;
+    lv.nsah_next[leaf] = my_nsah;
     int cur = g.parent[leaf];
     while (cur >= 0) {
-        if (atomic_add_acq_rel_gpu(&lv.counters[cb + cur], 1u) == 0u) return;
         const int x = base + cur;
+        int sib_cnt, sib_lvl;
+        float sib_nsah, sib_area;
+        bool local = false;
+        if (ranges) {
+            const int2 rg = ranges[cb + cur];
+            local = (int64_t)s0 + rg.x >= blo && (int64_t)s0 + rg.y <= bhi;
+            if (local) {
+                // Internal node cur covers [rg.x, rg.y] and is numbered by one
+                // of its ends, so its slot lies inside the block.
+                const int slot = (int)((int64_t)s0 + cur - blo);
+                const int side = my_first == rg.x ? 0 : 1;
+                s_rec[slot][side] = make_int4(my_cnt, my_lvl, __float_as_int(my_nsah), __float_as_int(my_area));
+                __threadfence_block();
+                if (atomicAdd(&s_ctr[slot], 1u) == 0u) return;
+                __threadfence_block();
+                const int4 r = s_rec[slot][side ^ 1];
+                sib_cnt = r.x;
+                sib_lvl = r.y;
+                sib_nsah = __int_as_float(r.z);
+                sib_area = __int_as_float(r.w);
+                my_first = rg.x;
+            }
+        }
         const int lc = ld_cg(g.left + x), rc = ld_cg(g.right + x);
-        const int l = base + lc, r = base + rc;
-        const int cnt = ld_cg(lv.subtree + l) + ld_cg(lv.subtree + r);
+        const int sib = lc == child ? rc : lc;
+        if (!local) {
+            if (atomic_add_acq_rel_gpu(&lv.counters[cb + cur], 1u) == 0u) return;
+            sib_cnt = ld_cg(lv.subtree + base + sib);
+            sib_lvl = is_internal(sib, n) ? ld_cg(lv.level + cb + sib) : 0;
+            sib_nsah = ld_cg(g.nsah + base + sib);
+            sib_area = ld_cg(g.area + base + sib);
+            if (ranges) my_first = min(my_first, ranges[cb + cur].x);
+        }
+        const bool mine_left = lc == child;
+        const int cnt = my_cnt + sib_cnt;
+        const float a = ld_cg(g.area + x);
         lv.subtree[x] = cnt;
-        lv.kids[cb + cur] = make_int4(lc, rc, __float_as_int(ld_cg(g.area + l)), __float_as_int(ld_cg(g.area + r)));
+        lv.kids[cb + cur] = make_int4(lc, rc, __float_as_int(mine_left ? my_area : sib_area),
+                                      __float_as_int(mine_left ? sib_area : my_area));
+        int lvl = 0;
+        float ns = 0.0f;
         if (cnt < gamma) {
-            const float v = __fadd_rn(__fadd_rn(__fmul_rn(ci, ld_cg(g.area + x)), ld_cg(g.nsah + l)), ld_cg(g.nsah + r));
-            g.nsah[x] = v;
-            lv.nsah_next[x] = v;
+            ns = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), mine_left ? my_nsah : sib_nsah), mine_left ? sib_nsah : my_nsah);
+            g.nsah[x] = ns;
+            lv.nsah_next[x] = ns;
             lv.level[cb + cur] = 0;
             lv.next[cb + cur] = 0;
         } else {
-            const int ll = is_internal(lc, n) ? ld_cg(lv.level + cb + lc) : 0;
-            const int lr = is_internal(rc, n) ? ld_cg(lv.level + cb + rc) : 0;
-            const int me = 1 + max(ll, lr);
-            lv.level[cb + cur] = me;
-            if (me <= L) {
-                atomicAdd(&lv.hist[me], 1u);
+            const int ll = mine_left ? my_lvl : sib_lvl, lr = mine_left ? sib_lvl : my_lvl;
+            lvl = 1 + max(ll, lr);
+            lv.level[cb + cur] = lvl;
+            if (lvl <= L) {
+                atomicAdd(&lv.hist[lvl], 1u);
             } else {
                 // A node left to the dataflow pass: its children that the
                 // level passes finish become climb starts.
@@ -630,6 +684,11 @@ __global__ void __launch_bounds__(256) k_levels(TreeRefs g, Segs segs, LevelRefs
                 if (lr <= L) lv.frontier[atomicAdd(lv.n_frontier, 1u)] = make_uint2(m, (uint32_t)rc);
             }
         }
+        my_cnt = cnt;
+        my_lvl = lvl;
+        my_nsah = ns;  // only read while the climb stays below the treelet roots (cnt < gamma)
+        my_area = a;
+        child = cur;
         cur = g.parent[x];
     }
 }
@@ -792,7 +851,7 @@ int atrbvh_group_width(int max_tsize) {
 // case `iterations` is their maximum and max_tsize the largest per-mesh size.
 int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t total_nodes, int tsize,
                int max_tsize, int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci,
-               float ct) {
+               float ct, const int2* karras_ranges) {
     if (iterations <= 0) return ATR_OK;
     const size_t inner = segs.n - segs.count;
     const int max_ts = seg_tsize ? max_tsize : tsize;
@@ -852,7 +911,9 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
             e = cudaMemsetAsync(lv.hist, 0, b_small, st);
             const unsigned gb = (segs.n + 255) / 256;
             if (it == 0)
-                k_levels<<<gb, 256, 0, st>>>(g, segs, lv, tsize, seg_tsize, seg_iters, it, ci, ct, L);
+                k_levels<<<(segs.n + kLvBlock - 1) / kLvBlock, kLvBlock, 0, st>>>(g, segs, lv, tsize, seg_tsize,
+                                                                                  seg_iters, it, ci, ct, L,
+                                                                                  karras_ranges);
             else
                 k_level_hist<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
             k_level_offsets<<<1, 32, 0, st>>>(lv, L);
@@ -904,5 +965,7 @@ extern "C" int atr_optimize_atrbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int 
     const uint32_t n = tree->n;
     TreeRefs g{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nullptr};
     Segs segs{nullptr, nullptr, 1u, n};
-    return atrbvh_run(ctx, g, segs, 2 * (size_t)n - 1, tsize, tsize, iterations, nullptr, nullptr, ci, ct);
+    const int2* ranges = tree->karras ? tree->range : nullptr;
+    if (iterations > 0) tree->karras = false;
+    return atrbvh_run(ctx, g, segs, 2 * (size_t)n - 1, tsize, tsize, iterations, nullptr, nullptr, ci, ct, ranges);
 }

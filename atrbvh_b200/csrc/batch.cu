@@ -118,7 +118,7 @@ int batch_run(atr_ctx* ctx, atr_batch* b, int optimizer, int tsize, int iteratio
     const int iters = b->per_mesh_params ? b->max_iters : iterations;
     if (optimizer == 1)
         return atrbvh_run(ctx, g, segs, b->total_nodes, tsize, b->per_mesh_params ? b->max_tsize : tsize, iters, ts, it,
-                          ci, ct);
+                          ci, ct, b->tree.range);
     if (optimizer == 2) return trbvh_run(ctx, g, segs, b->total_nodes, iters, it, ci, ct);
     return ATR_OK;
 }
@@ -157,7 +157,8 @@ int atr_batch_create(atr_ctx* ctx, const float* vertices, const uint32_t* tri_of
     int st = ctx->alloc(&b->meta, 2 * off_b + 2 * par_b + 2 * bnd_b);
     if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&b->verts), n * 48);
     const size_t nn = b->total_nodes, b4 = align256(nn * 4), b16 = align256(nn * 16);
-    if (st == ATR_OK) st = ctx->alloc(&b->block, 5 * b4 + 2 * b16);
+    const size_t b8 = align256((size_t)(n - count) * 8);
+    if (st == ATR_OK) st = ctx->alloc(&b->block, 5 * b4 + 2 * b16 + b8);
     if (st != ATR_OK) { atr_batch_destroy(b); return st; }
     char* p = static_cast<char*>(b->meta);
     b->d_tri_off = reinterpret_cast<uint32_t*>(p); p += off_b;
@@ -173,7 +174,8 @@ int atr_batch_create(atr_ctx* ctx, const float* vertices, const uint32_t* tri_of
     b->tree.data = reinterpret_cast<int32_t*>(q); q += b4;
     b->tree.area = reinterpret_cast<float*>(q); q += b4;
     b->tree.bmin = reinterpret_cast<float4*>(q); q += b16;
-    b->tree.bmax = reinterpret_cast<float4*>(q);
+    b->tree.bmax = reinterpret_cast<float4*>(q); q += b16;
+    b->tree.range = reinterpret_cast<int2*>(q);
     cudaStream_t s = ctx->stream;
     cudaMemcpyAsync(b->d_tri_off, b->h_tri_off.data(), (count + 1) * 4ull, cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(b->d_tile_off, b->h_tile_off.data(), (count + 1) * 4ull, cudaMemcpyHostToDevice, s);

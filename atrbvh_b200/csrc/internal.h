@@ -100,6 +100,10 @@ struct atr_tree {
     int32_t *parent = nullptr, *left = nullptr, *right = nullptr, *data = nullptr;
     float4 *bmin = nullptr, *bmax = nullptr;
     float* area = nullptr;
+    // Leaf ranges of the internal nodes, valid while `karras` (the topology is
+    // the LBVH build's own; optimisers clear it).
+    int2* range = nullptr;
+    bool karras = false;
     // Sort output kept from the build (keys as stored: uint32 or uint64).
     void* sorted_keys = nullptr;
     uint32_t* sorted_idx = nullptr;
@@ -135,6 +139,9 @@ struct TreeOut {
     int32_t *parent, *left, *right, *data;
     float4 *bmin, *bmax;
     float* area;
+    // Leaf range (first, last sorted leaf, local) of every internal node of a
+    // freshly built radix tree; written by the LBVH build when not NULL.
+    int2* range = nullptr;
 };
 
 // Collapsed-tree arrays (possibly batched: per-mesh node slices, per-mesh
@@ -175,7 +182,7 @@ int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4
                     uint32_t** keep_idx);
 int atrbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int tsize,
                int max_tsize, int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci,
-               float ct);
+               float ct, const int2* karras_ranges = nullptr);
 int atrbvh_group_width(int max_tsize);
 int atrbvh_prepare();  // kernel attributes; once per context
 int trbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int iterations,

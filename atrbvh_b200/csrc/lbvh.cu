@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ 
                                                 int32_t* __restrict__ left_all, int32_t* __restrict__ right_all,
                                                 int32_t* __restrict__ data_all, float4* __restrict__ bmin_all,
                                                 float4* __restrict__ bmax_all, float* __restrict__ area_all,
-                                                int32_t* __restrict__ slot_all) {
+                                                int32_t* __restrict__ slot_all, int2* __restrict__ range_all) {
     const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
     if (gi >= segs.n) return;
     const uint32_t m = segs.seg_of_tri(gi);
@@ -427,6 +427,7 @@ __global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ 
         left[p] = lc;
         right[p] = rc;
         data[p] = -1;
+        if (range_all) range_all[segs.inner_base(m) + p] = make_int2(pl, pr);
         parent[lc] = p;
         parent[rc] = p;
         bmin[p] = mn;
@@ -589,7 +590,7 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
     if (st == ATR_OK) {
         ctx->phase_begin("build");
         k_build<K><<<(n + 255) / 256, 256, 0, s>>>(segs, keys, idx, verts, t.parent, t.left, t.right, t.data, t.bmin,
-                                                  t.bmax, t.area, slot);
+                                                  t.bmax, t.area, slot, t.range);
         ctx->phase_end();
         ctx->launches += 1;
         cudaError_t e = cudaGetLastError();
@@ -639,7 +640,7 @@ int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* 
     t->morton_bits = morton_bits;
     Segs segs{nullptr, nullptr, 1u, n};
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
-    TreeOut out{t->parent, t->left, t->right, t->data, t->bmin, t->bmax, t->area};
+    TreeOut out{t->parent, t->left, t->right, t->data, t->bmin, t->bmax, t->area, t->range};
     void* keys = nullptr;
     uint32_t* idx = nullptr;
     ATR_TRY(lbvh_build_segs(ctx, segs, tiles, verts, d_bounds, morton_bits, out, &keys, &idx));
@@ -647,6 +648,7 @@ int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* 
     ctx->release(t->sorted_idx);
     t->sorted_keys = keys;
     t->sorted_idx = idx;
+    t->karras = true;
     return ATR_OK;
 }
 

@@ -354,5 +354,6 @@ extern "C" int atr_optimize_trbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int i
     const uint32_t n = tree->n;
     TreeRefs g{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nullptr};
     Segs segs{nullptr, nullptr, 1u, n};
+    tree->karras = false;
     return trbvh_run(ctx, g, segs, 2 * (size_t)n - 1, iterations, nullptr, ci, ct);
 }
