@@ -43,8 +43,18 @@ METRIC = "ATRBVH build Mtri/s at equal SAH, batched vs plain; Mrays/s; p99 laten
 WORKLOAD = ("clustered scene 4,194,304 tris (75% 64-Gaussian mixture, 25% 1024x512 ground-plane quads): "
             "LBVH 30-bit + ATRBVH(9,2) + collapse + Compact2, closest-hit trace of 1920x1080 primary "
             "rays + 1 diffuse bounce per hit")
-# Algorithmic bytes per triangle (reference data types) per HBM-bound phase.
-BYTES_PER_TRI = {"morton": 56.0, "sort": 4.0 + 16.0 * 4, "build": 40.0 + 180.0}
+# Algorithmic bytes per triangle (reference data types) per phase: Morton reads
+# 48 B and writes key + index; each of the 4 sort passes reads and writes key +
+# index after a 4-B histogram read; Karras build 40 B + refit 180 B; each ATRBVH
+# iteration reads every node's parent/left/right/area/box once (48 B x 2 nodes),
+# writes subtree count and nodesSah (8 B x 2) and a child record and counter per
+# internal node (24 B).
+BYTES_PER_TRI = {"morton": 56.0, "sort": 4.0 + 16.0 * 4, "build": 40.0 + 180.0, "atrbvh": 2 * 136.0}
+# DRAM bytes per triangle of the ATRBVH phase (both iterations) from the ncu
+# capture in profiles/launches_clustered4M_bench_step.md (2,097,152 triangles:
+# k_levels 140.8 MB, k_level_hist 18.4, k_level_scatter 16.8, k_level_groups
+# 2009.2, k_atrbvh 3.9), scaled by triangle count.
+ATRBVH_DRAM_BYTES_PER_TRI = (140.8 + 18.4 + 16.8 + 2009.2 + 3.9) * 1e6 / 2097152
 
 
 def _read_peaks() -> dict:
@@ -265,25 +275,19 @@ def run_ours(args, world, rank, local):
     for k, bpt in BYTES_PER_TRI.items():
         if ph_ms.get(k):
             roof[k] = n_tris * bpt / (ph_ms[k] * 1e-3) / 1e9
-    # Dominant phase by time (trace counted per launch).
+    # The dominant phase by time is ATRBVH: its kernels (phase A climb, level
+    # lists, one launch per treelet level, dataflow top) are issue- and
+    # latency-bound, so its HBM fraction is small; traffic is the ncu DRAM
+    # bytes of the same phase scaled to this triangle count.
     times = {k: (v2 / n_trace if k == "trace" and n_trace else v2) for k, v2 in ph_ms.items()}
     dominant = max(times, key=times.get)
-    if dominant in roof:
-        achieved = roof[dominant]
-        rl = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-              "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_src": peaks["src"]}
-    else:
-        # Latency/issue-bound phase: bytes it must move (tree arrays read once, written once).
-        if dominant == "atrbvh":
-            bpt = 2 * 52.0  # 52 B of SoA per node, ~2 nodes per triangle, read + write once
-        elif dominant == "trace":
-            bpt = 0.0
-        else:
-            bpt = 0.0
-        achieved = (n_tris * bpt / (times[dominant] * 1e-3) / 1e9) if bpt else 0.0
-        rl = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-              "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_src": peaks["src"],
-              "note": "latency/issue-bound phase; HBM fraction shown for reference"}
+    achieved = roof.get(dominant, 0.0)
+    rl = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+          "frac": achieved / peaks["hbm_gbs"], "peak_src": peaks["src"],
+          "traffic": (n_tris * ATRBVH_DRAM_BYTES_PER_TRI / 1e9 if dominant == "atrbvh" else None),
+          "traffic_unit": "GB per step (ncu DRAM bytes, scaled)",
+          "algorithmic_gb": n_tris * BYTES_PER_TRI.get(dominant, 0.0) / 1e9,
+          "note": "issue/latency-bound phase (ncu: ~50-70% issue active, long-scoreboard stalls)"}
     out = {
         "metric": METRIC,
         "value": world * n_tris / (build_ms_max * 1e-3) / 1e6,
