@@ -570,6 +570,8 @@ cudaError_t launch_atrbvh_g(int warps, uint32_t blocks, cudaStream_t s, const Tr
 // restructures each level's treelets at once, one thread per treelet; the
 // dataflow kernel then climbs from the frontier below the levels above L.
 
+constexpr int kMaxLevels = 64;  // largest L (ATR_TUNE_ATR_LEVELS)
+
 struct LevelRefs {
     int32_t* subtree;
     uint32_t* counters;
@@ -672,17 +674,8 @@ __global__ void __launch_bounds__(kLvBlock) k_levels(TreeRefs g, Segs segs, Leve
             lv.level[cb + cur] = 0;
             lv.next[cb + cur] = 0;
         } else {
-            const int ll = mine_left ? my_lvl : sib_lvl, lr = mine_left ? sib_lvl : my_lvl;
-            lvl = 1 + max(ll, lr);
+            lvl = 1 + max(my_lvl, sib_lvl);
             lv.level[cb + cur] = lvl;
-            if (lvl <= L) {
-                atomicAdd(&lv.hist[lvl], 1u);
-            } else {
-                // A node left to the dataflow pass: its children that the
-                // level passes finish become climb starts.
-                if (ll <= L) lv.frontier[atomicAdd(lv.n_frontier, 1u)] = make_uint2(m, (uint32_t)lc);
-                if (lr <= L) lv.frontier[atomicAdd(lv.n_frontier, 1u)] = make_uint2(m, (uint32_t)rc);
-            }
         }
         my_cnt = cnt;
         my_lvl = lvl;
@@ -690,6 +683,63 @@ __global__ void __launch_bounds__(kLvBlock) k_levels(TreeRefs g, Segs segs, Leve
         my_area = a;
         child = cur;
         cur = g.parent[x];
+    }
+}
+
+// Phase A of the first iteration on a tree straight from the LBVH build,
+// which left every node's nodesSah for the default constants: subtree counts
+// come from the radix tree's leaf ranges, so a streaming pass (one thread per
+// leaf and internal node) writes counts and child records, finishes the nodes
+// that are not treelet roots, and starts a climb at every treelet root whose
+// children are not roots (level 1).  The climbs visit treelet roots only and
+// wait at a root only when both of its children are roots.
+__global__ void __launch_bounds__(256) k_levels_pp(TreeRefs g, Segs segs, LevelRefs lv, const int2* __restrict__ ranges,
+                                                   int tsize_all, const uint8_t* __restrict__ seg_tsize,
+                                                   const uint8_t* __restrict__ seg_iters, int iteration) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= segs.n) return;
+    const uint32_t m = segs.seg_of_tri(i);
+    if (seg_iters && iteration >= (int)seg_iters[m]) return;
+    const uint32_t s0 = segs.tri_begin(m);
+    const uint32_t n = segs.tri_end(m) - s0;
+    const int base = segs.node_base(m), cb = segs.inner_base(m);
+    const int gamma = (seg_tsize ? (int)seg_tsize[m] : tsize_all) << iteration;
+    const int li = (int)(i - s0);
+    const int leaf = base + li + (int)n - 1;
+    lv.subtree[leaf] = 1;
+    lv.nsah_next[leaf] = g.nsah[leaf];
+    if (li >= (int)n - 1) return;
+    auto count = [&](int c) {
+        if (!is_internal(c, n)) return 1;
+        const int2 r = ranges[cb + c];
+        return r.y - r.x + 1;
+    };
+    int x = li;
+    const int lc = g.left[base + x], rc = g.right[base + x];
+    const int cnt = count(x);
+    lv.subtree[base + x] = cnt;
+    lv.kids[cb + x] = make_int4(lc, rc, __float_as_int(g.area[base + lc]), __float_as_int(g.area[base + rc]));
+    if (cnt < gamma) {
+        lv.level[cb + x] = 0;
+        lv.next[cb + x] = 0;
+        lv.nsah_next[base + x] = g.nsah[base + x];
+        return;
+    }
+    if (count(lc) >= gamma || count(rc) >= gamma) return;  // not a level-1 root: reached by a climb
+    int lvl = 1;
+    while (true) {
+        lv.level[cb + x] = lvl;
+        const int p = g.parent[base + x];
+        if (p < 0) return;
+        const int pl = g.left[base + p];
+        const int o = pl == x ? g.right[base + p] : pl;
+        int olvl = 0;
+        if (count(o) >= gamma) {
+            if (atomic_add_acq_rel_gpu(&lv.counters[cb + p], 1u) == 0u) return;
+            olvl = ld_cg(lv.level + cb + o);
+        }
+        lvl = 1 + max(lvl, olvl);
+        x = p;
     }
 }
 
@@ -701,8 +751,11 @@ __global__ void __launch_bounds__(kLvBlock) k_levels(TreeRefs g, Segs segs, Leve
 // one too, and list the frontier below the levels above L.
 __global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, const uint8_t* __restrict__ seg_iters,
                                                     int iteration, int L) {
+    __shared__ uint32_t s_hist[kMaxLevels + 2];
+    for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_hist[k] = 0;
+    __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    int me = 0, push = 0;
+    int push = 0;
     uint32_t m = 0;
     uint2 ent[2];
     if (i < segs.n) {
@@ -712,22 +765,20 @@ __global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, con
         const uint32_t li = i - s0;
         if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
             const int cb = segs.inner_base(m), nb = segs.node_base(m);
-            me = lv.level[cb + (int)li];
+            const int me = lv.level[cb + (int)li];
             if (me == 0) {
                 lv.next[cb + (int)li] = 0;
                 lv.nsah_next[nb + (int)li] = lv.nsah[nb + (int)li];
-            } else if (me > L) {
-                const int lc = lv.kids[cb + (int)li].x, rc = lv.kids[cb + (int)li].y;
-                if ((is_internal(lc, n) ? lv.level[cb + lc] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)lc);
-                if ((is_internal(rc, n) ? lv.level[cb + rc] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)rc);
-                me = 0;
+            } else if (me <= L) {
+                atomicAdd(&s_hist[me], 1u);
+            } else {
+                const int4 kd = lv.kids[cb + (int)li];
+                if ((is_internal(kd.x, n) ? lv.level[cb + kd.x] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)kd.x);
+                if ((is_internal(kd.y, n) ? lv.level[cb + kd.y] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)kd.y);
             }
         }
     }
-    // One atomic per level present in the warp, one for the frontier.
-    const uint32_t peers = __match_any_sync(kFull, me);
-    const int leader = __ffs(peers) - 1;
-    if (me > 0 && (threadIdx.x & 31) == leader) atomicAdd(&lv.hist[me], (uint32_t)__popc(peers));
+    // Frontier entries: one atomic per warp.
     uint32_t incl = push;
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(kFull, incl, o);
@@ -738,6 +789,10 @@ __global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, con
     if ((threadIdx.x & 31) == 31 && total) at = atomicAdd(lv.n_frontier, total);
     at = __shfl_sync(kFull, at, 31) + incl - push;
     for (int k = 0; k < push; ++k) lv.frontier[at + k] = ent[k];
+    // Level counts: one global atomic per level present in the block.
+    __syncthreads();
+    for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
+        if (s_hist[k]) atomicAdd(&lv.hist[k], s_hist[k]);
 }
 
 // Exclusive scan of the level histogram into offsets (one small block).
@@ -754,9 +809,13 @@ __global__ void k_level_offsets(LevelRefs lv, int L) {
 
 __global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, const uint8_t* __restrict__ seg_iters,
                                                        int iteration, int L) {
+    __shared__ uint32_t s_cnt[kMaxLevels + 2];
+    __shared__ uint32_t s_base[kMaxLevels + 2];
+    for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_cnt[k] = 0;
+    __syncthreads();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int me = 0;
-    uint32_t m = 0, li = 0;
+    uint32_t m = 0, li = 0, rank = 0;
     if (i < segs.n) {
         m = segs.seg_of_tri(i);
         const uint32_t s0 = segs.tri_begin(m);
@@ -767,13 +826,13 @@ __global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, 
             if (me > L) me = 0;
         }
     }
-    // One atomic per level present in the warp.
-    const uint32_t peers = __match_any_sync(kFull, me);
-    const int leader = __ffs(peers) - 1;
-    uint32_t at = 0;
-    if (me > 0 && (threadIdx.x & 31) == leader) at = atomicAdd(&lv.cursor[me], (uint32_t)__popc(peers));
-    at = __shfl_sync(kFull, at, leader);
-    if (me > 0) lv.order[lv.hist[me] + at + __popc(peers & lanemask_lt())] = make_uint2(m, li);
+    if (me > 0) rank = atomicAdd(&s_cnt[me], 1u);
+    __syncthreads();
+    // One global reservation per level present in the block.
+    for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
+        s_base[k] = s_cnt[k] ? atomicAdd(&lv.cursor[k], s_cnt[k]) : 0u;
+    __syncthreads();
+    if (me > 0) lv.order[lv.hist[me] + s_base[me] + rank] = make_uint2(m, li);
 }
 
 // Phase C: every treelet root of level `lev`; each warp takes 32/G roots at a
@@ -851,7 +910,7 @@ int atrbvh_group_width(int max_tsize) {
 // case `iterations` is their maximum and max_tsize the largest per-mesh size.
 int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t total_nodes, int tsize,
                int max_tsize, int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci,
-               float ct, const int2* karras_ranges) {
+               float ct, const int2* karras_ranges, const BuildPrepass* prepass) {
     if (iterations <= 0) return ATR_OK;
     const size_t inner = segs.n - segs.count;
     const int max_ts = seg_tsize ? max_tsize : tsize;
@@ -865,15 +924,23 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     const size_t b_lvl = align256(inner * 4), b_ord = L ? align256(inner * 8) : 0;
     const size_t b_front = L ? align256((size_t)segs.n * 8) : 0;
     const size_t b_small = L ? align256((size_t)(2 * (L + 2) + 1) * 4) : 0;
-    ATR_TRY(ctx->alloc(&scratch, b_sub + 2 * b_sah + b_ctr + b_kid + 2 * b_lvl + b_ord + b_front + b_small));
+    // The build's prepass (counts, first nodesSah, child records) serves as
+    // those arrays when its constants are this pass's.
+    const bool use_pp = prepass && prepass->nsah && karras_ranges && L > 0 && ci == kPrepassCi && ct == kPrepassCt;
+    ATR_TRY(ctx->alloc(&scratch, b_sub + (use_pp ? 1 : 2) * b_sah + b_kid + b_ctr + 2 * b_lvl + b_ord + b_front +
+                                     b_small));
     char* p = static_cast<char*>(scratch);
-    int32_t* subtree = reinterpret_cast<int32_t*>(p); p += b_sub;
     TreeRefs g = g_in;
+    int32_t* subtree = reinterpret_cast<int32_t*>(p); p += b_sub;
+    int4* kids = reinterpret_cast<int4*>(p); p += b_kid;
     float* ns[2];  // nodesSah: this iteration's and the next one's
-    ns[0] = reinterpret_cast<float*>(p); p += b_sah;
+    if (use_pp) {
+        ns[0] = prepass->nsah;
+    } else {
+        ns[0] = reinterpret_cast<float*>(p); p += b_sah;
+    }
     ns[1] = reinterpret_cast<float*>(p); p += b_sah;
     uint32_t* counters = reinterpret_cast<uint32_t*>(p); p += b_ctr;
-    int4* kids = reinterpret_cast<int4*>(p); p += b_kid;
     int32_t* lvl[2];
     lvl[0] = reinterpret_cast<int32_t*>(p); p += b_lvl;
     lvl[1] = reinterpret_cast<int32_t*>(p); p += b_lvl;
@@ -910,12 +977,17 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         if (L && e == cudaSuccess) {
             e = cudaMemsetAsync(lv.hist, 0, b_small, st);
             const unsigned gb = (segs.n + 255) / 256;
-            if (it == 0)
+            if (it == 0 && use_pp)
+                k_levels_pp<<<gb, 256, 0, st>>>(g, segs, lv, karras_ranges, tsize, seg_tsize, seg_iters, it);
+            else if (it == 0)
                 k_levels<<<(segs.n + kLvBlock - 1) / kLvBlock, kLvBlock, 0, st>>>(g, segs, lv, tsize, seg_tsize,
                                                                                   seg_iters, it, ci, ct, L,
                                                                                   karras_ranges);
-            else
-                k_level_hist<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
+            // Level counts and the frontier of the dataflow pass (after the
+            // first iteration's climb, or from the levels the previous
+            // iteration left).
+            k_level_hist<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
+            ctx->launches += 1;
             k_level_offsets<<<1, 32, 0, st>>>(lv, L);
             k_level_scatter<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
             ctx->launches += 3;
@@ -966,6 +1038,14 @@ extern "C" int atr_optimize_atrbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int 
     TreeRefs g{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nullptr};
     Segs segs{nullptr, nullptr, 1u, n};
     const int2* ranges = tree->karras ? tree->range : nullptr;
-    if (iterations > 0) tree->karras = false;
-    return atrbvh_run(ctx, g, segs, 2 * (size_t)n - 1, tsize, tsize, iterations, nullptr, nullptr, ci, ct, ranges);
+    const BuildPrepass* pp = tree->prepass_block ? &tree->prepass : nullptr;
+    if (iterations <= 0) return ATR_OK;
+    tree->karras = false;
+    const int st = atrbvh_run(ctx, g, segs, 2 * (size_t)n - 1, tsize, tsize, iterations, nullptr, nullptr, ci, ct,
+                              ranges, pp);
+    // The prepass arrays served as this pass's scratch; they are stale now.
+    ctx->release(tree->prepass_block);
+    tree->prepass_block = nullptr;
+    tree->prepass = BuildPrepass{};
+    return st;
 }

@@ -111,14 +111,26 @@ __global__ void k_seg_bounds_init(uint32_t count, uint32_t* __restrict__ enc) {
 
 int batch_run(atr_ctx* ctx, atr_batch* b, int optimizer, int tsize, int iterations, float ci, float ct) {
     const Segs segs{b->d_tri_off, b->d_tile_off, b->count, b->n};
-    ATR_TRY(lbvh_build_segs(ctx, segs, b->tiles, b->verts, b->d_bounds, 30, b->tree, nullptr, nullptr));
+    // The LBVH climb leaves its prepass for ATRBVH's first iteration.
+    void* ppb = nullptr;
+    BuildPrepass pp{};
+    const bool want_pp = optimizer == 1 && (b->per_mesh_params ? b->max_iters : iterations) > 0 &&
+                         ctx->atr_levels > 0 && ci == kPrepassCi && ct == kPrepassCt;
+    if (want_pp) ATR_TRY(prepass_alloc(ctx, b->total_nodes, b->n - b->count, &ppb, &pp));
+    int st = lbvh_build_segs(ctx, segs, b->tiles, b->verts, b->d_bounds, 30, b->tree, nullptr, nullptr,
+                             want_pp ? &pp : nullptr);
+    if (st != ATR_OK) { ctx->release(ppb); return st; }
     TreeRefs g{b->n, b->tree.parent, b->tree.left, b->tree.right, b->tree.bmin, b->tree.bmax, b->tree.area, nullptr};
     const uint8_t* ts = b->per_mesh_params ? b->d_tsize : nullptr;
     const uint8_t* it = b->per_mesh_params ? b->d_iters : nullptr;
     const int iters = b->per_mesh_params ? b->max_iters : iterations;
-    if (optimizer == 1)
-        return atrbvh_run(ctx, g, segs, b->total_nodes, tsize, b->per_mesh_params ? b->max_tsize : tsize, iters, ts, it,
-                          ci, ct, b->tree.range);
+    if (optimizer == 1) {
+        st = atrbvh_run(ctx, g, segs, b->total_nodes, tsize, b->per_mesh_params ? b->max_tsize : tsize, iters, ts, it,
+                        ci, ct, b->tree.range, want_pp ? &pp : nullptr);
+        ctx->release(ppb);
+        return st;
+    }
+    ctx->release(ppb);
     if (optimizer == 2) return trbvh_run(ctx, g, segs, b->total_nodes, iters, it, ci, ct);
     return ATR_OK;
 }

@@ -49,6 +49,16 @@ constexpr int kNumSms = 148;  // B200
 // Round up to a multiple of 256 bytes (alignment of every sub-array).
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// What the LBVH build's climb leaves for the first ATRBVH iteration: every
+// node's nodesSah under the reference's default constants, node-indexed in
+// the batch layout (NULL: not computed).  Subtree counts follow from the
+// radix tree's leaf ranges.
+struct BuildPrepass {
+    float* nsah = nullptr;
+};
+constexpr float kPrepassCi = 1.2f;  // AgglomerativeTreelet.h:75 defaults
+constexpr float kPrepassCt = 1.0f;
+
 }  // namespace atr
 
 struct atr_ctx {
@@ -104,6 +114,10 @@ struct atr_tree {
     // the LBVH build's own; optimisers clear it).
     int2* range = nullptr;
     bool karras = false;
+    // Prepass arrays of the last LBVH build for the first ATRBVH iteration
+    // (released by the first optimiser or refit that makes them stale).
+    void* prepass_block = nullptr;
+    atr::BuildPrepass prepass{};
     // Sort output kept from the build (keys as stored: uint32 or uint64).
     void* sorted_keys = nullptr;
     uint32_t* sorted_idx = nullptr;
@@ -179,10 +193,14 @@ int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* 
 // sorted keys and global triangle order.
 int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts,
                     const float* d_bounds, int morton_bits, const TreeOut& out, void** keep_keys,
-                    uint32_t** keep_idx);
+                    uint32_t** keep_idx, const BuildPrepass* prepass = nullptr);
+// Allocate the prepass arrays for total_nodes nodes and inner internal nodes
+// in one block (*block receives the allocation).
+int prepass_alloc(atr_ctx* ctx, size_t total_nodes, size_t inner, void** block, BuildPrepass* pp);
+
 int atrbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int tsize,
                int max_tsize, int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci,
-               float ct, const int2* karras_ranges = nullptr);
+               float ct, const int2* karras_ranges = nullptr, const BuildPrepass* prepass = nullptr);
 int atrbvh_group_width(int max_tsize);
 int atrbvh_prepare();  // kernel attributes; once per context
 int trbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int iterations,

@@ -368,7 +368,8 @@ __global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ 
                                                 int32_t* __restrict__ left_all, int32_t* __restrict__ right_all,
                                                 int32_t* __restrict__ data_all, float4* __restrict__ bmin_all,
                                                 float4* __restrict__ bmax_all, float* __restrict__ area_all,
-                                                int32_t* __restrict__ slot_all, int2* __restrict__ range_all) {
+                                                int32_t* __restrict__ slot_all, int2* __restrict__ range_all,
+                                                BuildPrepass pp) {
     const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
     if (gi >= segs.n) return;
     const uint32_t m = segs.seg_of_tri(gi);
@@ -396,7 +397,12 @@ __global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ 
     data[leaf] = (int32_t)(gtri - s0);
     bmin[leaf] = mn;
     bmax[leaf] = mx;
-    area[leaf] = box_area(mn, mx);
+    const float my_area = box_area(mn, mx);
+    area[leaf] = my_area;
+    // Prepass for the first ATRBVH iteration: this subtree's nodesSah under the
+    // default constants, (ci*A + left) + right bottom-up from ct*A at leaves.
+    float my_ns = __fmul_rn(kPrepassCt, my_area);
+    if (pp.nsah) pp.nsah[nb + leaf] = my_ns;
 
     const int last = (int)n - 1;
     int l = (int)i, r = (int)i;
@@ -432,7 +438,13 @@ __global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ 
         parent[rc] = p;
         bmin[p] = mn;
         bmax[p] = mx;
-        area[p] = box_area(mn, mx);
+        const float pa = box_area(mn, mx);
+        area[p] = pa;
+        if (pp.nsah) {
+            const float sns = ld_cg(pp.nsah + nb + sib);
+            my_ns = __fadd_rn(__fadd_rn(__fmul_rn(kPrepassCi, pa), is_left ? my_ns : sns), is_left ? sns : my_ns);
+            pp.nsah[nb + p] = my_ns;
+        }
         if (root) {
             parent[0] = -1;
             return;
@@ -560,7 +572,7 @@ int sort_pairs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, K** keys, uint32_
 
 template <typename K, int BITS>
 int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts, const float* d_bounds,
-                const TreeOut& t, void** keep_keys, uint32_t** keep_idx) {
+                const TreeOut& t, void** keep_keys, uint32_t** keep_idx, const BuildPrepass* prepass) {
     constexpr int P = SortPlan<K, BITS>::kPasses, D = SortPlan<K, BITS>::kDigits;
     const uint32_t n = segs.n;
     cudaStream_t s = ctx->stream;
@@ -590,7 +602,8 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
     if (st == ATR_OK) {
         ctx->phase_begin("build");
         k_build<K><<<(n + 255) / 256, 256, 0, s>>>(segs, keys, idx, verts, t.parent, t.left, t.right, t.data, t.bmin,
-                                                  t.bmax, t.area, slot, t.range);
+                                                  t.bmax, t.area, slot, t.range,
+                                                  prepass ? *prepass : BuildPrepass{});
         ctx->phase_end();
         ctx->launches += 1;
         cudaError_t e = cudaGetLastError();
@@ -626,13 +639,21 @@ int lbvh_prepare() {
 }
 
 int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts, const float* d_bounds,
-                    int morton_bits, const TreeOut& out, void** keep_keys, uint32_t** keep_idx) {
+                    int morton_bits, const TreeOut& out, void** keep_keys, uint32_t** keep_idx,
+                    const BuildPrepass* pp) {
     const bool ten = ctx->sort_bits == 10;
     if (morton_bits == 30)
-        return ten ? build_typed<uint32_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx)
-                   : build_typed<uint32_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx);
-    return ten ? build_typed<uint64_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx)
-               : build_typed<uint64_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx);
+        return ten ? build_typed<uint32_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp)
+                   : build_typed<uint32_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp);
+    return ten ? build_typed<uint64_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp)
+               : build_typed<uint64_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp);
+}
+
+int prepass_alloc(atr_ctx* ctx, size_t total_nodes, size_t inner, void** block, BuildPrepass* pp) {
+    (void)inner;
+    ATR_TRY(ctx->alloc(block, total_nodes * 4));
+    pp->nsah = static_cast<float*>(*block);
+    return ATR_OK;
 }
 
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds, int morton_bits,
@@ -643,7 +664,14 @@ int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* 
     TreeOut out{t->parent, t->left, t->right, t->data, t->bmin, t->bmax, t->area, t->range};
     void* keys = nullptr;
     uint32_t* idx = nullptr;
-    ATR_TRY(lbvh_build_segs(ctx, segs, tiles, verts, d_bounds, morton_bits, out, &keys, &idx));
+    // The prepass is kept with the tree for a following ATRBVH (level passes on).
+    ctx->release(t->prepass_block);
+    t->prepass_block = nullptr;
+    t->prepass = BuildPrepass{};
+    if (ctx->atr_levels > 0)
+        ATR_TRY(prepass_alloc(ctx, 2 * (size_t)n - 1, n - 1, &t->prepass_block, &t->prepass));
+    ATR_TRY(lbvh_build_segs(ctx, segs, tiles, verts, d_bounds, morton_bits, out, &keys, &idx,
+                            t->prepass_block ? &t->prepass : nullptr));
     ctx->release(t->sorted_keys);
     ctx->release(t->sorted_idx);
     t->sorted_keys = keys;
@@ -739,6 +767,10 @@ int atr_refit(atr_ctx* ctx, atr_tree* tree, const atr_scene* scene) {
     ATR_REQUIRE(ctx && tree && scene, ATR_ERR_INVALID_ARG, "atr_refit: NULL argument");
     ATR_REQUIRE(tree->n == scene->n, ATR_ERR_INVALID_ARG, "atr_refit: tree has %u triangles, scene %u",
                 tree->n, scene->n);
+    // New boxes make the build's prepass (areas, costs) stale.
+    ctx->release(tree->prepass_block);
+    tree->prepass_block = nullptr;
+    tree->prepass = BuildPrepass{};
     const TreeOut t{tree->parent, tree->left, tree->right, tree->data, tree->bmin, tree->bmax, tree->area};
     return refit_arrays(ctx, tree->n, t, scene->verts);
 }

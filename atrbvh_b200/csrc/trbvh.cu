@@ -355,5 +355,8 @@ extern "C" int atr_optimize_trbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int i
     TreeRefs g{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nullptr};
     Segs segs{nullptr, nullptr, 1u, n};
     tree->karras = false;
+    ctx->release(tree->prepass_block);
+    tree->prepass_block = nullptr;
+    tree->prepass = BuildPrepass{};
     return trbvh_run(ctx, g, segs, 2 * (size_t)n - 1, iterations, nullptr, ci, ct);
 }
