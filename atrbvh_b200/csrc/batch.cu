@@ -345,7 +345,7 @@ static int batch_alloc_outputs(atr_ctx* ctx, atr_batch* b) {
     }
     if (!b->cp_block) {
         const size_t bn = align256((n - b->count) * 64), bw = align256(n * 64), bt = align256(n * 16);
-        const size_t bs = align256(b->count * 16ull);
+        const size_t bs = align256(b->count * 16ull + 8);
         ATR_TRY(ctx->alloc(&b->cp_block, bn + bw + bt + bs));
         char* p = static_cast<char*>(b->cp_block);
         b->cp_nodes = reinterpret_cast<int4*>(p); p += bn;
@@ -387,11 +387,14 @@ int atr_batch_flatten(atr_ctx* ctx, atr_batch* b) {
     ATR_REQUIRE(b->col_block, ATR_ERR_INVALID_ARG, "atr_batch_flatten: collapse the batch first");
     const Segs segs{b->d_tri_off, b->d_tile_off, b->count, b->n};
     ctx->phase_begin("flatten");
-    int st = flatten_segs(ctx, segs, b->col, b->verts, b->cp_nodes, b->cp_woop, b->cp_tri, b->d_sizes, &b->max_depth);
+    int st = flatten_segs(ctx, segs, b->col, b->verts, b->cp_nodes, b->cp_woop, b->cp_tri, b->d_sizes);
     ctx->phase_end();
     ATR_TRY(st);
-    b->h_sizes.resize(2ull * b->count);
-    ATR_CUDA(cudaMemcpy(b->h_sizes.data(), b->d_sizes, b->h_sizes.size() * 8, cudaMemcpyDeviceToHost));
+    b->h_sizes.resize(2ull * b->count + 1);
+    ATR_CUDA(cudaMemcpyAsync(b->h_sizes.data(), b->d_sizes, b->h_sizes.size() * 8, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    ATR_CUDA(cudaStreamSynchronize(ctx->stream));
+    b->max_depth = (int32_t)b->h_sizes[2ull * b->count];
     b->flattened = true;
     return ATR_OK;
 }
@@ -476,15 +479,14 @@ int batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* ver
     const Segs one{nullptr, nullptr, 1u, n};
     const CollapsedOut c{b->col.parent + nb, b->col.left + nb, b->col.right + nb, b->col.data + nb,
                          b->col.count + nb, b->col.bmin + nb, b->col.bmax + nb, b->col.tri_indices + s0};
-    // sizes: Compact2 node and Woop counts, then (when asked) the SAH parts.
+    // sizes: Compact2 node and Woop counts, depth, then (when asked) the SAH parts.
     int64_t* sizes = nullptr;
     ATR_TRY(ctx->alloc(reinterpret_cast<void**>(&sizes), 32));
-    float* parts = h_sah ? reinterpret_cast<float*>(sizes + 2) : nullptr;
+    float* parts = h_sah ? reinterpret_cast<float*>(sizes + 3) : nullptr;
     int st = collapse_segs(ctx, one, 2 * (size_t)n - 1, t, c, b->col_ci, b->col_ct, b->col_max_leaf, parts);
-    int32_t depth = 0;
     if (st == ATR_OK)
         st = flatten_segs(ctx, one, c, b->verts + 3 * s0, b->cp_nodes + 4 * (s0 - mesh), b->cp_woop + 4 * s0,
-                          b->cp_tri + 4 * s0, sizes, &depth);
+                          b->cp_tri + 4 * s0, sizes);
     int64_t h[4] = {0, 0, 0, 0};
     if (st == ATR_OK) {
         cudaError_t e = cudaMemcpyAsync(h, sizes, 32, cudaMemcpyDeviceToHost, ctx->stream);
@@ -495,12 +497,12 @@ int batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* ver
     ATR_TRY(st);
     if (h_sah) {
         float p[2];
-        std::memcpy(p, h + 2, 8);
+        std::memcpy(p, h + 3, 8);
         *h_sah = p[0] / p[1];
     }
     b->h_sizes[mesh] = h[0];
     b->h_sizes[b->count + mesh] = h[1];
-    b->max_depth = std::max(b->max_depth, depth);
+    b->max_depth = std::max(b->max_depth, (int32_t)h[2]);
     return ATR_OK;
 }
 

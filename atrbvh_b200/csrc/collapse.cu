@@ -25,6 +25,7 @@ namespace {
 
 struct CollapseRefs {
     uint32_t n;
+    const float* area;
     const int32_t* parent;
     const int32_t* left;
     const int32_t* right;
@@ -43,9 +44,24 @@ struct CollapseRefs {
     uint32_t* emit_cnt;
 };
 
+// The collapsed tree starts as a copy of the tree (TreeCollapser.cu:13-30):
+// a streaming pass over every node of every mesh (data is -1 at internal
+// nodes in both).
+__global__ void __launch_bounds__(256) k_collapse_copy(CollapseRefs g, uint64_t total_nodes) {
+    const uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (x >= total_nodes) return;
+    g.c_parent[x] = g.parent[x];
+    g.c_left[x] = g.left[x];
+    g.c_right[x] = g.right[x];
+    g.c_data[x] = g.data[x];
+    g.c_bmin[x] = g.bmin[x];
+    g.c_bmax[x] = g.bmax[x];
+}
+
 // Segmented: thread i starts at the i-th leaf of the batch; node arrays are
 // addressed from the mesh's first node (local indices); each mesh's lists
-// live in its own slice [tri_begin, tri_end) of tri_indices.
+// live in its own slice [tri_begin, tri_end) of tri_indices.  A node's area
+// is its box's surface area (the tree's area array).
 __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs, uint32_t* __restrict__ counters,
                                                         float ci, float ct, int max_leaf) {
     const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
@@ -58,15 +74,8 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
     const int leaf = (int)(gi - s0) + (int)n - 1;
     {
         const int x = nb + leaf;
-        const float4 mn = g.bmin[x], mx = g.bmax[x];
-        g.c_parent[x] = g.parent[x];
-        g.c_left[x] = g.left[x];
-        g.c_right[x] = g.right[x];
-        g.c_data[x] = g.data[x];
-        g.c_bmin[x] = mn;
-        g.c_bmax[x] = mx;
         g.c_count[x] = 1;
-        g.cost[x] = __fmul_rn(ct, box_area(mn, mx));
+        g.cost[x] = __fmul_rn(ct, g.area[x]);
         g.pass[x] = 1;
     }
     int cur = g.parent[nb + leaf];
@@ -79,9 +88,8 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
         const int cl = ld_cg(g.c_count + nb + l), cr = ld_cg(g.c_count + nb + r);
         const float kl = ld_cg(g.cost + nb + l), kr = ld_cg(g.cost + nb + r);
         const int pl = ld_cg(g.pass + nb + l), pr = ld_cg(g.pass + nb + r);
-        const float4 mn = g.bmin[x], mx = g.bmax[x];
         const int cnt = cl + cr;
-        const float a = box_area(mn, mx);
+        const float a = g.area[x];
         float c = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), kl), kr);
         const float leaf_cost = __fmul_rn(__fmul_rn(ct, a), (float)cnt);
         const bool col = leaf_cost < c && (max_leaf <= 0 || cnt <= max_leaf);
@@ -91,12 +99,6 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
             if (cl > 1) g.emit_cnt[nb + l] = (uint32_t)cl;
             if (cr > 1) g.emit_cnt[nb + r] = (uint32_t)cr;
         }
-        g.c_parent[x] = g.parent[x];
-        g.c_left[x] = l;
-        g.c_right[x] = r;
-        g.c_data[x] = -1;
-        g.c_bmin[x] = mn;
-        g.c_bmax[x] = mx;
         g.c_count[x] = cnt;
         g.cost[x] = c;
         g.pass[x] = reached && col;
@@ -180,11 +182,12 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
     cudaMemsetAsync(emit, 0, nn * 4, s);
     cudaMemsetAsync(counters, 0, inner * 4, s);
     cudaMemsetAsync(dst.tri_indices, 0xff, (size_t)n * 4, s);
-    CollapseRefs r{n, src.parent, src.left, src.right, src.data, src.bmin, src.bmax, dst.parent, dst.left, dst.right,
-                   dst.data, dst.count, dst.bmin, dst.bmax, cost, pass, emit};
+    CollapseRefs r{n, src.area, src.parent, src.left, src.right, src.data, src.bmin, src.bmax, dst.parent, dst.left,
+                   dst.right, dst.data, dst.count, dst.bmin, dst.bmax, cost, pass, emit};
     const unsigned blocks = (n + 255) / 256;
+    k_collapse_copy<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(r, nn);
     k_collapse_cost<<<blocks, 256, 0, s>>>(r, segs, counters, ci, ct, max_leaf);
-    ctx->launches += 1;
+    ctx->launches += 2;
     int st = exclusive_scan_u32(ctx, emit, offs, nn, nullptr);
     if (st == ATR_OK) {
         k_collapse_emit<<<blocks, 256, 0, s>>>(r, segs, offs, dst.tri_indices);

@@ -28,7 +28,9 @@ int exclusive_scan_u32(atr_ctx* ctx, const uint32_t* in, uint32_t* out, uint64_t
 
 namespace {
 
-constexpr int kJumpRounds = 8;  // 2^8 ancestors per block of rounds; depth >= 256 runs more
+constexpr int kPendingWord = 8;    // flags[8 + r * kPendingStride]: jumps left after round r (r < 34)
+constexpr int kPendingStride = 8;  // one 32-byte sector per round
+constexpr size_t kFlagBytes = 4 * (kPendingWord + 34 * kPendingStride);
 
 struct FlatRefs {
     const int32_t* parent;
@@ -75,9 +77,7 @@ __global__ void __launch_bounds__(256) k_flat_counts(FlatRefs t, Segs segs, uint
     const SegPos q = seg_pos(segs, gi);
     int cur = t.parent[q.nb + (int)q.li + (int)q.n - 1];
     while (cur >= 0) {
-        fence_acq_rel_gpu();
-        if (atomicAdd(&counters[q.cb + cur], 1u) == 0u) return;
-        fence_acq_rel_gpu();
+        if (atomic_add_acq_rel_gpu(&counters[q.cb + cur], 1u) == 0u) return;
         const int l = t.left[q.nb + cur], r = t.right[q.nb + cur];
         const bool ll = c_leaf(t, q.nb, l), rl = c_leaf(t, q.nb, r);
         const uint32_t il = ll ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + q.cb + l);
@@ -115,23 +115,59 @@ __global__ void __launch_bounds__(256) k_flat_jump_init(FlatRefs t, Segs segs, c
     jmp[gx] = q.cb + p;
 }
 
-__global__ void __launch_bounds__(256) k_flat_jump(uint32_t m, const int2* __restrict__ acc_in,
-                                                    const int* __restrict__ jmp_in, int2* __restrict__ acc_out,
+// Round r of pointer jumping reads buffer r & 1 and writes buffer (r + 1) & 1;
+// pending[r * kPendingStride] records whether any jump is left after it (one
+// 32-byte sector per round, one store per block).  A round whose predecessor
+// left none does nothing, except the first such round of odd index, which
+// moves the finished sums into buffer 0: the host launches a fixed number of
+// rounds and never waits, and the result is always in buffer 0.  A node whose
+// jump ran out (-1) copies its sums into the other buffer once and marks both
+// jump words -2; later rounds skip it.  Readers of its jump word see -1 or -2,
+// both "no further ancestor".
+__global__ void __launch_bounds__(256) k_flat_jump(uint32_t m, int round, const int2* __restrict__ acc_in,
+                                                    int* jmp_in, int2* __restrict__ acc_out,
                                                     int* __restrict__ jmp_out, uint32_t* __restrict__ pending) {
-    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= m) return;
-    const int j = jmp_in[x];
-    int2 a = acc_in[x];
-    int nj = -1;
-    if (j >= 0) {
+    __shared__ int s_state;  // 0 jump, 1 idle, 2 idle and move buffer 1 to buffer 0
+    __shared__ int s_any;
+    if (threadIdx.x == 0) {
+        int st = 0;
+        if (round > 0 && pending[(round - 1) * kPendingStride] == 0u)
+            st = (round & 1) && (round == 1 || pending[(round - 2) * kPendingStride] != 0u) ? 2 : 1;
+        s_state = st;
+        s_any = 0;
+    }
+    __syncthreads();
+    const int st = s_state;
+    if (st == 1) return;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    bool any = false;
+    for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < m; x += stride) {
+        if (st == 2) {
+            acc_out[x] = acc_in[x];
+            continue;
+        }
+        const int j = jmp_in[x];
+        if (j < 0) {
+            if (j == -1) {
+                acc_out[x] = acc_in[x];
+                jmp_out[x] = -2;
+                jmp_in[x] = -2;
+            }
+            continue;
+        }
+        int2 a = acc_in[x];
         const int2 b = acc_in[j];
         a.x += b.x;
         a.y = ((a.y & 0xffff) + (b.y & 0xffff)) | ((a.y | b.y) & (1 << 30));
-        nj = jmp_in[j];
-        if (nj >= 0) *pending = 1u;
+        const int nj = jmp_in[j];
+        acc_out[x] = a;
+        jmp_out[x] = nj < 0 ? -1 : nj;
+        any |= nj >= 0;
     }
-    acc_out[x] = a;
-    jmp_out[x] = nj;
+    if (st != 0) return;
+    if (any) s_any = 1;
+    __syncthreads();
+    if (threadIdx.x == 0 && s_any) pending[round * kPendingStride] = 1u;
 }
 
 // Inner nodes of the layout are the reachable ones (no collapsed-tree leaf on
@@ -143,15 +179,22 @@ __global__ void __launch_bounds__(256) k_flat_scatter(Segs segs, const int2* __r
                                                        uint32_t* __restrict__ tw_by_rank,
                                                        int* __restrict__ max_depth) {
     const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gi >= segs.n) return;
-    const SegPos q = seg_pos(segs, gi);
-    if (q.li >= q.n - 1) return;
-    const int gx = q.cb + (int)q.li;
-    const int2 a = acc[gx];
-    if (a.y & (1 << 30)) return;
-    ic_by_rank[q.cb + a.x] = ic[gx];
-    tw_by_rank[q.cb + a.x] = tw[gx];
-    atomicMax(max_depth, (a.y & 0xffff) + 1);
+    int depth = 0;
+    if (gi < segs.n) {
+        const SegPos q = seg_pos(segs, gi);
+        if (q.li < q.n - 1) {
+            const int gx = q.cb + (int)q.li;
+            const int2 a = acc[gx];
+            if (!(a.y & (1 << 30))) {
+                ic_by_rank[q.cb + a.x] = ic[gx];
+                tw_by_rank[q.cb + a.x] = tw[gx];
+                depth = (a.y & 0xffff) + 1;
+            }
+        }
+    }
+    // One atomic per warp on the shared maximum.
+    depth = __reduce_max_sync(0xffffffffu, depth);
+    if ((threadIdx.x & 31) == 0 && depth > 0) atomicMax(max_depth, depth);
 }
 
 __device__ __forceinline__ float det3(const float s[3][3]) {
@@ -279,9 +322,11 @@ __global__ void __launch_bounds__(128) k_flat_write(FlatRefs t, Segs segs, const
 
 // Per-mesh sizes: inner nodes = 1 + inner children, Woop entries.
 __global__ void k_flat_sizes(Segs segs, const uint32_t* __restrict__ ic_scan, const uint32_t* __restrict__ tw_scan,
-                             const uint32_t* __restrict__ totals, int64_t* __restrict__ nodes_out,
-                             int64_t* __restrict__ woop_out) {
+                             const uint32_t* __restrict__ totals, const int* __restrict__ max_depth,
+                             int64_t* __restrict__ nodes_out, int64_t* __restrict__ woop_out,
+                             int64_t* __restrict__ depth_out) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m == 0) *depth_out = *max_depth;
     if (m >= segs.count) return;
     const int cb = segs.inner_base(m);
     const bool last = m + 1 == segs.count;
@@ -295,16 +340,17 @@ __global__ void k_flat_sizes(Segs segs, const uint32_t* __restrict__ ic_scan, co
 
 // Compact2 layout of every mesh of segs into per-mesh slices of nodes (mesh m
 // from node inner_base(m)), woop and tri_index (mesh m from entry 4 *
-// tri_begin(m)).  d_sizes receives 2 * count int64 (nodes, woop per mesh);
-// h_max_depth the deepest inner level over all meshes (host, synchronises).
+// tri_begin(m)).  d_sizes receives 2 * count + 1 int64: nodes per mesh, Woop
+// entries per mesh, then the deepest inner level over all meshes.  Stream
+// ordered: nothing here waits for the device.
 int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const float4* verts, int4* nodes,
-                 float4* woop, int32_t* tri_index, int64_t* d_sizes, int32_t* h_max_depth) {
+                 float4* woop, int32_t* tri_index, int64_t* d_sizes) {
     const uint32_t n = segs.n;
     const uint32_t m = n - segs.count;  // inner nodes over all meshes
     cudaStream_t s = ctx->stream;
     void* scratch = nullptr;
     const size_t bm = align256((size_t)m * 4), b2 = align256((size_t)m * 8);
-    ATR_TRY(ctx->alloc(&scratch, 9 * bm + 2 * b2 + 256));
+    ATR_TRY(ctx->alloc(&scratch, 9 * bm + 2 * b2 + kFlagBytes));
     char* p = static_cast<char*>(scratch);
     uint32_t* icnt = reinterpret_cast<uint32_t*>(p); p += bm;
     uint32_t* ic = reinterpret_cast<uint32_t*>(p); p += bm;
@@ -317,31 +363,28 @@ int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const fl
     int2* acc1 = reinterpret_cast<int2*>(p); p += b2;
     uint32_t* ic_r = reinterpret_cast<uint32_t*>(p); p += bm;
     uint32_t* tw_r = reinterpret_cast<uint32_t*>(p); p += bm;
-    uint32_t* flags = reinterpret_cast<uint32_t*>(p);  // [0] pending, [1] max depth, [2..3] totals
+    uint32_t* flags = reinterpret_cast<uint32_t*>(p);  // [1] max depth, [2..3] totals, then pending
     FlatRefs t{c.parent, c.left, c.right, c.data, c.count, c.bmin, c.bmax, c.tri_indices};
     const unsigned gb = (n + 255) / 256, gm = (m + 255) / 256;
     cudaMemsetAsync(counters, 0, (size_t)m * 4, s);
     cudaMemsetAsync(ic_r, 0, 2 * bm, s);
-    cudaMemsetAsync(flags, 0, 256, s);
+    cudaMemsetAsync(flags, 0, kFlagBytes, s);
     k_flat_counts<<<gb, 256, 0, s>>>(t, segs, icnt, ic, tw, counters);
     k_flat_jump_init<<<gb, 256, 0, s>>>(t, segs, icnt, acc0, jmp0);
     ctx->launches += 2;
-    int2* ai = acc0; int2* ao = acc1;
-    int* ji = jmp0; int* jo = jmp1;
-    for (int round = 0; round < 8 * kJumpRounds; ++round) {
-        const bool check = round % kJumpRounds == kJumpRounds - 1;
-        if (check) cudaMemsetAsync(flags, 0, 4, s);
-        k_flat_jump<<<gm, 256, 0, s>>>(m, ai, ji, ao, jo, flags);
-        ctx->launches += 1;
-        std::swap(ai, ao);
-        std::swap(ji, jo);
-        if (check) {
-            uint32_t pending = 0;
-            cudaMemcpyAsync(&pending, flags, 4, cudaMemcpyDeviceToHost, s);
-            cudaStreamSynchronize(s);
-            if (!pending) break;
-        }
+    // Depth <= m, and after round r every jump spans 2^(r+1) ancestors, so the
+    // last working round is below bits(m) and round bits(m) + 1 is idle.
+    if (m > 0) {
+        const int rounds = 34 - __builtin_clz(m);
+        int2* acc[2] = {acc0, acc1};
+        int* jmp[2] = {jmp0, jmp1};
+        const unsigned gj = std::min(gm, (unsigned)ctx->num_sms * 8u);
+        for (int r = 0; r < rounds; ++r)
+            k_flat_jump<<<gj, 256, 0, s>>>(m, r, acc[r & 1], jmp[r & 1], acc[(r + 1) & 1], jmp[(r + 1) & 1],
+                                           flags + kPendingWord);
+        ctx->launches += rounds;
     }
+    const int2* ai = acc0;
     k_flat_scatter<<<gb, 256, 0, s>>>(segs, ai, ic, tw, ic_r, tw_r, reinterpret_cast<int*>(flags + 1));
     ctx->launches += 1;
     int st = exclusive_scan_u32(ctx, ic_r, ic_r, m, flags + 2);
@@ -349,14 +392,10 @@ int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const fl
     if (st == ATR_OK) {
         k_flat_slots<<<gb, 256, 0, s>>>(t, segs, ai, ic_r, slot_of);
         k_flat_write<<<(n + 127) / 128, 128, 0, s>>>(t, segs, verts, ai, tw_r, slot_of, nodes, woop, tri_index);
-        k_flat_sizes<<<(segs.count + 255) / 256, 256, 0, s>>>(segs, ic_r, tw_r, flags + 2, d_sizes,
-                                                             d_sizes + segs.count);
+        k_flat_sizes<<<(segs.count + 255) / 256, 256, 0, s>>>(segs, ic_r, tw_r, flags + 2,
+                                                             reinterpret_cast<const int*>(flags + 1), d_sizes,
+                                                             d_sizes + segs.count, d_sizes + 2 * segs.count);
         ctx->launches += 3;
-        uint32_t h[4];
-        cudaMemcpyAsync(h, flags, 16, cudaMemcpyDeviceToHost, s);
-        cudaError_t e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) st = cuda_fail(e, "flatten kernels", __FILE__, __LINE__);
-        if (h_max_depth) *h_max_depth = (int32_t)h[1];
     }
     ctx->release(scratch);
     return st;
@@ -380,7 +419,7 @@ int atr_flatten_compact2(atr_ctx* ctx, const atr_collapsed* c, const atr_scene* 
     if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&cp->woop), (size_t)n * 4 * 16);
     if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&cp->tri_index), (size_t)n * 4 * 4);
     int64_t* sizes = nullptr;
-    if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&sizes), 16);
+    if (st == ATR_OK) st = ctx->alloc(reinterpret_cast<void**>(&sizes), 24);
     if (st != ATR_OK) {
         ctx->release(sizes);
         atr_compact_destroy(cp);
@@ -389,14 +428,16 @@ int atr_flatten_compact2(atr_ctx* ctx, const atr_collapsed* c, const atr_scene* 
     const Segs segs{nullptr, nullptr, 1u, n};
     const CollapsedOut co{c->parent, c->left, c->right, c->data, c->count, c->bmin, c->bmax, c->tri_indices};
     ctx->phase_begin("flatten");
-    st = flatten_segs(ctx, segs, co, scene->verts, cp->nodes, cp->woop, cp->tri_index, sizes, &cp->max_depth);
+    st = flatten_segs(ctx, segs, co, scene->verts, cp->nodes, cp->woop, cp->tri_index, sizes);
     ctx->phase_end();
     if (st == ATR_OK) {
-        int64_t h[2];
-        cudaError_t e = cudaMemcpy(h, sizes, 16, cudaMemcpyDeviceToHost);
-        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpy(sizes)", __FILE__, __LINE__);
+        int64_t h[3];
+        cudaError_t e = cudaMemcpyAsync(h, sizes, 24, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "flatten kernels", __FILE__, __LINE__);
         cp->num_nodes = h[0];
         cp->num_woop = h[1];
+        cp->max_depth = (int32_t)h[2];
     }
     ctx->release(sizes);
     if (st != ATR_OK) { atr_compact_destroy(cp); return st; }

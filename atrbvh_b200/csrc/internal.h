@@ -171,7 +171,7 @@ int tree_alloc(atr_ctx* ctx, uint32_t n, atr_tree** out);
 int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const TreeOut& src,
                   const CollapsedOut& dst, float ci, float ct, int max_leaf, float* d_sah_parts);
 int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const float4* verts, int4* nodes,
-                 float4* woop, int32_t* tri_index, int64_t* d_sizes, int32_t* h_max_depth);
+                 float4* woop, int32_t* tri_index, int64_t* d_sizes);
 struct RayMeshMap;  // trace.cu
 int trace_run(atr_ctx* ctx, const int4* nodes, const float4* woop, const int32_t* tri, const RayMeshMap& map,
               int max_depth, const float4* rays, int64_t n, int any_hit, int4* res);
