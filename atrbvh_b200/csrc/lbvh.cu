@@ -361,51 +361,177 @@ __device__ __forceinline__ int delta_adj(const uint64_t* keys, int k) {
 // Segmented: thread i finds its mesh; keys, slots and node arrays are
 // addressed from the mesh's first entry, so every mesh gets exactly the tree
 // a build of that mesh alone produces (local node and triangle indices).
+//
+// Two passes.  k_build_block: a block owns 256 consecutive sorted leaves and
+// finishes every node whose split position and the one after it lie in its
+// range, with the arrival slots, the adjacent-key deltas and the finished
+// boxes in shared memory.  Such a node's children lie in the block, so the
+// climb meets no other block.  A climb that reaches a split on the block's
+// first or last leaf stops and is recorded (at most one per block edge); at
+// the end the block writes its slots, a single arrival or -1, to the global
+// slot array.  k_build_top continues the recorded climbs with global atomic
+// exchanges; a slot written by the block pass carries its first arrival.
+struct BuildEdge {
+    int32_t mesh, node, l, r;  // mesh < 0: no climb stopped at this edge
+};
+
 template <typename K>
-__global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ keys_all,
-                                                const uint32_t* __restrict__ sidx,
-                                                const float4* __restrict__ verts, int32_t* __restrict__ parent_all,
-                                                int32_t* __restrict__ left_all, int32_t* __restrict__ right_all,
-                                                int32_t* __restrict__ data_all, float4* __restrict__ bmin_all,
-                                                float4* __restrict__ bmax_all, float* __restrict__ area_all,
-                                                int32_t* __restrict__ slot_all, int2* __restrict__ range_all,
-                                                BuildPrepass pp) {
-    const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gi >= segs.n) return;
-    const uint32_t m = segs.seg_of_tri(gi);
+struct BuildOut {
+    int32_t *parent, *left, *right, *data;
+    float4 *bmin, *bmax;
+    float* area;
+    int32_t* slot;
+    int2* range;
+    BuildPrepass pp;
+};
+
+// Record of the internal node p over leaves [pl, pr] with children lc, rc.
+template <typename K>
+__device__ __forceinline__ void write_inner(const BuildOut<K>& o, const Segs& segs, uint32_t m, int nb, int p, int pl,
+                                            int pr, int lc, int rc, float4 mn, float4 mx, float pa, float ns) {
+    o.left[nb + p] = lc;
+    o.right[nb + p] = rc;
+    o.data[nb + p] = -1;
+    if (o.range) o.range[segs.inner_base(m) + p] = make_int2(pl, pr);
+    o.parent[nb + lc] = p;
+    o.parent[nb + rc] = p;
+    o.bmin[nb + p] = mn;
+    o.bmax[nb + p] = mx;
+    o.area[nb + p] = pa;
+    if (o.pp.nsah) o.pp.nsah[nb + p] = ns;
+}
+
+constexpr int kBuildBlock = 256;
+
+template <typename K>
+__global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K* __restrict__ keys_all,
+                                                             const uint32_t* __restrict__ sidx,
+                                                             const float4* __restrict__ verts, BuildOut<K> o,
+                                                             BuildEdge* __restrict__ edges) {
+    __shared__ float4 s_lmn[kBuildBlock], s_lmx[kBuildBlock], s_imn[kBuildBlock], s_imx[kBuildBlock];
+    __shared__ float s_lns[kBuildBlock], s_ins[kBuildBlock];
+    __shared__ int s_slot[kBuildBlock];
+    __shared__ int s_delta[kBuildBlock + 1];  // delta at sorted position B0 - 1 + k
+    const int tid = threadIdx.x;
+    const uint32_t B0 = blockIdx.x * kBuildBlock;
+    const uint32_t gi = B0 + tid;
+    const bool live = gi < segs.n;
+    s_slot[tid] = -1;
+    if (tid < 2) edges[2 * blockIdx.x + tid] = BuildEdge{-1, -1, -1, -1};
+    uint32_t m = 0, s0 = 0, n = 1, i = 0;
+    int nb = 0, last = 0;
+    const K* keys = keys_all;
+    float4 mn = make_float4(0.f, 0.f, 0.f, 0.f), mx = mn;
+    float my_ns = 0.0f;
+    s_delta[tid] = -1;
+    if (tid == kBuildBlock - 1) s_delta[kBuildBlock] = -1;
+    if (live) {
+        m = segs.seg_of_tri(gi);
+        s0 = segs.tri_begin(m);
+        n = segs.tri_end(m) - s0;
+        i = gi - s0;
+        nb = segs.node_base(m);
+        last = (int)n - 1;
+        keys = keys_all + s0;
+        const uint32_t gtri = sidx[gi];
+        const float4 a = __ldg(verts + 3 * (size_t)gtri), b = __ldg(verts + 3 * (size_t)gtri + 1),
+                     c = __ldg(verts + 3 * (size_t)gtri + 2);
+        mn = make_float4(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z), 0.0f);
+        mx = make_float4(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z), 0.0f);
+        const int leaf = (int)i + last;
+        o.left[nb + leaf] = -1;
+        o.right[nb + leaf] = -1;
+        o.data[nb + leaf] = (int32_t)(gtri - s0);
+        o.bmin[nb + leaf] = mn;
+        o.bmax[nb + leaf] = mx;
+        const float my_area = box_area(mn, mx);
+        o.area[nb + leaf] = my_area;
+        // Prepass for the first ATRBVH iteration: this subtree's nodesSah under
+        // the default constants, (ci*A + left) + right bottom-up from ct*A at leaves.
+        my_ns = __fmul_rn(kPrepassCt, my_area);
+        if (o.pp.nsah) o.pp.nsah[nb + leaf] = my_ns;
+        s_lmn[tid] = mn;
+        s_lmx[tid] = mx;
+        s_lns[tid] = my_ns;
+        // Deltas within the mesh only: the climb never reads one across meshes.
+        if (i > 0) s_delta[tid] = delta_adj(keys, (int)i - 1);
+        if (tid == kBuildBlock - 1 && (int)i < last) s_delta[kBuildBlock] = delta_adj(keys, (int)i);
+    }
+    __syncthreads();
+    if (live) {
+        const int off = (int)s0 - (int)B0;  // block position of mesh-local sorted index 0
+        auto sd = [&](int x) { return s_delta[off + x + 1]; };
+        int l = (int)i, r = (int)i, node = (int)i + last;
+        int dl = l > 0 ? sd(l - 1) : -1;
+        int dr = r < last ? sd(r) : -1;
+        while (true) {
+            const bool is_left = dr > dl;
+            const int split = is_left ? r : l - 1;
+            const int bs = off + split;  // block position of the split
+            if (bs < 0 || bs >= kBuildBlock - 1) {
+                edges[2 * blockIdx.x + (bs < 0 ? 0 : 1)] = BuildEdge{(int32_t)m, node, l, r};
+                break;
+            }
+            __threadfence_block();
+            const int other = atomicExch(&s_slot[bs], is_left ? l : r);
+            if (other < 0) break;  // first of the two children
+            __threadfence_block();
+            const int pl = is_left ? l : other;
+            const int pr = is_left ? other : r;
+            const int lc = split == pl ? split + last : split;
+            const int rc = split + 1 == pr ? split + 1 + last : split + 1;
+            const bool sib_leaf = is_left ? split + 1 == pr : split == pl;
+            const int sib = is_left ? rc : lc;
+            const int sp = off + (sib_leaf ? sib - last : sib);
+            const float4 smn = sib_leaf ? s_lmn[sp] : s_imn[sp];
+            const float4 smx = sib_leaf ? s_lmx[sp] : s_imx[sp];
+            mn = make_float4(fminf(mn.x, smn.x), fminf(mn.y, smn.y), fminf(mn.z, smn.z), 0.0f);
+            mx = make_float4(fmaxf(mx.x, smx.x), fmaxf(mx.y, smx.y), fmaxf(mx.z, smx.z), 0.0f);
+            const bool root = pl == 0 && pr == last;
+            int p = 0;
+            if (!root) {
+                dl = pl > 0 ? sd(pl - 1) : -1;
+                dr = pr < last ? sd(pr) : -1;
+                p = dr > dl ? pr : pl;
+            }
+            const float pa = box_area(mn, mx);
+            if (o.pp.nsah) {
+                const float sns = sib_leaf ? s_lns[sp] : s_ins[sp];
+                my_ns = __fadd_rn(__fadd_rn(__fmul_rn(kPrepassCi, pa), is_left ? my_ns : sns), is_left ? sns : my_ns);
+            }
+            write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns);
+            s_imn[off + p] = mn;
+            s_imx[off + p] = mx;
+            s_ins[off + p] = my_ns;
+            if (root) {
+                o.parent[nb] = -1;
+                break;
+            }
+            node = p;
+            l = pl;
+            r = pr;
+        }
+    }
+    __syncthreads();
+    if (live && (int)i < last) o.slot[segs.inner_base(m) + i] = s_slot[tid];
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) k_build_top(Segs segs, const K* __restrict__ keys_all, BuildOut<K> o,
+                                                   const BuildEdge* __restrict__ edges, uint32_t count) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const BuildEdge e = edges[t];
+    if (e.mesh < 0) return;
+    const uint32_t m = (uint32_t)e.mesh;
     const uint32_t s0 = segs.tri_begin(m);
-    const uint32_t n = segs.tri_end(m) - s0;
-    const uint32_t i = gi - s0;
+    const int last = (int)(segs.tri_end(m) - s0) - 1;
     const int nb = segs.node_base(m);
     const K* keys = keys_all + s0;
-    int32_t* parent = parent_all + nb;
-    int32_t* left = left_all + nb;
-    int32_t* right = right_all + nb;
-    int32_t* data = data_all + nb;
-    float4* bmin = bmin_all + nb;
-    float4* bmax = bmax_all + nb;
-    float* area = area_all + nb;
-    int32_t* slot = slot_all + segs.inner_base(m);
-    const uint32_t gtri = sidx[gi];
-    const float4 a = __ldg(verts + 3 * (size_t)gtri), b = __ldg(verts + 3 * (size_t)gtri + 1),
-                 c = __ldg(verts + 3 * (size_t)gtri + 2);
-    float4 mn = make_float4(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z), 0.0f);
-    float4 mx = make_float4(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z), 0.0f);
-    const int leaf = (int)i + (int)n - 1;
-    left[leaf] = -1;
-    right[leaf] = -1;
-    data[leaf] = (int32_t)(gtri - s0);
-    bmin[leaf] = mn;
-    bmax[leaf] = mx;
-    const float my_area = box_area(mn, mx);
-    area[leaf] = my_area;
-    // Prepass for the first ATRBVH iteration: this subtree's nodesSah under the
-    // default constants, (ci*A + left) + right bottom-up from ct*A at leaves.
-    float my_ns = __fmul_rn(kPrepassCt, my_area);
-    if (pp.nsah) pp.nsah[nb + leaf] = my_ns;
-
-    const int last = (int)n - 1;
-    int l = (int)i, r = (int)i;
+    int32_t* slot = o.slot + segs.inner_base(m);
+    float4 mn = ld_cg(o.bmin + nb + e.node), mx = ld_cg(o.bmax + nb + e.node);
+    float my_ns = o.pp.nsah ? ld_cg(o.pp.nsah + nb + e.node) : 0.0f;
+    int l = e.l, r = e.r;
     int dl = l > 0 ? delta_adj(keys, l - 1) : -1;
     int dr = r < last ? delta_adj(keys, r) : -1;
     while (true) {
@@ -420,7 +546,7 @@ __global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ 
         const int lc = split == pl ? split + last : split;
         const int rc = split + 1 == pr ? split + 1 + last : split + 1;
         const int sib = is_left ? rc : lc;
-        const float4 smn = ld_cg(bmin + sib), smx = ld_cg(bmax + sib);
+        const float4 smn = ld_cg(o.bmin + nb + sib), smx = ld_cg(o.bmax + nb + sib);
         mn = make_float4(fminf(mn.x, smn.x), fminf(mn.y, smn.y), fminf(mn.z, smn.z), 0.0f);
         mx = make_float4(fmaxf(mx.x, smx.x), fmaxf(mx.y, smx.y), fmaxf(mx.z, smx.z), 0.0f);
         const bool root = pl == 0 && pr == last;
@@ -430,23 +556,14 @@ __global__ void __launch_bounds__(256) k_build(Segs segs, const K* __restrict__ 
             dr = pr < last ? delta_adj(keys, pr) : -1;
             p = dr > dl ? pr : pl;
         }
-        left[p] = lc;
-        right[p] = rc;
-        data[p] = -1;
-        if (range_all) range_all[segs.inner_base(m) + p] = make_int2(pl, pr);
-        parent[lc] = p;
-        parent[rc] = p;
-        bmin[p] = mn;
-        bmax[p] = mx;
         const float pa = box_area(mn, mx);
-        area[p] = pa;
-        if (pp.nsah) {
-            const float sns = ld_cg(pp.nsah + nb + sib);
+        if (o.pp.nsah) {
+            const float sns = ld_cg(o.pp.nsah + nb + sib);
             my_ns = __fadd_rn(__fadd_rn(__fmul_rn(kPrepassCi, pa), is_left ? my_ns : sns), is_left ? sns : my_ns);
-            pp.nsah[nb + p] = my_ns;
         }
+        write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns);
         if (root) {
-            parent[0] = -1;
+            o.parent[nb] = -1;
             return;
         }
         l = pl;
@@ -583,14 +700,16 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
     const size_t inner = n - segs.count;
     ATR_TRY(ctx->alloc(&kv, (size_t)n * sizeof(K)));
     int st = ctx->alloc(&iv, (size_t)n * 4);
-    if (st == ATR_OK) st = ctx->alloc(&aux, align256(hbytes) + align256(inner * 4));
+    const uint32_t bblocks = (n + kBuildBlock - 1) / kBuildBlock;
+    const size_t ebytes = (size_t)bblocks * 2 * sizeof(BuildEdge);
+    if (st == ATR_OK) st = ctx->alloc(&aux, align256(hbytes) + align256(inner * 4) + align256(ebytes));
     if (st != ATR_OK) { ctx->release(kv); ctx->release(iv); return st; }
     K* keys = static_cast<K*>(kv);
     uint32_t* idx = static_cast<uint32_t*>(iv);
     uint32_t* hist = static_cast<uint32_t*>(aux);
     int32_t* slot = reinterpret_cast<int32_t*>(static_cast<char*>(aux) + align256(hbytes));
+    BuildEdge* edges = reinterpret_cast<BuildEdge*>(static_cast<char*>(aux) + align256(hbytes) + align256(inner * 4));
     cudaMemsetAsync(hist, 0, hbytes, s);
-    cudaMemsetAsync(slot, 0xff, inner * 4, s);
 
     ctx->phase_begin("morton");
     k_morton<K, BITS><<<tiles, 256, 0, s>>>(segs, verts, d_bounds, keys, hist);
@@ -601,11 +720,13 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
     ctx->phase_end();
     if (st == ATR_OK) {
         ctx->phase_begin("build");
-        k_build<K><<<(n + 255) / 256, 256, 0, s>>>(segs, keys, idx, verts, t.parent, t.left, t.right, t.data, t.bmin,
-                                                  t.bmax, t.area, slot, t.range,
-                                                  prepass ? *prepass : BuildPrepass{});
+        const BuildOut<K> o{t.parent, t.left,  t.right, t.data,
+                            t.bmin,   t.bmax,  t.area,  slot,
+                            t.range,  prepass ? *prepass : BuildPrepass{}};
+        k_build_block<K><<<bblocks, kBuildBlock, 0, s>>>(segs, keys, idx, verts, o, edges);
+        k_build_top<K><<<(2 * bblocks + 255) / 256, 256, 0, s>>>(segs, keys, o, edges, 2 * bblocks);
         ctx->phase_end();
-        ctx->launches += 1;
+        ctx->launches += 2;
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) st = cuda_fail(e, "k_build launch", __FILE__, __LINE__);
     }
