@@ -39,8 +39,9 @@ struct CollapseRefs {
     int32_t* c_count;
     float4* c_bmin;
     float4* c_bmax;
-    float* cost;
-    int32_t* pass;
+    // Per node: (SAH cost bits, triangle count << 1 | pass flag), one 8-byte
+    // record so a climbing thread reads each child with one load.
+    int2* rec;
     uint32_t* emit_cnt;
 };
 
@@ -75,19 +76,17 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
     {
         const int x = nb + leaf;
         g.c_count[x] = 1;
-        g.cost[x] = __fmul_rn(ct, g.area[x]);
-        g.pass[x] = 1;
+        g.rec[x] = make_int2(__float_as_int(__fmul_rn(ct, g.area[x])), (1 << 1) | 1);
     }
     int cur = g.parent[nb + leaf];
     while (cur >= 0) {
-        fence_acq_rel_gpu();
-        if (atomicAdd(&ctr[cur], 1u) == 0u) return;
-        fence_acq_rel_gpu();
+        if (atomic_add_acq_rel_gpu(&ctr[cur], 1u) == 0u) return;
         const int x = nb + cur;
         const int l = g.left[x], r = g.right[x];
-        const int cl = ld_cg(g.c_count + nb + l), cr = ld_cg(g.c_count + nb + r);
-        const float kl = ld_cg(g.cost + nb + l), kr = ld_cg(g.cost + nb + r);
-        const int pl = ld_cg(g.pass + nb + l), pr = ld_cg(g.pass + nb + r);
+        const int2 el = __ldcg(g.rec + nb + l), er = __ldcg(g.rec + nb + r);
+        const int cl = el.y >> 1, cr = er.y >> 1;
+        const float kl = __int_as_float(el.x), kr = __int_as_float(er.x);
+        const int pl = el.y & 1, pr = er.y & 1;
         const int cnt = cl + cr;
         const float a = g.area[x];
         float c = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), kl), kr);
@@ -100,8 +99,7 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
             if (cr > 1) g.emit_cnt[nb + r] = (uint32_t)cr;
         }
         g.c_count[x] = cnt;
-        g.cost[x] = c;
-        g.pass[x] = reached && col;
+        g.rec[x] = make_int2(__float_as_int(c), (cnt << 1) | (reached && col ? 1 : 0));
         cur = g.parent[x];
     }
 }
@@ -117,7 +115,7 @@ __global__ void __launch_bounds__(256) k_collapse_emit(CollapseRefs g, Segs segs
     const int leaf = (int)(gi - s0) + (int)n - 1;
     int ch = leaf, a = g.parent[nb + leaf], top = -1;
     uint32_t rank = 0;
-    while (a >= 0 && g.pass[nb + a]) {
+    while (a >= 0 && (g.rec[nb + a].y & 1)) {
         if (g.left[nb + a] == ch) rank += (uint32_t)g.c_count[nb + g.right[nb + a]];
         top = a;
         ch = a;
@@ -129,12 +127,12 @@ __global__ void __launch_bounds__(256) k_collapse_emit(CollapseRefs g, Segs segs
     if (rank == 0) g.c_data[nb + top] = (int32_t)off;
 }
 
-__global__ void k_sah_parts(Segs segs, const float* __restrict__ cost, const float* __restrict__ area,
+__global__ void k_sah_parts(Segs segs, const int2* __restrict__ rec, const float* __restrict__ area,
                             float* __restrict__ out) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= segs.count) return;
     const int nb = segs.node_base(m);
-    out[2 * m] = cost[nb];
+    out[2 * m] = __int_as_float(rec[nb].x);
     out[2 * m + 1] = area[nb];
 }
 
@@ -171,10 +169,9 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
     void* scratch = nullptr;
     const size_t b4 = align256(nn * 4);
     const size_t inner = n - segs.count;
-    ATR_TRY(ctx->alloc(&scratch, 4 * b4 + align256(inner * 4)));
+    ATR_TRY(ctx->alloc(&scratch, align256(nn * 8) + 2 * b4 + align256(inner * 4)));
     char* p = static_cast<char*>(scratch);
-    float* cost = reinterpret_cast<float*>(p); p += b4;
-    int32_t* pass = reinterpret_cast<int32_t*>(p); p += b4;
+    int2* rec = reinterpret_cast<int2*>(p); p += align256(nn * 8);
     uint32_t* emit = reinterpret_cast<uint32_t*>(p); p += b4;
     uint32_t* offs = reinterpret_cast<uint32_t*>(p); p += b4;
     uint32_t* counters = reinterpret_cast<uint32_t*>(p);
@@ -183,7 +180,7 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
     cudaMemsetAsync(counters, 0, inner * 4, s);
     cudaMemsetAsync(dst.tri_indices, 0xff, (size_t)n * 4, s);
     CollapseRefs r{n, src.area, src.parent, src.left, src.right, src.data, src.bmin, src.bmax, dst.parent, dst.left,
-                   dst.right, dst.data, dst.count, dst.bmin, dst.bmax, cost, pass, emit};
+                   dst.right, dst.data, dst.count, dst.bmin, dst.bmax, rec, emit};
     const unsigned blocks = (n + 255) / 256;
     k_collapse_copy<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(r, nn);
     k_collapse_cost<<<blocks, 256, 0, s>>>(r, segs, counters, ci, ct, max_leaf);
@@ -193,7 +190,7 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
         k_collapse_emit<<<blocks, 256, 0, s>>>(r, segs, offs, dst.tri_indices);
         ctx->launches += 1;
         if (d_sah_parts) {
-            k_sah_parts<<<(segs.count + 255) / 256, 256, 0, s>>>(segs, cost, src.area, d_sah_parts);
+            k_sah_parts<<<(segs.count + 255) / 256, 256, 0, s>>>(segs, rec, src.area, d_sah_parts);
             ctx->launches += 1;
         }
         cudaError_t e = cudaGetLastError();

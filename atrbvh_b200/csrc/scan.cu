@@ -24,13 +24,24 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t* __restric
     __syncthreads();
     const uint32_t tile = s_tile;
     const uint64_t base = (uint64_t)tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+    // Each thread owns kScanItems consecutive values: four 16-byte loads when
+    // the pointers allow it (the L1 merges the warp's neighbouring halves).
+    const bool vec = ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15u) == 0 &&
+                     base + kScanItems <= n;
     uint32_t v[kScanItems];
+    if (vec) {
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            const uint4 u = __ldg(reinterpret_cast<const uint4*>(in + base) + q);
+            v[4 * q] = u.x; v[4 * q + 1] = u.y; v[4 * q + 2] = u.z; v[4 * q + 3] = u.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) v[k] = base + k < n ? in[base + k] : 0u;
+    }
     uint32_t sum = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        v[k] = base + k < n ? in[base + k] : 0u;
-        sum += v[k];
-    }
+    for (int k = 0; k < kScanItems; ++k) sum += v[k];
     // Block exclusive scan of the per-thread sums.
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     uint32_t inc = sum;
@@ -42,36 +53,66 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t* __restric
     if (lane == 31) s_warp[w] = inc;
     __syncthreads();
     uint32_t wb = 0, tile_sum = 0;
+#pragma unroll
     for (int j = 0; j < kScanThreads / 32; ++j) {
         if (j < w) wb += s_warp[j];
         tile_sum += s_warp[j];
     }
     const uint32_t excl = wb + inc - sum;
-    if (threadIdx.x == 0) {
+    // Decoupled look-back by warp 0, 32 predecessors per step: the nearest
+    // inclusive prefix plus the aggregates between it and this tile.
+    if (w == 0) {
         uint32_t prefix = 0;
         if (tile == 0) {
-            __stcg(status, kInc | tile_sum);
+            if (lane == 0) __stcg(status, kInc | tile_sum);
         } else {
-            __stcg(status + tile, kAgg | tile_sum);
-            int64_t k = (int64_t)tile - 1;
+            if (lane == 0) __stcg(status + tile, kAgg | tile_sum);
+            int64_t top = (int64_t)tile - 1;
             uint32_t polls = 0;
-            while (k >= 0) {
-                const uint32_t s = *reinterpret_cast<volatile uint32_t*>(status + k);
-                if (s & kInc) { prefix += s & kVal; break; }
-                if (s & kAgg) { prefix += s & kVal; --k; continue; }
-                if (++polls > kPollLimit) { set_error_bits(err, kErrCollapse); break; }
+            while (true) {
+                const int64_t k = top - lane;
+                const uint32_t st = k >= 0 ? *reinterpret_cast<volatile uint32_t*>(status + k) : kInc;
+                if (__any_sync(kFull, (st & (kAgg | kInc)) == 0u)) {
+                    if (++polls > kPollLimit) {
+                        if (lane == 0) set_error_bits(err, kErrCollapse);
+                        break;
+                    }
+                    continue;
+                }
+                const uint32_t incs = __ballot_sync(kFull, (st & kInc) != 0u);
+                if (incs) {
+                    const int first = __ffs(incs) - 1;
+                    prefix += __reduce_add_sync(kFull, lane <= first ? (st & kVal) : 0u);
+                    break;
+                }
+                prefix += __reduce_add_sync(kFull, st & kVal);
+                top -= 32;
             }
-            __stcg(status + tile, kInc | (prefix + tile_sum));
+            if (lane == 0) __stcg(status + tile, kInc | (prefix + tile_sum));
         }
-        s_prefix = prefix;
-        if (total && (uint64_t)(tile + 1) * kScanTile >= n) *total = prefix + tile_sum;
+        if (lane == 0) {
+            s_prefix = prefix;
+            if (total && (uint64_t)(tile + 1) * kScanTile >= n) *total = prefix + tile_sum;
+        }
     }
     __syncthreads();
     uint32_t run = s_prefix + excl;
+    if (vec) {
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < n) out[base + k] = run;
-        run += v[k];
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            uint4 u;
+            u.x = run; run += v[4 * q];
+            u.y = run; run += v[4 * q + 1];
+            u.z = run; run += v[4 * q + 2];
+            u.w = run; run += v[4 * q + 3];
+            reinterpret_cast<uint4*>(out + base)[q] = u;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            if (base + k < n) out[base + k] = run;
+            run += v[k];
+        }
     }
 }
 
