@@ -157,30 +157,28 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     float* const NS = g.nsah + nb;
 
     // ---- formTreelet (Treelet.cuh:57-114) ----
-    // Lane k holds treelet leaf k: its node, area and box, and (for an
-    // internal node) its children and their areas from the child record.
+    // Lane k holds treelet leaf k (node and area).  The child record of an
+    // internal leaf (children and their areas) is copied into the lane's
+    // shared slot with cp.async when the leaf joins; only the lane whose leaf
+    // is expanded waits, for its own copy, so a step never waits for the
+    // records of leaves that joined in the step before.  Boxes and nodesSah
+    // are loaded once the treelet is complete.
+    float* const dist = sm;
+    float4* const lmn = reinterpret_cast<float4*>(sm + Lay::kDistPad);
+    float4* const lmx = lmn + Lay::kLeaves;
+    int4* const lcn = reinterpret_cast<int4*>(lmx + Lay::kLeaves);
+    int4* const krec = lcn;  // child-record slots during formation
     int internal_node = gl == 0 ? root : -1;
-    int s_node = -1, s_cl = -1, s_cr = -1;
-    float s_area = 0.0f, s_cal = 0.0f, s_car = 0.0f, s_sah = 0.0f;
-    float4 s_mn = make_float4(0.f, 0.f, 0.f, 0.f), s_mx = s_mn;
-    auto load = [&](int node, float area) {
+    int s_node = -1;
+    float s_area = 0.0f;
+    auto join = [&](int node, float area) {
         s_node = node;
         s_area = area;
-        s_mn = ld_cg(BMN + node);
-        s_mx = ld_cg(BMX + node);
-        s_sah = ld_cg(NS + node);
-        s_cl = s_cr = -1;
-        if (is_internal(node, n)) {
-            const int4 k = __ldcg(KD + node);
-            s_cl = k.x;
-            s_cr = k.y;
-            s_cal = __int_as_float(k.z);
-            s_car = __int_as_float(k.w);
-        }
+        if (is_internal(node, n)) cp_async16_cg(krec + gl, KD + node);
     };
     if (active && gl < 2) {
         const int4 k = __ldcg(KD + root);
-        load(gl == 0 ? k.x : k.y, __int_as_float(gl == 0 ? k.z : k.w));
+        join(gl == 0 ? k.x : k.y, __int_as_float(gl == 0 ? k.z : k.w));
     }
     bool ok = true;
     for (int it = 0; it < maxts - 2; ++it) {
@@ -209,43 +207,53 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
             }
             largest = __shfl_sync(kFull, ix, gb);
         }
-        const int src = gb + largest;
-        const int rep = __shfl_sync(kFull, s_node, src);
-        const int cl = __shfl_sync(kFull, s_cl, src);
-        const int cr = __shfl_sync(kFull, s_cr, src);
-        const float al = __shfl_sync(kFull, s_cal, src);
-        const float ar = __shfl_sync(kFull, s_car, src);
+        const int rep = __shfl_sync(kFull, s_node, gb + largest);
+        const bool expand = act && is_internal(rep, n);
+        if (expand && gl == largest) cp_async_wait_all();
+        __syncwarp();
+        int4 rk = make_int4(-1, -1, 0, 0);
+        if (expand) rk = krec[largest];
+        __syncwarp();
         if (act) {
-            if (!is_internal(rep, n)) {
+            if (!expand) {
                 ok = false;
             } else {
                 if (gl == it + 1) internal_node = rep;
                 if (gl == largest || gl == it + 2) {
                     const bool isl = gl == largest;
-                    load(isl ? cl : cr, isl ? al : ar);
+                    join(isl ? rk.x : rk.y, __int_as_float(isl ? rk.z : rk.w));
                 }
             }
         }
     }
     const bool run = active && ok;
     if (active && !ok && gl == 0) set_error_bits(err, kErrTreeletClimb);
+    float4 s_mn = make_float4(0.f, 0.f, 0.f, 0.f), s_mx = s_mn;
+    float s_sah = 0.0f;
+    int s_cnt = 0, s_nlv = 0;
+    float s_nsn = 0.0f;
+    if (run && gl < tsize) {
+        s_mn = ld_cg(BMN + s_node);
+        s_mx = ld_cg(BMX + s_node);
+        s_sah = ld_cg(NS + s_node);
+        s_cnt = ld_cg(nx.sub + s_node);
+        s_nsn = ld_cg(nx.nsn + s_node);
+        s_nlv = is_internal(s_node, n) ? ld_cg(nx.nlv + s_node) : 0;
+    }
+    // Records of leaves that were never expanded may still be in flight into
+    // the slots the merge state reuses.
+    cp_async_wait_all();
+    __syncwarp();
 
     // ---- distance matrix (AgglomerativeTreelet.cu:18-63) ----
     // Slot k: (min.xyz, nodesSah), (max.xyz, node), (count, next level,
     // next nodesSah, -).  When the merge retires slot k (step last = k) it
     // takes the new node instead: (min.xyz, cost), (max.xyz, left child),
     // (count, next level, next nodesSah, right child).
-    float* const dist = sm;
-    float4* const lmn = reinterpret_cast<float4*>(sm + Lay::kDistPad);
-    float4* const lmx = lmn + Lay::kLeaves;
-    int4* const lcn = reinterpret_cast<int4*>(lmx + Lay::kLeaves);
     if (run && gl < tsize) {
-        const int cnt = ld_cg(nx.sub + s_node);
-        const float nsn = ld_cg(nx.nsn + s_node);
-        const int nlv = is_internal(s_node, n) ? ld_cg(nx.nlv + s_node) : 0;
         lmn[gl] = make_float4(s_mn.x, s_mn.y, s_mn.z, s_sah);
         lmx[gl] = make_float4(s_mx.x, s_mx.y, s_mx.z, __int_as_float(s_node));
-        lcn[gl] = make_int4(cnt, nlv, __float_as_int(nsn), 0);
+        lcn[gl] = make_int4(s_cnt, s_nlv, __float_as_int(s_nsn), 0);
     }
     __syncwarp();
     if (run) {
@@ -283,9 +291,47 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
             const uint32_t kmin = __reduce_min_sync(kFull, tk);
             mi = dmin == 0xffffffffu ? 0 : (int)(kmin & 255u);
         } else {
-            unsigned long long best = ~0ull;
-            if (act) {
-                const int msize = last * (last + 1) / 2;
+            // Fast path: the group minimum of the distances alone (32-bit), held
+            // by one lane whose scan met it once, is the reference's choice.
+            // Equal minima (two holders, or a holder that saw its minimum
+            // twice) take the exact (distance, brev5(j), j) key reduction.
+            const int msize = act ? last * (last + 1) / 2 : 0;
+            uint32_t bd = 0xffffffffu;
+            int bj = 0;
+            bool tie = false;
+            for (int j = gl; j < msize; j += G) {
+                uint32_t d = __float_as_uint(dist[j]);
+                d = d < 0x7f7fffffu ? d : 0xffffffffu;  // not below FLT_MAX: never chosen
+                if (d < bd) {
+                    bd = d;
+                    bj = j;
+                    tie = false;
+                } else if (d == bd) {
+                    tie = true;
+                }
+            }
+            uint32_t dmin = bd;
+            if ((G & (G - 1)) == 0) {
+#pragma unroll
+                for (int o = G >> 1; o > 0; o >>= 1) dmin = min(dmin, __shfl_xor_sync(kFull, dmin, o));
+            } else {
+                int c = G, sh = G >> 1;
+                while (c > 1) {
+                    const uint32_t od = __shfl_sync(kFull, dmin, lane + sh);
+                    if (gl < c - sh) dmin = min(dmin, od);
+                    c = (c + 1) >> 1;
+                    sh = c >> 1;
+                }
+                dmin = __shfl_sync(kFull, dmin, gb);
+            }
+            const uint32_t gmask = (G == 32 ? kFull : ((1u << G) - 1u)) << gb;
+            const bool holds = bd == dmin && dmin != 0xffffffffu;
+            const uint32_t holders = __ballot_sync(kFull, holds) & gmask;
+            const bool tied = (__ballot_sync(kFull, holds && tie) & gmask) != 0u || __popc(holders) > 1;
+            mi = __shfl_sync(kFull, bj, holders ? __ffs(holders) - 1 : gb);
+            if (!holders) mi = 0;
+            if (__any_sync(kFull, tied)) {
+                unsigned long long best = ~0ull;
                 for (int j = gl; j < msize; j += G) {
                     const float d = dist[j];
                     if (d < FLT_MAX) {
@@ -294,24 +340,24 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
                         best = k < best ? k : best;
                     }
                 }
-            }
-            if ((G & (G - 1)) == 0) {
+                if ((G & (G - 1)) == 0) {
 #pragma unroll
-                for (int o = G >> 1; o > 0; o >>= 1) {
-                    const unsigned long long ob = __shfl_xor_sync(kFull, best, o);
-                    best = ob < best ? ob : best;
+                    for (int o = G >> 1; o > 0; o >>= 1) {
+                        const unsigned long long ob = __shfl_xor_sync(kFull, best, o);
+                        best = ob < best ? ob : best;
+                    }
+                } else {
+                    int c = G, sh = G >> 1;
+                    while (c > 1) {
+                        const unsigned long long ob = __shfl_sync(kFull, best, lane + sh);
+                        if (gl < c - sh && ob < best) best = ob;
+                        c = (c + 1) >> 1;
+                        sh = c >> 1;
+                    }
+                    best = __shfl_sync(kFull, best, gb);
                 }
-            } else {
-                int c = G, sh = G >> 1;
-                while (c > 1) {
-                    const unsigned long long ob = __shfl_sync(kFull, best, lane + sh);
-                    if (gl < c - sh && ob < best) best = ob;
-                    c = (c + 1) >> 1;
-                    sh = c >> 1;
-                }
-                best = __shfl_sync(kFull, best, gb);
+                if (tied) mi = best == ~0ull ? 0 : (int)(best & 255u);
             }
-            mi = best == ~0ull ? 0 : (int)(best & 255u);
         }
         const int new_internal = __shfl_sync(kFull, internal_node, gb + (last >= 1 ? last - 1 : 0));
         // updateState (:101-150): the new node (union of rows jr and jc) takes

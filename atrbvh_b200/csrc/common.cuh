@@ -42,6 +42,14 @@ __device__ __forceinline__ uint32_t atomic_add_acq_rel_gpu(uint32_t* p, uint32_t
     return old;
 }
 
+// 16-byte global-to-shared copy through L2 (cp.async.cg) that leaves no
+// register pending: a later reader waits only for its own copies.
+__device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
