@@ -183,6 +183,10 @@ int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value) {
                         "atr_ctx_set_tuning: level passes %d outside [0, 64]", value);
             ctx->atr_levels = value;
             return ATR_OK;
+        case ATR_TUNE_QUAD_MIN:
+            ATR_REQUIRE(value >= -1, ATR_ERR_INVALID_ARG, "atr_ctx_set_tuning: quad threshold %d below -1", value);
+            ctx->atr_quad_min = value;
+            return ATR_OK;
         default:
             break;
     }
@@ -196,6 +200,7 @@ int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value) {
         case ATR_TUNE_ATR_GROUP_MIN: *value = ctx->atr_group_min; return ATR_OK;
         case ATR_TUNE_SORT_BITS: *value = ctx->sort_bits; return ATR_OK;
         case ATR_TUNE_ATR_LEVELS: *value = ctx->atr_levels; return ATR_OK;
+        case ATR_TUNE_QUAD_MIN: *value = ctx->atr_quad_min; return ATR_OK;
         default: break;
     }
     ATR_REQUIRE(false, ATR_ERR_INVALID_ARG, "atr_ctx_get_tuning: unknown knob %d", knob);

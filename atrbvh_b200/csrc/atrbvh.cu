@@ -881,14 +881,324 @@ __global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, 
     if (me > 0) lv.order[lv.hist[me] + s_base[me] + rank] = make_uint2(m, li);
 }
 
-// Phase C: every treelet root of level `lev`; each warp takes 32/G roots at a
-// time, one per lane group (the list is dense, so the groups stay full).
-template <int G, int W>
+// ---- quads: eight treelets per warp ----------------------------------------
+// The first levels hold most treelets (a quarter of a million in the first
+// level of a four-million-triangle scene) and the level pass is bound by
+// instruction issue.  There a group of four lanes restructures a treelet of
+// up to KL leaves, lane l owning leaves l, l + 4, ...: the searches and
+// updates are strided over four lanes and the reductions are two butterfly
+// steps, so a warp instruction serves eight treelets instead of three.  Same
+// operations, operands and order as process_group (same tie rules), hence the
+// same results bit for bit.
+template <int KL>
+struct QuadLayout {
+    static constexpr int kDist = KL * (KL - 1) / 2;
+    static constexpr int kDistPad = (kDist + 3) & ~3;
+    // dist, then per leaf slot three float4 (as GroupLayout), then the
+    // treelet's internal nodes.
+    static constexpr int kFloats = kDistPad + 12 * KL + ((KL + 3) & ~3);
+};
+constexpr int kQuadLeaves = 10;  // largest treelet the quad path takes
+
+template <int KL>
+__device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int nb, uint32_t n, int root,
+                                             int4* KD, const NextRefs& nx, float root_sah, int tsize, int maxts,
+                                             float ci, float* sm, const uint16_t* __restrict__ s_rc,
+                                             const uint8_t* __restrict__ s_prio, uint32_t* err) {
+    using Lay = QuadLayout<KL>;
+    const int lane = threadIdx.x & 31;
+    const int gb = lane & ~3;
+    const int gl = lane & 3;
+    const uint32_t gmask = 0xfu << gb;
+    int32_t* const P = g.parent + nb;
+    int32_t* const Lf = g.left + nb;
+    int32_t* const Rt = g.right + nb;
+    float4* const BMN = g.bmin + nb;
+    float4* const BMX = g.bmax + nb;
+    float* const AR = g.area + nb;
+    float* const NS = g.nsah + nb;
+    float* const dist = sm;
+    float4* const lmn = reinterpret_cast<float4*>(sm + Lay::kDistPad);
+    float4* const lmx = lmn + KL;
+    int4* const lcn = reinterpret_cast<int4*>(lmx + KL);
+    int* const inner = reinterpret_cast<int*>(lcn + KL);
+    int4* const krec = lcn;  // child-record slots during formation
+
+    // ---- formTreelet (Treelet.cuh:57-114) ----
+    // Slot k's node and area sit in lmx[k].w and lmn[k].w while the treelet
+    // grows; the owner lane (k mod 4) copies an internal leaf's child record
+    // into krec[k] with cp.async and is the only lane that waits for it.
+    auto join = [&](int k, int node, float area) {
+        lmx[k].w = __int_as_float(node);
+        lmn[k].w = area;
+        if (is_internal(node, n)) cp_async16_cg(krec + k, KD + node);
+    };
+    if (active) {
+        const int4 k = __ldcg(KD + root);
+        if (gl == 0) {
+            join(0, k.x, __int_as_float(k.z));
+            inner[0] = root;
+        }
+        if (gl == 1) join(1, k.y, __int_as_float(k.w));
+    }
+    __syncwarp();
+    bool ok = true;
+    for (int it = 0; it < maxts - 2; ++it) {
+        const bool act = active && ok && it < tsize - 2;
+        const int m = 2 + it;
+        // Largest area among internal leaves (others -FLT_MAX), ties to the
+        // lowest rank of the reference's reduction tree over m lanes.
+        float bv = -FLT_MAX;
+        int bk = gl < m ? gl : 0, brk = 255;
+        for (int k = gl; k < m; k += 4) {
+            const float v = is_internal(__float_as_int(lmx[k].w), n) ? lmn[k].w : -FLT_MAX;
+            const int rk = s_prio[m * 32 + k];
+            if (brk == 255 || v > bv || (v == bv && rk < brk)) {
+                bv = v;
+                bk = k;
+                brk = rk;
+            }
+        }
+#pragma unroll
+        for (int o = 1; o <= 2; o <<= 1) {
+            const float ov = __shfl_xor_sync(kFull, bv, o);
+            const int opk = __shfl_xor_sync(kFull, (brk << 8) | bk, o);
+            const int ork = opk >> 8;
+            if (ov > bv || (ov == bv && ork < brk)) {
+                bv = ov;
+                bk = opk & 255;
+                brk = ork;
+            }
+        }
+        const int largest = bk;
+        const int rep = act ? __float_as_int(lmx[largest].w) : -1;
+        const bool expand = act && is_internal(rep, n);
+        if (expand && gl == (largest & 3)) cp_async_wait_all();
+        __syncwarp();
+        int4 rk = make_int4(-1, -1, 0, 0);
+        if (expand) rk = krec[largest];
+        __syncwarp();
+        if (act) {
+            if (!expand) {
+                ok = false;
+            } else {
+                if (gl == 0) inner[it + 1] = rep;
+                if (gl == (largest & 3)) join(largest, rk.x, __int_as_float(rk.z));
+                if (gl == (m & 3)) join(m, rk.y, __int_as_float(rk.w));
+            }
+        }
+        __syncwarp();
+    }
+    const bool run = active && ok;
+    if (active && !ok && gl == 0) set_error_bits(err, kErrTreeletClimb);
+    cp_async_wait_all();
+    __syncwarp();
+
+    // ---- leaf data and distance matrix (AgglomerativeTreelet.cu:18-63) ----
+    // Slot k: (min.xyz, nodesSah), (max.xyz, node), (count, next level,
+    // next nodesSah, -); a retired slot holds the new node of its step:
+    // (min.xyz, cost), (max.xyz, left child), (count, next level, next
+    // nodesSah, right child).
+    if (run) {
+        for (int k = gl; k < tsize; k += 4) {
+            const int node = __float_as_int(lmx[k].w);
+            const float4 mn = ld_cg(BMN + node), mx = ld_cg(BMX + node);
+            const float sah = ld_cg(NS + node);
+            const int cnt = ld_cg(nx.sub + node);
+            const float nsn = ld_cg(nx.nsn + node);
+            const int nlv = is_internal(node, n) ? ld_cg(nx.nlv + node) : 0;
+            lmn[k] = make_float4(mn.x, mn.y, mn.z, sah);
+            lmx[k] = make_float4(mx.x, mx.y, mx.z, __int_as_float(node));
+            lcn[k] = make_int4(cnt, nlv, __float_as_int(nsn), 0);
+        }
+    }
+    __syncwarp();
+    if (run) {
+        const int np = tsize * (tsize - 1) / 2;
+        for (int j = gl; j < np; j += 4) {
+            const uint32_t rc = s_rc[j];
+            const float4 a0 = lmn[rc >> 8], a1 = lmx[rc >> 8], b0 = lmn[rc & 255u], b1 = lmx[rc & 255u];
+            dist[j] = union_area3(a0.x, a0.y, a0.z, a1.x, a1.y, a1.z, b0.x, b0.y, b0.z, b1.x, b1.y, b1.z);
+        }
+    }
+    __syncwarp();
+
+    // ---- agglomerative merge (AgglomerativeTreelet.cu:476-532) ----
+    for (int step = 0; step < maxts - 1; ++step) {
+        const int last = tsize - 1 - step;
+        const bool act = run && last >= 1;
+        const int msize = act ? last * (last + 1) / 2 : 0;
+        // findMinimumDistance as in process_group: distances alone unless the
+        // group minimum is held twice; then the exact key.
+        uint32_t bd = 0xffffffffu;
+        int bj = 0;
+        bool tie = false;
+        for (int j = gl; j < msize; j += 4) {
+            uint32_t d = __float_as_uint(dist[j]);
+            d = d < 0x7f7fffffu ? d : 0xffffffffu;
+            if (d < bd) {
+                bd = d;
+                bj = j;
+                tie = false;
+            } else if (d == bd) {
+                tie = true;
+            }
+        }
+        uint32_t dmin = min(bd, __shfl_xor_sync(kFull, bd, 1));
+        dmin = min(dmin, __shfl_xor_sync(kFull, dmin, 2));
+        const bool holds = bd == dmin && dmin != 0xffffffffu;
+        const uint32_t holders = __ballot_sync(kFull, holds) & gmask;
+        const bool tied = (__ballot_sync(kFull, holds && tie) & gmask) != 0u || __popc(holders) > 1;
+        int mi = __shfl_sync(kFull, bj, holders ? __ffs(holders) - 1 : gb);
+        if (!holders) mi = 0;
+        if (__any_sync(kFull, tied)) {
+            unsigned long long best = ~0ull;
+            for (int j = gl; j < msize; j += 4) {
+                const float d = dist[j];
+                if (d < FLT_MAX) {
+                    const unsigned long long k = ((unsigned long long)__float_as_uint(d) << 32) |
+                                                 (uint32_t)(((__brev((uint32_t)j) >> 27) << 8) | (uint32_t)j);
+                    best = k < best ? k : best;
+                }
+            }
+#pragma unroll
+            for (int o = 1; o <= 2; o <<= 1) {
+                const unsigned long long ob = __shfl_xor_sync(kFull, best, o);
+                best = ob < best ? ob : best;
+            }
+            if (tied) mi = best == ~0ull ? 0 : (int)(best & 255u);
+        }
+        // updateState (:101-150): the new node takes slot jc, the last leaf
+        // moves to slot jr, slot `last` retires with the new node.  Lanes 0,
+        // 1 and 2 of the group write those three slots.
+        int jr = 0, jc = 0;
+        float a0x = 0.f, a0y = 0.f, a0z = 0.f, a1x = 0.f, a1y = 0.f, a1z = 0.f;
+        float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f), w1 = w0;
+        int4 w2 = make_int4(0, 0, 0, 0);
+        int wslot = -1;
+        if (act) {
+            const uint32_t rc = s_rc[mi];
+            jr = (int)(rc >> 8);
+            jc = (int)(rc & 255u);
+            const int new_internal = inner[last - 1];
+            const float4 r0 = lmn[jr], r1 = lmx[jr], c0 = lmn[jc], c1 = lmx[jc];
+            const int4 r2 = lcn[jr], c2 = lcn[jc];
+            a0x = fminf(c0.x, r0.x); a0y = fminf(c0.y, r0.y); a0z = fminf(c0.z, r0.z);
+            a1x = fmaxf(c1.x, r1.x); a1y = fmaxf(c1.y, r1.y); a1z = fmaxf(c1.z, r1.z);
+            const float area_new = box_area(a0x, a0y, a0z, a1x, a1y, a1z);
+            const float la = __fadd_rn(__fadd_rn(r0.w, c0.w), __fmul_rn(ci, area_new));
+            const int cnt = r2.x + c2.x;
+            const float nsn = __fadd_rn(__fadd_rn(__fmul_rn(ci, area_new), __int_as_float(r2.z)), __int_as_float(c2.z));
+            const int nlv = cnt >= nx.gamma ? 1 + max(r2.y, c2.y) : 0;
+            if (gl == 0) {  // slot jc: the new node
+                wslot = jc;
+                w0 = make_float4(a0x, a0y, a0z, la);
+                w1 = make_float4(a1x, a1y, a1z, __int_as_float(new_internal));
+                w2 = make_int4(cnt, nlv, __float_as_int(nsn), 0);
+            } else if (gl == 1) {  // slot jr: the last leaf (nothing when jr is last)
+                if (jr != last) {
+                    wslot = jr;
+                    w0 = lmn[last];
+                    w1 = lmx[last];
+                    w2 = lcn[last];
+                }
+            } else if (gl == 2) {  // slot last: retired, left = row jr, right = column jc
+                wslot = last;
+                w0 = make_float4(a0x, a0y, a0z, la);
+                w1 = make_float4(a1x, a1y, a1z, r1.w);
+                w2 = make_int4(cnt, nlv, __float_as_int(nsn), __float_as_int(c1.w));
+            }
+        }
+        // updateDistancesMatrix (:152-188): row `last` moves to row jr, then
+        // the distances to the new node at jc are recomputed.
+        const bool du = act && last > 1;
+        float mv[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int c = gl + 4 * q;
+            if (du && c < last && c != jr) mv[q] = dist[trm_idx(last, c)];
+        }
+        __syncwarp();
+        if (wslot >= 0) {
+            lmn[wslot] = w0;
+            lmx[wslot] = w1;
+            lcn[wslot] = w2;
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int c = gl + 4 * q;
+            if (du && c < last && c != jr) dist[trm_idx(max(jr, c), min(jr, c))] = mv[q];
+        }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int c = gl + 4 * q;
+            if (du && c < last && c != jc) {
+                const float4 b0 = lmn[c], b1 = lmx[c];
+                dist[trm_idx(max(jc, c), min(jc, c))] =
+                    union_area3(a0x, a0y, a0z, a1x, a1y, a1z, b0.x, b0.y, b0.z, b1.x, b1.y, b1.z);
+            }
+        }
+        __syncwarp();
+    }
+
+    // ---- updateTreelet (:190-212) ----
+    const bool accept = run && lmn[1].w < root_sah;
+    int fls[3], frs[3], nis[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const int sl = 1 + gl + 4 * q;
+        nis[q] = -1;
+        if (accept && sl < tsize) {
+            const float4 f0 = lmn[sl], f1 = lmx[sl];
+            const int4 f2 = lcn[sl];
+            const int ni = inner[sl - 1];
+            const int fl = __float_as_int(f1.w), fr = f2.w;
+            nis[q] = ni;
+            fls[q] = fl;
+            frs[q] = fr;
+            Lf[ni] = fl;
+            Rt[ni] = fr;
+            P[fl] = ni;
+            P[fr] = ni;
+            NS[ni] = f0.w;
+            const float4 mn = make_float4(f0.x, f0.y, f0.z, 0.0f);
+            const float4 mx = make_float4(f1.x, f1.y, f1.z, 0.0f);
+            BMN[ni] = mn;
+            BMX[ni] = mx;
+            AR[ni] = box_area(mn, mx);
+            nx.sub[ni] = f2.x;
+            nx.nlv[ni] = f2.y;
+            nx.nsn[ni] = __int_as_float(f2.z);
+        }
+    }
+    __syncwarp();
+    // The rewritten nodes' child records, once every new area is stored.
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        if (nis[q] >= 0)
+            KD[nis[q]] = make_int4(fls[q], frs[q], __float_as_int(__ldcg(AR + fls[q])),
+                                   __float_as_int(__ldcg(AR + frs[q])));
+    // A treelet left as it was: its root's next level and next nodesSah.
+    if (run && !accept && gl == 0) {
+        const int lc = ld_cg(Lf + root), rc = ld_cg(Rt + root);
+        const int a = is_internal(lc, n) ? ld_cg(nx.nlv + lc) : 0;
+        const int b = is_internal(rc, n) ? ld_cg(nx.nlv + rc) : 0;
+        nx.nlv[root] = ld_cg(nx.sub + root) >= nx.gamma ? 1 + max(a, b) : 0;
+        nx.nsn[root] = __fadd_rn(__fadd_rn(__fmul_rn(ci, ld_cg(AR + root)), ld_cg(nx.nsn + lc)), ld_cg(nx.nsn + rc));
+    }
+    __syncwarp();
+}
+
+// Phase C: every treelet root of level `lev`.  Each warp takes `per` roots
+// at a time: 32/G in lane groups of G, or (QUADS) eight in four-lane groups.
+template <int G, int W, bool QUADS>
 __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Segs segs, LevelRefs lv, int lev,
                                                                  int tsize_all, const uint8_t* __restrict__ seg_tsize,
                                                                  int iteration, float ci, uint32_t* err) {
-    constexpr int NG = GroupLayout<G>::kGroups;
-    __shared__ __align__(16) float s_mem[W][GroupLayout<G>::kFloats * NG];
+    constexpr int per = QUADS ? 8 : GroupLayout<G>::kGroups;
+    constexpr int kGroupFloats = QUADS ? QuadLayout<kQuadLeaves>::kFloats : GroupLayout<G>::kFloats;
+    __shared__ __align__(16) float s_mem[W][kGroupFloats * per];
     __shared__ uint16_t s_rc[kMaxDist];
     __shared__ __align__(4) uint8_t s_prio[(kMaxTreelet + 1) * 32];
     for (int k = threadIdx.x; k < kMaxDist; k += blockDim.x) {
@@ -900,12 +1210,13 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Seg
         reinterpret_cast<uint32_t*>(s_prio)[k] = reinterpret_cast<const uint32_t*>(&g_argmax_priority.rank[0][0])[k];
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int grp = lane / G;
+    const int gw = QUADS ? 4 : G;
+    const int grp = lane / gw;
     const uint32_t beg = lv.hist[lev], end = lv.hist[lev + 1];
     const uint32_t warp = blockIdx.x * W + w, nwarps = gridDim.x * W;
-    for (uint32_t e0 = beg + warp * NG; e0 < end; e0 += nwarps * NG) {
+    for (uint32_t e0 = beg + warp * per; e0 < end; e0 += nwarps * per) {
         const uint32_t e = e0 + (uint32_t)grp;
-        const bool has = grp < NG && e < end;
+        const bool has = grp < per && e < end;
         int nb = 0, x = 0, tsize = 0;
         uint32_t n = 2;
         int4* kd = lv.kids;
@@ -923,24 +1234,27 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Seg
             const int4 k = __ldcg(kd + x);
             root_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, __ldcg(g.area + nb + x)), __ldcg(g.nsah + nb + k.x)),
                                  __ldcg(g.nsah + nb + k.y));
-            if (lane == grp * G) g.nsah[nb + x] = root_sah;
+            if (lane == grp * gw) g.nsah[nb + x] = root_sah;
         }
         const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)tsize : 0u);
         __syncwarp();
         const NextRefs nx{lv.subtree + nb, nl, lv.nsah_next + nb, tsize << (iteration + 1)};
-        process_group<G>(g, has, nb, n, x, kd, nx, root_sah, tsize, maxts, ci,
-                         &s_mem[w][0] + (grp < NG ? grp : NG - 1) * GroupLayout<G>::kFloats, s_rc, s_prio, err);
+        float* const sm = &s_mem[w][0] + (grp < per ? grp : per - 1) * kGroupFloats;
+        if constexpr (QUADS)
+            process_quad<kQuadLeaves>(g, has, nb, n, x, kd, nx, root_sah, tsize, maxts, ci, sm, s_rc, s_prio, err);
+        else
+            process_group<G>(g, has, nb, n, x, kd, nx, root_sah, tsize, maxts, ci, sm, s_rc, s_prio, err);
     }
 }
 
-template <int G>
+template <int G, bool QUADS>
 void launch_level_g(int warps, unsigned blocks, cudaStream_t s, const TreeRefs& g, const Segs& segs,
                     const LevelRefs& lv, int lev, int tsize, const uint8_t* seg_tsize, int it, float ci,
                     uint32_t* err) {
     switch (warps) {
-        case 2: k_level_groups<G, 2><<<blocks, 64, 0, s>>>(g, segs, lv, lev, tsize, seg_tsize, it, ci, err); break;
-        case 8: k_level_groups<G, 8><<<blocks, 256, 0, s>>>(g, segs, lv, lev, tsize, seg_tsize, it, ci, err); break;
-        default: k_level_groups<G, 4><<<blocks, 128, 0, s>>>(g, segs, lv, lev, tsize, seg_tsize, it, ci, err); break;
+        case 2: k_level_groups<G, 2, QUADS><<<blocks, 64, 0, s>>>(g, segs, lv, lev, tsize, seg_tsize, it, ci, err); break;
+        case 8: k_level_groups<G, 8, QUADS><<<blocks, 256, 0, s>>>(g, segs, lv, lev, tsize, seg_tsize, it, ci, err); break;
+        default: k_level_groups<G, 4, QUADS><<<blocks, 128, 0, s>>>(g, segs, lv, lev, tsize, seg_tsize, it, ci, err); break;
     }
 }
 
@@ -1038,12 +1352,22 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
             k_level_scatter<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
             ctx->launches += 3;
             const unsigned lg = (unsigned)ctx->num_sms * (256 / threads) * 4;
-            for (int lev = 1; lev <= L; ++lev) {
-                switch (gw) {
-                    case 8: launch_level_g<8>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
-                    case 10: launch_level_g<10>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
-                    case 16: launch_level_g<16>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
-                    default: launch_level_g<32>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
+            // Roots per level fall by about 0.62 per level from n / (1.5 gamma)
+            // at level 1 (gamma = tsize << it); levels expected to hold at
+            // least atr_quad_min roots run in four-lane groups.
+            const double gamma = (double)(tsize << it);
+            double expect = (double)segs.n / (1.5 * gamma);
+            for (int lev = 1; lev <= L; ++lev, expect *= 0.62) {
+                const bool quads = max_ts <= kQuadLeaves && ctx->atr_quad_min >= 0 && expect >= ctx->atr_quad_min;
+                if (quads) {
+                    launch_level_g<8, true>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error);
+                } else {
+                    switch (gw) {
+                        case 8: launch_level_g<8, false>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
+                        case 10: launch_level_g<10, false>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
+                        case 16: launch_level_g<16, false>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
+                        default: launch_level_g<32, false>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;
+                    }
                 }
                 ++ctx->launches;
             }

@@ -112,14 +112,19 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
  *                           4 passes over 30-bit codes, 8 over 63-bit) or 10
  *                           (3 and 7 passes).
  *   ATR_TUNE_ATR_LEVELS     ATRBVH levels of treelet roots restructured level
- *                           by level, one thread per treelet (0..64; default
- *                           16; 0 = all by the bottom-up warp pass); used when
- *                           every treelet size is at most 10. */
+ *                           by level in lane groups (0..64; default 16; 0 =
+ *                           all by the bottom-up warp pass); used when every
+ *                           treelet size is at most 10.
+ *   ATR_TUNE_QUAD_MIN       fewest treelet roots of one level that the level
+ *                           pass restructures in four-lane groups, eight per
+ *                           warp, instead of 32/G per warp (-1 = never;
+ *                           default 80000). */
 enum atr_tune_knob {
     ATR_TUNE_ATR_WARPS = 0,
     ATR_TUNE_ATR_GROUP_MIN = 1,
     ATR_TUNE_SORT_BITS = 2,
-    ATR_TUNE_ATR_LEVELS = 3
+    ATR_TUNE_ATR_LEVELS = 3,
+    ATR_TUNE_QUAD_MIN = 4
 };
 int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value);
 int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value);
