@@ -306,13 +306,41 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(
         const int d = threadIdx.x * R + r;
         uint32_t prefix = 0;
         if (tile != first_tile) {
+            // Eight predecessors per poll (tiles before the mesh's first read
+            // as an inclusive zero): add aggregates in order up to the first
+            // inclusive prefix, or stop at the first tile not yet published.
+            constexpr int kWin = 8;
             int64_t k = (int64_t)tile - 1;
             uint32_t polls = 0;
-            while (k >= (int64_t)first_tile) {
-                const uint32_t sv = *reinterpret_cast<volatile uint32_t*>(status + (size_t)k * D + d);
-                if (sv & kFlagInc) { prefix += sv & kValueMask; break; }
-                if (sv & kFlagAgg) { prefix += sv & kValueMask; --k; continue; }
-                if (++polls > kLookbackLimit) { set_error_bits(err, kErrSortLookback); break; }
+            bool done = false;
+            while (!done) {
+                uint32_t sv[kWin];
+#pragma unroll
+                for (int u = 0; u < kWin; ++u) {
+                    sv[u] = 0x80000000u;  // kFlagInc with value 0
+                    if (k - u >= (int64_t)first_tile)
+                        sv[u] = *reinterpret_cast<volatile uint32_t*>(status + (size_t)(k - u) * D + d);
+                }
+                int used = 0;
+                bool stop = false;
+#pragma unroll
+                for (int u = 0; u < kWin; ++u) {
+                    if (stop || done) continue;
+                    if (sv[u] & kFlagInc) {
+                        prefix += sv[u] & kValueMask;
+                        done = true;
+                    } else if (sv[u] & kFlagAgg) {
+                        prefix += sv[u] & kValueMask;
+                        ++used;
+                    } else {
+                        stop = true;
+                    }
+                }
+                k -= used;
+                if (!done && used == 0 && ++polls > kLookbackLimit) {
+                    set_error_bits(err, kErrSortLookback);
+                    break;
+                }
             }
             __threadfence();
             __stcg(st + r, kFlagInc | (prefix + count[r]));
