@@ -50,11 +50,12 @@ WORKLOAD = ("clustered scene 4,194,304 tris (75% 64-Gaussian mixture, 25% 1024x5
 # writes subtree count and nodesSah (8 B x 2) and a child record and counter per
 # internal node (24 B).
 BYTES_PER_TRI = {"morton": 56.0, "sort": 4.0 + 16.0 * 4, "build": 40.0 + 180.0, "atrbvh": 2 * 136.0}
-# DRAM bytes per triangle of the ATRBVH phase (both iterations) from the ncu
-# capture in profiles/launches_clustered4M_bench_step.md (2,097,152 triangles:
-# k_levels 140.8 MB, k_level_hist 18.4, k_level_scatter 16.8, k_level_groups
-# 2009.2, k_atrbvh 3.9), scaled by triangle count.
-ATRBVH_DRAM_BYTES_PER_TRI = (140.8 + 18.4 + 16.8 + 2009.2 + 3.9) * 1e6 / 2097152
+# DRAM bytes per triangle of the ATRBVH phase (both iterations) from an ncu
+# capture of this bench step at 2,097,152 triangles (dram__bytes_read.sum +
+# dram__bytes_write.sum: k_levels_pp 136.6 MB, k_level_hist 38.1,
+# k_level_scatter 16.8, k_level_groups 1914.4, k_atrbvh 3.8), scaled by
+# triangle count.
+ATRBVH_DRAM_BYTES_PER_TRI = (136.6 + 38.1 + 16.8 + 1914.4 + 3.8) * 1e6 / 2097152
 
 
 def _read_peaks() -> dict:
