@@ -42,6 +42,14 @@ __device__ __forceinline__ uint32_t atomic_add_acq_rel_gpu(uint32_t* p, uint32_t
     return old;
 }
 
+// Atomic exchange with acquire-release semantics at GPU scope (the arrival
+// slots of the LBVH climb): one instruction in place of fence, exchange, fence.
+__device__ __forceinline__ int atomic_exch_acq_rel_gpu(int* p, int v) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.exch.b32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 // 16-byte global-to-shared copy through L2 (cp.async.cg) that leaves no
 // register pending: a later reader waits only for its own copies.
 __device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {

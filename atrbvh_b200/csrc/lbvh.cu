@@ -565,10 +565,8 @@ __global__ void __launch_bounds__(256) k_build_top(Segs segs, const K* __restric
     while (true) {
         const bool is_left = dr > dl;
         const int split = is_left ? r : l - 1;
-        fence_acq_rel_gpu();
-        const int other = atomicExch(&slot[split], is_left ? l : r);
+        const int other = atomic_exch_acq_rel_gpu(&slot[split], is_left ? l : r);
         if (other < 0) return;  // first of the two children: the sibling finishes the parent
-        fence_acq_rel_gpu();
         const int pl = is_left ? l : other;
         const int pr = is_left ? other : r;
         const int lc = split == pl ? split + last : split;
