@@ -480,6 +480,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
     __shared__ __align__(16) float s_mem[W][kWarpFloats];
     __shared__ uint16_t s_rc[kMaxDist];
     __shared__ __align__(4) uint8_t s_prio[(kMaxTreelet + 1) * 32];
+    if (start && blockIdx.x * blockDim.x >= *start_count) return;  // no frontier node for this block
     for (int k = threadIdx.x; k < kMaxDist; k += blockDim.x) {
         int r, c;
         trm_rc(k, r, c);
@@ -524,14 +525,17 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
             cur = g.parent[leaf];
         }
     }
+    // The arrival atomic is acquire-release; after a treelet rewrite, whose
+    // stores other lanes of the warp made, a fence first publishes those too.
+    bool rewrote = false;
     while (__any_sync(kFull, cur >= 0 || next < n_start)) {
         if (cur < 0 && next < n_start) take_start();
         const int gamma = tsize << iteration;
         bool second = false;
         if (cur >= 0) {
-            fence_acq_rel_gpu();
-            if (atomicAdd(&counters[cbase + cur], 1u) == 0u) cur = -1;
-            else { second = true; fence_acq_rel_gpu(); }
+            if (rewrote) fence_acq_rel_gpu();
+            if (atomic_add_acq_rel_gpu(&counters[cbase + cur], 1u) == 0u) cur = -1;
+            else second = true;
         }
         int cnt = 0;
         float my_sah = 0.0f;
@@ -553,6 +557,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
             }
         }
         unsigned vote = __ballot_sync(kFull, cnt >= gamma);
+        rewrote = vote != 0;
         if (vote) __syncwarp();
         while (vote) {
             if (G < 32 && __popc(vote) >= group_min) {
@@ -741,7 +746,8 @@ __global__ void __launch_bounds__(kLvBlock) k_levels(TreeRefs g, Segs segs, Leve
 // wait at a root only when both of its children are roots.
 __global__ void __launch_bounds__(256) k_levels_pp(TreeRefs g, Segs segs, LevelRefs lv, const int2* __restrict__ ranges,
                                                    int tsize_all, const uint8_t* __restrict__ seg_tsize,
-                                                   const uint8_t* __restrict__ seg_iters, int iteration) {
+                                                   const uint8_t* __restrict__ seg_iters, int iteration,
+                                                   bool levels_known) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= segs.n) return;
     const uint32_t m = segs.seg_of_tri(i);
@@ -771,6 +777,7 @@ __global__ void __launch_bounds__(256) k_levels_pp(TreeRefs g, Segs segs, LevelR
         lv.nsah_next[base + x] = g.nsah[base + x];
         return;
     }
+    if (levels_known) return;  // the build left every level in lv.level
     if (count(lc) >= gamma || count(rc) >= gamma) return;  // not a level-1 root: reached by a climb
     int lvl = 1;
     while (true) {
@@ -1201,6 +1208,8 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Seg
     __shared__ __align__(16) float s_mem[W][kGroupFloats * per];
     __shared__ uint16_t s_rc[kMaxDist];
     __shared__ __align__(4) uint8_t s_prio[(kMaxTreelet + 1) * 32];
+    const uint32_t beg = lv.hist[lev], end = lv.hist[lev + 1];
+    if (beg + blockIdx.x * (uint32_t)(W * per) >= end) return;  // no root for this block
     for (int k = threadIdx.x; k < kMaxDist; k += blockDim.x) {
         int r, c;
         trm_rc(k, r, c);
@@ -1212,7 +1221,6 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Seg
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int gw = QUADS ? 4 : G;
     const int grp = lane / gw;
-    const uint32_t beg = lv.hist[lev], end = lv.hist[lev + 1];
     const uint32_t warp = blockIdx.x * W + w, nwarps = gridDim.x * W;
     for (uint32_t e0 = beg + warp * per; e0 < end; e0 += nwarps * per) {
         const uint32_t e = e0 + (uint32_t)grp;
@@ -1287,6 +1295,9 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     // The build's prepass (counts, first nodesSah, child records) serves as
     // those arrays when its constants are this pass's.
     const bool use_pp = prepass && prepass->nsah && karras_ranges && L > 0 && ci == kPrepassCi && ct == kPrepassCt;
+    // ... and its levels serve as the first iteration's when gamma is this
+    // pass's treelet size for every mesh.
+    const bool use_pp_levels = use_pp && prepass->level && !seg_tsize && tsize == prepass->gamma;
     ATR_TRY(ctx->alloc(&scratch, b_sub + (use_pp ? 1 : 2) * b_sah + b_kid + b_ctr + 2 * b_lvl + b_ord + b_front +
                                      b_small));
     char* p = static_cast<char*>(scratch);
@@ -1325,7 +1336,7 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     cudaError_t e = cudaSuccess;
     ctx->phase_begin("atrbvh");
     for (int it = 0; it < iterations && e == cudaSuccess; ++it) {
-        lv.level = lvl[it & 1];
+        lv.level = it == 0 && use_pp_levels ? prepass->level : lvl[it & 1];
         lv.next = lvl[(it + 1) & 1];
         g.nsah = lv.nsah = ns[it & 1];
         lv.nsah_next = ns[(it + 1) & 1];
@@ -1338,7 +1349,8 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
             e = cudaMemsetAsync(lv.hist, 0, b_small, st);
             const unsigned gb = (segs.n + 255) / 256;
             if (it == 0 && use_pp)
-                k_levels_pp<<<gb, 256, 0, st>>>(g, segs, lv, karras_ranges, tsize, seg_tsize, seg_iters, it);
+                k_levels_pp<<<gb, 256, 0, st>>>(g, segs, lv, karras_ranges, tsize, seg_tsize, seg_iters, it,
+                                                use_pp_levels);
             else if (it == 0)
                 k_levels<<<(segs.n + kLvBlock - 1) / kLvBlock, kLvBlock, 0, st>>>(g, segs, lv, tsize, seg_tsize,
                                                                                   seg_iters, it, ci, ct, L,

@@ -416,7 +416,8 @@ struct BuildOut {
 // Record of the internal node p over leaves [pl, pr] with children lc, rc.
 template <typename K>
 __device__ __forceinline__ void write_inner(const BuildOut<K>& o, const Segs& segs, uint32_t m, int nb, int p, int pl,
-                                            int pr, int lc, int rc, float4 mn, float4 mx, float pa, float ns) {
+                                            int pr, int lc, int rc, float4 mn, float4 mx, float pa, float ns,
+                                            int lvl) {
     o.left[nb + p] = lc;
     o.right[nb + p] = rc;
     o.data[nb + p] = -1;
@@ -427,6 +428,7 @@ __device__ __forceinline__ void write_inner(const BuildOut<K>& o, const Segs& se
     o.bmax[nb + p] = mx;
     o.area[nb + p] = pa;
     if (o.pp.nsah) o.pp.nsah[nb + p] = ns;
+    if (o.pp.level) o.pp.level[segs.inner_base(m) + p] = lvl;
 }
 
 constexpr int kBuildBlock = 256;
@@ -438,6 +440,7 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
                                                              BuildEdge* __restrict__ edges) {
     __shared__ float4 s_lmn[kBuildBlock], s_lmx[kBuildBlock], s_imn[kBuildBlock], s_imx[kBuildBlock];
     __shared__ float s_lns[kBuildBlock], s_ins[kBuildBlock];
+    __shared__ int s_ilv[kBuildBlock];  // prepass levels of the block's finished internal nodes
     __shared__ int s_slot[kBuildBlock];
     __shared__ int s_delta[kBuildBlock + 1];  // delta at sorted position B0 - 1 + k
     const int tid = threadIdx.x;
@@ -490,6 +493,7 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
         const int off = (int)s0 - (int)B0;  // block position of mesh-local sorted index 0
         auto sd = [&](int x) { return s_delta[off + x + 1]; };
         int l = (int)i, r = (int)i, node = (int)i + last;
+        int my_lv = 0;
         int dl = l > 0 ? sd(l - 1) : -1;
         int dr = r < last ? sd(r) : -1;
         while (true) {
@@ -527,10 +531,12 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
                 const float sns = sib_leaf ? s_lns[sp] : s_ins[sp];
                 my_ns = __fadd_rn(__fadd_rn(__fmul_rn(kPrepassCi, pa), is_left ? my_ns : sns), is_left ? sns : my_ns);
             }
-            write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns);
+            if (o.pp.level) my_lv = pr - pl + 1 >= o.pp.gamma ? 1 + max(my_lv, sib_leaf ? 0 : s_ilv[sp]) : 0;
+            write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns, my_lv);
             s_imn[off + p] = mn;
             s_imx[off + p] = mx;
             s_ins[off + p] = my_ns;
+            s_ilv[off + p] = my_lv;
             if (root) {
                 o.parent[nb] = -1;
                 break;
@@ -559,6 +565,8 @@ __global__ void __launch_bounds__(256) k_build_top(Segs segs, const K* __restric
     int32_t* slot = o.slot + segs.inner_base(m);
     float4 mn = ld_cg(o.bmin + nb + e.node), mx = ld_cg(o.bmax + nb + e.node);
     float my_ns = o.pp.nsah ? ld_cg(o.pp.nsah + nb + e.node) : 0.0f;
+    const int32_t* const plv = o.pp.level + segs.inner_base(m);
+    int my_lv = o.pp.level && e.node < last ? ld_cg(plv + e.node) : 0;
     int l = e.l, r = e.r;
     int dl = l > 0 ? delta_adj(keys, l - 1) : -1;
     int dr = r < last ? delta_adj(keys, r) : -1;
@@ -587,7 +595,9 @@ __global__ void __launch_bounds__(256) k_build_top(Segs segs, const K* __restric
             const float sns = ld_cg(o.pp.nsah + nb + sib);
             my_ns = __fadd_rn(__fadd_rn(__fmul_rn(kPrepassCi, pa), is_left ? my_ns : sns), is_left ? sns : my_ns);
         }
-        write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns);
+        if (o.pp.level)
+            my_lv = pr - pl + 1 >= o.pp.gamma ? 1 + max(my_lv, sib < last ? ld_cg(plv + sib) : 0) : 0;
+        write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns, my_lv);
         if (root) {
             o.parent[nb] = -1;
             return;
@@ -797,9 +807,10 @@ int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4
 }
 
 int prepass_alloc(atr_ctx* ctx, size_t total_nodes, size_t inner, void** block, BuildPrepass* pp) {
-    (void)inner;
-    ATR_TRY(ctx->alloc(block, total_nodes * 4));
+    ATR_TRY(ctx->alloc(block, align256(total_nodes * 4) + inner * 4));
     pp->nsah = static_cast<float*>(*block);
+    pp->level = reinterpret_cast<int32_t*>(static_cast<char*>(*block) + align256(total_nodes * 4));
+    pp->gamma = kPrepassGamma;
     return ATR_OK;
 }
 
