@@ -532,7 +532,17 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
         if (cur < 0 && next < n_start) take_start();
         const int gamma = tsize << iteration;
         bool second = false;
+        // A node's links, area and parent stay as they are until it is
+        // reached (only a treelet rooted at it or above rewrites them), so
+        // they are loaded before the arrival atomic.
+        int lc = 0, rc = 0, up = -1;
+        float a = 0.0f;
         if (cur >= 0) {
+            const int x = base + cur;
+            lc = ld_cg(g.left + x);
+            rc = ld_cg(g.right + x);
+            up = ld_cg(g.parent + x);
+            a = ld_cg(g.area + x);
             if (rewrote) fence_acq_rel_gpu();
             if (atomic_add_acq_rel_gpu(&counters[cbase + cur], 1u) == 0u) cur = -1;
             else second = true;
@@ -541,9 +551,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
         float my_sah = 0.0f;
         if (second) {
             const int x = base + cur;
-            const int lc = ld_cg(g.left + x), rc = ld_cg(g.right + x);
             const int l = base + lc, r = base + rc;
-            const float a = ld_cg(g.area + x);
             cnt = ld_cg(subtree + l) + ld_cg(subtree + r);
             my_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), ld_cg(g.nsah + l)), ld_cg(g.nsah + r));
             subtree[x] = cnt;
@@ -593,7 +601,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                 vote &= vote - 1;
             }
         }
-        if (cur >= 0) cur = ld_cg(g.parent + base + cur);
+        if (cur >= 0) cur = up;
     }
 }
 

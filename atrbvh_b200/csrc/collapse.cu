@@ -80,15 +80,18 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
     }
     int cur = g.parent[nb + leaf];
     while (cur >= 0) {
-        if (atomic_add_acq_rel_gpu(&ctr[cur], 1u) == 0u) return;
+        // The tree is read-only here: its links and area are loaded before
+        // the arrival atomic, so the second arrival waits only for the
+        // children's records.
         const int x = nb + cur;
-        const int l = g.left[x], r = g.right[x];
+        const int l = g.left[x], r = g.right[x], up = g.parent[x];
+        const float a = g.area[x];
+        if (atomic_add_acq_rel_gpu(&ctr[cur], 1u) == 0u) return;
         const int2 el = __ldcg(g.rec + nb + l), er = __ldcg(g.rec + nb + r);
         const int cl = el.y >> 1, cr = er.y >> 1;
         const float kl = __int_as_float(el.x), kr = __int_as_float(er.x);
         const int pl = el.y & 1, pr = er.y & 1;
         const int cnt = cl + cr;
-        const float a = g.area[x];
         float c = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), kl), kr);
         const float leaf_cost = __fmul_rn(__fmul_rn(ct, a), (float)cnt);
         const bool col = leaf_cost < c && (max_leaf <= 0 || cnt <= max_leaf);
@@ -100,7 +103,7 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
         }
         g.c_count[x] = cnt;
         g.rec[x] = make_int2(__float_as_int(c), (cnt << 1) | (reached && col ? 1 : 0));
-        cur = g.parent[x];
+        cur = up;
     }
 }
 

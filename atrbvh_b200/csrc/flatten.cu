@@ -77,15 +77,17 @@ __global__ void __launch_bounds__(256) k_flat_counts(FlatRefs t, Segs segs, uint
     const SegPos q = seg_pos(segs, gi);
     int cur = t.parent[q.nb + (int)q.li + (int)q.n - 1];
     while (cur >= 0) {
-        if (atomic_add_acq_rel_gpu(&counters[q.cb + cur], 1u) == 0u) return;
-        const int l = t.left[q.nb + cur], r = t.right[q.nb + cur];
+        // Links are read-only here: loaded before the arrival atomic.
+        const int l = t.left[q.nb + cur], r = t.right[q.nb + cur], up = t.parent[q.nb + cur];
         const bool ll = c_leaf(t, q.nb, l), rl = c_leaf(t, q.nb, r);
+        const bool cleaf = c_leaf(t, q.nb, cur);
+        if (atomic_add_acq_rel_gpu(&counters[q.cb + cur], 1u) == 0u) return;
         const uint32_t il = ll ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + q.cb + l);
         const uint32_t ir = rl ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + q.cb + r);
-        icnt[q.cb + cur] = c_leaf(t, q.nb, cur) ? 0u : 1u + il + ir;
+        icnt[q.cb + cur] = cleaf ? 0u : 1u + il + ir;
         ic[q.cb + cur] = (ll ? 0u : 1u) + (rl ? 0u : 1u);
         tw[q.cb + cur] = (ll ? woop_entries(t, q.nb, l) : 0u) + (rl ? woop_entries(t, q.nb, r) : 0u);
-        cur = t.parent[q.nb + cur];
+        cur = up;
     }
 }
 
