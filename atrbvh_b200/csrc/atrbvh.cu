@@ -1014,17 +1014,38 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
     // next nodesSah, -); a retired slot holds the new node of its step:
     // (min.xyz, cost), (max.xyz, left child), (count, next level, next
     // nodesSah, right child).
-    if (run) {
-        for (int k = gl; k < tsize; k += 4) {
-            const int node = __float_as_int(lmx[k].w);
-            const float4 mn = ld_cg(BMN + node), mx = ld_cg(BMX + node);
-            const float sah = ld_cg(NS + node);
-            const int cnt = ld_cg(nx.sub + node);
-            const float nsn = ld_cg(nx.nsn + node);
-            const int nlv = is_internal(node, n) ? ld_cg(nx.nlv + node) : 0;
-            lmn[k] = make_float4(mn.x, mn.y, mn.z, sah);
-            lmx[k] = make_float4(mx.x, mx.y, mx.z, __int_as_float(node));
-            lcn[k] = make_int4(cnt, nlv, __float_as_int(nsn), 0);
+    // A lane's leaves arrive by cp.async, all in flight at once: boxes into
+    // lmn/lmx, count, next level, next nodesSah into lcn and nodesSah parked
+    // in lcn.w, then moved to lmn.w.  Nothing else in this level pass writes
+    // a treelet leaf's records.
+    {
+        int node[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const int k = gl + 4 * q;
+            node[q] = run && k < tsize ? __float_as_int(lmx[k].w) : -1;
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            if (node[q] < 0) continue;
+            const int k = gl + 4 * q;
+            int* const c = reinterpret_cast<int*>(lcn + k);
+            cp_async16_cg(lmn + k, BMN + node[q]);
+            cp_async16_cg(lmx + k, BMX + node[q]);
+            cp_async4_ca(c, nx.sub + node[q]);
+            cp_async4_ca(c + 2, nx.nsn + node[q]);
+            cp_async4_ca(c + 3, NS + node[q]);
+            if (is_internal(node[q], n)) cp_async4_ca(c + 1, nx.nlv + node[q]);
+            else c[1] = 0;
+        }
+        cp_async_wait_all();
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            if (node[q] < 0) continue;
+            const int k = gl + 4 * q;
+            lmn[k].w = __int_as_float(lcn[k].w);
+            lmx[k].w = __int_as_float(node[q]);
+            lcn[k].w = 0;
         }
     }
     __syncwarp();

@@ -56,6 +56,12 @@ __device__ __forceinline__ void cp_async16_cg(void* smem, const void* gmem) {
     const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
 }
+// 4-byte form (cp.async.ca: through L1; for data no other thread of the
+// running launch writes).
+__device__ __forceinline__ void cp_async4_ca(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
