@@ -1112,6 +1112,7 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
         float4 w0 = make_float4(0.f, 0.f, 0.f, 0.f), w1 = w0;
         int4 w2 = make_int4(0, 0, 0, 0);
         int wslot = -1;
+        float ral = 0.f, rar = 0.f;
         if (act) {
             const uint32_t rc = s_rc[mi];
             jr = (int)(rc >> 8);
@@ -1143,6 +1144,10 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
                 w0 = make_float4(a0x, a0y, a0z, la);
                 w1 = make_float4(a1x, a1y, a1z, r1.w);
                 w2 = make_int4(cnt, nlv, __float_as_int(nsn), __float_as_int(c1.w));
+                // The children's areas (their boxes' surface areas, as the
+                // area array holds them) for the child record at the rewrite.
+                ral = box_area(r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
+                rar = box_area(c0.x, c0.y, c0.z, c1.x, c1.y, c1.z);
             }
         }
         // updateDistancesMatrix (:152-188): row `last` moves to row jr, then
@@ -1160,6 +1165,7 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
             lmx[wslot] = w1;
             lcn[wslot] = w2;
         }
+
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             const int c = gl + 4 * q;
@@ -1174,6 +1180,14 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
                 dist[trm_idx(max(jc, c), min(jc, c))] =
                     union_area3(a0x, a0y, a0z, a1x, a1y, a1z, b0.x, b0.y, b0.z, b1.x, b1.y, b1.z);
             }
+        }
+        // The retired node's child areas for the rewrite: in row `last` of the
+        // matrix, dead now (slot 1's, the final step's, in slot 0, which the
+        // rewrite does not read).
+        if (act && gl == 2) {
+            float* const ca = last >= 2 ? dist + trm_idx(last, 0) : reinterpret_cast<float*>(lmn);
+            ca[0] = ral;
+            ca[1] = rar;
         }
         __syncwarp();
     }
@@ -1209,12 +1223,15 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
         }
     }
     __syncwarp();
-    // The rewritten nodes' child records, once every new area is stored.
+    // The rewritten nodes' child records, with the child areas kept in the
+    // dead matrix rows.
 #pragma unroll
     for (int q = 0; q < 3; ++q)
-        if (nis[q] >= 0)
-            KD[nis[q]] = make_int4(fls[q], frs[q], __float_as_int(__ldcg(AR + fls[q])),
-                                   __float_as_int(__ldcg(AR + frs[q])));
+        if (nis[q] >= 0) {
+            const int sl = 1 + gl + 4 * q;
+            const float* const ca = sl >= 2 ? dist + trm_idx(sl, 0) : reinterpret_cast<const float*>(lmn);
+            KD[nis[q]] = make_int4(fls[q], frs[q], __float_as_int(ca[0]), __float_as_int(ca[1]));
+        }
     // A treelet left as it was: its root's next level and next nodesSah.
     if (run && !accept && gl == 0) {
         const int lc = ld_cg(Lf + root), rc = ld_cg(Rt + root);
