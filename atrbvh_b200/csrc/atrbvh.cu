@@ -141,7 +141,8 @@ __device__ __forceinline__ float union_area3(float ax0, float ay0, float az0, fl
 // the shuffles stay warp-wide.  sm is this group's shared memory.
 template <int G>
 __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, int nb, uint32_t n, int root,
-                                              int4* KD, const NextRefs& nx, float root_sah, int tsize, int maxts,
+                                              int4 rk, int4* KD, const NextRefs& nx, float root_sah, int tsize,
+                                              int maxts,
                                               float ci, float* sm, const uint16_t* __restrict__ s_rc,
                                               const uint8_t* __restrict__ s_prio, uint32_t* err) {
     using Lay = GroupLayout<G>;
@@ -176,10 +177,7 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
         s_area = area;
         if (is_internal(node, n)) cp_async16_cg(krec + gl, KD + node);
     };
-    if (active && gl < 2) {
-        const int4 k = __ldcg(KD + root);
-        join(gl == 0 ? k.x : k.y, __int_as_float(gl == 0 ? k.z : k.w));
-    }
+    if (active && gl < 2) join(gl == 0 ? rk.x : rk.y, __int_as_float(gl == 0 ? rk.z : rk.w));
     bool ok = true;
     for (int it = 0; it < maxts - 2; ++it) {
         const bool act = active && ok && it < tsize - 2;
@@ -549,6 +547,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
         }
         int cnt = 0;
         float my_sah = 0.0f;
+        int4 myk = make_int4(-1, -1, 0, 0);
         if (second) {
             const int x = base + cur;
             const int l = base + lc, r = base + rc;
@@ -558,7 +557,8 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
             g.nsah[x] = my_sah;
             // Child record for treelet formation: one load yields both
             // children and their areas.
-            kids[cbase + cur] = make_int4(lc, rc, __float_as_int(ld_cg(g.area + l)), __float_as_int(ld_cg(g.area + r)));
+            myk = make_int4(lc, rc, __float_as_int(ld_cg(g.area + l)), __float_as_int(ld_cg(g.area + r)));
+            kids[cbase + cur] = myk;
             if (cnt < gamma) {  // not a treelet root now, nor next iteration
                 next_lv[cbase + cur] = 0;
                 nsah_next[x] = my_sah;
@@ -582,8 +582,10 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                 const uint32_t rn = __shfl_sync(kFull, nm, rl);
                 const int rts = __shfl_sync(kFull, tsize, rl);
                 const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)rts : 0u);
+                const int4 rk = make_int4(__shfl_sync(kFull, myk.x, rl), __shfl_sync(kFull, myk.y, rl),
+                                          __shfl_sync(kFull, myk.z, rl), __shfl_sync(kFull, myk.w, rl));
                 const NextRefs nx{subtree + rbase, next_lv + rcb, nsah_next + rbase, rts << (iteration + 1)};
-                process_group<G>(g, has, rbase, rn, root, kids + rcb, nx, rsah, rts, maxts, ci,
+                process_group<G>(g, has, rbase, rn, root, rk, kids + rcb, nx, rsah, rts, maxts, ci,
                                  &s_mem[w][0] + (grp < NG ? grp : NG - 1) * GroupLayout<G>::kFloats, s_rc, s_prio, err);
 #pragma unroll
                 for (int k = 0; k < NG; ++k) vote &= vote - 1;
@@ -595,9 +597,11 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                 const int rcb = __shfl_sync(kFull, cbase, rl);
                 const uint32_t rn = __shfl_sync(kFull, nm, rl);
                 const int rts = __shfl_sync(kFull, tsize, rl);
+                const int4 rk = make_int4(__shfl_sync(kFull, myk.x, rl), __shfl_sync(kFull, myk.y, rl),
+                                          __shfl_sync(kFull, myk.z, rl), __shfl_sync(kFull, myk.w, rl));
                 const NextRefs nx{subtree + rbase, next_lv + rcb, nsah_next + rbase, rts << (iteration + 1)};
-                process_group<32>(g, true, rbase, rn, root, kids + rcb, nx, rsah, rts, rts, ci, &s_mem[w][0], s_rc,
-                                  s_prio, err);
+                process_group<32>(g, true, rbase, rn, root, rk, kids + rcb, nx, rsah, rts, rts, ci, &s_mem[w][0],
+                                  s_rc, s_prio, err);
                 vote &= vote - 1;
             }
         }
@@ -917,7 +921,8 @@ constexpr int kQuadLeaves = 10;  // largest treelet the quad path takes
 
 template <int KL>
 __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int nb, uint32_t n, int root,
-                                             int4* KD, const NextRefs& nx, float root_sah, int tsize, int maxts,
+                                             int4 rk, int4* KD, const NextRefs& nx, float root_sah, int tsize,
+                                             int maxts,
                                              float ci, float* sm, const uint16_t* __restrict__ s_rc,
                                              const uint8_t* __restrict__ s_prio, uint32_t* err) {
     using Lay = QuadLayout<KL>;
@@ -949,12 +954,11 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
         if (is_internal(node, n)) cp_async16_cg(krec + k, KD + node);
     };
     if (active) {
-        const int4 k = __ldcg(KD + root);
         if (gl == 0) {
-            join(0, k.x, __int_as_float(k.z));
+            join(0, rk.x, __int_as_float(rk.z));
             inner[0] = root;
         }
-        if (gl == 1) join(1, k.y, __int_as_float(k.w));
+        if (gl == 1) join(1, rk.y, __int_as_float(rk.w));
     }
     __syncwarp();
     bool ok = true;
@@ -1276,6 +1280,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Seg
         int4* kd = lv.kids;
         int32_t* nl = lv.next;
         float root_sah = 0.0f;
+        int4 rk = make_int4(-1, -1, 0, 0);
         if (has) {
             const uint2 q = lv.order[e];
             const uint32_t s0 = segs.tri_begin(q.x);
@@ -1285,9 +1290,9 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Seg
             nl = lv.next + segs.inner_base(q.x);
             x = (int)q.y;
             tsize = seg_tsize ? (int)seg_tsize[q.x] : tsize_all;
-            const int4 k = __ldcg(kd + x);
-            root_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, __ldcg(g.area + nb + x)), __ldcg(g.nsah + nb + k.x)),
-                                 __ldcg(g.nsah + nb + k.y));
+            rk = __ldcg(kd + x);
+            root_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, __ldcg(g.area + nb + x)), __ldcg(g.nsah + nb + rk.x)),
+                                 __ldcg(g.nsah + nb + rk.y));
             if (lane == grp * gw) g.nsah[nb + x] = root_sah;
         }
         const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)tsize : 0u);
@@ -1295,9 +1300,10 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Seg
         const NextRefs nx{lv.subtree + nb, nl, lv.nsah_next + nb, tsize << (iteration + 1)};
         float* const sm = &s_mem[w][0] + (grp < per ? grp : per - 1) * kGroupFloats;
         if constexpr (QUADS)
-            process_quad<kQuadLeaves>(g, has, nb, n, x, kd, nx, root_sah, tsize, maxts, ci, sm, s_rc, s_prio, err);
+            process_quad<kQuadLeaves>(g, has, nb, n, x, rk, kd, nx, root_sah, tsize, maxts, ci, sm, s_rc, s_prio,
+                                      err);
         else
-            process_group<G>(g, has, nb, n, x, kd, nx, root_sah, tsize, maxts, ci, sm, s_rc, s_prio, err);
+            process_group<G>(g, has, nb, n, x, rk, kd, nx, root_sah, tsize, maxts, ci, sm, s_rc, s_prio, err);
     }
 }
 
