@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
     __shared__ __align__(16) float s_mem[W][kWarpFloats];
     __shared__ uint16_t s_rc[kMaxDist];
     __shared__ __align__(4) uint8_t s_prio[(kMaxTreelet + 1) * 32];
-    if (start && blockIdx.x * blockDim.x >= *start_count) return;  // no frontier node for this block
+    if (start && blockIdx.x * W >= *start_count) return;  // no frontier node for this block
     for (int k = threadIdx.x; k < kMaxDist; k += blockDim.x) {
         int r, c;
         trm_rc(k, r, c);
@@ -494,11 +494,15 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
     // Frontier mode: climb from the frontier below the nodes the level passes
     // left over (everything under a start node is final); a thread takes the
     // next start whenever its climb ends, so any frontier size fits the grid.
+    // Starts go to lane 0 of every warp first, then lane 1, ...: a warp
+    // restructures the treelets its lanes reach one after another, so a small
+    // frontier is spread over as many warps as possible.
     const uint32_t n_start = start ? *start_count : 0u;
-    uint32_t next = i;
+    const uint32_t nwarps = gridDim.x * W;
+    uint32_t next = (uint32_t)lane * nwarps + blockIdx.x * W + (uint32_t)w;
     auto take_start = [&]() {
         const uint2 e = start[next];
-        next += gridDim.x * blockDim.x;
+        next += 32u * nwarps;
         const uint32_t s0 = segs.tri_begin(e.x);
         nm = segs.tri_end(e.x) - s0;
         base = segs.node_base(e.x);
