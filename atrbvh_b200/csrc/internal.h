@@ -84,7 +84,7 @@ struct atr_ctx {
     int sort_bits = 8;
     // ATRBVH levels restructured by the level passes (one thread per
     // treelet) before the dataflow pass takes the rest; 0 = dataflow only.
-    int atr_levels = 16;
+    int atr_levels = 12;
     // A level pass over at least this many treelet roots restructures them in
     // four-lane groups (eight per warp); -1 = never.
     int atr_quad_min = 80000;

@@ -112,7 +112,7 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
  *                           4 passes over 30-bit codes, 8 over 63-bit) or 10
  *                           (3 and 7 passes).
  *   ATR_TUNE_ATR_LEVELS     ATRBVH levels of treelet roots restructured level
- *                           by level in lane groups (0..64; default 16; 0 =
+ *                           by level in lane groups (0..64; default 12; 0 =
  *                           all by the bottom-up warp pass); used when every
  *                           treelet size is at most 10.
  *   ATR_TUNE_QUAD_MIN       fewest treelet roots of one level that the level
