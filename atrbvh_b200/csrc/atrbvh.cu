@@ -812,6 +812,72 @@ __global__ void __launch_bounds__(256) k_levels_pp(TreeRefs g, Segs segs, LevelR
     }
 }
 
+// Phase A of the first iteration when the LBVH build left the levels too:
+// one streaming pass writes the counts, child records and next-iteration
+// values of the nodes that are not big, counts the levels 1..L and lists
+// the frontier below the levels above L (k_level_hist's work as well).
+__global__ void __launch_bounds__(256) k_levels_pp_hist(TreeRefs g, Segs segs, LevelRefs lv,
+                                                        const int2* __restrict__ ranges, int tsize_all,
+                                                        const uint8_t* __restrict__ seg_tsize,
+                                                        const uint8_t* __restrict__ seg_iters, int L) {
+    __shared__ uint32_t s_hist[kMaxLevels + 2];
+    for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_hist[k] = 0;
+    __syncthreads();
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    int push = 0;
+    uint2 ent[2];
+    if (i < segs.n) {
+        const uint32_t m = segs.seg_of_tri(i);
+        const uint32_t s0 = segs.tri_begin(m);
+        const uint32_t n = segs.tri_end(m) - s0;
+        if (!seg_iters || 0 < (int)seg_iters[m]) {
+            const int base = segs.node_base(m), cb = segs.inner_base(m);
+            const int gamma = seg_tsize ? (int)seg_tsize[m] : tsize_all;
+            const int li = (int)(i - s0);
+            const int leaf = base + li + (int)n - 1;
+            lv.subtree[leaf] = 1;
+            lv.nsah_next[leaf] = g.nsah[leaf];
+            if (li < (int)n - 1) {
+                const int x = li;
+                const int lc = g.left[base + x], rc = g.right[base + x];
+                const int2 r = ranges[cb + x];
+                const int cnt = r.y - r.x + 1;
+                lv.subtree[base + x] = cnt;
+                lv.kids[cb + x] =
+                    make_int4(lc, rc, __float_as_int(g.area[base + lc]), __float_as_int(g.area[base + rc]));
+                if (cnt < gamma) {
+                    lv.level[cb + x] = 0;
+                    lv.next[cb + x] = 0;
+                    lv.nsah_next[base + x] = g.nsah[base + x];
+                } else {
+                    const int me = lv.level[cb + x];
+                    if (me <= L) {
+                        atomicAdd(&s_hist[me], 1u);
+                    } else {
+                        if ((is_internal(lc, n) ? lv.level[cb + lc] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)lc);
+                        if ((is_internal(rc, n) ? lv.level[cb + rc] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)rc);
+                    }
+                }
+            }
+        }
+    }
+    // Frontier entries: one atomic per warp.
+    uint32_t incl = push;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, incl, o);
+        if ((threadIdx.x & 31) >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    uint32_t at = 0;
+    if ((threadIdx.x & 31) == 31 && total) at = atomicAdd(lv.n_frontier, total);
+    at = __shfl_sync(kFull, at, 31) + incl - push;
+    for (int k = 0; k < push; ++k) lv.frontier[at + k] = ent[k];
+    // Level counts: one global atomic per level present in the block.
+    __syncthreads();
+    for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
+        if (s_hist[k]) atomicAdd(&lv.hist[k], s_hist[k]);
+}
+
 // Phase A of iterations after the first: the previous iteration left every
 // internal node's level for this one (next levels of the nodes it finished,
 // kept current by treelet rewrites), and subtree counts, nodesSah and child
@@ -1404,7 +1470,10 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         if (L && e == cudaSuccess) {
             e = cudaMemsetAsync(lv.hist, 0, b_small, st);
             const unsigned gb = (segs.n + 255) / 256;
-            if (it == 0 && use_pp)
+            const bool hist_done = it == 0 && use_pp_levels;
+            if (hist_done)
+                k_levels_pp_hist<<<gb, 256, 0, st>>>(g, segs, lv, karras_ranges, tsize, seg_tsize, seg_iters, L);
+            else if (it == 0 && use_pp)
                 k_levels_pp<<<gb, 256, 0, st>>>(g, segs, lv, karras_ranges, tsize, seg_tsize, seg_iters, it,
                                                 use_pp_levels);
             else if (it == 0)
@@ -1414,7 +1483,7 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
             // Level counts and the frontier of the dataflow pass (after the
             // first iteration's climb, or from the levels the previous
             // iteration left).
-            k_level_hist<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
+            if (!hist_done) k_level_hist<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
             ctx->launches += 1;
             k_level_offsets<<<1, 32, 0, st>>>(lv, L);
             k_level_scatter<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);

@@ -47,7 +47,7 @@ struct CollapseRefs {
 
 // The collapsed tree starts as a copy of the tree (TreeCollapser.cu:13-30):
 // a streaming pass over every node of every mesh (data is -1 at internal
-// nodes in both).
+// nodes in both), which also clears the emission counts.
 __global__ void __launch_bounds__(256) k_collapse_copy(CollapseRefs g, uint64_t total_nodes) {
     const uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (x >= total_nodes) return;
@@ -57,6 +57,7 @@ __global__ void __launch_bounds__(256) k_collapse_copy(CollapseRefs g, uint64_t 
     g.c_data[x] = g.data[x];
     g.c_bmin[x] = g.bmin[x];
     g.c_bmax[x] = g.bmax[x];
+    g.emit_cnt[x] = 0u;
 }
 
 // Segmented: thread i starts at the i-th leaf of the batch; node arrays are
@@ -179,7 +180,6 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
     uint32_t* offs = reinterpret_cast<uint32_t*>(p); p += b4;
     uint32_t* counters = reinterpret_cast<uint32_t*>(p);
     cudaStream_t s = ctx->stream;
-    cudaMemsetAsync(emit, 0, nn * 4, s);
     cudaMemsetAsync(counters, 0, inner * 4, s);
     cudaMemsetAsync(dst.tri_indices, 0xff, (size_t)n * 4, s);
     CollapseRefs r{n, src.area, src.parent, src.left, src.right, src.data, src.bmin, src.bmax, dst.parent, dst.left,
