@@ -52,10 +52,10 @@ WORKLOAD = ("clustered scene 4,194,304 tris (75% 64-Gaussian mixture, 25% 1024x5
 BYTES_PER_TRI = {"morton": 56.0, "sort": 4.0 + 16.0 * 4, "build": 40.0 + 180.0, "atrbvh": 2 * 136.0}
 # DRAM bytes per triangle of the ATRBVH phase (both iterations) from an ncu
 # capture of this bench step at 2,097,152 triangles (dram__bytes_read.sum +
-# dram__bytes_write.sum: k_levels_pp 136.6 MB, k_level_hist 38.1,
-# k_level_scatter 16.8, k_level_groups 1914.4, k_atrbvh 3.8), scaled by
+# dram__bytes_write.sum: k_levels_pp_hist 111.8 MB, k_level_hist 19.3,
+# k_level_scatter 16.8, k_level_groups 1896.6, k_atrbvh 13.0), scaled by
 # triangle count.
-ATRBVH_DRAM_BYTES_PER_TRI = (136.6 + 38.1 + 16.8 + 1914.4 + 3.8) * 1e6 / 2097152
+ATRBVH_DRAM_BYTES_PER_TRI = (111.8 + 19.3 + 16.8 + 1896.6 + 13.0) * 1e6 / 2097152
 
 
 def _read_peaks() -> dict:
