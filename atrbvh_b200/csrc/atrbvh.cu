@@ -1448,7 +1448,7 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         lv.cursor = lv.hist + (L + 2);
         lv.n_frontier = lv.cursor + (L + 2);
     }
-    const int warps = ctx->atr_warps == 2 || ctx->atr_warps == 8 ? ctx->atr_warps : 4;
+    const int warps = ctx->atr_warps == 2 || ctx->atr_warps == 4 ? ctx->atr_warps : 8;
     const int threads = warps * 32;
     const uint32_t leaf_blocks = (segs.n + threads - 1) / threads;
     const uint32_t front_blocks = (uint32_t)ctx->num_sms * (256 / threads) * 4;  // grid-stride over the frontier

@@ -77,7 +77,7 @@ struct atr_ctx {
     // Launch tuning (atr_ctx_set_tuning): ATRBVH warps per block (2, 4, 8);
     // fewest simultaneous treelet roots in a warp that are restructured in
     // lane groups (33: never; a single root always takes the whole warp).
-    int atr_warps = 4;
+    int atr_warps = 8;
     int atr_group_min = 2;
     // Radix sort digit width of LBVH builds: 8 (4 passes for 30-bit codes)
     // or 10 (3 passes).

@@ -104,7 +104,7 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
 /* Launch tuning of this context's kernels (no counterpart in the reference,
  * whose launch shapes are fixed: AgglomerativeTreelet.cu:556-595).  Results
  * do not depend on the tuning; only speed does.
- *   ATR_TUNE_ATR_WARPS      ATRBVH warps per block: 2, 4 (default) or 8.
+ *   ATR_TUNE_ATR_WARPS      ATRBVH warps per block: 2, 4 or 8 (default).
  *   ATR_TUNE_ATR_GROUP_MIN  fewest treelet roots reached by one warp at once
  *                           that are restructured side by side in lane groups
  *                           (2..32; 33 = never; default 2).

@@ -62,6 +62,7 @@ def test_tuning_rejects_bad_values(tuned_ctx):
 
 
 def test_autotune_table_and_tuned_batch(tuned_ctx):
+    warps0, bits0 = tuned_ctx.get_tuning(ab.TUNE_ATR_WARPS), tuned_ctx.get_tuning(ab.TUNE_SORT_BITS)
     table = ab.autotune(tuned_ctx, min_class=8, max_class=11, sample_triangles=1 << 15, reps=1)
     cls = table.classes()
     assert sorted(cls) == [8, 9, 10, 11]
@@ -72,7 +73,7 @@ def test_autotune_table_and_tuned_batch(tuned_ctx):
         assert 0.0 < e["build_ms"] <= e["reference_ms"], e
         assert e["sample_meshes"] >= 2
     # The tuning context's own knobs are restored.
-    assert tuned_ctx.get_tuning(ab.TUNE_ATR_WARPS) == 4 and tuned_ctx.get_tuning(ab.TUNE_SORT_BITS) == 8
+    assert tuned_ctx.get_tuning(ab.TUNE_ATR_WARPS) == warps0 and tuned_ctx.get_tuning(ab.TUNE_SORT_BITS) == bits0
     ts, it = table.class_arrays()
     assert ts[8] == cls[8]["treelet"] and ts[20] == cls[11]["treelet"] and ts[3] == cls[8]["treelet"]
 
