@@ -1417,9 +1417,11 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     // The build's prepass (counts, first nodesSah, child records) serves as
     // those arrays when its constants are this pass's.
     const bool use_pp = prepass && prepass->nsah && karras_ranges && L > 0 && ci == kPrepassCi && ct == kPrepassCt;
-    // ... and its levels serve as the first iteration's when gamma is this
-    // pass's treelet size for every mesh.
-    const bool use_pp_levels = use_pp && prepass->level && !seg_tsize && tsize == prepass->gamma;
+    // ... and its levels serve as the first iteration's when its gamma is this
+    // pass's treelet size (per mesh, when the sizes are per mesh).
+    const bool use_pp_levels = use_pp && prepass->level &&
+                               (seg_tsize ? prepass->seg_gamma == seg_tsize
+                                          : !prepass->seg_gamma && tsize == prepass->gamma);
     ATR_TRY(ctx->alloc(&scratch, b_sub + (use_pp ? 1 : 2) * b_sah + b_kid + b_ctr + 2 * b_lvl + b_ord + b_front +
                                      b_small));
     char* p = static_cast<char*>(scratch);

@@ -116,7 +116,11 @@ int batch_run(atr_ctx* ctx, atr_batch* b, int optimizer, int tsize, int iteratio
     BuildPrepass pp{};
     const bool want_pp = optimizer == 1 && (b->per_mesh_params ? b->max_iters : iterations) > 0 &&
                          ctx->atr_levels > 0 && ci == kPrepassCi && ct == kPrepassCt;
-    if (want_pp) ATR_TRY(prepass_alloc(ctx, b->total_nodes, b->n - b->count, &ppb, &pp));
+    if (want_pp) {
+        ATR_TRY(prepass_alloc(ctx, b->total_nodes, b->n - b->count, &ppb, &pp));
+        if (b->per_mesh_params) pp.seg_gamma = b->d_tsize;  // first iteration: gamma = each mesh's treelet size
+        else pp.gamma = tsize;
+    }
     int st = lbvh_build_segs(ctx, segs, b->tiles, b->verts, b->d_bounds, 30, b->tree, nullptr, nullptr,
                              want_pp ? &pp : nullptr);
     if (st != ATR_OK) { ctx->release(ppb); return st; }

@@ -53,12 +53,14 @@ inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 // node's nodesSah under the reference's default constants, node-indexed in
 // the batch layout, and every internal node's level among the nodes of at
 // least `gamma` triangles (0 below gamma, else 1 + the larger level of its
-// children), indexed by internal node in the batch layout (NULL: not
-// computed).  Subtree counts follow from the radix tree's leaf ranges.
+// children; gamma per mesh when seg_gamma is set), indexed by internal node
+// in the batch layout (NULL: not computed).  Subtree counts follow from the
+// radix tree's leaf ranges.
 struct BuildPrepass {
     float* nsah = nullptr;
     int32_t* level = nullptr;
     int gamma = 0;
+    const uint8_t* seg_gamma = nullptr;  // per-mesh gamma (device), in place of gamma when set
 };
 constexpr float kPrepassCi = 1.2f;  // AgglomerativeTreelet.h:75 defaults
 constexpr float kPrepassCt = 1.0f;

@@ -531,7 +531,10 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
                 const float sns = sib_leaf ? s_lns[sp] : s_ins[sp];
                 my_ns = __fadd_rn(__fadd_rn(__fmul_rn(kPrepassCi, pa), is_left ? my_ns : sns), is_left ? sns : my_ns);
             }
-            if (o.pp.level) my_lv = pr - pl + 1 >= o.pp.gamma ? 1 + max(my_lv, sib_leaf ? 0 : s_ilv[sp]) : 0;
+            if (o.pp.level) {
+                const int gam = o.pp.seg_gamma ? (int)o.pp.seg_gamma[m] : o.pp.gamma;
+                my_lv = pr - pl + 1 >= gam ? 1 + max(my_lv, sib_leaf ? 0 : s_ilv[sp]) : 0;
+            }
             write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns, my_lv);
             s_imn[off + p] = mn;
             s_imx[off + p] = mx;
@@ -596,7 +599,9 @@ __global__ void __launch_bounds__(256) k_build_top(Segs segs, const K* __restric
             my_ns = __fadd_rn(__fadd_rn(__fmul_rn(kPrepassCi, pa), is_left ? my_ns : sns), is_left ? sns : my_ns);
         }
         if (o.pp.level)
-            my_lv = pr - pl + 1 >= o.pp.gamma ? 1 + max(my_lv, sib < last ? ld_cg(plv + sib) : 0) : 0;
+            my_lv = pr - pl + 1 >= (o.pp.seg_gamma ? (int)o.pp.seg_gamma[m] : o.pp.gamma)
+                        ? 1 + max(my_lv, sib < last ? ld_cg(plv + sib) : 0)
+                        : 0;
         write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns, my_lv);
         if (root) {
             o.parent[nb] = -1;
