@@ -631,11 +631,13 @@ cudaError_t launch_atrbvh_g(int warps, uint32_t blocks, cudaStream_t s, const Tr
 // root; its results depend only on its subtree, so any order that finishes a
 // node's big descendants first gives the reference's result.  The level of a
 // big node is 1 + the largest level of its big children (0 for the others).
-// Phase A (k_levels) climbs once from every leaf and finishes every node that
-// is not big (subtree count, nodesSah, child record) and levels the big ones;
-// phase B sorts big nodes of levels 1..L into per-level lists; phase C
-// restructures each level's treelets at once, one thread per treelet; the
-// dataflow kernel then climbs from the frontier below the levels above L.
+// Phase A finishes every node that is not big (subtree count, nodesSah, child
+// record) and levels the big ones: k_levels climbs once from every leaf;
+// k_levels_pp and k_levels_pp_hist take counts, nodesSah (and levels) from
+// the LBVH build.  Phase B sorts big nodes of levels 1..L into per-level
+// lists; phase C restructures each level's treelets in one launch, several
+// per warp in lane groups; the dataflow kernel then climbs from the frontier
+// below the levels above L.
 
 constexpr int kMaxLevels = 64;  // largest L (ATR_TUNE_ATR_LEVELS)
 
