@@ -89,7 +89,7 @@ struct atr_ctx {
     int atr_levels = 12;
     // A level pass over at least this many treelet roots restructures them in
     // four-lane groups (eight per warp); -1 = never.
-    int atr_quad_min = 80000;
+    int atr_quad_min = 50000;
     struct Phase {
         std::string name;
         cudaEvent_t a, b;

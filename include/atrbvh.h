@@ -118,7 +118,7 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
  *   ATR_TUNE_QUAD_MIN       fewest treelet roots of one level that the level
  *                           pass restructures in four-lane groups, eight per
  *                           warp, instead of 32/G per warp (-1 = never;
- *                           default 80000). */
+ *                           default 50000). */
 enum atr_tune_knob {
     ATR_TUNE_ATR_WARPS = 0,
     ATR_TUNE_ATR_GROUP_MIN = 1,
