@@ -649,7 +649,8 @@ struct LevelRefs {
     int32_t* next;         // the next iteration's levels, filled as nodes are finished
     float* nsah;           // this iteration's nodesSah (node-indexed)
     float* nsah_next;      // the next iteration's nodesSah
-    uint32_t* hist;        // [L + 2]: level histogram, then per-level offsets
+    uint32_t* hist;        // [L + 2]: level histogram
+    uint32_t* off;         // [L + 2]: per-level offsets into `order` (written by phase B)
     uint32_t* cursor;      // [L + 2]
     uint2* order;          // (mesh, local node) of big nodes by level
     uint2* frontier;       // climb starts of the dataflow pass
@@ -933,23 +934,24 @@ __global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, con
 }
 
 // Exclusive scan of the level histogram into offsets (one small block).
-__global__ void k_level_offsets(LevelRefs lv, int L) {
-    if (threadIdx.x != 0) return;
-    uint32_t run = 0;
-    for (int l = 0; l <= L + 1; ++l) {
-        const uint32_t c = lv.hist[l];
-        lv.hist[l] = run;
-        lv.cursor[l] = 0;
-        run += c;
-    }
-}
-
 __global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, const uint8_t* __restrict__ seg_iters,
                                                        int iteration, int L) {
     __shared__ uint32_t s_cnt[kMaxLevels + 2];
     __shared__ uint32_t s_base[kMaxLevels + 2];
+    __shared__ uint32_t s_off[kMaxLevels + 2];
     for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_cnt[k] = 0;
+    // Offsets of the level lists: every block scans the (small) histogram;
+    // block 0 publishes them for the level passes.
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int l = 0; l <= L + 1; ++l) {
+            s_off[l] = run;
+            run += lv.hist[l];
+        }
+    }
     __syncthreads();
+    if (blockIdx.x == 0)
+        for (int k = threadIdx.x; k < L + 2; k += blockDim.x) lv.off[k] = s_off[k];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     int me = 0;
     uint32_t m = 0, li = 0, rank = 0;
@@ -969,7 +971,7 @@ __global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, 
     for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
         s_base[k] = s_cnt[k] ? atomicAdd(&lv.cursor[k], s_cnt[k]) : 0u;
     __syncthreads();
-    if (me > 0) lv.order[lv.hist[me] + s_base[me] + rank] = make_uint2(m, li);
+    if (me > 0) lv.order[s_off[me] + s_base[me] + rank] = make_uint2(m, li);
 }
 
 // ---- quads: eight treelets per warp ----------------------------------------
@@ -1330,7 +1332,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Seg
     __shared__ __align__(16) float s_mem[W][kGroupFloats * per];
     __shared__ uint16_t s_rc[kMaxDist];
     __shared__ __align__(4) uint8_t s_prio[(kMaxTreelet + 1) * 32];
-    const uint32_t beg = lv.hist[lev], end = lv.hist[lev + 1];
+    const uint32_t beg = lv.off[lev], end = lv.off[lev + 1];
     if (beg + blockIdx.x * (uint32_t)(W * per) >= end) return;  // no root for this block
     for (int k = threadIdx.x; k < kMaxDist; k += blockDim.x) {
         int r, c;
@@ -1415,7 +1417,7 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     // Two level arrays: this iteration's and the next one's.
     const size_t b_lvl = align256(inner * 4), b_ord = L ? align256(inner * 8) : 0;
     const size_t b_front = L ? align256((size_t)segs.n * 8) : 0;
-    const size_t b_small = L ? align256((size_t)(2 * (L + 2) + 1) * 4) : 0;
+    const size_t b_small = L ? align256((size_t)(3 * (L + 2) + 1) * 4) : 0;
     // The build's prepass (counts, first nodesSah, child records) serves as
     // those arrays when its constants are this pass's.
     const bool use_pp = prepass && prepass->nsah && karras_ranges && L > 0 && ci == kPrepassCi && ct == kPrepassCt;
@@ -1449,7 +1451,8 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         lv.order = reinterpret_cast<uint2*>(p); p += b_ord;
         lv.frontier = reinterpret_cast<uint2*>(p); p += b_front;
         lv.hist = reinterpret_cast<uint32_t*>(p);
-        lv.cursor = lv.hist + (L + 2);
+        lv.off = lv.hist + (L + 2);
+        lv.cursor = lv.off + (L + 2);
         lv.n_frontier = lv.cursor + (L + 2);
     }
     const int warps = ctx->atr_warps == 2 || ctx->atr_warps == 4 ? ctx->atr_warps : 8;
@@ -1467,14 +1470,16 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         g.nsah = lv.nsah = ns[it & 1];
         lv.nsah_next = ns[(it + 1) & 1];
         int32_t* const next_lv = lv.next;
-        e = cudaMemsetAsync(counters, 0, inner * 4, st);
+        const bool hist_done = L && it == 0 && use_pp_levels;
+        // Arrival counters: for the first iteration's climbs, else only for
+        // the dataflow pass (cleared again below).
+        if (!L || (it == 0 && !hist_done)) e = cudaMemsetAsync(counters, 0, inner * 4, st);
         const uint2* start = nullptr;
         const uint32_t* start_count = nullptr;
         uint32_t blocks = leaf_blocks;
         if (L && e == cudaSuccess) {
             e = cudaMemsetAsync(lv.hist, 0, b_small, st);
             const unsigned gb = (segs.n + 255) / 256;
-            const bool hist_done = it == 0 && use_pp_levels;
             if (hist_done)
                 k_levels_pp_hist<<<gb, 256, 0, st>>>(g, segs, lv, karras_ranges, tsize, seg_tsize, seg_iters, L);
             else if (it == 0 && use_pp)
@@ -1484,14 +1489,16 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
                 k_levels<<<(segs.n + kLvBlock - 1) / kLvBlock, kLvBlock, 0, st>>>(g, segs, lv, tsize, seg_tsize,
                                                                                   seg_iters, it, ci, ct, L,
                                                                                   karras_ranges);
+            if (it == 0) ++ctx->launches;
             // Level counts and the frontier of the dataflow pass (after the
             // first iteration's climb, or from the levels the previous
             // iteration left).
-            if (!hist_done) k_level_hist<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
-            ctx->launches += 1;
-            k_level_offsets<<<1, 32, 0, st>>>(lv, L);
+            if (!hist_done) {
+                k_level_hist<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
+                ++ctx->launches;
+            }
             k_level_scatter<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
-            ctx->launches += 3;
+            ++ctx->launches;
             const unsigned lg = (unsigned)ctx->num_sms * (256 / threads) * 4;
             // Roots per level fall by about 0.62 per level from n / (1.5 gamma)
             // at level 1 (gamma = tsize << it); levels expected to hold at
