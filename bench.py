@@ -55,7 +55,7 @@ BYTES_PER_TRI = {"morton": 56.0, "sort": 4.0 + 16.0 * 4, "build": 40.0 + 180.0, 
 # dram__bytes_write.sum: k_levels_pp_hist 111.8 MB, k_level_hist 19.3,
 # k_level_scatter 16.8, k_level_groups 1896.6, k_atrbvh 13.0), scaled by
 # triangle count.
-ATRBVH_DRAM_BYTES_PER_TRI = (111.8 + 19.3 + 16.8 + 1896.6 + 13.0) * 1e6 / 2097152
+ATRBVH_DRAM_BYTES_PER_TRI = (111.3 + 19.3 + 16.8 + 1923.6 + 12.9) * 1e6 / 2097152
 
 
 def _read_peaks() -> dict:
