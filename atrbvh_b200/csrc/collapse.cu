@@ -64,31 +64,49 @@ __global__ void __launch_bounds__(256) k_collapse_copy(CollapseRefs g, uint64_t 
 // addressed from the mesh's first node (local indices); each mesh's lists
 // live in its own slice [tri_begin, tri_end) of tri_indices.  A node's area
 // is its box's surface area (the tree's area array).
-__global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs, uint32_t* __restrict__ counters,
-                                                        float ci, float ct, int max_leaf) {
+//
+// A child's record travels to its parent through the parent's 64-bit slot:
+// the first arrival exchanges its record in and stops, the second takes the
+// sibling's record out of the exchange.  Nothing else is read that another
+// thread of this pass writes, so the exchanges need no ordering, and the next
+// node's links are loaded while the exchange is in flight.  A record is never
+// zero (its count is at least one); zero marks an empty slot.
+__device__ __forceinline__ unsigned long long pack_rec(int2 v) {
+    return (unsigned long long)(uint32_t)v.x | ((unsigned long long)(uint32_t)v.y << 32);
+}
+
+__global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs,
+                                                        unsigned long long* __restrict__ slots, float ci, float ct,
+                                                        int max_leaf) {
     const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
     if (gi >= segs.n) return;
     const uint32_t m = segs.seg_of_tri(gi);
     const uint32_t s0 = segs.tri_begin(m);
     const uint32_t n = segs.tri_end(m) - s0;
     const int nb = segs.node_base(m);
-    uint32_t* ctr = counters + segs.inner_base(m);
-    const int leaf = (int)(gi - s0) + (int)n - 1;
-    {
-        const int x = nb + leaf;
-        g.c_count[x] = 1;
-        g.rec[x] = make_int2(__float_as_int(__fmul_rn(ct, g.area[x])), (1 << 1) | 1);
-    }
-    int cur = g.parent[nb + leaf];
-    while (cur >= 0) {
-        // The tree is read-only here: its links and area are loaded before
-        // the arrival atomic, so the second arrival waits only for the
-        // children's records.
-        const int x = nb + cur;
-        const int l = g.left[x], r = g.right[x], up = g.parent[x];
-        const float a = g.area[x];
-        if (atomic_add_acq_rel_gpu(&ctr[cur], 1u) == 0u) return;
-        const int2 el = __ldcg(g.rec + nb + l), er = __ldcg(g.rec + nb + r);
+    unsigned long long* const slot = slots + segs.inner_base(m);
+    int ch = (int)(gi - s0) + (int)n - 1;
+    int cur = g.parent[nb + ch];
+    int2 mine = make_int2(__float_as_int(__fmul_rn(ct, g.area[nb + ch])), (1 << 1) | 1);
+    g.c_count[nb + ch] = 1;
+    g.rec[nb + ch] = mine;
+    if (cur < 0) return;
+    int l = g.left[nb + cur], r = g.right[nb + cur], up = g.parent[nb + cur];
+    float a = g.area[nb + cur];
+    while (true) {
+        int nl = 0, nr = 0, nup = -1;
+        float na = 0.0f;
+        if (up >= 0) {
+            nl = g.left[nb + up];
+            nr = g.right[nb + up];
+            nup = g.parent[nb + up];
+            na = g.area[nb + up];
+        }
+        const unsigned long long other = atomicExch(slot + cur, pack_rec(mine));
+        if (other == 0ull) return;
+        const int2 sib = make_int2((int)(uint32_t)other, (int)(uint32_t)(other >> 32));
+        const bool from_left = ch == l;
+        const int2 el = from_left ? mine : sib, er = from_left ? sib : mine;
         const int cl = el.y >> 1, cr = er.y >> 1;
         const float kl = __int_as_float(el.x), kr = __int_as_float(er.x);
         const int pl = el.y & 1, pr = er.y & 1;
@@ -98,13 +116,21 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
         const bool col = leaf_cost < c && (max_leaf <= 0 || cnt <= max_leaf);
         if (col) c = leaf_cost;
         const bool reached = pl && pr;
+        const int x = nb + cur;
         if (reached && !col) {
             if (cl > 1) g.emit_cnt[nb + l] = (uint32_t)cl;
             if (cr > 1) g.emit_cnt[nb + r] = (uint32_t)cr;
         }
+        mine = make_int2(__float_as_int(c), (cnt << 1) | (reached && col ? 1 : 0));
         g.c_count[x] = cnt;
-        g.rec[x] = make_int2(__float_as_int(c), (cnt << 1) | (reached && col ? 1 : 0));
+        g.rec[x] = mine;
+        if (up < 0) return;
+        ch = cur;
         cur = up;
+        l = nl;
+        r = nr;
+        up = nup;
+        a = na;
     }
 }
 
@@ -178,15 +204,17 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
     int2* rec = reinterpret_cast<int2*>(p); p += align256(nn * 8);
     uint32_t* emit = reinterpret_cast<uint32_t*>(p); p += b4;
     uint32_t* offs = reinterpret_cast<uint32_t*>(p); p += b4;
-    uint32_t* counters = reinterpret_cast<uint32_t*>(p);
+    // The exchange slots (8 B per inner node, at most 4 B per node) are dead
+    // once the cost pass ends, before the scan writes the list offsets.
+    unsigned long long* slots = reinterpret_cast<unsigned long long*>(offs);
     cudaStream_t s = ctx->stream;
-    cudaMemsetAsync(counters, 0, inner * 4, s);
+    cudaMemsetAsync(slots, 0, inner * 8, s);
     cudaMemsetAsync(dst.tri_indices, 0xff, (size_t)n * 4, s);
     CollapseRefs r{n, src.area, src.parent, src.left, src.right, src.data, src.bmin, src.bmax, dst.parent, dst.left,
                    dst.right, dst.data, dst.count, dst.bmin, dst.bmax, rec, emit};
     const unsigned blocks = (n + 255) / 256;
     k_collapse_copy<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(r, nn);
-    k_collapse_cost<<<blocks, 256, 0, s>>>(r, segs, counters, ci, ct, max_leaf);
+    k_collapse_cost<<<blocks, 256, 0, s>>>(r, segs, slots, ci, ct, max_leaf);
     ctx->launches += 2;
     int st = exclusive_scan_u32(ctx, emit, offs, nn, nullptr);
     if (st == ATR_OK) {
