@@ -69,25 +69,50 @@ __device__ __forceinline__ uint32_t woop_entries(const FlatRefs& t, int nb, int 
 
 // Pass 1: per inner node, inner nodes in its subtree, inner children, Woop
 // entries of its leaf children (inner arrays are indexed cb + local index).
+// A child's inner-node count reaches its parent through the parent's 64-bit
+// slot (bit 32 marks it present): the first arrival exchanges its count in
+// and stops, the second takes the sibling's out of the exchange.  Nothing
+// else read here is written by this pass, so the exchanges need no ordering,
+// and the next node's links load while the exchange is in flight.
 __global__ void __launch_bounds__(256) k_flat_counts(FlatRefs t, Segs segs, uint32_t* __restrict__ icnt,
                                                       uint32_t* __restrict__ ic, uint32_t* __restrict__ tw,
-                                                      uint32_t* __restrict__ counters) {
+                                                      unsigned long long* __restrict__ slots) {
     const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
     if (gi >= segs.n) return;
     const SegPos q = seg_pos(segs, gi);
-    int cur = t.parent[q.nb + (int)q.li + (int)q.n - 1];
-    while (cur >= 0) {
-        // Links are read-only here: loaded before the arrival atomic.
-        const int l = t.left[q.nb + cur], r = t.right[q.nb + cur], up = t.parent[q.nb + cur];
+    int ch = (int)q.li + (int)q.n - 1;
+    int cur = t.parent[q.nb + ch];
+    if (cur < 0) return;
+    uint32_t mine = 0u;  // inner nodes below ch counted by the parent (none under a leaf)
+    int l = t.left[q.nb + cur], r = t.right[q.nb + cur], up = t.parent[q.nb + cur];
+    bool cleaf = c_leaf(t, q.nb, cur);
+    while (true) {
+        int nl = 0, nr = 0, nup = -1;
+        bool ncleaf = false;
+        if (up >= 0) {
+            nl = t.left[q.nb + up];
+            nr = t.right[q.nb + up];
+            nup = t.parent[q.nb + up];
+            ncleaf = c_leaf(t, q.nb, up);
+        }
         const bool ll = c_leaf(t, q.nb, l), rl = c_leaf(t, q.nb, r);
-        const bool cleaf = c_leaf(t, q.nb, cur);
-        if (atomic_add_acq_rel_gpu(&counters[q.cb + cur], 1u) == 0u) return;
-        const uint32_t il = ll ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + q.cb + l);
-        const uint32_t ir = rl ? 0u : (uint32_t)ld_cg(reinterpret_cast<const int*>(icnt) + q.cb + r);
-        icnt[q.cb + cur] = cleaf ? 0u : 1u + il + ir;
+        const unsigned long long other = atomicExch(slots + q.cb + cur, (1ull << 32) | mine);
+        if (other == 0ull) return;
+        const uint32_t sib = (uint32_t)other;
+        const bool from_left = ch == l;
+        const uint32_t il = from_left ? mine : sib, ir = from_left ? sib : mine;
+        const uint32_t v = cleaf ? 0u : 1u + il + ir;
+        icnt[q.cb + cur] = v;
         ic[q.cb + cur] = (ll ? 0u : 1u) + (rl ? 0u : 1u);
         tw[q.cb + cur] = (ll ? woop_entries(t, q.nb, l) : 0u) + (rl ? woop_entries(t, q.nb, r) : 0u);
+        if (up < 0) return;
+        mine = v;
+        ch = cur;
         cur = up;
+        l = nl;
+        r = nr;
+        up = nup;
+        cleaf = ncleaf;
     }
 }
 
@@ -357,7 +382,7 @@ int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const fl
     uint32_t* icnt = reinterpret_cast<uint32_t*>(p); p += bm;
     uint32_t* ic = reinterpret_cast<uint32_t*>(p); p += bm;
     uint32_t* tw = reinterpret_cast<uint32_t*>(p); p += bm;
-    uint32_t* counters = reinterpret_cast<uint32_t*>(p); p += bm;
+    p += bm;  // spare word per inner node: the scratch keeps its size (and its place in the pool)
     int* jmp0 = reinterpret_cast<int*>(p); p += bm;
     int* jmp1 = reinterpret_cast<int*>(p); p += bm;
     int* slot_of = reinterpret_cast<int*>(p); p += bm;
@@ -368,10 +393,13 @@ int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const fl
     uint32_t* flags = reinterpret_cast<uint32_t*>(p);  // [1] max depth, [2..3] totals, then pending
     FlatRefs t{c.parent, c.left, c.right, c.data, c.count, c.bmin, c.bmax, c.tri_indices};
     const unsigned gb = (n + 255) / 256, gm = (m + 255) / 256;
-    cudaMemsetAsync(counters, 0, (size_t)m * 4, s);
+    // The exchange slots of pass 1 (8 B per inner node) live in acc0, which
+    // k_flat_jump_init overwrites for every inner node afterwards.
+    unsigned long long* const slots = reinterpret_cast<unsigned long long*>(acc0);
+    cudaMemsetAsync(slots, 0, (size_t)m * 8, s);
     cudaMemsetAsync(ic_r, 0, 2 * bm, s);
     cudaMemsetAsync(flags, 0, kFlagBytes, s);
-    k_flat_counts<<<gb, 256, 0, s>>>(t, segs, icnt, ic, tw, counters);
+    k_flat_counts<<<gb, 256, 0, s>>>(t, segs, icnt, ic, tw, slots);
     k_flat_jump_init<<<gb, 256, 0, s>>>(t, segs, icnt, acc0, jmp0);
     ctx->launches += 2;
     // Depth <= m, and after round r every jump spans 2^(r+1) ancestors, so the
