@@ -1,10 +1,10 @@
 // Leaf collapse (BVHRT-Core/src/TreeCollapser.cu:13-285, BVHTreeCollapser.cpp:21-93).
 //
-// Pass 1 (bottom-up, one thread per leaf, second arrival continues) copies the
-// tree into the collapsed layout and computes, per node: triangle count,
-// SAH cost (ci*A + cL + cR, or ct*A*count when that is cheaper -- :47-84), the
-// collapse flag, and whether a climbing thread of the reference's emission
-// kernel (:173-237) would pass the node upward.  The reference emits, at every
+// A streaming pass copies the tree into the collapsed layout.  Pass 1
+// (bottom-up, one thread per leaf, second arrival continues) computes, per
+// node: triangle count, SAH cost (ci*A + cL + cR, or ct*A*count when that is
+// cheaper -- :47-84), the collapse flag, and whether a climbing thread of the
+// reference's emission kernel (:173-237) would pass the node upward.  The reference emits, at every
 // node reached by two such threads that is not collapsed, each child holding
 // more than one triangle as a multi-triangle leaf; pass 1 records those
 // children.  A scan gives their list offsets in node order (the reference
