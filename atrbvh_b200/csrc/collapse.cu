@@ -208,8 +208,13 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
     // once the cost pass ends, before the scan writes the list offsets.
     unsigned long long* slots = reinterpret_cast<unsigned long long*>(offs);
     cudaStream_t s = ctx->stream;
-    cudaMemsetAsync(slots, 0, inner * 8, s);
-    cudaMemsetAsync(dst.tri_indices, 0xff, (size_t)n * 4, s);
+    // The climb reads a zero slot as "no sibling yet": a failed clear must stop here.
+    cudaError_t me = cudaMemsetAsync(slots, 0, inner * 8, s);
+    if (me == cudaSuccess) me = cudaMemsetAsync(dst.tri_indices, 0xff, (size_t)n * 4, s);
+    if (me != cudaSuccess) {
+        ctx->release(scratch);
+        return cuda_fail(me, "collapse scratch clear", __FILE__, __LINE__);
+    }
     CollapseRefs r{n, src.area, src.parent, src.left, src.right, src.data, src.bmin, src.bmax, dst.parent, dst.left,
                    dst.right, dst.data, dst.count, dst.bmin, dst.bmax, rec, emit};
     const unsigned blocks = (n + 255) / 256;

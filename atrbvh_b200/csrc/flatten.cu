@@ -396,9 +396,14 @@ int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const fl
     // The exchange slots of pass 1 (8 B per inner node) live in acc0, which
     // k_flat_jump_init overwrites for every inner node afterwards.
     unsigned long long* const slots = reinterpret_cast<unsigned long long*>(acc0);
-    cudaMemsetAsync(slots, 0, (size_t)m * 8, s);
-    cudaMemsetAsync(ic_r, 0, 2 * bm, s);
-    cudaMemsetAsync(flags, 0, kFlagBytes, s);
+    // The count climb reads a zero slot as "no sibling yet": a failed clear must stop here.
+    cudaError_t me = cudaMemsetAsync(slots, 0, (size_t)m * 8, s);
+    if (me == cudaSuccess) me = cudaMemsetAsync(ic_r, 0, 2 * bm, s);
+    if (me == cudaSuccess) me = cudaMemsetAsync(flags, 0, kFlagBytes, s);
+    if (me != cudaSuccess) {
+        ctx->release(scratch);
+        return cuda_fail(me, "flatten scratch clear", __FILE__, __LINE__);
+    }
     k_flat_counts<<<gb, 256, 0, s>>>(t, segs, icnt, ic, tw, slots);
     k_flat_jump_init<<<gb, 256, 0, s>>>(t, segs, icnt, acc0, jmp0);
     ctx->launches += 2;

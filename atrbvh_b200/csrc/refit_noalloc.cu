@@ -19,9 +19,13 @@
 //     overlaps on the GPU (different streams, no ordering between them) race
 //     on the array and give wrong boxes.  Serialise calls on one stream or
 //     order them with events.
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before capturing the stream into a CUDA graph.
+//   * every call made outside stream capture looks up the array's device
+//     address (cudaGetSymbolAddress, a host-side lookup that allocates
+//     nothing) with the caller's device current, so a device reset, which
+//     reloads the module and can move the array, never leaves a stale
+//     address behind.  A call made while its stream is being captured uses
+//     the address the last uncaptured call on that device found; make one
+//     uncaptured call on a device (after any reset) before capturing.
 
 #include <mutex>
 
@@ -39,18 +43,26 @@ static __device__ __align__(256) uint32_t g_refit_counters[kNoAllocMaxTriangles 
 std::mutex g_addr_mutex;
 uint32_t* g_addr[kMaxDevices] = {};
 
-// Device address of g_refit_counters on the current device (looked up once).
-int counters_address(uint32_t** out) {
+// Device address of g_refit_counters on the current device.  Outside stream
+// capture it is looked up afresh (the module, and with it the array, moves
+// when the device's primary context is reset and recreated); inside a capture
+// the address from the last uncaptured call on this device is used.
+int counters_address(cudaStream_t s, uint32_t** out) {
     int dev = 0;
     ATR_CUDA(cudaGetDevice(&dev));
     ATR_REQUIRE(dev >= 0 && dev < kMaxDevices, ATR_ERR_NO_DEVICE, "atr_refit_noalloc: device %d", dev);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    ATR_CUDA(cudaStreamIsCapturing(s, &cap));
     std::lock_guard<std::mutex> lock(g_addr_mutex);
-    if (!g_addr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_refit_counters);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_refit_counters)", __FILE__, __LINE__);
         g_addr[dev] = static_cast<uint32_t*>(p);
     }
+    ATR_REQUIRE(g_addr[dev] != nullptr, ATR_ERR_INVALID_ARG,
+                "atr_refit_noalloc: first call on device %d made during stream capture; make one call outside "
+                "capture first", dev);
     *out = g_addr[dev];
     return ATR_OK;
 }
@@ -106,9 +118,9 @@ extern "C" int atr_refit_noalloc(void* stream, uint32_t num_triangles, const flo
     ATR_REQUIRE(num_triangles <= kNoAllocMaxTriangles, ATR_ERR_INVALID_ARG,
                 "atr_refit_noalloc: %u triangles exceed the fixed maximum of %u; use atr_refit", num_triangles,
                 kNoAllocMaxTriangles);
-    uint32_t* counters = nullptr;
-    ATR_TRY(counters_address(&counters));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t* counters = nullptr;
+    ATR_TRY(counters_address(s, &counters));
     ATR_CUDA(cudaMemsetAsync(counters, 0, (size_t)(num_triangles - 1) * 4, s));
     k_refit_noalloc<<<(num_triangles + 255) / 256, 256, 0, s>>>(
         reinterpret_cast<const float4*>(vertices), num_triangles, parent, left, right, data,

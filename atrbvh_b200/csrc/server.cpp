@@ -52,6 +52,7 @@ struct Request {
     atr_request req{};
     Clock::time_point t_submit, t_taken, t_done;
     bool done = false;
+    bool waited = false;  // a thread is in atr_server_wait on this ticket
     int status = ATR_OK;
     float sah = 0.0f;
     uint32_t batch_requests = 0, lane = 0;
@@ -637,6 +638,11 @@ int atr_server_wait(atr_server* s, uint64_t ticket, atr_request_result* out) {
     ATR_REQUIRE(it != s->tickets.end(), ATR_ERR_INVALID_ARG, "atr_server_wait: unknown ticket %llu",
                 (unsigned long long)ticket);
     Request* r = it->second.get();
+    // The waiter erases the ticket (and frees the request) when it returns, so
+    // a second concurrent waiter would read freed memory: refuse it.
+    ATR_REQUIRE(!r->waited, ATR_ERR_INVALID_ARG, "atr_server_wait: ticket %llu already has a waiter",
+                (unsigned long long)ticket);
+    r->waited = true;
     s->cv_done.wait(lock, [&] { return r->done; });
     std::memset(out, 0, sizeof(*out));
     out->status = r->status;

@@ -633,7 +633,7 @@ def run_reference(args, world, rank, local):
     }
     out["reference_cuda"] = {
         "unavailable": "the reference's ATRBVH CUDA kernel, compiled here for sm_100a, did not terminate on "
-                       "4,096- and 65,536-triangle inputs on this pool (unfenced cross-SM reads; see DESIGN.md); "
+                       "4,096- and 65,536-triangle inputs on this pool (unfenced cross-SM reads of treelet rewrites); "
                        "it is not run again"}
     print(json.dumps(out), flush=True)
 

@@ -205,8 +205,11 @@ int atr_refit(atr_ctx* ctx, atr_tree* tree, const atr_scene* scene);
  * library: at most 1,048,576 triangles (larger meshes are rejected; use
  * atr_refit), one array per device for the life of the process, shared by all
  * calls -- calls that overlap on the GPU race, so order them on one stream.
- * The first call on a device looks up the array's address; make it before
- * any stream capture.  stream may be NULL (legacy default stream). */
+ * Each call made outside stream capture looks up the array's address afresh
+ * (so a device reset cannot leave a stale one); a call inside a capture uses
+ * the address of the last uncaptured call on that device, so make one
+ * uncaptured call on a device, and again after a reset, before capturing.
+ * stream may be NULL (legacy default stream). */
 int atr_refit_noalloc(void* stream, uint32_t num_triangles, const float* vertices,
                       const int32_t* parent, const int32_t* left, const int32_t* right,
                       const int32_t* data, float* bbox_min, float* bbox_max, float* area);
@@ -402,7 +405,8 @@ typedef struct atr_server_stats {
 
 int atr_server_create(int device, const atr_server_config* config, atr_server** out);
 int atr_server_submit(atr_server* server, const atr_request* request, uint64_t* ticket);
-/* Blocks until the request is done; each ticket can be waited on once. */
+/* Blocks until the request is done; each ticket can be waited on once, by one
+ * thread (a second concurrent waiter gets ATR_ERR_INVALID_ARG). */
 int atr_server_wait(atr_server* server, uint64_t ticket, atr_request_result* result);
 /* Drop a resident mesh (its memory is freed once no lane uses it). */
 int atr_server_release(atr_server* server, uint64_t mesh_id);

@@ -1,9 +1,8 @@
 """ORACLE -- test infrastructure only.
 
-ctypes access to the CPU restatement (liboracle.so, from atr_oracle.cpp) and to
-the reference's own CUDA build (oracle/_ref/libbvhrt_ref*.so, from
-oracle/build.py).  Only tests/, __graft_entry__.smoke() and the CPU-baseline
-leg of bench.py use this package, and only as the checker.
+ctypes access to the CPU restatement (liboracle.so, from atr_oracle.cpp).
+Only tests/, __graft_entry__.smoke() and the CPU-baseline legs of bench.py use
+this package, and only as the checker.
 """
 from __future__ import annotations
 
@@ -15,8 +14,6 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "liboracle.so"
-REF_LIB = HERE / "_ref" / "libbvhrt_ref.so"
-REF_LIB_FMAD = HERE / "_ref" / "libbvhrt_ref_fmad.so"
 
 _p = C.c_void_p
 _lib = None
@@ -245,50 +242,3 @@ def atrbvh_schedule(treelet: int, warp: int = 32) -> np.ndarray:
     out = np.zeros(4096, np.int32)
     k = lib().orc_atrbvh_schedule(treelet, warp, _ptr(out), len(out))
     return out[:k]
-
-
-# ---- the reference's own CUDA build (GPU machine only) ------------------------
-
-_ref = {}
-
-
-def ref_available(fmad: bool = False) -> bool:
-    return (REF_LIB_FMAD if fmad else REF_LIB).exists()
-
-
-def ref_lib(fmad: bool = False) -> C.CDLL:
-    key = bool(fmad)
-    if key not in _ref:
-        L = C.CDLL(str(REF_LIB_FMAD if fmad else REF_LIB))
-        L.ref_run.restype = C.c_int
-        L.ref_run.argtypes = [_p, C.c_uint, _p, _p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int] + \
-            [_p] * 15 + [_p, _p]
-        _ref[key] = L
-    return _ref[key]
-
-
-def ref_run(v: np.ndarray, bbmin, bbmax, *, use64=False, optimizer=0, treelet=9, iterations=2,
-            collapse=False, fmad=False):
-    """Run the reference pipeline on the GPU; returns (Tree, Collapsed|None, times_ms)."""
-    v = np.ascontiguousarray(v, np.float32)
-    n = v.shape[0]
-    t = Tree.empty(n)
-    nn = 2 * n - 1
-    c = None
-    if collapse:
-        c = Collapsed(*(np.zeros(nn, np.int32) for _ in range(5)), np.zeros((nn, 4), np.float32),
-                      np.zeros((nn, 4), np.float32), np.zeros(n, np.int32), np.zeros(0, np.float32), 0.0)
-    sah_out = np.zeros(1, np.float32)
-    times = np.zeros(3, np.float64)
-    mn = np.asarray(bbmin, np.float32)
-    mx = np.asarray(bbmax, np.float32)
-    cp = [None] * 8 if c is None else [_ptr(c.parent), _ptr(c.left), _ptr(c.right), _ptr(c.data),
-                                      _ptr(c.triangle_count), _ptr(c.bbox_min), _ptr(c.bbox_max),
-                                      _ptr(c.triangle_indices)]
-    rc = ref_lib(fmad).ref_run(_ptr(v), n, _ptr(mn), _ptr(mx), 1 if use64 else 0, optimizer, treelet, iterations,
-                               1 if collapse else 0, 1, *t.ptrs(), *cp, _ptr(sah_out), _ptr(times))
-    if rc != 0:
-        raise RuntimeError(f"reference run failed: cuda error {rc}")
-    if c is not None:
-        c.sah = float(sah_out[0])
-    return t, c, times

@@ -90,3 +90,33 @@ def test_noalloc_refit_rejects_oversize_and_null(ctx):
     assert b"fixed maximum" in ab.lib().atr_last_error()
     assert ab.lib().atr_refit_noalloc(None, 1, *args) == 1
     assert ab.lib().atr_refit_noalloc(None, 100, None, *args[1:]) == 1
+
+
+def _pool_used(device: int = 0) -> int:
+    """Bytes in use in the device's default stream-ordered pool (the pool the
+    library's allocating entry points draw from)."""
+    from cuda.bindings import runtime as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(device)
+    assert err == rt.cudaError_t.cudaSuccess
+    err, used = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+    assert err == rt.cudaError_t.cudaSuccess
+    return int(used)
+
+
+@pytest.mark.gpu
+def test_noalloc_refit_allocates_nothing(ctx):
+    """After the first call on the device (which may load the library's module
+    and with it the fixed array), further calls change neither the device's
+    free memory, the stream-ordered pool's usage nor torch's allocator."""
+    import torch
+    scene, tree = _tree(ctx, scene_case("c1"))
+    _noalloc(ctx, scene, tree)
+    for seed in range(5):
+        scene.set_vertices(_jitter(scene_case("c1"), 200 + seed))
+        torch.cuda.synchronize()
+        before = (torch.cuda.mem_get_info(0)[0], _pool_used(0), torch.cuda.memory_allocated(0))
+        _noalloc(ctx, scene, tree)
+        _noalloc(ctx, scene, tree)
+        torch.cuda.synchronize()
+        after = (torch.cuda.mem_get_info(0)[0], _pool_used(0), torch.cuda.memory_allocated(0))
+        assert after == before, (seed, before, after)
