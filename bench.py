@@ -14,11 +14,16 @@ input, CUDA events on the library's stream), summed over ranks; traversal
 Mrays/s is reported beside it.  e2e repeats the build through the public C ABI
 from pinned host vertices (H2D inside the timed region) to the SAH read back
 on the host.  With --gpus N > 1 every rank builds its own replica (the path
-has no data exchange for a single mesh).
+has no data exchange for a single mesh).  After the K timed steps the default
+line also carries: a sustained run of the same step (>= 1 s, with its own
+clock record), the timed build's SAH against the oracle's committed value,
+the 4096-mesh batched-vs-plain figures and serving p50/p99 at three arrival
+rates, and the host-core baseline on the whole scene.
 
---impl reference times the CPU restatement of the same pipeline on the host
-cores (the reference has no CPU implementation of this path) and, where its
-compiled CUDA build is present, the reference's own CUDA builder.
+--impl reference times the checker's CPU restatement of the same pipeline on
+all host cores, on the whole workload scene per step (the reference has no CPU
+implementation of this path, and its CUDA build is not run); it loads nothing
+from the product library.
 """
 from __future__ import annotations
 
@@ -76,8 +81,9 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, interval_ms: int = 10):
         self.device = device
+        self.interval_ms = interval_ms
         self.proc = None
         self.lines: list[str] = []
         self.thread = None
@@ -85,7 +91,7 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -173,15 +179,33 @@ def cpu_pipeline(v: np.ndarray, threads: int) -> float:
     return time.perf_counter() - t0
 
 
-def cpu_baseline(v_full: np.ndarray) -> dict:
+def cpu_baseline(reps: int = 5) -> dict:
+    """The host-core pipeline on the whole workload scene (generated by the
+    checker's own generator), best of `reps` after one warm-up."""
     import oracle as O
     threads = O.max_threads()
-    m = min(len(v_full), 1 << 20)
-    v = np.ascontiguousarray(v_full[:m])
-    cpu_pipeline(v[: 1 << 14], threads)  # warm-up
-    secs = min(cpu_pipeline(v, threads) for _ in range(2))
-    return {"value": m / secs / 1e6, "unit": "Mtri/s", "cores": threads, "kind": "port",
-            "sample": f"first {m} triangles of the workload scene, LBVH+ATRBVH(9,2)+collapse, best of 2"}
+    v = O.gen_scene(O.SCENE_CLUSTERED, N_TRIS, 0)
+    cpu_pipeline(v, threads)  # warm-up
+    secs = min(cpu_pipeline(v, threads) for _ in range(reps))
+    return {"value": N_TRIS / secs / 1e6, "unit": "Mtri/s", "cores": threads, "kind": "port",
+            "sample": f"the whole {N_TRIS}-triangle workload scene, LBVH+ATRBVH(9,2)+collapse, best of {reps} after "
+                      f"1 warm-up"}
+
+
+def golden_c2() -> dict | None:
+    """Oracle SAH and digests of the clustered 4,194,304-triangle workload."""
+    p = ROOT / "tests" / "golden" / "fullsize_oracle.json"
+    if not p.exists():
+        return None
+    return json.loads(p.read_text()).get("c2")
+
+
+def clustered_config(n_tris: int, world: int, rays_per_step: int) -> dict:
+    """The workload description both arms print (identical for equal runs)."""
+    return {"workload": WORKLOAD if n_tris == N_TRIS else f"{n_tris}-triangle instance of: {WORKLOAD}",
+            "triangles": n_tris, "rays_per_step": int(rays_per_step), "treelet": 9, "iterations": 2,
+            "morton_bits": 30, "collapse_max_leaf": 0, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (201 MB of vertices); no flush"}
 
 
 def run_ours(args, world, rank, local):
@@ -202,7 +226,7 @@ def run_ours(args, world, rank, local):
         res2 = torch.zeros_like(res)
     torch.cuda.synchronize()
 
-    def step(timed: bool):
+    def step(keep: bool = False):
         tree = ab.LBVHBuilder(False).BuildTree(scene)
         ab.AgglomerativeTreeletOptimizer(9, 2).Optimize(tree)
         col, _ = ab.BVHTreeCollapser().Collapse(tree, want_sah=False)
@@ -211,15 +235,18 @@ def run_ours(args, world, rank, local):
         ab.check(ab.lib().atr_gen_bounce_rays(ctx.handle, scene.handle, rays.data_ptr(), res.data_ptr(), nr, 1,
                                               bounce.data_ptr()))
         bvh.trace(bounce.data_ptr(), nr, res2.data_ptr())
+        if keep:
+            return tree, col, bvh
         bvh.close()
         col.close()
         tree.close()
+        return None
 
     for _ in range(args.warmup):
-        step(False)
+        step()
     ctx.synchronize()
 
-    # ---- device-resident timed region ----
+    # ---- device-resident timed region: exactly K steps ----
     ctx.set_timing(True)
     clocks = ClockSampler(local)
     launches0 = ctx.launch_count()
@@ -230,7 +257,7 @@ def run_ours(args, world, rank, local):
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        step(True)
+        step()
     ev1.record(stream)
     ctx.synchronize()
     torch.cuda.synchronize()
@@ -251,6 +278,47 @@ def run_ours(args, world, rank, local):
     build_ms_max = max_over_ranks(build_ms, world)
     trace_ms_max = max_over_ranks(trace_ms, world)
     step_ms_max = max_over_ranks(total_ms / args.steps, world)
+
+    # ---- sustained: the same step repeated for at least a second, its own clock record ----
+    sustained = None
+    if args.sustain_s > 0:
+        clocks2 = ClockSampler(local, interval_ms=50)
+        barrier(world)
+        torch.cuda.synchronize()
+        clocks2.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t0 = time.perf_counter()
+        reps = 0
+        while time.perf_counter() - t0 < args.sustain_s or reps < 2:
+            step()
+            reps += 1
+            if reps % 16 == 0:
+                ctx.synchronize()
+        e1.record(stream)
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        clk2 = clocks2.stop()
+        s_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        sustained = {"steps": reps, "seconds": s_ms / 1e3, "ms_per_step": s_ms / reps,
+                     "note": "whole steps (build, flatten, both traces) back to back; the same step as the timed region",
+                     "clocks": clk2}
+
+    # ---- the timed build's SAH against the oracle's, outside the timed region ----
+    sah_check = None
+    gold = golden_c2() if n_tris == N_TRIS else None
+    if gold is not None:
+        tree, col, bvh = step(keep=True)
+        got_tree = float(tree.sah())
+        _, got_col = ab.BVHTreeCollapser().Collapse(tree)
+        bvh.close()
+        col.close()
+        tree.close()
+        sah_check = {"tree_sah": got_tree, "oracle_tree_sah": gold["tree_sah"],
+                     "collapsed_sah": float(got_col), "oracle_collapsed_sah": gold["collapsed_sah"],
+                     "equal": bool(np.float32(got_tree) == np.float32(gold["tree_sah"])
+                                   and np.float32(got_col) == np.float32(gold["collapsed_sah"]))}
 
     # ---- e2e through the public API from pinned host memory ----
     pinned = torch.from_numpy(v.reshape(-1)).pin_memory().numpy().reshape(v.shape)
@@ -302,10 +370,7 @@ def run_ours(args, world, rank, local):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded Philox: clustered scene + pinhole/diffuse rays)",
-        "config": {"workload": WORKLOAD if n_tris == N_TRIS else f"{n_tris}-triangle instance of: {WORKLOAD}",
-                   "triangles": n_tris, "rays_per_step": int(rays_per_step),
-                   "treelet": 9, "iterations": 2, "morton_bits": 30, "collapse_max_leaf": 0,
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (201 MB of vertices)"},
+        "config": clustered_config(n_tris, world, rays_per_step),
         "mrays_per_s": world * rays_per_step / (trace_ms_max * 1e-3) / 1e6 if trace_ms_max else None,
         "phase_ms": {k: round(x, 4) for k, x in ph_ms.items()},
         "build_ms": build_ms_max,
@@ -317,11 +382,23 @@ def run_ours(args, world, rank, local):
                         "atr_collapse (SAH read back)"},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "sustained": sustained,
+        "sah_check": sah_check,
     }
+    scene.close()
+    del rays, res, bounce, res2
+    torch.cuda.synchronize()
+    if world == 1 and not args.no_batch:
+        out["batch"] = measure_batch(ctx, stream, world, rank, device=local, steps=5, warmup=2, plain_reps=2,
+                                     autotune=False, e2e=False)
+    if world == 1 and not args.no_serve and rank == 0:
+        out["serving"] = measure_serve(rates=[500.0, 2000.0, 5000.0], requests=1000, pool_size=16, lanes=args.lanes,
+                                       device=local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(v)
+        out["cpu_baseline"] = cpu_baseline()
     if rank == 0:
         print(json.dumps(out), flush=True)
+    ctx.close()
 
 
 BATCH_MESHES = 4096
@@ -346,17 +423,15 @@ def _cuda_ms(stream, fn, reps: int) -> list[float]:
     return out
 
 
-def run_batch(args, world, rank, local):
+def measure_batch(ctx, stream, world, rank, *, device: int = 0, meshes: int = BATCH_MESHES, steps: int = 5,
+                  warmup: int = 2, plain_reps: int = 3, autotune: bool = True, e2e: bool = True) -> dict:
     """Segmented batched builds of the 4096-mesh workload against per-mesh
-    plain launches of the same library on the same GPU (equal trees, so equal
-    SAH: every 64th mesh's SAH is compared bit for bit)."""
+    plain launches of the same library on the same GPU.  The trees are equal,
+    so the SAH is equal: every 64th mesh's SAH is compared bit for bit."""
     import torch
     import atrbvh_b200 as ab
-    torch.cuda.set_device(local)
-    ctx = ab.Context(local)
-    stream = torch.cuda.ExternalStream(ctx.stream)
     from atrbvh_b200.shard import rank_meshes
-    sizes_all = ab.gen_batch_sizes(args.meshes, BATCH_MIN, BATCH_MAX, 0)
+    sizes_all = ab.gen_batch_sizes(meshes, BATCH_MIN, BATCH_MAX, 0)
     v_all = ab.gen_batch_scene(sizes_all, 0)
     total_tris = int(sizes_all.sum())
     if world > 1:
@@ -369,36 +444,34 @@ def run_batch(args, world, rank, local):
     else:
         v, sizes = v_all, sizes_all
     off = np.concatenate([[0], np.cumsum(sizes, dtype=np.uint64)]).astype(np.uint32)
-    n_tris = int(off[-1])
     batch = ab.Batch(ctx, v, off)
-    launches0 = ctx.launch_count()
 
     def build_batched():
         batch.build(1, 9, 2, graph=True)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         build_batched()
     ctx.synchronize()
     barrier(world)
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(device, interval_ms=50)
     clocks.start()
     l0 = ctx.launch_count()
-    bt = _cuda_ms(stream, build_batched, args.steps)
-    launches = (ctx.launch_count() - l0) // max(1, args.steps)
+    bt = _cuda_ms(stream, build_batched, steps)
+    launches = (ctx.launch_count() - l0) // max(1, steps)
     clk = clocks.stop()
     sah_b = batch.sah()
 
     # Autotuned arm: per-class treelet/iterations at SAH no worse than
     # ATRBVH(9,2), ATRBVH block size and sort digit width of the dominant class.
     tuned = None
-    if not args.no_autotune:
+    if autotune:
         t0 = time.perf_counter()
         table = ab.autotune(ctx, min_class=8, max_class=18, sample_triangles=1 << 21, reps=2)
         tune_s = time.perf_counter() - t0
         batch.apply_tuning(table)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             build_batched()
-        tt = _cuda_ms(stream, build_batched, args.steps)
+        tt = _cuda_ms(stream, build_batched, steps)
         sah_t = batch.sah()
         t_ms = max_over_ranks(statistics.median(tt), world)
         tuned = {"mtri_per_s": total_tris / (t_ms * 1e-3) / 1e6, "ms": t_ms,
@@ -423,7 +496,7 @@ def run_batch(args, world, rank, local):
 
     build_plain()
     ctx.synchronize()
-    pt = _cuda_ms(stream, build_plain, max(1, min(args.steps, 3)))
+    pt = _cuda_ms(stream, build_plain, max(1, plain_reps))
     sah_equal = True
     checked = 0
     for m in range(0, len(sizes), 64):
@@ -434,42 +507,61 @@ def run_batch(args, world, rank, local):
         t.close()
     for sc in scenes:
         sc.close()
-    # e2e: pinned host vertices -> atr_batch_create -> build -> per-mesh SAH on the host.
-    pinned = torch.from_numpy(v.reshape(-1)).pin_memory().numpy().reshape(v.shape)
-    e2e = []
-    for it in range(0 if args.no_e2e else 2):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        b2 = ab.Batch(ctx, pinned, off)
-        b2.build(1, 9, 2)
-        b2.sah()
-        e2e.append(time.perf_counter() - t0)
-        b2.close()
+    e2e_t = []
+    if e2e:
+        # pinned host vertices -> atr_batch_create -> build -> per-mesh SAH on the host.
+        pinned = torch.from_numpy(v.reshape(-1)).pin_memory().numpy().reshape(v.shape)
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b2 = ab.Batch(ctx, pinned, off)
+            b2.build(1, 9, 2)
+            b2.sah()
+            e2e_t.append(time.perf_counter() - t0)
+            b2.close()
+        del pinned
     batch.close()
     b_ms = max_over_ranks(statistics.median(bt), world)
     p_ms = max_over_ranks(statistics.median(pt), world)
+    return {"workload": BATCH_WORKLOAD, "meshes": len(sizes_all), "triangles": total_tris,
+            "batched_mtri_per_s": total_tris / (b_ms * 1e-3) / 1e6, "batched_ms": b_ms, "batched_steps": steps,
+            "plain_mtri_per_s": total_tris / (p_ms * 1e-3) / 1e6, "plain_ms": p_ms, "plain_reps": max(1, plain_reps),
+            "batched_vs_plain": p_ms / b_ms, "sah_equal_checked_meshes": checked, "sah_equal": sah_equal,
+            "autotuned": tuned, "gpu_launches_per_batched_step": int(launches), "clocks": clk,
+            "e2e_s": (max_over_ranks(statistics.median(e2e_t), world) if e2e_t else None),
+            "h2d_bytes": int(v.nbytes), "timing": "CUDA events on the library stream, median of the timed steps"}
+
+
+def run_batch(args, world, rank, local):
+    import torch
+    import atrbvh_b200 as ab
+    torch.cuda.set_device(local)
+    ctx = ab.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    r = measure_batch(ctx, stream, world, rank, device=local, meshes=args.meshes, steps=args.steps,
+                      warmup=args.warmup,
+                      plain_reps=min(args.steps, 3), autotune=not args.no_autotune, e2e=not args.no_e2e)
+    total = r["triangles"]
     out = {
-        "metric": METRIC, "value": total_tris / (b_ms * 1e-3) / 1e6, "unit": "Mtri/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms, "higher_is_better": True,
+        "metric": METRIC, "value": r["batched_mtri_per_s"], "unit": "Mtri/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["batched_ms"], "higher_is_better": True,
         "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox)",
-        "config": {"workload": BATCH_WORKLOAD, "meshes": len(sizes_all), "triangles": total_tris, "treelet": 9,
+        "config": {"workload": BATCH_WORKLOAD, "meshes": r["meshes"], "triangles": total, "treelet": 9,
                    "iterations": 2, "morton_bits": 30,
                    "parallelism": "meshes sharded by size over ranks" if world > 1 else "one GPU",
-                   "l2": f"inputs larger than L2 ({total_tris * 48 / 1e9:.1f} GB of vertices)"},
-        "plain_mtri_per_s": total_tris / (p_ms * 1e-3) / 1e6,
-        "plain_ms": p_ms,
-        "batched_vs_plain": p_ms / b_ms,
-        "sah_equal_checked_meshes": checked, "sah_equal": sah_equal,
-        "autotuned": tuned,
-        "gpu_launches": int(launches),
-        "e2e": {"value": (total_tris / max_over_ranks(statistics.median(e2e), world) / 1e6) if e2e else None,
-                "unit": "Mtri/s",
-                "h2d_bytes_per_step": int(v.nbytes), "d2h_bytes_per_step": 4 * len(sizes),
+                   "l2": f"inputs larger than L2 ({total * 48 / 1e9:.1f} GB of vertices)"},
+        "plain_mtri_per_s": r["plain_mtri_per_s"], "plain_ms": r["plain_ms"],
+        "batched_vs_plain": r["batched_vs_plain"],
+        "sah_equal_checked_meshes": r["sah_equal_checked_meshes"], "sah_equal": r["sah_equal"],
+        "autotuned": r["autotuned"], "gpu_launches": r["gpu_launches_per_batched_step"] * args.steps,
+        "e2e": {"value": (total / r["e2e_s"] / 1e6) if r["e2e_s"] else None, "unit": "Mtri/s",
+                "h2d_bytes_per_step": r["h2d_bytes"], "d2h_bytes_per_step": 4 * r["meshes"],
                 "path": "atr_batch_create(pinned host vertices) -> atr_batch_build -> atr_batch_sah"},
-        "clocks": clk,
+        "clocks": r["clocks"],
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
+    ctx.close()
 
 
 SERVE_WORKLOAD = ("serving loop: Poisson arrivals; each request builds a mesh (log-uniform 1k-2M triangles, "
@@ -477,13 +569,13 @@ SERVE_WORKLOAD = ("serving loop: Poisson arrivals; each request builds a mesh (l
                   "64k-1M random rays; 120 GB device-memory budget")
 
 
-def run_serve(args, world, rank, local):
+def measure_serve(*, rates, requests: int, pool_size: int, lanes: int, device: int = 0) -> list[dict]:
     """The serving loop under Poisson arrivals: p50/p99 request latency beside
-    build and trace throughput, one JSON line per arrival rate."""
+    build and trace throughput, one record per arrival rate."""
     import atrbvh_b200 as ab
     rng = np.random.default_rng(0)
     pool = []
-    for k in range(args.pool):
+    for k in range(pool_size):
         n = int(np.exp(rng.uniform(np.log(1000), np.log(2_000_000))))
         v = ab.gen_scene(ab.SCENE_UNIFORM, n, 1000 + k)
         j = (v + rng.normal(0.0, 0.001, v.shape).astype(np.float32)).astype(np.float32)
@@ -493,15 +585,16 @@ def run_serve(args, world, rank, local):
         rays = ab.gen_rays_random(nr, p.min(0), p.max(0), seed=2000 + k)
         pool.append((v, j, rays))
     max_rays = max(len(r) for _, _, r in pool)
-    for rate in [float(x) for x in args.rates.split(",")]:
-        srv = ab.Server(device=local, hbm_budget=120 << 30, lanes=args.lanes, max_batch_requests=32,
+    rows = []
+    for rate in rates:
+        srv = ab.Server(device=device, hbm_budget=120 << 30, lanes=lanes, max_batch_requests=32,
                         max_batch_triangles=1 << 25)
-        outs = [np.empty((max_rays, 4), np.int32) for _ in range(2 * args.lanes * 32 + 8)]
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, args.requests))
+        outs = [np.empty((max_rays, 4), np.int32) for _ in range(2 * lanes * 32 + 8)]
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, requests))
         resident: list[int] = []
         tickets = []
         t0 = time.perf_counter()
-        for i in range(args.requests):
+        for i in range(requests):
             delay = arrivals[i] - (time.perf_counter() - t0)
             if delay > 0:
                 time.sleep(delay)
@@ -528,19 +621,28 @@ def run_serve(args, world, rank, local):
         wall = time.perf_counter() - t0
         st = srv.stats()
         srv.close()
+        rows.append({"rate_per_s": rate, "requests": requests, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                     "mean_ms": st["mean_ms"], "max_ms": st["max_ms"], "completed": st["completed"],
+                     "failed": st["failed"], "builds": st["builds"], "refits": st["refits"],
+                     "build_mtri_per_s": st["triangles_built"] / wall / 1e6,
+                     "trace_mrays_per_s": st["rays_traced"] / wall / 1e6, "wall_s": wall,
+                     "lane_batches": st["lane_batches"], "max_batch_requests_seen": st["max_batch_requests_seen"],
+                     "overlap_fraction": st["overlap_fraction"], "peak_gb": st["peak_bytes"] / 1e9})
+    return rows
+
+
+def run_serve(args, world, rank, local):
+    rows = measure_serve(rates=[float(x) for x in args.rates.split(",")], requests=args.requests,
+                         pool_size=args.pool, lanes=args.lanes, device=local)
+    for r in rows:
         out = {
-            "metric": METRIC, "value": st["p99_ms"], "unit": "ms (p99 request latency)", "n_gpus": 1,
-            "steps": args.requests, "warmup": 0, "ms_per_step": wall * 1e3 / args.requests,
+            "metric": METRIC, "value": r["p99_ms"], "unit": "ms (p99 request latency)", "n_gpus": 1,
+            "steps": args.requests, "warmup": 0, "ms_per_step": r["wall_s"] * 1e3 / args.requests,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded)",
-            "config": {"workload": SERVE_WORKLOAD, "requests": args.requests, "rate_per_s": rate,
+            "config": {"workload": SERVE_WORKLOAD, "requests": args.requests, "rate_per_s": r["rate_per_s"],
                        "pool_meshes": args.pool, "lanes": args.lanes},
-            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
-            "completed": st["completed"], "failed": st["failed"], "builds": st["builds"], "refits": st["refits"],
-            "build_mtri_per_s": st["triangles_built"] / wall / 1e6,
-            "trace_mrays_per_s": st["rays_traced"] / wall / 1e6,
-            "lane_batches": st["lane_batches"], "max_batch_requests_seen": st["max_batch_requests_seen"],
-            "overlap_fraction": st["overlap_fraction"], "peak_gb": st["peak_bytes"] / 1e9,
+            **{k: v for k, v in r.items() if k not in ("rate_per_s", "requests")},
         }
         print(json.dumps(out), flush=True)
 
@@ -608,44 +710,55 @@ def run_sweep(args, world, rank, local):
 
 
 def run_reference(args, world, rank, local):
+    """The host-core pipeline on the whole workload scene, one build per step.
+    The reference has no CPU implementation of this path, and its CUDA build
+    is not run here; the checker's restatement of the same pipeline
+    (LBVH 30-bit + ATRBVH(9,2) + collapse) stands in for it.  Nothing from the
+    product library is loaded: the scene comes from the checker's own
+    generator (the same bits as the product's)."""
     if rank != 0:
         return
     import oracle as O
-    import atrbvh_b200 as ab
-    v = ab.gen_scene(ab.SCENE_CLUSTERED, N_TRIS, 0)
+    v = O.gen_scene(O.SCENE_CLUSTERED, N_TRIS, 0)
     threads = O.max_threads()
-    m = 1 << 20
-    sample = np.ascontiguousarray(v[:m])
     for _ in range(args.warmup):
-        cpu_pipeline(sample[: 1 << 16], threads)
-    secs = [cpu_pipeline(sample, threads) for _ in range(args.steps)]
-    value = m / statistics.mean(secs) / 1e6
+        cpu_pipeline(v, threads)
+    secs = [cpu_pipeline(v, threads) for _ in range(args.steps)]
+    mean_s = statistics.mean(secs)
+    value = N_TRIS / mean_s / 1e6
     out = {
         "metric": METRIC, "value": value, "unit": "Mtri/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": statistics.mean(secs) * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox)",
+        "warmup": args.warmup, "ms_per_step": mean_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Philox: clustered scene + pinhole/diffuse rays)",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "sample_triangles": m},
+        "config": clustered_config(N_TRIS, world, WIDTH * HEIGHT * 2),
+        "best_of_steps": N_TRIS / min(secs) / 1e6,
         "cpu_baseline": {"value": value, "unit": "Mtri/s", "cores": threads, "kind": "port",
-                         "sample": f"first {m} triangles of the workload scene per step: LBVH+ATRBVH(9,2)+collapse "
-                                   f"on {threads} host threads"},
+                         "sample": f"the whole {N_TRIS}-triangle workload scene per step (no sample): "
+                                   f"LBVH+ATRBVH(9,2)+collapse on {threads} host threads, mean of {args.steps} steps "
+                                   f"after {args.warmup} warm-ups"},
         "e2e": {"value": value, "unit": "Mtri/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cuda": {
+            "unavailable": "the reference's ATRBVH CUDA kernel, compiled here for sm_100a, did not terminate on a "
+                           "4,096-triangle input on this pool (unfenced cross-SM reads of treelet rewrites); it is "
+                           "not run again"},
     }
-    out["reference_cuda"] = {
-        "unavailable": "the reference's ATRBVH CUDA kernel, compiled here for sm_100a, did not terminate on "
-                       "4,096- and 65,536-triangle inputs on this pool (unfenced cross-SM reads of treelet rewrites); "
-                       "it is not run again"}
     print(json.dumps(out), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="default line: skip the 4096-mesh batched-vs-plain keys")
+    ap.add_argument("--no-serve", action="store_true", help="default line: skip the serving p50/p99 keys")
+    ap.add_argument("--sustain-s", type=float, default=1.0,
+                    help="default line: seconds of back-to-back steps timed after the K steps, with their own clocks")
     ap.add_argument("--triangles", type=int, default=N_TRIS,
                     help="scene size (default: the workload's 4,194,304); smaller values are for profiling")
     ap.add_argument("--workload", default="clustered", choices=["clustered", "batch", "serve", "sweep"],

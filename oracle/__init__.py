@@ -52,6 +52,14 @@ def lib() -> C.CDLL:
         L.orc_trace.argtypes = [_p, _p, _p, _p, C.c_int64, C.c_int, _p, C.c_int]
         L.orc_atrbvh_schedule.argtypes = [C.c_int, C.c_int, _p, C.c_int]
         L.orc_atrbvh_schedule.restype = C.c_int
+        L.orc_gen_scene.argtypes = [C.c_int, C.c_uint32, C.c_uint64, _p]
+        L.orc_gen_rays_pinhole.argtypes = [C.c_uint32, C.c_uint32, _p, C.c_float, _p]
+        L.orc_gen_rays_random.argtypes = [C.c_uint64, C.c_uint64, _p, _p, _p]
+        L.orc_gen_batch_sizes.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _p]
+        L.orc_gen_batch_scene.argtypes = [C.c_uint32, _p, C.c_uint64, _p]
+        for f in (L.orc_gen_scene, L.orc_gen_rays_pinhole, L.orc_gen_rays_random, L.orc_gen_batch_sizes,
+                  L.orc_gen_batch_scene):
+            f.restype = C.c_int
     return _lib
 
 
@@ -157,6 +165,14 @@ def trbvh(t: Tree, treelet: int = 7, iterations: int = 3, ci: float = 1.2, ct: f
     return out
 
 
+def refit(t: Tree, v: np.ndarray, threads: int = 0) -> Tree:
+    """Boxes and areas of t's topology recomputed from vertices v."""
+    out = t.copy()
+    v = np.ascontiguousarray(v, np.float32)
+    lib().orc_refit(_ptr(v), out.n, *out.ptrs(), threads)
+    return out
+
+
 def sah(t: Tree, ci: float = 1.2, ct: float = 1.0) -> float:
     return float(lib().orc_sah(t.n, _ptr(t.area), 0, ci, ct))
 
@@ -242,3 +258,48 @@ def atrbvh_schedule(treelet: int, warp: int = 32) -> np.ndarray:
     out = np.zeros(4096, np.int32)
     k = lib().orc_atrbvh_schedule(treelet, warp, _ptr(out), len(out))
     return out[:k]
+
+
+# ---- seeded workloads (the checker's own generators) --------------------------
+
+SCENE_UNIFORM, SCENE_CLUSTERED = 0, 1
+
+
+def _ok(rc: int, what: str) -> None:
+    if rc != 0:
+        raise ValueError(f"{what}: invalid arguments")
+
+
+def gen_scene(kind: int, n: int, seed: int = 0) -> np.ndarray:
+    """(n, 3, 4) float32 triangle soup of the unit-cube (0) or clustered (1) scene."""
+    out = np.empty((n, 3, 4), np.float32)
+    _ok(lib().orc_gen_scene(kind, n, seed, _ptr(out)), "gen_scene")
+    return out
+
+
+def gen_rays_pinhole(w: int, h: int, eye=(0.5, 0.5, -1.5), fov_deg: float = 60.0) -> np.ndarray:
+    out = np.empty((w * h, 2, 4), np.float32)
+    e = np.asarray(eye, np.float32)
+    _ok(lib().orc_gen_rays_pinhole(w, h, _ptr(e), fov_deg, _ptr(out)), "gen_rays_pinhole")
+    return out
+
+
+def gen_rays_random(n: int, bbmin, bbmax, seed: int = 0) -> np.ndarray:
+    out = np.empty((n, 2, 4), np.float32)
+    mn = np.asarray(bbmin, np.float32)
+    mx = np.asarray(bbmax, np.float32)
+    _ok(lib().orc_gen_rays_random(n, seed, _ptr(mn), _ptr(mx), _ptr(out)), "gen_rays_random")
+    return out
+
+
+def gen_batch_sizes(count: int, lo: int, hi: int, seed: int = 0) -> np.ndarray:
+    out = np.empty(count, np.uint32)
+    _ok(lib().orc_gen_batch_sizes(count, lo, hi, seed, _ptr(out)), "gen_batch_sizes")
+    return out
+
+
+def gen_batch_scene(sizes: np.ndarray, seed: int = 0) -> np.ndarray:
+    sizes = np.ascontiguousarray(sizes, np.uint32)
+    out = np.empty((int(sizes.sum(dtype=np.uint64)), 3, 4), np.float32)
+    _ok(lib().orc_gen_batch_scene(len(sizes), _ptr(sizes), seed, _ptr(out)), "gen_batch_scene")
+    return out

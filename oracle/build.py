@@ -1,7 +1,8 @@
 """ORACLE -- test infrastructure only.
 
 Builds the checker:
-  oracle/liboracle.so   CPU restatement (atr_oracle.cpp), g++ -O2
+  oracle/liboracle.so   CPU restatement (atr_oracle.cpp) and the seeded
+                        workload generators (workload_oracle.cpp), g++ -O2
                         -ffp-contract=off -fopenmp.
 
 The reference's own sources are located through the ATRBVH_REFERENCE
@@ -34,11 +35,11 @@ def _run(cmd: list[str], **kw) -> None:
 
 def build_oracle() -> Path:
     out = HERE / "liboracle.so"
-    src = HERE / "atr_oracle.cpp"
-    if out.exists() and out.stat().st_mtime >= src.stat().st_mtime:
+    srcs = [HERE / "atr_oracle.cpp", HERE / "workload_oracle.cpp"]
+    if out.exists() and out.stat().st_mtime >= max(p.stat().st_mtime for p in srcs):
         return out
     _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
-          "-shared", "-o", str(out), str(src)])
+          "-shared", "-o", str(out), *map(str, srcs)])
     return out
 
 

@@ -65,17 +65,38 @@ def tree_digests(parent, left, right, data, bmin, bmax, area) -> dict:
     }
 
 
+def reachable_leaves(left, right, data, count, tri_indices):
+    """Leaves reachable from the root of a collapsed tree, ascending by node,
+    with their triangle counts and their triangle lists end to end (level by
+    level over numpy arrays, so it stays quick at millions of nodes)."""
+    left, right, data, count = (np.asarray(a) for a in (left, right, data, count))
+    tri_indices = np.asarray(tri_indices)
+    leaves = []
+    frontier = np.zeros(1, np.int64)
+    while frontier.size:
+        ch = np.concatenate([left[frontier], right[frontier]]).astype(np.int64)
+        is_leaf = data[ch] >= 0
+        leaves.append(ch[is_leaf])
+        frontier = ch[~is_leaf]
+    nodes = np.sort(np.concatenate(leaves)) if leaves else np.zeros(0, np.int64)
+    cnt = np.maximum(count[nodes].astype(np.int64), 1)
+    start = np.where(count[nodes] > 1, data[nodes], -1).astype(np.int64)
+    # Flat list: leaf k contributes tri_indices[start_k : start_k + cnt_k], or
+    # its own data index when it holds one triangle.
+    first = np.repeat(np.cumsum(cnt) - cnt, cnt)
+    within = np.arange(int(cnt.sum()), dtype=np.int64) - first
+    owner = np.repeat(np.arange(len(nodes)), cnt)
+    multi = start[owner] >= 0
+    flat = np.where(multi, tri_indices[np.where(multi, start[owner] + within, 0)], data[nodes][owner])
+    return nodes, cnt, flat.astype(np.int64)
+
+
 def collapsed_digests(left, right, data, count, tri_indices, n) -> dict:
     """Order-independent digest of a collapsed tree: reachable leaves with
     their triangle lists (the reference assigns list offsets by atomicAdd)."""
-    import oracle as O
-    ll = O.leaf_lists(left, right, data, count, tri_indices, n)
-    flat = []
-    for node in sorted(ll):
-        flat.append(node)
-        flat.append(len(ll[node]))
-        flat.extend(ll[node])
-    return {"leaves": digest(np.asarray(flat, np.int64)), "num_leaves": len(ll)}
+    nodes, cnt, flat = reachable_leaves(left, right, data, count, tri_indices)
+    return {"leaf_nodes": digest(nodes), "leaf_counts": digest(cnt), "leaf_lists": digest(flat),
+            "num_leaves": int(len(nodes))}
 
 
 def check_tree(t, n: int) -> None:

@@ -257,3 +257,65 @@ def test_library_reports_errors_without_device():
     assert st in (2, 6)
     assert ab.lib().atr_last_error()
     assert ab.lib().atr_build_lbvh(None, None, 30, C.byref(h)) == 1
+
+
+def test_oracle_workload_generators_match_product_and_digests():
+    """The checker's own scene and ray generators (used by the host-core
+    baseline and the reference arm of bench.py, which load nothing from the
+    product library) produce the same bits as the product's generators and
+    as the committed workload digests."""
+    from tests._util import CASES, digest
+    want = json.loads((GOLDEN / "workload_digests.json").read_text())
+    kinds = {"uniform": O.SCENE_UNIFORM, "clustered": O.SCENE_CLUSTERED}
+    for name, (kind, n, seed) in CASES.items():
+        if kind in kinds:
+            v = O.gen_scene(kinds[kind], n, seed)
+            assert digest(v) == want[name], name
+    for kind, n, seed in [(O.SCENE_CLUSTERED, 1 << 16, 0), (O.SCENE_UNIFORM, 3000, 4)]:
+        a, b = O.gen_scene(kind, n, seed), ab.gen_scene(kind, n, seed)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (kind, n)
+    a, b = O.gen_rays_pinhole(320, 200), ab.gen_rays_pinhole(320, 200)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    a, b = O.gen_rays_random(5000, [0, 0, 0], [1, 2, 3], 5), ab.gen_rays_random(5000, [0, 0, 0], [1, 2, 3], 5)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    sa, sb = O.gen_batch_sizes(4096, 256, 262144, 0), ab.gen_batch_sizes(4096, 256, 262144, 0)
+    assert np.array_equal(sa, sb)
+    assert np.array_equal(O.gen_batch_scene(sa[:40]).view(np.uint32), ab.gen_batch_scene(sb[:40]).view(np.uint32))
+
+
+def test_cpu_golden_fullsize():
+    """The committed full-size digests (tests/golden/fullsize_oracle.json,
+    which the full-size GPU tests and bench.py's SAH check read) are the
+    oracle's own outputs: the clustered 4,194,304-triangle pipeline end to
+    end, and the 16,777,216-triangle LBVH and ATRBVH(9,2) trees."""
+    from tests._util import collapsed_digests, digest, tree_digests
+    gold = json.loads((GOLDEN / "fullsize_oracle.json").read_text())
+    g = gold["c2"]
+    v = O.gen_scene(O.SCENE_CLUSTERED, 4194304, 0)
+    assert digest(v) == g["scene"]
+    mn, mx = O.scene_aabb(v)
+    base, _, _ = O.build_lbvh(v, mn, mx, threads=0)
+    t = O.atrbvh(base, 9, 2, threads=0)
+
+    def tdig(x):
+        return tree_digests(x.parent, x.left, x.right, x.data, x.bbox_min, x.bbox_max, x.area)
+
+    assert tdig(base) == g["lbvh_tree"] and tdig(t) == g["tree"]
+    assert np.float32(O.sah(t)) == np.float32(g["tree_sah"])
+    c = O.collapse(t)
+    assert np.float32(c.sah) == np.float32(g["collapsed_sah"])
+    assert collapsed_digests(c.left, c.right, c.data, c.triangle_count, c.triangle_indices, len(v)) == g["collapsed"]
+    cp = O.flatten(c, v)
+    assert digest(cp.nodes) == g["compact2"]["nodes"] and digest(cp.tri_index) == g["compact2"]["tri_index"]
+    assert digest(cp.woop) == g["compact2"]["woop"]
+    rays = O.gen_rays_pinhole(1920, 1080)
+    res = O.trace(cp, rays)
+    assert digest(res[:, 0].copy()) == g["primary_hits"]["ids"] and digest(res[:, 1].copy()) == g["primary_hits"]["t"]
+    g3 = gold["c3"]
+    v = O.gen_scene(O.SCENE_UNIFORM, 16777216, 0)
+    assert digest(v) == g3["scene"]
+    mn, mx = O.scene_aabb(v)
+    base, _, _ = O.build_lbvh(v, mn, mx, threads=0)
+    assert tdig(base) == g3["variants"]["lbvh"]["tree"]
+    t = O.atrbvh(base, 9, 2, threads=0)
+    assert tdig(t) == g3["variants"]["atrbvh_9_2"]["tree"]
