@@ -52,6 +52,16 @@ def lib() -> C.CDLL:
         L.orc_trace.argtypes = [_p, _p, _p, _p, C.c_int64, C.c_int, _p, C.c_int]
         L.orc_atrbvh_schedule.argtypes = [C.c_int, C.c_int, _p, C.c_int]
         L.orc_atrbvh_schedule.restype = C.c_int
+        L.orc_expand_bits.argtypes = [C.c_uint32]
+        L.orc_expand_bits.restype = C.c_uint32
+        L.orc_morton30_point.argtypes = [C.c_float] * 3
+        L.orc_morton30_point.restype = C.c_uint32
+        L.orc_morton63_point.argtypes = [C.c_float] * 3
+        L.orc_morton63_point.restype = C.c_uint64
+        L.orc_box_area.argtypes = [_p, _p]
+        L.orc_box_area.restype = C.c_float
+        L.orc_union_area.argtypes = [_p, _p, _p, _p]
+        L.orc_union_area.restype = C.c_float
         L.orc_gen_scene.argtypes = [C.c_int, C.c_uint32, C.c_uint64, _p]
         L.orc_gen_rays_pinhole.argtypes = [C.c_uint32, C.c_uint32, _p, C.c_float, _p]
         L.orc_gen_rays_random.argtypes = [C.c_uint64, C.c_uint64, _p, _p, _p]
@@ -303,3 +313,85 @@ def gen_batch_scene(sizes: np.ndarray, seed: int = 0) -> np.ndarray:
     out = np.empty((int(sizes.sum(dtype=np.uint64)), 3, 4), np.float32)
     _ok(lib().orc_gen_batch_scene(len(sizes), _ptr(sizes), seed, _ptr(out)), "gen_batch_scene")
     return out
+
+
+# ---- the reference's own code on the host (oracle/_ref/libbvhrt_ref_host.so) ----
+
+REF_HOST_LIB = HERE / "_ref" / "libbvhrt_ref_host.so"
+_ref_host = None
+
+
+def ref_host_available() -> bool:
+    return REF_HOST_LIB.exists()
+
+
+def ref_host_lib() -> C.CDLL:
+    """The reference's BVHRT-Core sources compiled for the host execution
+    model (oracle/ref_cpu/, built by oracle/build.py where the reference tree
+    is present)."""
+    global _ref_host
+    if _ref_host is None:
+        L = C.CDLL(str(REF_HOST_LIB))
+        L.ref_host_run.restype = C.c_int
+        L.ref_host_run.argtypes = [_p, C.c_uint, _p, _p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int] + \
+            [_p] * 15 + [_p, _p]
+        L.ref_host_morton.argtypes = [_p, C.c_uint, _p, _p, C.c_int, _p, _p, _p]
+        L.ref_host_morton.restype = C.c_int
+        L.ref_host_morton30_point.argtypes = [C.c_float] * 3
+        L.ref_host_morton30_point.restype = C.c_uint32
+        L.ref_host_morton63_point.argtypes = [C.c_float] * 3
+        L.ref_host_morton63_point.restype = C.c_uint64
+        L.ref_host_expand_bits.argtypes = [C.c_uint32]
+        L.ref_host_expand_bits.restype = C.c_uint32
+        for f in (L.ref_host_box_area3, L.ref_host_box_area4, L.ref_host_box_area_arr):
+            f.argtypes = [_p, _p]
+            f.restype = C.c_float
+        for f in (L.ref_host_union_area3, L.ref_host_union_area4):
+            f.argtypes = [_p, _p, _p, _p]
+            f.restype = C.c_float
+        L.ref_host_sah.argtypes = [C.c_uint, _p, C.c_float, C.c_float]
+        L.ref_host_sah.restype = C.c_float
+        _ref_host = L
+    return _ref_host
+
+
+def ref_host_run(v: np.ndarray, bbmin, bbmax, *, use64=False, optimizer=0, treelet=9, iterations=2,
+                 collapse=False):
+    """The reference's own pipeline (LBVHBuilder, optimiser, collapser) on the
+    host; returns (Tree, Collapsed | None, times_ms)."""
+    v = np.ascontiguousarray(v, np.float32)
+    n = v.shape[0]
+    t = Tree.empty(n)
+    nn = 2 * n - 1
+    c = None
+    if collapse:
+        c = Collapsed(*(np.zeros(nn, np.int32) for _ in range(5)), np.zeros((nn, 4), np.float32),
+                      np.zeros((nn, 4), np.float32), np.zeros(n, np.int32), np.zeros(0, np.float32), 0.0)
+    sah_out = np.zeros(1, np.float32)
+    times = np.zeros(3, np.float64)
+    mn = np.asarray(bbmin, np.float32)
+    mx = np.asarray(bbmax, np.float32)
+    cp = [None] * 8 if c is None else [_ptr(c.parent), _ptr(c.left), _ptr(c.right), _ptr(c.data),
+                                      _ptr(c.triangle_count), _ptr(c.bbox_min), _ptr(c.bbox_max),
+                                      _ptr(c.triangle_indices)]
+    ref_host_lib().ref_host_run(_ptr(v), n, _ptr(mn), _ptr(mx), 1 if use64 else 0, optimizer, treelet, iterations,
+                                1 if collapse else 0, 1, *t.ptrs(), *cp, _ptr(sah_out), _ptr(times))
+    if c is not None:
+        c.sah = float(sah_out[0])
+    return t, c, times
+
+
+def ref_host_morton(v: np.ndarray, bbmin, bbmax, bits: int = 30):
+    """The reference's Morton kernel output (keys in triangle order, indices)."""
+    v = np.ascontiguousarray(v, np.float32)
+    n = v.shape[0]
+    mn = np.asarray(bbmin, np.float32)
+    mx = np.asarray(bbmax, np.float32)
+    idx = np.zeros(n, np.uint32)
+    if bits == 30:
+        k = np.zeros(n, np.uint32)
+        ref_host_lib().ref_host_morton(_ptr(v), n, _ptr(mn), _ptr(mx), 0, _ptr(k), None, _ptr(idx))
+    else:
+        k = np.zeros(n, np.uint64)
+        ref_host_lib().ref_host_morton(_ptr(v), n, _ptr(mn), _ptr(mx), 1, None, _ptr(k), _ptr(idx))
+    return k, idx

@@ -560,6 +560,23 @@ extern "C" {
 // Number of host threads the parallel entry points use when asked for 0.
 int orc_max_threads(void) { return nthreads_or_max(0); }
 
+// Point-level forms of the arithmetic above, for the pins against the
+// reference's own helpers (BVHRT-Core/src/Commons.cuh:99-194, 481-510, 606-662):
+// a point already normalised to the unit cube, boxes as three floats.
+uint32_t orc_expand_bits(uint32_t v) { return expand_bits(v); }
+uint32_t orc_morton30_point(float x, float y, float z) {
+    const float c[3] = {x, y, z}, lo[3] = {0.0f, 0.0f, 0.0f}, hi[3] = {1.0f, 1.0f, 1.0f};
+    return morton30(c, lo, hi);
+}
+uint64_t orc_morton63_point(float x, float y, float z) {
+    const float c[3] = {x, y, z}, lo[3] = {0.0f, 0.0f, 0.0f}, hi[3] = {1.0f, 1.0f, 1.0f};
+    return morton63(c, lo, hi);
+}
+float orc_box_area(const float* mn, const float* mx) { return box_area(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]); }
+float orc_union_area(const float* mn1, const float* mx1, const float* mn2, const float* mx2) {
+    return union_area(mn1, mx1, mn2, mx2);
+}
+
 // Scene AABB over all vertices: gpu-ray-traversal/src/rt/SceneConverter.cpp:28-60.
 // The max is seeded with numeric_limits<float>::min() (the smallest positive
 // normal float), as in the reference.
