@@ -330,6 +330,17 @@ class Context:
             pass
 
 
+def scene_bounds(vertices) -> tuple[np.ndarray, np.ndarray]:
+    """Host-side scene box as the reference's SceneConverter computes it
+    (gpu-ray-traversal/src/rt/SceneConverter.cpp:19-72): the minimum over all
+    vertices, and the maximum seeded with FLT_MIN (the smallest positive
+    normal float), for SceneWrapper's bbmin/bbmax."""
+    v = np.asarray(vertices, dtype=np.float32).reshape(-1, 4)[:, :3]
+    mn = v.min(axis=0)
+    mx = np.maximum(v.max(axis=0), np.finfo(np.float32).tiny)
+    return mn.astype(np.float32), mx.astype(np.float32)
+
+
 class SceneWrapper:
     """BVHRT::SceneWrapper: device copy of the triangle soup and its box."""
 

@@ -856,6 +856,18 @@ int refit_arrays(atr_ctx* ctx, uint32_t n, const TreeOut& t, const float4* verts
     return ATR_OK;
 }
 
+// Caller-given scene bounds written by the device from kernel arguments, so
+// that creating a scene from host bounds enqueues without waiting for the
+// vertex upload (no host buffer has to outlive the call).
+__global__ void k_set_bounds(float* __restrict__ out, float x0, float y0, float z0, float x1, float y1, float z1) {
+    out[0] = x0;
+    out[1] = y0;
+    out[2] = z0;
+    out[3] = x1;
+    out[4] = y1;
+    out[5] = z1;
+}
+
 int scene_bounds_device(atr_ctx* ctx, const float4* verts, uint32_t n, float* d_out) {
     const uint64_t nv = 3ull * n;
     const int blocks = grid_for(ctx, nv, 2, 256);
@@ -894,10 +906,11 @@ int atr_scene_create(atr_ctx* ctx, const float* vertices, uint32_t n, const floa
                                     on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream);
     if (e != cudaSuccess) { atr_scene_destroy(s); return cuda_fail(e, "cudaMemcpyAsync(vertices)", __FILE__, __LINE__); }
     if (bbmin) {
-        float h[6] = {bbmin[0], bbmin[1], bbmin[2], bbmax[0], bbmax[1], bbmax[2]};
-        e = cudaMemcpyAsync(s->d_bounds, h, sizeof(h), cudaMemcpyHostToDevice, ctx->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // h is a stack array
-        if (e != cudaSuccess) { atr_scene_destroy(s); return cuda_fail(e, "cudaMemcpyAsync(bounds)", __FILE__, __LINE__); }
+        k_set_bounds<<<1, 1, 0, ctx->stream>>>(s->d_bounds, bbmin[0], bbmin[1], bbmin[2], bbmax[0], bbmax[1],
+                                               bbmax[2]);
+        ctx->launches += 1;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) { atr_scene_destroy(s); return cuda_fail(e, "k_set_bounds", __FILE__, __LINE__); }
     } else {
         st = scene_bounds_device(ctx, s->verts, n, s->d_bounds);
         if (st != ATR_OK) { atr_scene_destroy(s); return st; }

@@ -75,16 +75,31 @@ HOST_LIB = REF_OUT / "libbvhrt_ref_host.so"
 #     treeletLeavesAreas[1] < nodesSah[root] and lane 1 then stores the
 #     root's new nodesSah; in lock-step all lanes compare before that store,
 #     so the comparison is taken, then the warp syncs, then it branches.
+#   * TRBVH.cu updateTreelet, the treelet rewrite's work stack: every lane
+#     reads stackSize (the loop condition, then lastStackSize) before lane 0
+#     clears it, and every lane pushes its left child (atomicAdd on
+#     currentInternalNode and stackSize, in lane order) before any lane
+#     pushes its right child.  Warp syncs go before the loop condition, after
+#     the lastStackSize read and before the right-child block.
 LOCKSTEP_SYNCS = [
-    ("AgglomerativeTreelet.cu", r"void\s+findMinimumDistance\s*\([^)]*\)\s*\{", " SIMT_WARP_SYNC();"),
+    ("AgglomerativeTreelet.cu", r"void\s+findMinimumDistance\s*\([^)]*\)\s*\{", " SIMT_WARP_SYNC(1);"),
+    ("TRBVH.cu", r"int\s+lastStackSize\s*=\s*stackSize\[globalWarpIndex\]\s*;", " SIMT_WARP_SYNC(4);"),
 ]
 # (file, anchor regex, replacement) for the comparison above.
 LOCKSTEP_REWRITES = [
     ("AgglomerativeTreelet.cu",
      r"if\s*\(\s*treeletLeavesAreas\[1\]\s*<\s*nodesSah\[treeletInternalNodes\[0\]\]\s*\)",
-     "const bool simtAccept = treeletLeavesAreas[1] < nodesSah[treeletInternalNodes[0]]; SIMT_WARP_SYNC(); "
+     "const bool simtAccept = treeletLeavesAreas[1] < nodesSah[treeletInternalNodes[0]]; SIMT_WARP_SYNC(2); "
      "if (simtAccept)"),
+    ("TRBVH.cu", r"while\s*\(\s*stackSize\[globalWarpIndex\]\s*>\s*0\s*\)",
+     "while ((SIMT_WARP_SYNC(3), stackSize[globalWarpIndex] > 0))"),
+    ("TRBVH.cu", r"if\s*\(\s*__popc\(partitionComplement\)\s*>\s*1\s*\)",
+     "SIMT_WARP_SYNC(5); if (__popc(partitionComplement) > 1)"),
 ]
+# Translation units whose code must keep source order in its layout: the host
+# model orders divergent collectives by code address (TRBVH.cu calls
+# __shfl_down inside a branch that some lanes skip, in processSubsets).
+SOURCE_ORDER = {"TRBVH.cu"}
 
 
 def _matching(text: str, i: int, open_ch: str, close_ch: str) -> int:
@@ -174,8 +189,8 @@ def build_reference_host() -> Path | None:
     REF_OUT.mkdir(exist_ok=True)
     objdir = REF_OUT / "obj_host"
     objdir.mkdir(exist_ok=True)
-    base = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fpermissive", "-w",
-            "-I", str(OWN / "include"), "-I", str(OWN), "-I", str(src)]
+    base = ["g++", "-std=c++17", "-O2", "-fno-omit-frame-pointer", "-fPIC", "-ffp-contract=off", "-fno-fast-math",
+            "-fpermissive", "-w", "-I", str(OWN / "include"), "-I", str(OWN), "-I", str(src)]
     jobs = []
     objs = []
     for f in REF_KERNELS:
@@ -183,7 +198,8 @@ def build_reference_host() -> Path | None:
         objs.append(o)
         text = cuda_source_for_host((src / f).read_text(errors="replace"), f)
         text = f'#line 1 "{src / f}"\n' + text
-        jobs.append((base + ["-D__CUDA_ARCH__=350", "-x", "c++", "-c", "-", "-o", str(o)], text))
+        opt = ["-O0"] if f in SOURCE_ORDER else []
+        jobs.append((base + opt + ["-D__CUDA_ARCH__=350", "-x", "c++", "-c", "-", "-o", str(o)], text))
     for f in REF_HOST:
         o = objdir / (f + ".o")
         objs.append(o)

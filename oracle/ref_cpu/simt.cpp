@@ -46,6 +46,7 @@ enum State { kReady, kInCollective, kAtBarrier, kDone };
 
 struct Thread {
     void* sp = nullptr;
+    char* stack = nullptr;
     uint3 tid{0, 0, 0};
     int state = kDone;
     int kind = 0;
@@ -53,6 +54,14 @@ struct Thread {
     uint64_t value = 0;
     uint64_t result = 0;
 };
+
+// Lanes wait in the same collective when they wait in collectives of the same
+// kind (and, for inserted warp syncs, the same id).  Code addresses cannot
+// tell this: an optimising compiler may duplicate one source-level
+// collective into several code paths.
+bool same_collective(const Thread& a, const Thread& b) {
+    return a.kind == b.kind && (a.kind != kWarpSync || a.arg == b.arg);
+}
 
 constexpr size_t kStackBytes = 256 * 1024;
 
@@ -115,24 +124,79 @@ void yield() {
     simt_switch(&t->sp, g.sched_sp);
 }
 
-// All live lanes of [lo, hi) wait in a collective: compute every lane's
-// result from the operands as deposited, then release the lanes.
+// Return addresses of a suspended thread's frames, outermost first (frame
+// pointers are kept in every object of the host model).
+std::vector<const void*> call_chain(const Thread& t) {
+    std::vector<const void*> chain;
+    void* const* regs = static_cast<void* const*>(t.sp);
+    chain.push_back(regs[6]);
+    const char* lo = t.stack;
+    const char* hi = t.stack + kStackBytes;
+    const char* fp = static_cast<const char*>(regs[5]);
+    while (fp && fp >= lo && fp + 16 <= hi) {
+        chain.push_back(reinterpret_cast<void* const*>(fp)[1]);
+        fp = static_cast<const char*>(reinterpret_cast<void* const*>(fp)[0]);
+    }
+    std::reverse(chain.begin(), chain.end());
+    return chain;
+}
+
+// True when a's call chain lies before b's in program order: compared at the
+// first frame where they differ, by code address.
+bool chain_before(const std::vector<const void*>& a, const std::vector<const void*>& b) {
+    const size_t m = std::min(a.size(), b.size());
+    for (size_t k = 0; k < m; ++k)
+        if (a[k] != b[k]) return a[k] < b[k];
+    return a.size() < b.size();
+}
+
+// All live lanes of [lo, hi) wait in collectives.  When they wait in the same
+// one, all take part.  When they wait in different ones (a collective inside
+// a branch some lanes skipped), the lanes furthest back in program order (by
+// call chain; the code concerned keeps source order in its layout) take part
+// and the others keep waiting: the divergent path runs to its reconvergence
+// point first, as on a warp of the pre-Volta SIMT model.  Each lane taking
+// part gets its result from the operands as deposited; a source lane that
+// takes no part gives the reader its own operand.
 void complete_collective(size_t lo, size_t hi) {
-    int first_kind = -1;
+    std::vector<char> part(hi - lo, 0);
+    bool one_site = true;
+    const Thread* ref = nullptr;
     for (size_t i = lo; i < hi; ++i) {
         const Thread& t = g.threads[i];
         if (t.state != kInCollective) continue;
-        if (first_kind < 0) first_kind = t.kind;
-        if (t.kind != first_kind) fail("lanes of one warp wait in different kinds of collective");
+        if (!ref) ref = &t;
+        else if (!same_collective(t, *ref)) one_site = false;
     }
-    auto lane_live = [&](size_t i) { return i < hi && g.threads[i].state == kInCollective; };
+    if (one_site) {
+        for (size_t i = lo; i < hi; ++i) part[i - lo] = g.threads[i].state == kInCollective;
+    } else {
+        std::vector<std::vector<const void*>> chains(hi - lo);
+        std::vector<const void*>* best = nullptr;
+        for (size_t i = lo; i < hi; ++i) {
+            if (g.threads[i].state != kInCollective) continue;
+            chains[i - lo] = call_chain(g.threads[i]);
+            if (!best || chain_before(chains[i - lo], *best)) best = &chains[i - lo];
+        }
+        for (size_t i = lo; i < hi; ++i)
+            part[i - lo] = g.threads[i].state == kInCollective && chains[i - lo] == *best;
+        ++g.stats.divergent;
+    }
+    int first_kind = -1;
+    for (size_t i = lo; i < hi; ++i) {
+        if (!part[i - lo]) continue;
+        const Thread& t = g.threads[i];
+        if (first_kind < 0) first_kind = t.kind;
+        if (t.kind != first_kind) fail("lanes at one call site wait in different kinds of collective");
+    }
+    auto lane_live = [&](size_t i) { return i < hi && part[i - lo]; };
     uint32_t ballot = 0;
     if (first_kind == kBallot)
         for (size_t i = lo; i < hi; ++i)
             if (lane_live(i) && g.threads[i].value) ballot |= 1u << (i - lo);
     for (size_t i = lo; i < hi; ++i) {
         Thread& t = g.threads[i];
-        if (t.state != kInCollective) continue;
+        if (!part[i - lo]) continue;
         switch (first_kind) {
             case kShfl: {
                 const size_t src = lo + ((unsigned)t.arg & 31u);
@@ -163,7 +227,7 @@ void complete_collective(size_t lo, size_t hi) {
         }
     }
     for (size_t i = lo; i < hi; ++i)
-        if (g.threads[i].state == kInCollective) g.threads[i].state = kReady;
+        if (part[i - lo]) g.threads[i].state = kReady;
     ++g.stats.collectives;
 }
 
@@ -175,7 +239,8 @@ void run_block() {
         t.tid = uint3{(unsigned)(i % g.bdim.x), (unsigned)((i / g.bdim.x) % g.bdim.y),
                       (unsigned)(i / ((size_t)g.bdim.x * g.bdim.y))};
         t.state = kReady;
-        t.sp = initial_sp(stack_for(i));
+        t.stack = stack_for(i);
+        t.sp = initial_sp(t.stack);
     }
     const size_t warps = (n + 31) / 32;
     while (true) {
@@ -228,7 +293,7 @@ const dim3& block_dim() { return g.bdim; }
 const dim3& grid_dim() { return g.gdim; }
 void* dynamic_shared() { return g.shared.data(); }
 
-uint64_t warp_collective(int kind, uint64_t value, int arg) {
+__attribute__((noinline)) uint64_t warp_collective(int kind, uint64_t value, int arg) {
     Thread* t = g.cur;
     if (!t) fail("warp intrinsic called outside a kernel");
     t->kind = kind;

@@ -11,14 +11,17 @@
 //   * a thread runs until it reaches a warp collective (__shfl, __shfl_down,
 //     __ballot), __syncthreads() or its end; lanes of a warp run in lane
 //     order between collectives;
-//   * a warp collective completes when every live lane of the warp has
-//     reached one (all of the same kind); __syncthreads() completes when
+//   * a warp collective completes when every live lane of the warp waits in
+//     one; when they wait at different call sites (a collective inside a
+//     branch that some lanes skipped), the lanes furthest back in program
+//     order complete theirs first, as a divergent path of a pre-Volta warp
+//     runs to its reconvergence point first.  __syncthreads() completes when
 //     every live thread of the block waits in one.  Threads that have
 //     returned take no part, as on the hardware;
 //   * atomics are plain read-modify-writes (one fiber runs at a time).
 // Code written for the pre-Volta lock-step warp (a lane reading what another
 // lane wrote with no collective in between) needs an explicit warp sync at
-// that point; the build recipe inserts SIMT_WARP_SYNC() where the reference
+// that point; the build recipe inserts SIMT_WARP_SYNC(id) where the reference
 // relies on it, and documents each place.
 #pragma once
 
@@ -80,7 +83,7 @@ void run(const Launch& cfg, const std::function<void()>& body);
 
 // Counters of the last run(), for tests of the model itself.
 struct Stats {
-    uint64_t blocks, threads, collectives, barriers, inactive_sources;
+    uint64_t blocks, threads, collectives, barriers, inactive_sources, divergent;
 };
 Stats last_stats();
 
@@ -114,7 +117,8 @@ inline T from_bits(uint64_t b) {
 #define __shared__ static
 #define __restrict__
 
-#define SIMT_WARP_SYNC() ((void)::simt::warp_collective(::simt::kWarpSync, 0, 0))
+// A warp sync inserted into the reference's source; each place has its own id.
+#define SIMT_WARP_SYNC(id) ((void)::simt::warp_collective(::simt::kWarpSync, 0, (id)))
 
 // Legacy (mask-less) warp intrinsics over the lanes that reach them.
 template <class T>

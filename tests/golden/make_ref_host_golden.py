@@ -1,6 +1,6 @@
 """Write tests/golden/ref_host_golden.json: outputs of the reference's own
-BVHRT-Core code (its Morton, sort call, Karras, refit, ATRBVH and collapse
-kernels and host classes, compiled from the reference tree by oracle/build.py
+BVHRT-Core code (its Morton, sort call, Karras, refit, ATRBVH, TRBVH and
+collapse kernels and host classes, compiled from the reference tree by oracle/build.py
 for the host execution model of oracle/ref_cpu/) on the seeded test cases.
 
 Each record holds digests of the tree arrays, the SAH, and for collapsed runs
@@ -33,7 +33,9 @@ RUNS = ([(c, "lbvh", 0, 0, 30, True) for c in SMALL] + [(c, "lbvh", 0, 0, 63, Fa
         + [(c, "lbvh", 0, 0, 30, True) for c in ("c1", "clu65536")]
         + [(c, "lbvh", 0, 0, 63, False) for c in ("c1", "clu65536")]
         + [(c, "atrbvh", 9, 2, 30, True) for c in ("c1", "clu65536")]
-        + [("c1", "atrbvh", 5, 1, 30, False), ("c1", "atrbvh", 7, 3, 30, False)])
+        + [("c1", "atrbvh", 5, 1, 30, False), ("c1", "atrbvh", 7, 3, 30, False)]
+        + [(c, "trbvh", 7, i, 30, i == 3) for c in SMALL for i in (1, 2, 3)]
+        + [("c1", "trbvh", 7, 3, 30, True), ("clu65536", "trbvh", 7, 2, 30, False)])
 
 
 def main() -> None:
@@ -45,7 +47,7 @@ def main() -> None:
         v = scene_case(case)
         mn, mx = O.scene_aabb(v)
         t0 = time.perf_counter()
-        t, c, _ = O.ref_host_run(v, mn, mx, use64=bits == 63, optimizer={"lbvh": 0, "atrbvh": 1}[opt],
+        t, c, _ = O.ref_host_run(v, mn, mx, use64=bits == 63, optimizer={"lbvh": 0, "atrbvh": 1, "trbvh": 2}[opt],
                                  treelet=ts, iterations=it, collapse=col)
         keys, idx = O.ref_host_morton(v, mn, mx, bits)
         rec = {"case": case, "optimizer": opt, "treelet": ts, "iterations": it, "bits": bits,
@@ -60,7 +62,7 @@ def main() -> None:
         print(case, opt, ts, it, bits, rec["sah"], f"{time.perf_counter() - t0:.1f}s", flush=True)
     doc = {"generator": "tests/golden/make_ref_host_golden.py",
            "reference_build": "oracle/_ref/libbvhrt_ref_host.so: BVHRT-Core/src/{LBVH,AgglomerativeTreelet,"
-                              "TreeCollapser}.cu and the host classes, compiled from the reference tree by "
+                              "TRBVH,TreeCollapser}.cu and the host classes, compiled from the reference tree by "
                               "oracle/build.py for the host execution model (oracle/ref_cpu/)",
            "records": records}
     OUT.write_text(json.dumps(doc, indent=1))

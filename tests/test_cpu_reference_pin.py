@@ -1,7 +1,7 @@
 """The oracle pinned to the reference's own code, on the CPU.
 
 oracle/_ref/libbvhrt_ref_host.so is the reference's BVHRT-Core sources (its
-LBVH, ATRBVH and collapse kernels and its host classes) compiled from the
+LBVH, ATRBVH, TRBVH and collapse kernels and its host classes) compiled from the
 reference tree by oracle/build.py for a host execution model in which every
 CUDA thread is a fiber (oracle/ref_cpu/).  tests/golden/ref_host_golden.json
 records its outputs on the seeded cases (tests/golden/make_ref_host_golden.py).
@@ -37,13 +37,16 @@ def _oracle_run(rec):
     t, _, _ = O.build_lbvh(v, mn, mx, bits=rec["bits"], threads=0)
     if rec["optimizer"] == "atrbvh":
         t = O.atrbvh(t, rec["treelet"], rec["iterations"], threads=0)
+    elif rec["optimizer"] == "trbvh":
+        t = O.trbvh(t, rec["treelet"], rec["iterations"], threads=0)
     return v, mn, mx, t
 
 
 def test_oracle_matches_reference_records():
-    """Morton keys, LBVH (30- and 63-bit), ATRBVH (treelet 3-20) and collapse
-    of the oracle equal the reference's own outputs on every recorded case,
-    multi-block inputs of up to 65,536 triangles included."""
+    """Morton keys, LBVH (30- and 63-bit), ATRBVH (treelet 3-20), TRBVH
+    (treelet 7, 1-3 iterations) and collapse of the oracle equal the
+    reference's own outputs on every recorded case, multi-block inputs of up to
+    65,536 triangles included."""
     assert len(GOLD["records"]) >= 100
     for rec in GOLD["records"]:
         v, mn, mx, t = _oracle_run(rec)
@@ -69,7 +72,7 @@ def test_reference_library_reproduces_records():
         v = scene_case(rec["case"])
         mn, mx = O.scene_aabb(v)
         t, c, _ = O.ref_host_run(v, mn, mx, use64=rec["bits"] == 63,
-                                 optimizer={"lbvh": 0, "atrbvh": 1}[rec["optimizer"]], treelet=rec["treelet"],
+                                 optimizer={"lbvh": 0, "atrbvh": 1, "trbvh": 2}[rec["optimizer"]], treelet=rec["treelet"],
                                  iterations=rec["iterations"], collapse="collapsed" in rec)
         what = f"{rec['case']} {rec['optimizer']}({rec['treelet']},{rec['iterations']})"
         assert _tdig(t) == rec["tree"], what
