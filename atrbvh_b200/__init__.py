@@ -92,6 +92,11 @@ class ServerStats(C.Structure):
                 ("max_ms", C.c_double), ("overlap_fraction", C.c_double), ("busy_ms", C.c_double)]
 
 
+class CacheParams(C.Structure):
+    _fields_ = [("morton_bits", C.c_int32), ("optimizer", C.c_int32), ("treelet_size", C.c_int32),
+                ("iterations", C.c_int32), ("ci", C.c_float), ("ct", C.c_float), ("max_leaf", C.c_int32)]
+
+
 class TuneEntry(C.Structure):
     _fields_ = [("treelet", C.c_uint8), ("iterations", C.c_uint8), ("atr_warps", C.c_uint8),
                 ("sort_bits", C.c_uint8), ("build_ms", C.c_float), ("reference_ms", C.c_float),
@@ -166,6 +171,9 @@ _SIGS = [
     ("atr_compact_destroy", C.c_int, [_p]),
     ("atr_compact_view_get", C.c_int, [_p, C.POINTER(CompactView)]),
     ("atr_compact_download", C.c_int, [_p, _p, _p, _p, _p]),
+    ("atr_compact_serialize", C.c_int, [_p, _p, _p, C.c_uint64, C.POINTER(C.c_uint64)]),
+    ("atr_compact_deserialize", C.c_int, [_p, _p, C.c_uint64, C.POINTER(_p)]),
+    ("atr_cache_key", C.c_int, [_p, C.c_uint32, C.POINTER(CacheParams), C.POINTER(C.c_uint64)]),
     ("atr_trace", C.c_int, [_p, _p, _p, C.c_int64, C.c_int, _p]),
     ("atr_batch_create", C.c_int, [_p, _p, _p, C.c_uint32, _p, C.c_int, C.POINTER(_p)]),
     ("atr_batch_destroy", C.c_int, [_p]),
@@ -712,6 +720,26 @@ class CudaBVH:
         check(lib().atr_compact_download(self.ctx.handle, self.handle, _ptr(nodes), _ptr(woop), _ptr(tri)))
         return nodes, woop, tri
 
+    @classmethod
+    def from_image(cls, ctx: "Context", image: bytes) -> "CudaBVH":
+        """A traversal layout loaded from a cache image (atr_compact_deserialize)."""
+        buf = np.frombuffer(image, dtype=np.uint8)
+        h = C.c_void_p()
+        check(lib().atr_compact_deserialize(ctx.handle, _ptr(buf), len(buf), C.byref(h)))
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.handle = h
+        ctx._adopt(self)
+        return self
+
+    def serialize(self) -> bytes:
+        """The cache image in the reference's CudaBVH stream format."""
+        size = C.c_uint64()
+        check(lib().atr_compact_serialize(self.ctx.handle, self.handle, None, 0, C.byref(size)))
+        out = np.empty(size.value, np.uint8)
+        check(lib().atr_compact_serialize(self.ctx.handle, self.handle, _ptr(out), size.value, C.byref(size)))
+        return out.tobytes()
+
     def trace(self, rays_ptr: int, num_rays: int, results_ptr: int, any_hit: bool = False) -> None:
         """rays: device float4 pairs; results: device int4 per ray."""
         check(lib().atr_trace(self.ctx.handle, self.handle, C.c_void_p(rays_ptr), num_rays,
@@ -727,6 +755,44 @@ class CudaBVH:
             self.close()
         except Exception:
             pass
+
+
+def cache_key(vertices, morton_bits: int = 30, optimizer: int = 1, treelet: int = 9, iterations: int = 2,
+              ci: float = 1.2, ct: float = 1.0, max_leaf: int = 0) -> int:
+    """64-bit cache key of a scene and the build parameters (atr_cache_key)."""
+    v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3, 4)
+    p = CacheParams(morton_bits, optimizer, treelet, iterations, ci, ct, max_leaf)
+    k = C.c_uint64()
+    check(lib().atr_cache_key(_ptr(v), v.shape[0], C.byref(p), C.byref(k)))
+    return k.value
+
+
+class BVHCache:
+    """Directory of cache images named by cache key ("<key as 16 hex
+    digits>.dat"), as Renderer::getCudaBVH names its files
+    (gpu-ray-traversal/src/rt/cuda/Renderer.cpp:137-158): load() returns the
+    stored layout or None, store() writes one atomically."""
+
+    def __init__(self, directory):
+        from pathlib import Path
+        self.dir = Path(directory)
+        self.dir.mkdir(parents=True, exist_ok=True)
+
+    def path(self, key: int):
+        return self.dir / f"{key:016x}.dat"
+
+    def load(self, ctx: "Context", key: int) -> "CudaBVH | None":
+        p = self.path(key)
+        if not p.exists():
+            return None
+        return CudaBVH.from_image(ctx, p.read_bytes())
+
+    def store(self, key: int, bvh: "CudaBVH") -> None:
+        import os
+        p = self.path(key)
+        tmp = p.with_suffix(f".tmp{os.getpid()}")
+        tmp.write_bytes(bvh.serialize())
+        os.replace(tmp, p)
 
 
 def autotune(ctx: Context, min_class: int = 8, max_class: int = 21, sample_triangles: int = 1 << 21,

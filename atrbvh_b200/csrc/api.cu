@@ -52,7 +52,7 @@ int tree_alloc(atr_ctx* ctx, uint32_t n, atr_tree** out) {
 int atr_ctx::alloc(void** p, size_t bytes) {
     *p = nullptr;
     if (bytes == 0) return ATR_OK;
-    cudaError_t e = cudaMallocAsync(p, bytes, stream);
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, stream);
     if (e != cudaSuccess) {
         *p = nullptr;
         return atr::cuda_fail(e, "cudaMallocAsync", __FILE__, __LINE__);
@@ -106,17 +106,29 @@ int atr_ctx_create(int device, void* stream, atr_ctx** out) {
         if (e != cudaSuccess) { delete c; return atr::cuda_fail(e, "cudaStreamCreate", __FILE__, __LINE__); }
         c->own_stream = true;
     }
-    // Keep freed pool memory cached for the next build.
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    // The context's own stream-ordered pool; freed memory stays cached in it
+    // for the next build.
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaError_t e = cudaMemPoolCreate(&c->pool, &props);
+    if (e == cudaSuccess) {
         uint64_t thr = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
-    cudaError_t e = cudaMalloc(&c->d_error, sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        if (c->pool) cudaMemPoolDestroy(c->pool);
+        if (c->own_stream) cudaStreamDestroy(c->stream);
+        delete c;
+        return atr::cuda_fail(e, "cudaMemPoolCreate", __FILE__, __LINE__);
+    }
+    e = cudaMalloc(&c->d_error, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(c->d_error, 0, sizeof(uint32_t));
     if (e == cudaSuccess && atr::lbvh_prepare() != ATR_OK) e = cudaErrorInvalidValue;
     if (e == cudaSuccess && atr::atrbvh_prepare() != ATR_OK) e = cudaErrorInvalidValue;
     if (e != cudaSuccess) {
+        cudaMemPoolDestroy(c->pool);
         if (c->own_stream) cudaStreamDestroy(c->stream);
         delete c;
         return atr::cuda_fail(e, "cudaMalloc(error word)", __FILE__, __LINE__);
@@ -130,6 +142,9 @@ int atr_ctx_destroy(atr_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (auto& p : ctx->phases) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     cudaFree(ctx->d_error);
+    // Memory still allocated from the pool (objects the caller has not yet
+    // destroyed) stays valid; the pool goes once the last of it is freed.
+    cudaMemPoolDestroy(ctx->pool);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return ATR_OK;

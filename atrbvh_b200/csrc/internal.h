@@ -98,7 +98,11 @@ struct atr_ctx {
     std::vector<float> phase_ms;
     std::string phase_names;  // comma-separated names of the last atr_ctx_phase_times
 
-    // Stream-ordered allocation from the device's default pool.
+    // Stream-ordered allocation from this context's own pool.  A pool per
+    // context keeps contexts that run side by side on one device from
+    // waiting on each other: a pool shared by several streams may make an
+    // allocation on one stream wait for a free enqueued on another.
+    cudaMemPool_t pool = nullptr;
     int alloc(void** p, size_t bytes);
     void release(void* p);
     // Phase timing helpers (no-ops unless timing is enabled).

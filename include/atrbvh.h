@@ -248,6 +248,33 @@ int atr_compact_download(atr_ctx* ctx, const atr_compact* compact, int32_t* node
 int atr_trace(atr_ctx* ctx, const atr_compact* compact, const float* rays, int64_t num_rays,
               int any_hit, int32_t* results);
 
+/* ---- on-disk cache of the traversal layout ----------------------------------
+ * CudaBVH::serialize / CudaBVH(InputStream&)
+ * (gpu-ray-traversal/src/rt/cuda/CudaBVH.cpp:108-123; Buffer stream format
+ * framework/gpu/Buffer.cpp:331-362): the image is the layout as a
+ * little-endian S32 (BVHLayout_Compact2 = 5), then the node, Woop and
+ * triangle-index buffers, each a little-endian S64 byte count and the bytes,
+ * so files load in either implementation.  atr_compact_serialize with out =
+ * NULL only reports the size.  atr_compact_deserialize checks the sizes and
+ * every child reference before copying to the device, and recomputes the
+ * layout depth from the references.  atr_cache_key stands in for the file name
+ * hash of Renderer::getCudaBVH (gpu-ray-traversal/src/rt/cuda/Renderer.cpp:137-141:
+ * scene, platform and build-parameter hashes with the layout): a 64-bit hash of
+ * the vertex bytes, the layout and every build parameter below. */
+typedef struct atr_cache_params {
+    int32_t morton_bits;   /* 30 or 63 */
+    int32_t optimizer;     /* 0 none, 1 ATRBVH, 2 TRBVH */
+    int32_t treelet_size;
+    int32_t iterations;
+    float ci, ct;          /* collapse costs */
+    int32_t max_leaf;      /* collapse leaf cap, 0 = uncapped */
+} atr_cache_params;
+int atr_compact_serialize(atr_ctx* ctx, const atr_compact* compact, void* out, uint64_t capacity,
+                          uint64_t* size);
+int atr_compact_deserialize(atr_ctx* ctx, const void* image, uint64_t size, atr_compact** out);
+int atr_cache_key(const float* vertices, uint32_t num_triangles, const atr_cache_params* params,
+                  uint64_t* key);
+
 /* ---- segmented batch builds (no counterpart in the reference, which builds
  * one mesh per call: LBVHBuilder.cpp:21-130 and the optimisers per mesh) ------
  * Meshes laid end to end: mesh m owns triangles [tri_offsets[m],

@@ -93,8 +93,8 @@ def test_noalloc_refit_rejects_oversize_and_null(ctx):
 
 
 def _pool_used(device: int = 0) -> int:
-    """Bytes in use in the device's default stream-ordered pool (the pool the
-    library's allocating entry points draw from)."""
+    """Bytes in use in the device's default stream-ordered pool (where any
+    cudaMallocAsync without an explicit pool would draw from)."""
     from cuda.bindings import runtime as rt
     err, pool = rt.cudaDeviceGetDefaultMemPool(device)
     assert err == rt.cudaError_t.cudaSuccess
