@@ -92,6 +92,12 @@ class ServerStats(C.Structure):
                 ("max_ms", C.c_double), ("overlap_fraction", C.c_double), ("busy_ms", C.c_double)]
 
 
+class PlanParams(C.Structure):
+    _fields_ = [("morton_bits", C.c_int32), ("optimizer", C.c_int32), ("treelet_size", C.c_int32),
+                ("iterations", C.c_int32), ("ci", C.c_float), ("ct", C.c_float), ("max_leaf", C.c_int32),
+                ("flatten", C.c_int32)]
+
+
 class CacheParams(C.Structure):
     _fields_ = [("morton_bits", C.c_int32), ("optimizer", C.c_int32), ("treelet_size", C.c_int32),
                 ("iterations", C.c_int32), ("ci", C.c_float), ("ct", C.c_float), ("max_leaf", C.c_int32)]
@@ -171,6 +177,14 @@ _SIGS = [
     ("atr_compact_destroy", C.c_int, [_p]),
     ("atr_compact_view_get", C.c_int, [_p, C.POINTER(CompactView)]),
     ("atr_compact_download", C.c_int, [_p, _p, _p, _p, _p]),
+    ("atr_plan_create", C.c_int, [_p, _p, C.POINTER(PlanParams), C.POINTER(_p)]),
+    ("atr_plan_run", C.c_int, [_p, _p, C.c_int]),
+    ("atr_plan_tree", C.c_int, [_p, C.POINTER(_p)]),
+    ("atr_plan_collapsed", C.c_int, [_p, C.POINTER(_p)]),
+    ("atr_plan_compact", C.c_int, [_p, _p, C.POINTER(_p)]),
+    ("atr_plan_sah", C.c_int, [_p, _p, C.POINTER(C.c_float)]),
+    ("atr_plan_times", C.c_int, [_p, _p, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    ("atr_plan_destroy", C.c_int, [_p]),
     ("atr_compact_serialize", C.c_int, [_p, _p, _p, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("atr_compact_deserialize", C.c_int, [_p, _p, C.c_uint64, C.POINTER(_p)]),
     ("atr_cache_key", C.c_int, [_p, C.c_uint32, C.POINTER(CacheParams), C.POINTER(C.c_uint64)]),
@@ -748,6 +762,80 @@ class CudaBVH:
     def close(self) -> None:
         if getattr(self, "handle", None):
             lib().atr_compact_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Borrowed:
+    """A plan-owned tree, collapsed tree or layout: usable like the objects the
+    builders return, but freed with the plan (close() does nothing)."""
+
+    def close(self) -> None:
+        self.handle = None
+
+
+class BuildPlan:
+    """The steady-state build of one scene (atr_plan): LBVH -> optimiser ->
+    collapse (-> Compact2) into plan-owned outputs; run(graph=True) replays it
+    from a CUDA graph with one launch."""
+
+    def __init__(self, scene: SceneWrapper, morton_bits: int = 30, optimizer: int = 1, treelet: int = 9,
+                 iterations: int = 2, ci: float = 1.2, ct: float = 1.0, max_leaf: int = 0, flatten: bool = True):
+        self.ctx = scene.ctx
+        self.scene = scene
+        self.n = scene.n
+        p = PlanParams(morton_bits, optimizer, treelet, iterations, ci, ct, max_leaf, 1 if flatten else 0)
+        h = C.c_void_p()
+        check(lib().atr_plan_create(self.ctx.handle, scene.handle, C.byref(p), C.byref(h)))
+        self.handle = h
+        self.ctx._adopt(self)
+
+    def run(self, graph: bool = True) -> None:
+        check(lib().atr_plan_run(self.ctx.handle, self.handle, 1 if graph else 0))
+
+    def tree(self) -> BVHTree:
+        h = C.c_void_p()
+        check(lib().atr_plan_tree(self.handle, C.byref(h)))
+        t = BVHTree.__new__(BVHTree)
+        t.ctx, t.handle, t.n = self.ctx, h, self.n
+        t.close = _Borrowed.close.__get__(t)
+        return t
+
+    def collapsed(self) -> BVHCollapsedTree:
+        h = C.c_void_p()
+        check(lib().atr_plan_collapsed(self.handle, C.byref(h)))
+        c = BVHCollapsedTree.__new__(BVHCollapsedTree)
+        c.ctx, c.handle, c.n = self.ctx, h, self.n
+        c.close = _Borrowed.close.__get__(c)
+        return c
+
+    def compact(self) -> "CudaBVH":
+        h = C.c_void_p()
+        check(lib().atr_plan_compact(self.ctx.handle, self.handle, C.byref(h)))
+        b = CudaBVH.__new__(CudaBVH)
+        b.ctx, b.handle = self.ctx, h
+        b.close = _Borrowed.close.__get__(b)
+        return b
+
+    def sah(self) -> float:
+        s = C.c_float()
+        check(lib().atr_plan_sah(self.ctx.handle, self.handle, C.byref(s)))
+        return s.value
+
+    def times(self) -> tuple[float, float]:
+        """Device ms of the last run: (Morton through collapse, flatten)."""
+        a, b = C.c_float(), C.c_float()
+        check(lib().atr_plan_times(self.ctx.handle, self.handle, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            lib().atr_plan_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -199,6 +199,12 @@ int refit_arrays(atr_ctx* ctx, uint32_t n, const TreeOut& t, const float4* verts
 int batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* vertices, int on_device,
                      float* h_sah);
 
+// Collapsed-tree arrays for n triangles in one block, and the single-mesh
+// collapse into them (d_sah_parts, may be NULL: cost and area of the root).
+int collapsed_alloc(atr_ctx* ctx, uint32_t n, atr_collapsed** out);
+int collapse_into(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int max_leaf, atr_collapsed* c,
+                  float* d_sah_parts);
+
 // Single-mesh LBVH into an allocated tree (keeps the sort output).
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds,
                     int morton_bits, atr_tree* t);

@@ -39,6 +39,7 @@ typedef struct atr_tree atr_tree;
 typedef struct atr_collapsed atr_collapsed;
 typedef struct atr_compact atr_compact;
 typedef struct atr_batch atr_batch;
+typedef struct atr_plan atr_plan;
 
 /* Device-resident tree in the reference's structure-of-arrays layout
  * (BVHRT-Core/src/SoABVHTree.h:21-34): 2N-1 nodes, internal nodes [0, N-2],
@@ -247,6 +248,37 @@ int atr_compact_download(atr_ctx* ctx, const atr_compact* compact, int32_t* node
  * float bits of t, 0, 0) on the device. */
 int atr_trace(atr_ctx* ctx, const atr_compact* compact, const float* rays, int64_t num_rays,
               int any_hit, int32_t* results);
+
+/* ---- build plans: the steady-state single-mesh build as one CUDA graph -----
+ * The sequence Renderer::getCudaBVH runs per rebuild -- LBVHBuilder::BuildTree,
+ * an optimiser, BVHTreeCollapser::Collapse (BVHRT-Core/src/LBVHBuilder.cpp:60-97,
+ * AgglomerativeTreeletOptimizer.cpp:75-92, BVHTreeCollapser.cpp:21-93) and,
+ * with flatten, CudaBVH's Compact2 conversion -- into outputs the plan owns
+ * for one scene.  atr_plan_run enqueues the whole build; with use_graph the
+ * first run captures it into a CUDA graph and later runs replay it with one
+ * launch (captured again when the context's launch tuning changes).  A run
+ * reads the scene's current vertices and bounds, so a plan also rebuilds a
+ * deforming mesh.  The results are read through atr_plan_tree /
+ * atr_plan_collapsed / atr_plan_compact (the last reads the layout sizes and
+ * synchronises) and atr_plan_sah; atr_plan_times gives the device time of the
+ * last run's build (Morton through collapse) and flatten. */
+typedef struct atr_plan_params {
+    int32_t morton_bits;   /* 30 or 63 */
+    int32_t optimizer;     /* 0 none, 1 ATRBVH, 2 TRBVH */
+    int32_t treelet_size;
+    int32_t iterations;
+    float ci, ct;
+    int32_t max_leaf;      /* collapse leaf cap, 0 = uncapped (the reference) */
+    int32_t flatten;       /* also build the Compact2 layout */
+} atr_plan_params;
+int atr_plan_create(atr_ctx* ctx, const atr_scene* scene, const atr_plan_params* params, atr_plan** out);
+int atr_plan_run(atr_ctx* ctx, atr_plan* plan, int use_graph);
+int atr_plan_tree(const atr_plan* plan, const atr_tree** tree);
+int atr_plan_collapsed(const atr_plan* plan, const atr_collapsed** collapsed);
+int atr_plan_compact(atr_ctx* ctx, atr_plan* plan, const atr_compact** compact);
+int atr_plan_sah(atr_ctx* ctx, atr_plan* plan, float* sah);
+int atr_plan_times(atr_ctx* ctx, atr_plan* plan, float* build_ms, float* flatten_ms);
+int atr_plan_destroy(atr_plan* plan);
 
 /* ---- on-disk cache of the traversal layout ----------------------------------
  * CudaBVH::serialize / CudaBVH(InputStream&)
