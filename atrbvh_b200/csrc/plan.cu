@@ -53,7 +53,8 @@ int plan_enqueue(atr_ctx* ctx, atr_plan* P) {
     const atr_plan_params& p = P->p;
     atr_tree* t = P->tree;
     const uint32_t n = t->n;
-    ATR_CUDA(cudaEventRecord(P->ev[0], ctx->stream));
+    // External records, so that a captured graph records them when it runs.
+    ATR_CUDA(cudaEventRecordWithFlags(P->ev[0], ctx->stream, cudaEventRecordExternal));
     ATR_TRY(lbvh_build_into(ctx, P->scene->verts, n, P->scene->d_bounds, p.morton_bits, t));
     if (p.optimizer == 1) {
         ATR_TRY(atr_optimize_atrbvh(ctx, t, p.treelet_size, p.iterations, p.ci, p.ct));
@@ -69,7 +70,7 @@ int plan_enqueue(atr_ctx* ctx, atr_plan* P) {
     t->sorted_keys = nullptr;
     t->sorted_idx = nullptr;
     ATR_TRY(collapse_into(ctx, t, p.ci, p.ct, p.max_leaf, P->col, P->d_sah));
-    ATR_CUDA(cudaEventRecord(P->ev[1], ctx->stream));
+    ATR_CUDA(cudaEventRecordWithFlags(P->ev[1], ctx->stream, cudaEventRecordExternal));
     if (p.flatten) {
         const Segs segs{nullptr, nullptr, 1u, n};
         const atr_collapsed* c = P->col;
@@ -77,7 +78,7 @@ int plan_enqueue(atr_ctx* ctx, atr_plan* P) {
         ATR_TRY(flatten_segs(ctx, segs, co, P->scene->verts, P->cp->nodes, P->cp->woop, P->cp->tri_index,
                              P->d_sizes));
     }
-    ATR_CUDA(cudaEventRecord(P->ev[2], ctx->stream));
+    ATR_CUDA(cudaEventRecordWithFlags(P->ev[2], ctx->stream, cudaEventRecordExternal));
     return ATR_OK;
 }
 

@@ -347,14 +347,16 @@ def run_ours(args, world, rank, local):
     # Each step: atr_scene_create from pinned host vertices with the host scene
     # box (as the reference's SceneWrapper takes it) -> atr_build_lbvh ->
     # atr_optimize_atrbvh -> atr_collapse with the SAH read back to the host.
-    # Two steps are in flight, on two library contexts (streams) driven by two
-    # host threads, so one step's upload overlaps the other's kernels.
+    # Several steps are in flight (--e2e-inflight, default 4), each on its own
+    # library context (stream) driven by its own host thread, so uploads overlap
+    # other steps' kernels and the host link stays busy.
     pinned = torch.from_numpy(v.reshape(-1)).pin_memory().numpy().reshape(v.shape)
     bmin_h, bmax_h = ab.scene_bounds(pinned)  # input preparation, outside the timed region
     e2e = None
     if not args.no_e2e:
-        ctxs = [ctx, ab.Context(local)]
-        sahs: list[list[float]] = [[], []]
+        inflight = max(1, args.e2e_inflight)
+        ctxs = [ctx] + [ab.Context(local) for _ in range(inflight - 1)]
+        sahs: list[list[float]] = [[] for _ in range(inflight)]
 
         def e2e_step(c: "ab.Context", k: int) -> None:
             sc = ab.SceneWrapper(c, pinned, bmin_h, bmax_h)
@@ -367,7 +369,7 @@ def run_ours(args, world, rank, local):
             sc.close()
 
         def e2e_run(total: int) -> float:
-            counts = [(total + 1) // 2, total // 2]
+            counts = [total // inflight + (1 if k < total % inflight else 0) for k in range(inflight)]
             errors: list[BaseException] = []
 
             def worker(k: int) -> None:
@@ -380,7 +382,7 @@ def run_ours(args, world, rank, local):
             barrier(world)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            ths = [threading.Thread(target=worker, args=(k,)) for k in range(2)]
+            ths = [threading.Thread(target=worker, args=(k,)) for k in range(inflight)]
             for th in ths:
                 th.start()
             for th in ths:
@@ -390,18 +392,20 @@ def run_ours(args, world, rank, local):
                 raise errors[0]
             return dt
 
-        e2e_run(max(2, args.warmup))
-        sahs = [[], []]
+        e2e_run(max(inflight, args.warmup))
+        for k in range(inflight):
+            sahs[k].clear()
         e2e_dt = max_over_ranks(e2e_run(args.steps), world)
-        got = {np.float32(x) for k in range(2) for x in sahs[k]}
+        got = {np.float32(x) for k in range(inflight) for x in sahs[k]}
         e2e = {"value": world * n_tris * args.steps / e2e_dt / 1e6, "unit": "Mtri/s",
                "h2d_bytes_per_step": int(v.nbytes) + 24, "d2h_bytes_per_step": 8,
                "steps": args.steps, "seconds": e2e_dt,
                "path": "atr_scene_create(pinned host vertices, host scene box) -> atr_build_lbvh -> "
-                       "atr_optimize_atrbvh -> atr_collapse (SAH read back); two steps in flight on two "
-                       "contexts (streams), one host thread each",
+                       f"atr_optimize_atrbvh -> atr_collapse (SAH read back); {inflight} steps in flight on "
+                       f"{inflight} contexts (streams), one host thread each",
                "collapsed_sah_values": sorted(float(x) for x in got)}
-        ctxs[1].close()
+        for c in ctxs[1:]:
+            c.close()
 
     peaks = _read_peaks()
     roof = {}
@@ -820,6 +824,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-inflight", type=int, default=4, help="e2e: steps in flight (one context and thread each)")
     ap.add_argument("--no-batch", action="store_true", help="default line: skip the 4096-mesh batched-vs-plain keys")
     ap.add_argument("--no-serve", action="store_true", help="default line: skip the serving p50/p99 keys")
     ap.add_argument("--sustain-s", type=float, default=1.0,
