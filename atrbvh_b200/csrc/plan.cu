@@ -48,13 +48,20 @@ void plan_tuning_key(const atr_ctx* ctx, int key[5]) {
     key[4] = ctx->atr_quad_min;
 }
 
+// Marks a point of the run; while capturing, as an external record node so
+// that the graph records the event each time it runs.
+int plan_mark(atr_ctx* ctx, cudaEvent_t ev, bool capturing) {
+    ATR_CUDA(capturing ? cudaEventRecordWithFlags(ev, ctx->stream, cudaEventRecordExternal)
+                       : cudaEventRecord(ev, ctx->stream));
+    return ATR_OK;
+}
+
 // The whole build, enqueued on the context's stream into the plan's arrays.
-int plan_enqueue(atr_ctx* ctx, atr_plan* P) {
+int plan_enqueue(atr_ctx* ctx, atr_plan* P, bool capturing) {
     const atr_plan_params& p = P->p;
     atr_tree* t = P->tree;
     const uint32_t n = t->n;
-    // External records, so that a captured graph records them when it runs.
-    ATR_CUDA(cudaEventRecordWithFlags(P->ev[0], ctx->stream, cudaEventRecordExternal));
+    ATR_TRY(plan_mark(ctx, P->ev[0], capturing));
     ATR_TRY(lbvh_build_into(ctx, P->scene->verts, n, P->scene->d_bounds, p.morton_bits, t));
     if (p.optimizer == 1) {
         ATR_TRY(atr_optimize_atrbvh(ctx, t, p.treelet_size, p.iterations, p.ci, p.ct));
@@ -70,7 +77,7 @@ int plan_enqueue(atr_ctx* ctx, atr_plan* P) {
     t->sorted_keys = nullptr;
     t->sorted_idx = nullptr;
     ATR_TRY(collapse_into(ctx, t, p.ci, p.ct, p.max_leaf, P->col, P->d_sah));
-    ATR_CUDA(cudaEventRecordWithFlags(P->ev[1], ctx->stream, cudaEventRecordExternal));
+    ATR_TRY(plan_mark(ctx, P->ev[1], capturing));
     if (p.flatten) {
         const Segs segs{nullptr, nullptr, 1u, n};
         const atr_collapsed* c = P->col;
@@ -78,7 +85,7 @@ int plan_enqueue(atr_ctx* ctx, atr_plan* P) {
         ATR_TRY(flatten_segs(ctx, segs, co, P->scene->verts, P->cp->nodes, P->cp->woop, P->cp->tri_index,
                              P->d_sizes));
     }
-    ATR_CUDA(cudaEventRecordWithFlags(P->ev[2], ctx->stream, cudaEventRecordExternal));
+    ATR_TRY(plan_mark(ctx, P->ev[2], capturing));
     return ATR_OK;
 }
 
@@ -153,7 +160,7 @@ int atr_plan_run(atr_ctx* ctx, atr_plan* P, int use_graph) {
     P->sizes_read = false;
     if (!use_graph) {
         ctx->phase_begin("plan");
-        const int st = plan_enqueue(ctx, P);
+        const int st = plan_enqueue(ctx, P, false);
         ctx->phase_end();
         P->ran = st == ATR_OK;
         return st;
@@ -170,7 +177,7 @@ int atr_plan_run(atr_ctx* ctx, atr_plan* P, int use_graph) {
         const uint64_t l0 = ctx->launches;
         cudaGraph_t graph = nullptr;
         ATR_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        const int st = plan_enqueue(ctx, P);
+        const int st = plan_enqueue(ctx, P, true);
         const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
         ctx->timing = timing;
         if (st != ATR_OK) {
