@@ -184,6 +184,8 @@ _SIGS = [
     ("atr_plan_compact", C.c_int, [_p, _p, C.POINTER(_p)]),
     ("atr_plan_sah", C.c_int, [_p, _p, C.POINTER(C.c_float)]),
     ("atr_plan_times", C.c_int, [_p, _p, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    ("atr_plan_phase_times", C.c_int, [_p, _p, _p, C.c_int, C.POINTER(C.c_int)]),
+    ("atr_plan_phase_names", C.c_char_p, [_p]),
     ("atr_plan_destroy", C.c_int, [_p]),
     ("atr_compact_serialize", C.c_int, [_p, _p, _p, C.c_uint64, C.POINTER(C.c_uint64)]),
     ("atr_compact_deserialize", C.c_int, [_p, _p, C.c_uint64, C.POINTER(_p)]),
@@ -826,6 +828,14 @@ class BuildPlan:
         s = C.c_float()
         check(lib().atr_plan_sah(self.ctx.handle, self.handle, C.byref(s)))
         return s.value
+
+    def phase_times(self) -> list[tuple[str, float]]:
+        """(phase, device ms) of the last graph replay."""
+        ms = (C.c_float * 64)()
+        k = C.c_int()
+        check(lib().atr_plan_phase_times(self.ctx.handle, self.handle, ms, 64, C.byref(k)))
+        names = lib().atr_plan_phase_names(self.handle).decode().split(",")
+        return list(zip(names, ms[:k.value]))
 
     def times(self) -> tuple[float, float]:
         """Device ms of the last run: (Morton through collapse, flatten)."""

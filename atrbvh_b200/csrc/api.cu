@@ -70,13 +70,15 @@ void atr_ctx::phase_begin(const char* name) {
     ph.name = name;
     cudaEventCreate(&ph.a);
     cudaEventCreate(&ph.b);
-    cudaEventRecord(ph.a, stream);
+    if (capture_marks) cudaEventRecordWithFlags(ph.a, stream, cudaEventRecordExternal);
+    else cudaEventRecord(ph.a, stream);
     phases.push_back(ph);
 }
 
 void atr_ctx::phase_end() {
     if (!timing || phases.empty()) return;
-    cudaEventRecord(phases.back().b, stream);
+    if (capture_marks) cudaEventRecordWithFlags(phases.back().b, stream, cudaEventRecordExternal);
+    else cudaEventRecord(phases.back().b, stream);
 }
 
 extern "C" {

@@ -95,6 +95,9 @@ struct atr_ctx {
         cudaEvent_t a, b;
     };
     std::vector<Phase> phases;
+    // While a build plan captures its graph: phase marks become external
+    // record nodes, so each replay records them again.
+    bool capture_marks = false;
     std::vector<float> phase_ms;
     std::string phase_names;  // comma-separated names of the last atr_ctx_phase_times
 

@@ -15,6 +15,8 @@
 // and sizes are read on request.
 
 #include <cstring>
+#include <string>
+#include <vector>
 
 #include "common.cuh"
 #include "internal.h"
@@ -35,6 +37,11 @@ struct atr_plan {
     uint64_t graph_launches = 0;
     bool ran = false;
     bool sizes_read = false;
+    // Phase marks recorded inside the graph (morton, sort, build, atrbvh or
+    // trbvh, collapse, flatten), re-recorded by every replay.
+    std::vector<atr_ctx::Phase> phases;
+    std::string phase_names;
+    bool graph_ran = false;
 };
 
 namespace atr {
@@ -76,14 +83,20 @@ int plan_enqueue(atr_ctx* ctx, atr_plan* P, bool capturing) {
     ctx->release(t->sorted_idx);
     t->sorted_keys = nullptr;
     t->sorted_idx = nullptr;
-    ATR_TRY(collapse_into(ctx, t, p.ci, p.ct, p.max_leaf, P->col, P->d_sah));
+    ctx->phase_begin("collapse");
+    const int cst = collapse_into(ctx, t, p.ci, p.ct, p.max_leaf, P->col, P->d_sah);
+    ctx->phase_end();
+    ATR_TRY(cst);
     ATR_TRY(plan_mark(ctx, P->ev[1], capturing));
     if (p.flatten) {
         const Segs segs{nullptr, nullptr, 1u, n};
         const atr_collapsed* c = P->col;
         const CollapsedOut co{c->parent, c->left, c->right, c->data, c->count, c->bmin, c->bmax, c->tri_indices};
-        ATR_TRY(flatten_segs(ctx, segs, co, P->scene->verts, P->cp->nodes, P->cp->woop, P->cp->tri_index,
-                             P->d_sizes));
+        ctx->phase_begin("flatten");
+        const int fst = flatten_segs(ctx, segs, co, P->scene->verts, P->cp->nodes, P->cp->woop, P->cp->tri_index,
+                                     P->d_sizes);
+        ctx->phase_end();
+        ATR_TRY(fst);
     }
     ATR_TRY(plan_mark(ctx, P->ev[2], capturing));
     return ATR_OK;
@@ -172,14 +185,26 @@ int atr_plan_run(atr_ctx* ctx, atr_plan* P, int use_graph) {
             cudaGraphExecDestroy(P->graph);
             P->graph = nullptr;
         }
+        for (auto& ph : P->phases) {
+            cudaEventDestroy(ph.a);
+            cudaEventDestroy(ph.b);
+        }
+        P->phases.clear();
+        // The capture records its own phase marks (kept by the plan).
         const bool timing = ctx->timing;
-        ctx->timing = false;
+        std::vector<atr_ctx::Phase> outer;
+        outer.swap(ctx->phases);
+        ctx->timing = true;
+        ctx->capture_marks = true;
         const uint64_t l0 = ctx->launches;
         cudaGraph_t graph = nullptr;
-        ATR_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        const int st = plan_enqueue(ctx, P, true);
-        const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        cudaError_t be = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        const int st = be == cudaSuccess ? plan_enqueue(ctx, P, true) : ATR_OK;
+        const cudaError_t e = be == cudaSuccess ? cudaStreamEndCapture(ctx->stream, &graph) : be;
         ctx->timing = timing;
+        ctx->capture_marks = false;
+        P->phases.swap(ctx->phases);
+        ctx->phases.swap(outer);
         if (st != ATR_OK) {
             if (graph) cudaGraphDestroy(graph);
             return st;
@@ -200,8 +225,29 @@ int atr_plan_run(atr_ctx* ctx, atr_plan* P, int use_graph) {
     ctx->phase_end();
     ctx->launches += P->graph_launches;
     P->ran = true;
+    P->graph_ran = true;
     return ATR_OK;
 }
+
+int atr_plan_phase_times(atr_ctx* ctx, atr_plan* P, float* ms, int capacity, int* count) {
+    ATR_REQUIRE(ctx && P && count, ATR_ERR_INVALID_ARG, "atr_plan_phase_times: NULL argument");
+    ATR_REQUIRE(P->graph_ran, ATR_ERR_INVALID_ARG, "atr_plan_phase_times: no graph replay yet");
+    ATR_CUDA(cudaEventSynchronize(P->ev[2]));
+    int k = 0;
+    P->phase_names.clear();
+    for (auto& ph : P->phases) {
+        float t = 0.0f;
+        ATR_CUDA(cudaEventElapsedTime(&t, ph.a, ph.b));
+        if (ms && k < capacity) ms[k] = t;
+        if (!P->phase_names.empty()) P->phase_names += ",";
+        P->phase_names += ph.name;
+        ++k;
+    }
+    *count = k;
+    return ATR_OK;
+}
+
+const char* atr_plan_phase_names(const atr_plan* P) { return P ? P->phase_names.c_str() : ""; }
 
 int atr_plan_tree(const atr_plan* P, const atr_tree** tree) {
     ATR_REQUIRE(P && tree, ATR_ERR_INVALID_ARG, "atr_plan_tree: NULL argument");
@@ -254,6 +300,10 @@ int atr_plan_times(atr_ctx* ctx, atr_plan* P, float* build_ms, float* flatten_ms
 int atr_plan_destroy(atr_plan* P) {
     if (!P) return ATR_OK;
     if (P->graph) cudaGraphExecDestroy(P->graph);
+    for (auto& ph : P->phases) {
+        cudaEventDestroy(ph.a);
+        cudaEventDestroy(ph.b);
+    }
     for (cudaEvent_t e : P->ev)
         if (e) cudaEventDestroy(e);
     atr_tree_destroy(P->tree);

@@ -278,6 +278,11 @@ int atr_plan_collapsed(const atr_plan* plan, const atr_collapsed** collapsed);
 int atr_plan_compact(atr_ctx* ctx, atr_plan* plan, const atr_compact** compact);
 int atr_plan_sah(atr_ctx* ctx, atr_plan* plan, float* sah);
 int atr_plan_times(atr_ctx* ctx, atr_plan* plan, float* build_ms, float* flatten_ms);
+/* Device ms of each phase of the last graph replay (marks recorded inside the
+ * graph), and their comma-separated names, as atr_ctx_phase_times does for
+ * eager calls. */
+int atr_plan_phase_times(atr_ctx* ctx, atr_plan* plan, float* ms, int capacity, int* count);
+const char* atr_plan_phase_names(const atr_plan* plan);
 int atr_plan_destroy(atr_plan* plan);
 
 /* ---- on-disk cache of the traversal layout ----------------------------------
