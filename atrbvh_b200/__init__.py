@@ -206,6 +206,8 @@ _SIGS = [
     ("atr_batch_trace", C.c_int, [_p, _p, _p, C.c_int64, _p, _p, C.c_uint32, C.c_int, _p]),
     ("atr_batch_refit_mesh", C.c_int, [_p, _p, C.c_uint32, _p, C.c_int]),
     ("atr_gen_bounce_rays", C.c_int, [_p, _p, _p, _p, C.c_int64, C.c_uint64, _p]),
+    ("atr_gen_ao_rays", C.c_int, [_p, _p, _p, _p, C.c_int64, C.c_int64, C.c_int, C.c_float, C.c_uint32, _p]),
+    ("atr_sort_rays", C.c_int, [_p, _p, _p, C.c_int64, _p, _p, _p]),
     ("atr_gen_scene", C.c_int, [C.c_int, C.c_uint32, C.c_uint64, _p]),
     ("atr_gen_batch_sizes", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64, _p]),
     ("atr_gen_batch_scene", C.c_int, [C.c_uint32, _p, C.c_uint64, _p]),
@@ -853,6 +855,34 @@ class BuildPlan:
             self.close()
         except Exception:
             pass
+
+
+def ray_batches(num_input_rays: int, num_samples: int, max_batch: int = 1 << 20):
+    """Slices [lo, hi) of an input ray batch whose secondary rays fit in
+    max_batch rays, as RayGen::batching cuts them
+    (gpu-ray-traversal/src/rt/ray/RayGen.cpp:240-258; the benchmark's batches
+    hold 2^20 rays)."""
+    lo = 0
+    step = max(1, max_batch // num_samples)
+    while lo < num_input_rays:
+        hi = min(num_input_rays, lo + step)
+        yield lo, hi
+        lo = hi
+
+
+def gen_ao_rays(scene: SceneWrapper, rays_ptr: int, results_ptr: int, first: int, count: int, num_samples: int,
+                max_dist: float, seed: int, out_ptr: int) -> None:
+    """Ambient-occlusion rays for rays[first:first+count] (device arrays), see atr_gen_ao_rays."""
+    check(lib().atr_gen_ao_rays(scene.ctx.handle, scene.handle, C.c_void_p(rays_ptr), C.c_void_p(results_ptr),
+                                first, count, num_samples, max_dist, seed & 0xFFFFFFFF, C.c_void_p(out_ptr)))
+
+
+def sort_rays(ctx: "Context", rays_ptr: int, num_rays: int, out_rays_ptr: int, slot_to_id_ptr: int | None = None,
+              out_slot_to_id_ptr: int | None = None, out_id_to_slot_ptr: int | None = None) -> None:
+    """Morton sort of a ray batch on the device (atr_sort_rays)."""
+    p = lambda x: None if x is None else C.c_void_p(x)  # noqa: E731
+    check(lib().atr_sort_rays(ctx.handle, C.c_void_p(rays_ptr), p(slot_to_id_ptr), num_rays, C.c_void_p(out_rays_ptr),
+                              p(out_slot_to_id_ptr), p(out_id_to_slot_ptr)))
 
 
 def cache_key(vertices, morton_bits: int = 30, optimizer: int = 1, treelet: int = 9, iterations: int = 2,

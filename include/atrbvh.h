@@ -484,6 +484,26 @@ int atr_server_destroy(atr_server* server);
 int atr_gen_bounce_rays(atr_ctx* ctx, const atr_scene* scene, const float* rays,
                         const int32_t* results, int64_t num_rays, uint64_t seed, float* out_rays);
 
+/* Ambient-occlusion rays, RayGen::ao / rayGenAOKernel
+ * (gpu-ray-traversal/src/rt/ray/RayGen.cpp:120-150, RayGenKernels.cu:114-223):
+ * num_samples rays per input ray of rays[first, first + count) (device
+ * arrays; results as atr_trace writes them), written to out_rays[0,
+ * count * num_samples) in input order, sample-minor.  The range is the
+ * reference's batching of secondary rays (firstInputSlot / numInputRays):
+ * a large primary batch is processed in slices that bound the output.  Misses
+ * give rays with tmax = -1.  seed is RayGenAOInput::randomSeed. */
+int atr_gen_ao_rays(atr_ctx* ctx, const atr_scene* scene, const float* rays, const int32_t* results,
+                    int64_t first, int64_t count, int num_samples, float max_dist, uint32_t seed,
+                    float* out_rays);
+/* RayBuffer::mortonSort (gpu-ray-traversal/src/rt/ray/RayBuffer.cpp:103-160), on
+ * the device: rays sorted by the 192-bit Morton key of origin (in the box of
+ * the origins and end points) and direction, into out_rays (must not alias
+ * rays); slot_to_id (may be NULL = identity) is carried to out_slot_to_id,
+ * and out_id_to_slot is its inverse (either output may be NULL).  Equal keys
+ * keep their input order. */
+int atr_sort_rays(atr_ctx* ctx, const float* rays, const int32_t* slot_to_id, int64_t num_rays,
+                  float* out_rays, int32_t* out_slot_to_id, int32_t* out_id_to_slot);
+
 /* ---- synthetic workloads (host memory; deterministic in seed) ---------- */
 int atr_gen_scene(int kind, uint32_t num_triangles, uint64_t seed, float* vertices);
 int atr_gen_batch_sizes(uint32_t count, uint32_t min_tris, uint32_t max_tris, uint64_t seed,

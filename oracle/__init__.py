@@ -62,6 +62,8 @@ def lib() -> C.CDLL:
         L.orc_box_area.restype = C.c_float
         L.orc_union_area.argtypes = [_p, _p, _p, _p]
         L.orc_union_area.restype = C.c_float
+        L.orc_gen_ao_rays.argtypes = [_p, _p, _p, C.c_int64, C.c_int64, C.c_int, C.c_float, C.c_uint32, _p]
+        L.orc_sort_rays.argtypes = [_p, C.c_int64, _p, _p]
         L.orc_gen_scene.argtypes = [C.c_int, C.c_uint32, C.c_uint64, _p]
         L.orc_gen_rays_pinhole.argtypes = [C.c_uint32, C.c_uint32, _p, C.c_float, _p]
         L.orc_gen_rays_random.argtypes = [C.c_uint64, C.c_uint64, _p, _p, _p]
@@ -395,3 +397,24 @@ def ref_host_morton(v: np.ndarray, bbmin, bbmax, bits: int = 30):
         k = np.zeros(n, np.uint64)
         ref_host_lib().ref_host_morton(_ptr(v), n, _ptr(mn), _ptr(mx), 1, None, _ptr(k), _ptr(idx))
     return k, idx
+
+
+def gen_ao_rays(v: np.ndarray, rays: np.ndarray, results: np.ndarray, samples: int, max_dist: float, seed: int,
+                first: int = 0, count: int | None = None) -> np.ndarray:
+    """Ambient-occlusion rays (count * samples, 2, 4) from the hits of rays[first:first+count]."""
+    v = np.ascontiguousarray(v, np.float32)
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    results = np.ascontiguousarray(results, np.int32).reshape(-1, 4)
+    count = len(rays) - first if count is None else count
+    out = np.empty((count * samples, 2, 4), np.float32)
+    lib().orc_gen_ao_rays(_ptr(v), _ptr(rays), _ptr(results), first, count, samples, max_dist, seed, _ptr(out))
+    return out
+
+
+def sort_rays(rays: np.ndarray):
+    """(perm, box): perm[j] = old slot of the ray at sorted position j."""
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    perm = np.empty(len(rays), np.uint32)
+    box = np.empty(6, np.float32)
+    lib().orc_sort_rays(_ptr(rays), len(rays), _ptr(perm), _ptr(box))
+    return perm, box

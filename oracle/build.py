@@ -1,8 +1,9 @@
 """ORACLE -- test infrastructure only.
 
 Builds the checkers:
-  oracle/liboracle.so                CPU restatement (atr_oracle.cpp) and the
-                                     seeded workload generators
+  oracle/liboracle.so                CPU restatement (atr_oracle.cpp,
+                                     raygen_oracle.cpp) and the seeded
+                                     workload generators
                                      (workload_oracle.cpp), g++ -O2
                                      -ffp-contract=off -fopenmp.
   oracle/_ref/libbvhrt_ref_host.so   the reference's own BVHRT-Core sources
@@ -42,7 +43,7 @@ def _run(cmd: list[str], **kw) -> None:
 
 def build_oracle() -> Path:
     out = HERE / "liboracle.so"
-    srcs = [HERE / "atr_oracle.cpp", HERE / "workload_oracle.cpp"]
+    srcs = [HERE / "atr_oracle.cpp", HERE / "workload_oracle.cpp", HERE / "raygen_oracle.cpp"]
     if out.exists() and out.stat().st_mtime >= max(p.stat().st_mtime for p in srcs):
         return out
     _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC",
