@@ -89,7 +89,8 @@ class ServerStats(C.Structure):
                 ("rays_traced", C.c_uint64), ("lane_batches", C.c_uint64), ("max_batch_requests_seen", C.c_uint32),
                 ("max_lanes_busy", C.c_uint32), ("resident_meshes", C.c_uint32), ("resident_bytes", C.c_uint64),
                 ("peak_bytes", C.c_uint64), ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
-                ("max_ms", C.c_double), ("overlap_fraction", C.c_double), ("busy_ms", C.c_double)]
+                ("max_ms", C.c_double), ("overlap_fraction", C.c_double), ("busy_ms", C.c_double),
+                ("host_copy_ms", C.c_double), ("lane_batch_ms", C.c_double)]
 
 
 class PlanParams(C.Structure):
@@ -354,6 +355,16 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+def pinned_like(a: np.ndarray) -> np.ndarray:
+    """A page-locked host copy of a (through torch's pinned allocator), for
+    request buffers that the server and the upload paths copy directly."""
+    import torch
+    t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+    out = t.numpy().view(a.dtype).reshape(a.shape)
+    out[...] = a
+    return out  # the view's base is the tensor, which keeps the pinned storage alive
 
 
 def scene_bounds(vertices) -> tuple[np.ndarray, np.ndarray]:

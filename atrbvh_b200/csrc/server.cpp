@@ -122,6 +122,19 @@ int grow_pinned(void** p, size_t* cap, size_t need) {
     return ATR_OK;
 }
 
+// True for page-locked host memory (cudaHostAlloc'd or cudaHostRegister'ed):
+// such request buffers are copied to and from the device directly, without
+// the host staging copy.
+bool is_pinned(const void* p) {
+    if (!p) return false;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 }  // namespace
 
 struct atr_server {
@@ -303,19 +316,27 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
     std::vector<Request*> builds, refits;
     for (Request* r : work) (r->req.kind == ATR_REQ_BUILD ? builds : refits).push_back(r);
 
-    // Rays of every request into one pinned buffer, in `work` order.
+    const Clock::time_point t_start = Clock::now();
+    // Rays of every request into one device queue, in `work` order: a request
+    // whose buffer is page-locked is copied from it directly, the others
+    // through this lane's pinned staging buffer.
     uint64_t total_rays = 0;
     for (Request* r : work) total_rays += r->req.num_rays;
     ATR_TRY(grow_pinned(&L.h_rays, &L.h_rays_cap, std::max<uint64_t>(total_rays, 1) * 32));
     ATR_TRY(grow_pinned(&L.h_res, &L.h_res_cap, std::max<uint64_t>(total_rays, 1) * 16));
     std::vector<uint64_t> ray_at(work.size() + 1, 0);
+    std::vector<char> rays_pinned(work.size(), 0), res_pinned(work.size(), 0), verts_pinned(work.size(), 0);
     std::vector<CopyJob> jobs;
     for (size_t i = 0; i < work.size(); ++i) {
         ray_at[i + 1] = ray_at[i] + work[i]->req.num_rays;
-        if (work[i]->req.num_rays)
+        if (!work[i]->req.num_rays) continue;
+        rays_pinned[i] = is_pinned(work[i]->req.rays);
+        res_pinned[i] = is_pinned(work[i]->req.results);
+        if (!rays_pinned[i])
             jobs.push_back({static_cast<char*>(L.h_rays) + ray_at[i] * 32, work[i]->req.rays,
                             (size_t)work[i]->req.num_rays * 32});
     }
+    for (size_t i = 0; i < work.size(); ++i) verts_pinned[i] = is_pinned(work[i]->req.vertices);
     // Refit vertices go to their own staging buffer (copied before any launch).
     uint64_t refit_tris = 0;
     std::vector<size_t> refit_at(work.size(), 0);
@@ -333,7 +354,7 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
     {
         std::lock_guard<std::mutex> lock(mu);
         for (size_t i = 0; i < work.size(); ++i) {
-            if (work[i]->req.kind != ATR_REQ_REFIT) continue;
+            if (work[i]->req.kind != ATR_REQ_REFIT || verts_pinned[i]) continue;
             auto f = resident.find(work[i]->req.mesh_id);
             if (f == resident.end()) continue;
             jobs.push_back({static_cast<char*>(L.h_rverts) + refit_at[i] * 48, work[i]->req.vertices,
@@ -341,13 +362,21 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
         }
     }
     par_copy(jobs);
+    double copy_ms = ms_between(t_start, Clock::now());
     void* d_rays = nullptr;
     void* d_res = nullptr;
     if (total_rays) {
         ATR_TRY(ctx->alloc(&d_rays, total_rays * 32));
         int s = ctx->alloc(&d_res, total_rays * 16);
         if (s != ATR_OK) { ctx->release(d_rays); return s; }
-        cudaError_t e = cudaMemcpyAsync(d_rays, L.h_rays, total_rays * 32, cudaMemcpyHostToDevice, ctx->stream);
+        cudaError_t e = cudaSuccess;
+        for (size_t i = 0; i < work.size() && e == cudaSuccess; ++i) {
+            if (!work[i]->req.num_rays) continue;
+            const void* src = rays_pinned[i] ? work[i]->req.rays
+                                             : static_cast<const void*>(static_cast<char*>(L.h_rays) + ray_at[i] * 32);
+            e = cudaMemcpyAsync(static_cast<char*>(d_rays) + ray_at[i] * 32, src, (size_t)work[i]->req.num_rays * 32,
+                                cudaMemcpyHostToDevice, ctx->stream);
+        }
         if (e != cudaSuccess) {
             ctx->release(d_rays);
             ctx->release(d_res);
@@ -376,16 +405,45 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
         std::vector<uint32_t> off(builds.size() + 1, 0);
         std::vector<uint8_t> ts(builds.size()), it(builds.size());
         std::vector<CopyJob> vjobs;
+        bool all_pinned = true;
         for (size_t m = 0; m < builds.size(); ++m) {
             const uint32_t n = builds[m]->req.num_triangles;
-            vjobs.push_back({static_cast<char*>(L.h_verts) + (size_t)off[m] * 48, builds[m]->req.vertices, (size_t)n * 48});
+            if (!verts_pinned[m])
+                vjobs.push_back({static_cast<char*>(L.h_verts) + (size_t)off[m] * 48, builds[m]->req.vertices,
+                                 (size_t)n * 48});
+            all_pinned = all_pinned && verts_pinned[m];
             off[m + 1] = off[m] + n;
             params_for(n, &ts[m], &it[m]);
         }
+        const Clock::time_point tv = Clock::now();
         par_copy(vjobs);
+        copy_ms += ms_between(tv, Clock::now());
         atr_batch* b = nullptr;
-        s = atr_batch_create(ctx, static_cast<const float*>(L.h_verts), off.data(), (uint32_t)builds.size(), nullptr,
-                             0, &b);
+        if (all_pinned && builds.size() == 1) {
+            s = atr_batch_create(ctx, static_cast<const float*>(builds[0]->req.vertices), off.data(), 1u, nullptr, 0,
+                                 &b);
+        } else if (all_pinned || vjobs.size() < builds.size()) {
+            // Gather on the device: each mesh from its own pinned buffer or
+            // from the staging buffer, then the batch copies the span.
+            void* d_verts = nullptr;
+            s = ctx->alloc(&d_verts, (size_t)tris * 48);
+            cudaError_t e = cudaSuccess;
+            for (size_t m = 0; s == ATR_OK && m < builds.size() && e == cudaSuccess; ++m) {
+                const void* src = verts_pinned[m] ? builds[m]->req.vertices
+                                                  : static_cast<const void*>(static_cast<char*>(L.h_verts) +
+                                                                             (size_t)off[m] * 48);
+                e = cudaMemcpyAsync(static_cast<char*>(d_verts) + (size_t)off[m] * 48, src,
+                                    (size_t)builds[m]->req.num_triangles * 48, cudaMemcpyHostToDevice, ctx->stream);
+            }
+            if (s == ATR_OK && e != cudaSuccess) s = atr::cuda_fail(e, "cudaMemcpyAsync(vertices)", __FILE__, __LINE__);
+            if (s == ATR_OK)
+                s = atr_batch_create(ctx, static_cast<const float*>(d_verts), off.data(), (uint32_t)builds.size(),
+                                     nullptr, 1, &b);
+            ctx->release(d_verts);
+        } else {
+            s = atr_batch_create(ctx, static_cast<const float*>(L.h_verts), off.data(), (uint32_t)builds.size(),
+                                 nullptr, 0, &b);
+        }
         if (s == ATR_OK) s = atr_batch_set_params(ctx, b, ts.data(), it.data());
         if (s == ATR_OK) s = atr_batch_build(ctx, b, 1, cfg.treelet_size, cfg.iterations, 1.2f, 1.0f, 0);
         std::vector<float> sah(builds.size(), 0.0f);
@@ -431,9 +489,10 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
         }
         float sah = 0.0f;
         const size_t p = work_pos(r);
-        int s = atr::batch_refit_mesh(ctx, res.rec->batch, res.index,
-                                      reinterpret_cast<const float*>(static_cast<char*>(L.h_rverts) + refit_at[p] * 48),
-                                      0, &sah);
+        const float* src = verts_pinned[p]
+                               ? r->req.vertices
+                               : reinterpret_cast<const float*>(static_cast<char*>(L.h_rverts) + refit_at[p] * 48);
+        int s = atr::batch_refit_mesh(ctx, res.rec->batch, res.index, src, 0, &sah);
         if (s == ATR_OK && r->req.num_rays) {
             const uint32_t roff[2] = {0, r->req.num_rays};
             const uint32_t gm[1] = {res.index};
@@ -444,20 +503,32 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
         if (s != ATR_OK) { r->status = s; set_msg(r, s); }
     }
 
-    // 3. Results back to host memory.
-    if (total_rays) {
-        cudaError_t e = cudaMemcpyAsync(L.h_res, d_res, total_rays * 16, cudaMemcpyDeviceToHost, ctx->stream);
+    // 3. Results back to host memory: straight into page-locked result
+    // buffers, through the staging buffer for the others.
+    for (size_t i = 0; i < work.size(); ++i) {
+        if (!work[i]->req.num_rays) continue;
+        void* dst = res_pinned[i] ? static_cast<void*>(work[i]->req.results)
+                                  : static_cast<void*>(static_cast<char*>(L.h_res) + ray_at[i] * 16);
+        cudaError_t e = cudaMemcpyAsync(dst, static_cast<char*>(d_res) + ray_at[i] * 16,
+                                        (size_t)work[i]->req.num_rays * 16, cudaMemcpyDeviceToHost, ctx->stream);
         if (e != cudaSuccess) { release_rays(); return atr::cuda_fail(e, "cudaMemcpyAsync(results)", __FILE__, __LINE__); }
     }
     const int s = atr_ctx_synchronize(ctx);
     release_rays();
+    const Clock::time_point t_done = Clock::now();
     ATR_TRY(s);
     std::vector<CopyJob> out;
     for (size_t i = 0; i < work.size(); ++i)
-        if (work[i]->req.num_rays && work[i]->status == ATR_OK)
+        if (work[i]->req.num_rays && work[i]->status == ATR_OK && !res_pinned[i])
             out.push_back({work[i]->req.results, static_cast<char*>(L.h_res) + ray_at[i] * 16,
                            (size_t)work[i]->req.num_rays * 16});
     par_copy(out);
+    const double out_ms = ms_between(t_done, Clock::now());
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        st.host_copy_ms += copy_ms + out_ms;
+        st.lane_batch_ms += ms_between(t_start, Clock::now());
+    }
     return ATR_OK;
 }
 

@@ -623,11 +623,15 @@ SERVE_WORKLOAD = ("serving loop: Poisson arrivals; each request builds a mesh (l
                   "64k-1M random rays; 120 GB device-memory budget")
 
 
-def measure_serve(*, rates, requests: int, pool_size: int, lanes: int, device: int = 0) -> list[dict]:
+def measure_serve(*, rates, requests: int, pool_size: int, lanes: int, device: int = 0,
+                  pinned: bool = True) -> list[dict]:
     """The serving loop under Poisson arrivals: p50/p99 request latency beside
-    build and trace throughput, one record per arrival rate."""
+    build and trace throughput, one record per arrival rate.  With pinned, the
+    requests' vertex, ray and result buffers are page-locked host memory,
+    which the server copies to and from the device directly."""
     import atrbvh_b200 as ab
     rng = np.random.default_rng(0)
+    host = ab.pinned_like if pinned else (lambda a: a)
     pool = []
     for k in range(pool_size):
         n = int(np.exp(rng.uniform(np.log(1000), np.log(2_000_000))))
@@ -637,13 +641,14 @@ def measure_serve(*, rates, requests: int, pool_size: int, lanes: int, device: i
         p = v[:, :, :3].reshape(-1, 3)
         nr = int(np.exp(rng.uniform(np.log(65536), np.log(1 << 20))))
         rays = ab.gen_rays_random(nr, p.min(0), p.max(0), seed=2000 + k)
-        pool.append((v, j, rays))
+        pool.append((host(v), host(j), host(rays)))
     max_rays = max(len(r) for _, _, r in pool)
+    n_outs = 2 * lanes * 32 + 8
+    outs = [host(np.zeros((max_rays, 4), np.int32)) for _ in range(n_outs)]
     rows = []
     for rate in rates:
         srv = ab.Server(device=device, hbm_budget=120 << 30, lanes=lanes, max_batch_requests=32,
                         max_batch_triangles=1 << 25)
-        outs = [np.empty((max_rays, 4), np.int32) for _ in range(2 * lanes * 32 + 8)]
         arrivals = np.cumsum(rng.exponential(1.0 / rate, requests))
         resident: list[int] = []
         tickets = []
@@ -681,7 +686,9 @@ def measure_serve(*, rates, requests: int, pool_size: int, lanes: int, device: i
                      "build_mtri_per_s": st["triangles_built"] / wall / 1e6,
                      "trace_mrays_per_s": st["rays_traced"] / wall / 1e6, "wall_s": wall,
                      "lane_batches": st["lane_batches"], "max_batch_requests_seen": st["max_batch_requests_seen"],
-                     "overlap_fraction": st["overlap_fraction"], "peak_gb": st["peak_bytes"] / 1e9})
+                     "overlap_fraction": st["overlap_fraction"], "peak_gb": st["peak_bytes"] / 1e9,
+                     "host_copy_ms": st["host_copy_ms"], "lane_batch_ms": st["lane_batch_ms"],
+                     "pinned_request_buffers": pinned})
     return rows
 
 

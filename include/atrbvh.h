@@ -465,8 +465,13 @@ typedef struct atr_server_stats {
     double p50_ms, p99_ms, mean_ms, max_ms;
     double overlap_fraction;       /* share of busy time with >= 2 lanes busy */
     double busy_ms;                /* time with >= 1 lane busy */
+    double host_copy_ms;           /* lane time in host staging copies (pageable buffers) */
+    double lane_batch_ms;          /* lane time from a batch's first copy to its results */
 } atr_server_stats;
 
+/* Request buffers (vertices, rays, results) in page-locked host memory
+ * (cudaHostAlloc or cudaHostRegister) are copied to and from the device
+ * directly; pageable ones go through a lane's pinned staging buffer. */
 int atr_server_create(int device, const atr_server_config* config, atr_server** out);
 int atr_server_submit(atr_server* server, const atr_request* request, uint64_t* ticket);
 /* Blocks until the request is done; each ticket can be waited on once, by one

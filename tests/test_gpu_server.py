@@ -141,3 +141,30 @@ def test_server_rejects_bad_requests():
     r = srv.wait(srv.submit(ab.REQ_REFIT, 123, v[:10]))
     assert r["status"] == ab.ERR_NOT_RESIDENT
     srv.close()
+
+
+def test_server_pinned_request_buffers_equal_pageable():
+    """Requests whose vertex, ray and result buffers are page-locked (copied to
+    and from the device directly, no staging copy), mixed in one lane batch
+    with pageable ones, give the same results as pageable requests alone."""
+    reqs = _workload(1)
+    pinned = []
+    for k, (kind, mid, v, rays) in enumerate(reqs):
+        if k % 2 == 0:
+            v, rays = ab.pinned_like(v), ab.pinned_like(rays)
+        pinned.append((kind, mid, v, rays))
+    mix = ab.Server(lanes=2, max_batch_requests=8)
+    outs = [np.full((len(r[3]), 4), -7, np.int32) for r in pinned]
+    outs = [ab.pinned_like(o) if k % 3 == 0 else o for k, o in enumerate(outs)]
+    tickets = [mix.submit(kind, mid, v, rays, out) for (kind, mid, v, rays), out in zip(pinned, outs)]
+    res_mix = [mix.wait(t) for t in tickets]
+    st = mix.stats()
+    mix.close()
+    alone = ab.Server(lanes=1, max_batch_requests=1)
+    outs_alone, res_alone = _run(alone, reqs, together=False)
+    alone.close()
+    assert all(r["status"] == 0 for r in res_mix), [r["error"] for r in res_mix if r["status"]]
+    assert st["host_copy_ms"] >= 0 and st["lane_batch_ms"] > 0
+    for k in range(len(reqs)):
+        assert np.array_equal(outs[k], outs_alone[k]), f"request {k}"
+        assert np.float32(res_mix[k]["sah"]) == np.float32(res_alone[k]["sah"]), k
