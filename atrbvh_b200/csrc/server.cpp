@@ -112,11 +112,11 @@ void par_copy(const std::vector<CopyJob>& jobs) {
 
 int grow_pinned(void** p, size_t* cap, size_t need) {
     if (need <= *cap) return ATR_OK;
+    // Grow by doubling: pinning host memory is slow, so reallocations must be rare.
+    const size_t c = std::max({need, (size_t)1 << 20, 2 * *cap});
     if (*p) cudaFreeHost(*p);
     *p = nullptr;
     *cap = 0;
-    size_t c = std::max(need, (size_t)1 << 20);
-    c += c / 4;
     ATR_CUDA(cudaHostAlloc(p, c, cudaHostAllocDefault));
     *cap = c;
     return ATR_OK;
@@ -320,37 +320,44 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
     // Rays of every request into one device queue, in `work` order: a request
     // whose buffer is page-locked is copied from it directly, the others
     // through this lane's pinned staging buffer.
+    // Staging holds only the pageable buffers, packed: stage_at[i] is request
+    // i's offset (in rays) in the ray and result staging buffers.
     uint64_t total_rays = 0;
     for (Request* r : work) total_rays += r->req.num_rays;
-    ATR_TRY(grow_pinned(&L.h_rays, &L.h_rays_cap, std::max<uint64_t>(total_rays, 1) * 32));
-    ATR_TRY(grow_pinned(&L.h_res, &L.h_res_cap, std::max<uint64_t>(total_rays, 1) * 16));
-    std::vector<uint64_t> ray_at(work.size() + 1, 0);
+    std::vector<uint64_t> ray_at(work.size() + 1, 0), stage_at(work.size(), 0);
     std::vector<char> rays_pinned(work.size(), 0), res_pinned(work.size(), 0), verts_pinned(work.size(), 0);
-    std::vector<CopyJob> jobs;
+    uint64_t stage_rays = 0, stage_res = 0;
     for (size_t i = 0; i < work.size(); ++i) {
         ray_at[i + 1] = ray_at[i] + work[i]->req.num_rays;
+        verts_pinned[i] = is_pinned(work[i]->req.vertices);
         if (!work[i]->req.num_rays) continue;
         rays_pinned[i] = is_pinned(work[i]->req.rays);
         res_pinned[i] = is_pinned(work[i]->req.results);
-        if (!rays_pinned[i])
-            jobs.push_back({static_cast<char*>(L.h_rays) + ray_at[i] * 32, work[i]->req.rays,
-                            (size_t)work[i]->req.num_rays * 32});
+        stage_at[i] = std::max(stage_rays, stage_res);
+        if (!rays_pinned[i]) stage_rays = stage_at[i] + work[i]->req.num_rays;
+        if (!res_pinned[i]) stage_res = stage_at[i] + work[i]->req.num_rays;
     }
-    for (size_t i = 0; i < work.size(); ++i) verts_pinned[i] = is_pinned(work[i]->req.vertices);
-    // Refit vertices go to their own staging buffer (copied before any launch).
+    if (stage_rays) ATR_TRY(grow_pinned(&L.h_rays, &L.h_rays_cap, stage_rays * 32));
+    if (stage_res) ATR_TRY(grow_pinned(&L.h_res, &L.h_res_cap, stage_res * 16));
+    std::vector<CopyJob> jobs;
+    for (size_t i = 0; i < work.size(); ++i)
+        if (work[i]->req.num_rays && !rays_pinned[i])
+            jobs.push_back({static_cast<char*>(L.h_rays) + stage_at[i] * 32, work[i]->req.rays,
+                            (size_t)work[i]->req.num_rays * 32});
+    // Pageable refit vertices go to their own staging buffer (copied before any launch).
     uint64_t refit_tris = 0;
     std::vector<size_t> refit_at(work.size(), 0);
     {
         std::lock_guard<std::mutex> lock(mu);
         for (size_t i = 0; i < work.size(); ++i) {
-            if (work[i]->req.kind != ATR_REQ_REFIT) continue;
+            if (work[i]->req.kind != ATR_REQ_REFIT || verts_pinned[i]) continue;
             auto f = resident.find(work[i]->req.mesh_id);
             if (f == resident.end()) continue;
             refit_at[i] = refit_tris;
             refit_tris += f->second.n;
         }
     }
-    ATR_TRY(grow_pinned(&L.h_rverts, &L.h_rverts_cap, std::max<uint64_t>(refit_tris, 1) * 48));
+    if (refit_tris) ATR_TRY(grow_pinned(&L.h_rverts, &L.h_rverts_cap, refit_tris * 48));
     {
         std::lock_guard<std::mutex> lock(mu);
         for (size_t i = 0; i < work.size(); ++i) {
@@ -373,7 +380,7 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
         for (size_t i = 0; i < work.size() && e == cudaSuccess; ++i) {
             if (!work[i]->req.num_rays) continue;
             const void* src = rays_pinned[i] ? work[i]->req.rays
-                                             : static_cast<const void*>(static_cast<char*>(L.h_rays) + ray_at[i] * 32);
+                                             : static_cast<const void*>(static_cast<char*>(L.h_rays) + stage_at[i] * 32);
             e = cudaMemcpyAsync(static_cast<char*>(d_rays) + ray_at[i] * 32, src, (size_t)work[i]->req.num_rays * 32,
                                 cudaMemcpyHostToDevice, ctx->stream);
         }
@@ -398,9 +405,12 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
 
     // 1. One segmented build of every new mesh.
     if (!builds.empty()) {
-        uint64_t tris = 0;
-        for (Request* r : builds) tris += r->req.num_triangles;
-        int s = grow_pinned(&L.h_verts, &L.h_verts_cap, tris * 48);
+        uint64_t tris = 0, stage_tris = 0;
+        for (size_t m = 0; m < builds.size(); ++m) {
+            tris += builds[m]->req.num_triangles;
+            if (!verts_pinned[m]) stage_tris += builds[m]->req.num_triangles;
+        }
+        int s = stage_tris ? grow_pinned(&L.h_verts, &L.h_verts_cap, tris * 48) : ATR_OK;
         if (s != ATR_OK) { release_rays(); return s; }
         std::vector<uint32_t> off(builds.size() + 1, 0);
         std::vector<uint8_t> ts(builds.size()), it(builds.size());
@@ -508,7 +518,7 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
     for (size_t i = 0; i < work.size(); ++i) {
         if (!work[i]->req.num_rays) continue;
         void* dst = res_pinned[i] ? static_cast<void*>(work[i]->req.results)
-                                  : static_cast<void*>(static_cast<char*>(L.h_res) + ray_at[i] * 16);
+                                  : static_cast<void*>(static_cast<char*>(L.h_res) + stage_at[i] * 16);
         cudaError_t e = cudaMemcpyAsync(dst, static_cast<char*>(d_res) + ray_at[i] * 16,
                                         (size_t)work[i]->req.num_rays * 16, cudaMemcpyDeviceToHost, ctx->stream);
         if (e != cudaSuccess) { release_rays(); return atr::cuda_fail(e, "cudaMemcpyAsync(results)", __FILE__, __LINE__); }
@@ -520,7 +530,7 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
     std::vector<CopyJob> out;
     for (size_t i = 0; i < work.size(); ++i)
         if (work[i]->req.num_rays && work[i]->status == ATR_OK && !res_pinned[i])
-            out.push_back({work[i]->req.results, static_cast<char*>(L.h_res) + ray_at[i] * 16,
+            out.push_back({work[i]->req.results, static_cast<char*>(L.h_res) + stage_at[i] * 16,
                            (size_t)work[i]->req.num_rays * 16});
     par_copy(out);
     const double out_ms = ms_between(t_done, Clock::now());
