@@ -446,8 +446,8 @@ def run_ours(args, world, rank, local):
         out["batch"] = measure_batch(ctx, stream, world, rank, device=local, steps=5, warmup=2, plain_reps=2,
                                      autotune=False, e2e=False)
     if world == 1 and not args.no_serve and rank == 0:
-        out["serving"] = measure_serve(rates=[500.0, 2000.0, 5000.0], requests=1000, pool_size=16, lanes=args.lanes,
-                                       device=local)
+        out["serving"] = measure_serve(rates=[500.0, 1000.0, 2000.0, 5000.0], requests=1000, pool_size=16,
+                                       lanes=args.lanes, device=local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline()
     if rank == 0:
@@ -845,8 +845,9 @@ def main():
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES, help="batch: number of meshes")
     ap.add_argument("--no-autotune", action="store_true", help="batch: skip the autotuned arm")
     ap.add_argument("--requests", type=int, default=20000, help="serve: requests per arrival rate")
-    ap.add_argument("--rates", default="1000,5000", help="serve: comma-separated arrival rates per second")
-    ap.add_argument("--lanes", type=int, default=2, help="serve: concurrent lanes")
+    ap.add_argument("--rates", default="100,200,500,1000,2000,5000",
+                    help="serve: comma-separated arrival rates per second")
+    ap.add_argument("--lanes", type=int, default=3, help="serve: concurrent lanes")
     ap.add_argument("--pool", type=int, default=48, help="serve: distinct meshes drawn by the requests")
     ap.add_argument("--sweep-triangles", type=int, default=1 << 24, help="sweep: scene size")
     args = ap.parse_args()
