@@ -134,6 +134,11 @@ class TuneTable(C.Structure):
         return ts, it
 
 
+class TuneOutcome(C.Structure):
+    _fields_ = [("default_ms", C.c_float), ("tuned_ms", C.c_float), ("default_sah", C.c_double),
+                ("tuned_sah", C.c_double), ("kept", C.c_int32)]
+
+
 class AutotuneConfig(C.Structure):
     _fields_ = [("min_class", C.c_uint32), ("max_class", C.c_uint32), ("sample_triangles", C.c_uint64),
                 ("sah_tolerance", C.c_float), ("reps", C.c_uint32), ("seed", C.c_uint64)]
@@ -217,6 +222,8 @@ _SIGS = [
     ("atr_autotune", C.c_int, [_p, C.POINTER(AutotuneConfig), C.POINTER(TuneTable)]),
     ("atr_tune_lookup", C.c_int, [C.POINTER(TuneTable), C.c_uint32, C.POINTER(TuneEntry)]),
     ("atr_batch_apply_tuning", C.c_int, [_p, _p, C.POINTER(TuneTable)]),
+    ("atr_batch_autotune", C.c_int, [_p, _p, C.POINTER(AutotuneConfig), C.POINTER(TuneTable),
+                                     C.POINTER(TuneOutcome)]),
     ("atr_server_create", C.c_int, [C.c_int, C.POINTER(ServerConfig), C.POINTER(_p)]),
     ("atr_server_submit", C.c_int, [_p, C.POINTER(ServerRequest), C.POINTER(C.c_uint64)]),
     ("atr_server_wait", C.c_int, [_p, C.c_uint64, C.POINTER(ServerResult)]),
@@ -943,6 +950,17 @@ def autotune(ctx: Context, min_class: int = 8, max_class: int = 21, sample_trian
     t = TuneTable()
     check(lib().atr_autotune(ctx.handle, C.byref(cfg), C.byref(t)))
     return t
+
+
+def batch_autotune(ctx: Context, batch: "Batch", sample_triangles: int = 1 << 22, sah_tolerance: float = 0.0,
+                   reps: int = 3, seed: int = 0) -> tuple[TuneTable, dict]:
+    """Tune the batch's size classes, keep the table only if the batch itself
+    builds faster with it (atr_batch_autotune); returns (table, outcome)."""
+    cfg = AutotuneConfig(1, 29, sample_triangles, sah_tolerance, reps, seed)
+    t = TuneTable()
+    o = TuneOutcome()
+    check(lib().atr_batch_autotune(ctx.handle, batch.handle, C.byref(cfg), C.byref(t), C.byref(o)))
+    return t, {name: getattr(o, name) for name, _ in TuneOutcome._fields_}
 
 
 # ---- serving loop ----------------------------------------------------------------

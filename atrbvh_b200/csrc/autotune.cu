@@ -142,8 +142,9 @@ int atr_autotune(atr_ctx* ctx, const atr_autotune_config* cfg, atr_tune_table* o
         st = atr_gen_batch_scene(count, sizes.data(), cfg->seed + c, verts.data());
         if (st == ATR_OK) st = atr_batch_create(ctx, verts.data(), s.off.data(), count, nullptr, 0, &s.b);
         if (st != ATR_OK) break;
-        ctx->atr_warps = 4;
-        ctx->sort_bits = 8;
+        // The reference point: ATRBVH(9,2) at the context's own launch shape.
+        ctx->atr_warps = warps0;
+        ctx->sort_bits = bits0;
         double sah_ref = 0.0, sah = 0.0;
         float ms_ref = 0.0f;
         st = time_builds(ctx, s.b, 9, 2, cfg->reps, &ms_ref);
@@ -164,10 +165,10 @@ int atr_autotune(atr_ctx* ctx, const atr_autotune_config* cfg, atr_tune_table* o
                     best_sah = sah;
                 }
             }
-        int best_w = 4, best_b = 8;
+        int best_w = warps0, best_b = bits0;
         for (int w : {2, 4, 8})
             for (int bits : {8, 10}) {
-                if (st != ATR_OK || (w == 4 && bits == 8)) continue;
+                if (st != ATR_OK || (w == warps0 && bits == bits0)) continue;
                 ctx->atr_warps = w;
                 ctx->sort_bits = bits;
                 float ms = 0.0f;
@@ -200,6 +201,42 @@ int atr_autotune(atr_ctx* ctx, const atr_autotune_config* cfg, atr_tune_table* o
     ctx->atr_warps = warps0;
     ctx->sort_bits = bits0;
     return st;
+}
+
+// Median device time of `reps` builds of a whole batch (graph replays) after
+// one warm-up, and its summed per-mesh SAH.
+int time_batch(atr_ctx* ctx, atr_batch* b, uint32_t reps, float* ms, double* sah) {
+    ATR_TRY(atr_batch_build(ctx, b, 1, 9, 2, 1.2f, 1.0f, 1));
+    cudaEvent_t e0, e1;
+    ATR_CUDA(cudaEventCreate(&e0));
+    ATR_CUDA(cudaEventCreate(&e1));
+    std::vector<float> t;
+    int st = ATR_OK;
+    for (uint32_t r = 0; r < reps && st == ATR_OK; ++r) {
+        cudaEventRecord(e0, ctx->stream);
+        st = atr_batch_build(ctx, b, 1, 9, 2, 1.2f, 1.0f, 1);
+        cudaEventRecord(e1, ctx->stream);
+        if (st != ATR_OK) break;
+        const cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) { st = cuda_fail(e, "batch autotune timing", __FILE__, __LINE__); break; }
+        float x = 0.0f;
+        cudaEventElapsedTime(&x, e0, e1);
+        t.push_back(x);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ATR_TRY(st);
+    std::sort(t.begin(), t.end());
+    *ms = t[t.size() / 2];
+    uint32_t count = 0, n = 0;
+    uint64_t nodes = 0;
+    ATR_TRY(atr_batch_info(b, &count, &n, &nodes));
+    std::vector<float> per(count);
+    ATR_TRY(atr_batch_sah(ctx, b, 1.2f, 1.0f, per.data()));
+    double sum = 0.0;
+    for (float x : per) sum += x;
+    *sah = sum;
+    return ATR_OK;
 }
 
 // Class entry used for a mesh of n triangles: its own class when tuned, else
@@ -244,6 +281,66 @@ int atr_batch_apply_tuning(atr_ctx* ctx, atr_batch* b, const atr_tune_table* t) 
     ctx->atr_warps = t->cls[dom].atr_warps;
     ctx->sort_bits = t->cls[dom].sort_bits;
     return atr_batch_set_params(ctx, b, ts.data(), it.data());
+}
+
+// Tunes the size classes present in a batch on class samples, then builds the
+// batch itself with ATRBVH(9,2) at the context's launch shape and with the
+// tuned table, and keeps the table only when the batch builds faster with it
+// at a summed SAH within the tolerance; otherwise every entry is reset to
+// the reference point, so the table applied to this batch is never slower
+// than the defaults.  The batch is left with the kept parameters applied.
+int atr_batch_autotune(atr_ctx* ctx, atr_batch* b, const atr_autotune_config* cfg, atr_tune_table* out,
+                       atr_tune_outcome* outcome) {
+    ATR_REQUIRE(ctx && b && cfg && out && outcome, ATR_ERR_INVALID_ARG, "atr_batch_autotune: NULL argument");
+    std::memset(out, 0, sizeof(*out));
+    std::memset(outcome, 0, sizeof(*outcome));
+    uint32_t count = 0, n = 0;
+    uint64_t nodes = 0;
+    ATR_TRY(atr_batch_info(b, &count, &n, &nodes));
+    uint32_t present = 0;
+    for (uint32_t m = 0; m < count; ++m) {
+        atr_tree_view v;
+        ATR_TRY(atr_batch_mesh_view(b, m, &v));
+        present |= 1u << (31 - __builtin_clz(v.num_triangles));
+    }
+    const int warps0 = ctx->atr_warps, bits0 = ctx->sort_bits;
+    // Reference: the batch with ATRBVH(9,2) everywhere at the context's launch shape.
+    ATR_TRY(atr_batch_set_params(ctx, b, nullptr, nullptr));
+    ATR_TRY(time_batch(ctx, b, cfg->reps, &outcome->default_ms, &outcome->default_sah));
+    for (uint32_t c = 1; c < 30; ++c) {
+        if (!(present >> c & 1u)) continue;
+        atr_autotune_config one = *cfg;
+        one.min_class = one.max_class = c;
+        atr_tune_table t;
+        ATR_TRY(atr_autotune(ctx, &one, &t));
+        out->cls[c] = t.cls[c];
+        out->tuned_mask |= 1u << c;
+    }
+    int st = atr_batch_apply_tuning(ctx, b, out);
+    if (st == ATR_OK) st = time_batch(ctx, b, cfg->reps, &outcome->tuned_ms, &outcome->tuned_sah);
+    if (st != ATR_OK) {
+        ctx->atr_warps = warps0;
+        ctx->sort_bits = bits0;
+        return st;
+    }
+    outcome->kept = outcome->tuned_ms < outcome->default_ms &&
+                    outcome->tuned_sah <= outcome->default_sah * (1.0 + (double)cfg->sah_tolerance);
+    if (!outcome->kept) {
+        for (uint32_t c = 0; c < 32; ++c) {
+            if (!(out->tuned_mask >> c & 1u)) continue;
+            atr_tune_entry& e = out->cls[c];
+            e.treelet = 9;
+            e.iterations = 2;
+            e.atr_warps = (uint8_t)warps0;
+            e.sort_bits = (uint8_t)bits0;
+            e.build_ms = e.reference_ms;
+            e.sah_ratio = 1.0f;
+        }
+        ctx->atr_warps = warps0;
+        ctx->sort_bits = bits0;
+        ATR_TRY(atr_batch_set_params(ctx, b, nullptr, nullptr));
+    }
+    return ATR_OK;
 }
 
 }  // extern "C"

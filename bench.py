@@ -519,10 +519,12 @@ def measure_batch(ctx, stream, world, rank, *, device: int = 0, meshes: int = BA
     # ATRBVH(9,2), ATRBVH block size and sort digit width of the dominant class.
     tuned = None
     if autotune:
+        # Classes tuned on samples of up to 4M triangles, the table then checked
+        # on this batch against the defaults and kept only if faster.
+        w0, b0 = ctx.get_tuning(ab.TUNE_ATR_WARPS), ctx.get_tuning(ab.TUNE_SORT_BITS)
         t0 = time.perf_counter()
-        table = ab.autotune(ctx, min_class=8, max_class=18, sample_triangles=1 << 21, reps=2)
+        table, outcome = ab.batch_autotune(ctx, batch, sample_triangles=1 << 22, reps=3)
         tune_s = time.perf_counter() - t0
-        batch.apply_tuning(table)
         for _ in range(warmup):
             build_batched()
         tt = _cuda_ms(stream, build_batched, steps)
@@ -530,12 +532,13 @@ def measure_batch(ctx, stream, world, rank, *, device: int = 0, meshes: int = BA
         t_ms = max_over_ranks(statistics.median(tt), world)
         tuned = {"mtri_per_s": total_tris / (t_ms * 1e-3) / 1e6, "ms": t_ms,
                  "sah_ratio_vs_atrbvh_9_2": float(np.sum(sah_t, dtype=np.float64) / np.sum(sah_b, dtype=np.float64)),
-                 "tuning_seconds": tune_s,
+                 "tuning_seconds": tune_s, "kept": bool(outcome["kept"]),
+                 "tuner_batch_ms": {"default": outcome["default_ms"], "tuned": outcome["tuned_ms"]},
                  "table": {str(c): {k: e[k] for k in ("treelet", "iterations", "atr_warps", "sort_bits", "sah_ratio")}
                            for c, e in table.classes().items()}}
         batch.set_params(None)
-        ctx.set_tuning(ab.TUNE_ATR_WARPS, 4)
-        ctx.set_tuning(ab.TUNE_SORT_BITS, 8)
+        ctx.set_tuning(ab.TUNE_ATR_WARPS, w0)
+        ctx.set_tuning(ab.TUNE_SORT_BITS, b0)
 
     # Per-mesh plain launches: one scene per mesh made up front (like the
     # batch's own upload), then LBVH + ATRBVH per mesh in the timed loop.

@@ -377,7 +377,7 @@ typedef struct atr_tune_entry {
     uint8_t atr_warps;
     uint8_t sort_bits;
     float build_ms;          /* median LBVH+ATRBVH time of the class sample, tuned */
-    float reference_ms;      /* same with ATRBVH(9,2), 4 warps, 8-bit digits */
+    float reference_ms;      /* same with ATRBVH(9,2) at the context's launch shape */
     float sah_ratio;         /* summed SAH of the tuned build / that of ATRBVH(9,2) */
     uint32_t sample_triangles;
     uint32_t sample_meshes;
@@ -397,6 +397,21 @@ typedef struct atr_autotune_config {
 } atr_autotune_config;
 
 int atr_autotune(atr_ctx* ctx, const atr_autotune_config* config, atr_tune_table* table);
+/* Outcome of atr_batch_autotune: the batch's own build time (CUDA-graph
+ * replays, median) and summed per-mesh SAH with ATRBVH(9,2) at the context's
+ * launch shape and with the tuned table, and whether the table was kept. */
+typedef struct atr_tune_outcome {
+    float default_ms, tuned_ms;
+    double default_sah, tuned_sah;
+    int32_t kept;
+} atr_tune_outcome;
+/* Tunes the size classes present in the batch (atr_autotune on class
+ * samples), then times the batch itself both ways and keeps the table only
+ * when it builds the batch faster at a summed SAH within the tolerance;
+ * otherwise every entry is reset to ATRBVH(9,2) at the context's launch
+ * shape.  The batch and the context are left with the kept parameters. */
+int atr_batch_autotune(atr_ctx* ctx, atr_batch* batch, const atr_autotune_config* config,
+                       atr_tune_table* table, atr_tune_outcome* outcome);
 /* The entry for a mesh of num_triangles: its class, or the nearest tuned one. */
 int atr_tune_lookup(const atr_tune_table* table, uint32_t num_triangles, atr_tune_entry* entry);
 /* Per-mesh treelet size and iterations of a batch from the table

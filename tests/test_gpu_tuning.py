@@ -93,3 +93,37 @@ def test_autotune_table_and_tuned_batch(tuned_ctx):
         want = O.atrbvh(base, cls[c]["treelet"], cls[c]["iterations"], threads=8)
         assert_trees_equal(b.mesh(m), want, f"mesh {m} ({n} tris, class {c})")
     b.close()
+
+
+def test_batch_autotune_never_slower_than_defaults(tuned_ctx):
+    """atr_batch_autotune keeps its table only when the batch itself builds
+    faster with it; either way the batch is left with parameters whose build
+    equals the oracle's at those parameters, and the table's entries match
+    what the batch uses."""
+    sizes = ab.gen_batch_sizes(48, 256, 20000, 6)
+    v = ab.gen_batch_scene(sizes, 6)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint32)
+    b = ab.Batch(tuned_ctx, v, off)
+    warps0, bits0 = tuned_ctx.get_tuning(ab.TUNE_ATR_WARPS), tuned_ctx.get_tuning(ab.TUNE_SORT_BITS)
+    table, out = ab.batch_autotune(tuned_ctx, b, sample_triangles=1 << 15, reps=2)
+    assert out["default_ms"] > 0 and out["tuned_ms"] > 0
+    if out["kept"]:
+        assert out["tuned_ms"] < out["default_ms"]
+        assert out["tuned_sah"] <= out["default_sah"] * (1 + 1e-12)
+    else:
+        for e in table.classes().values():
+            assert (e["treelet"], e["iterations"], e["atr_warps"], e["sort_bits"]) == (9, 2, warps0, bits0), e
+        assert tuned_ctx.get_tuning(ab.TUNE_ATR_WARPS) == warps0
+    present = {int(n).bit_length() - 1 for n in sizes}
+    assert set(table.classes()) == present
+    b.build(1, 9, 2, graph=True)
+    for m in range(0, len(sizes), 5):
+        e = table.classes()[int(sizes[m]).bit_length() - 1]
+        vm = np.ascontiguousarray(v[off[m]:off[m + 1]])
+        mn, mx = O.scene_aabb(vm)
+        base, _, _ = O.build_lbvh(vm, mn, mx, threads=8)
+        want = O.atrbvh(base, e["treelet"], e["iterations"], threads=8)
+        assert_trees_equal(b.mesh(m), want, f"mesh {m}")
+    b.close()
+    tuned_ctx.set_tuning(ab.TUNE_ATR_WARPS, warps0)
+    tuned_ctx.set_tuning(ab.TUNE_SORT_BITS, bits0)
