@@ -279,6 +279,7 @@ int atr_scene_bounds(atr_ctx* ctx, const atr_scene* s, float* bmin, float* bmax)
 
 int atr_tree_destroy(atr_tree* t) {
     if (!t) return ATR_OK;
+    atr::refit_plan_free(t->ctx, t->refit_plan);
     t->ctx->release(t->block);
     t->ctx->release(t->prepass_block);
     t->ctx->release(t->sorted_keys);

@@ -1559,6 +1559,7 @@ extern "C" int atr_optimize_atrbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int 
     const BuildPrepass* pp = tree->prepass_block ? &tree->prepass : nullptr;
     if (iterations <= 0) return ATR_OK;
     tree->karras = false;
+    tree_topology_changed(tree);
     const int st = atrbvh_run(ctx, g, segs, 2 * (size_t)n - 1, tsize, tsize, iterations, nullptr, nullptr, ci, ct,
                               ranges, pp);
     // The prepass arrays served as this pass's scratch; they are stale now.

@@ -4,7 +4,7 @@
 // ATRBVH and TRBVH stages runs once over the whole batch (one launch per
 // stage and iteration), with each thread, tile or treelet working inside its
 // own mesh: per-mesh scene boxes and Morton normalisation, per-mesh digit
-// histograms and look-back chains in the onesweep sort, per-mesh radix trees
+// histograms and tile-prefix scans that restart at each mesh in the sort, per-mesh radix trees
 // with local node indices, and treelets formed and rewritten within one
 // mesh.  Every mesh's arrays therefore equal those of a build of that mesh
 // alone.  Steady-state builds can be captured once into a CUDA graph and

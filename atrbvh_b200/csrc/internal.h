@@ -120,6 +120,25 @@ struct atr_scene {
     float* d_bounds = nullptr;  // min.xyz, max.xyz on the device
 };
 
+namespace atr {
+// Plan of the refit of one topology (refit.cu): per level, CTA slot offsets,
+// the inputs (source and node, parent slot) and the internal nodes (node,
+// parent slot, child slots) in CTA-local slot order.
+struct RefitPlan {
+    static constexpr int kMaxLevels = 8;
+    struct Level {
+        uint32_t ctas = 0, inputs = 0, internal = 0;
+        uint32_t *cta_in = nullptr, *cta_int = nullptr;
+        int32_t *in_src = nullptr, *in_node = nullptr, *it_node = nullptr;
+        uint16_t *in_par = nullptr, *it_par = nullptr;
+        uint32_t* it_kids = nullptr;
+    };
+    int levels = 0;
+    Level lv[kMaxLevels];
+    std::vector<void*> blocks;  // device allocations of the levels
+};
+}  // namespace atr
+
 struct atr_tree {
     atr_ctx* ctx = nullptr;
     uint32_t n = 0;
@@ -139,6 +158,11 @@ struct atr_tree {
     void* sorted_keys = nullptr;
     uint32_t* sorted_idx = nullptr;
     int morton_bits = 30;
+    // Refit plan of the current topology (built by the first refit; released
+    // whenever the topology changes).  no_refit_plan: the topology has no
+    // plan (too deep a top); refits climb instead.
+    atr::RefitPlan* refit_plan = nullptr;
+    bool no_refit_plan = false;
 };
 
 struct atr_collapsed {
@@ -197,6 +221,12 @@ int trace_batch(atr_ctx* ctx, const int4* nodes, const float4* woop, const int32
                 const float4* rays, int64_t n, int any_hit, int4* res);
 // Bottom-up box refit of one tree (local indices) from vertices of its mesh.
 int refit_arrays(atr_ctx* ctx, uint32_t n, const TreeOut& t, const float4* verts);
+// Refit plans (refit.cu): build for a topology (ATR_ERR_UNSUPPORTED: the
+// topology has no plan), run, free.  tree_topology_changed drops a tree's plan.
+int refit_plan_build(atr_ctx* ctx, uint32_t n, const TreeOut& t, RefitPlan** out);
+int refit_plan_run(atr_ctx* ctx, const RefitPlan& p, const TreeOut& t, const float4* verts);
+void refit_plan_free(atr_ctx* ctx, RefitPlan* p);
+void tree_topology_changed(atr_tree* t);
 // atr_batch_refit_mesh that also returns the mesh's collapsed-tree SAH
 // (h_sah may be NULL).
 int batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* vertices, int on_device,
@@ -229,7 +259,7 @@ int atrbvh_prepare();  // kernel attributes; once per context
 int trbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int iterations,
               const uint8_t* seg_iters, float ci, float ct);
 
-constexpr uint32_t kSortTileSize = 4096;  // triangles per sort tile (lbvh.cu)
+constexpr uint32_t kSortTileSize = 3072;  // triangles per sort tile (lbvh.cu)
 int lbvh_prepare();                       // kernel attributes; once per context
 
 }  // namespace atr

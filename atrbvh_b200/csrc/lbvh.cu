@@ -1,6 +1,6 @@
 // LBVH construction on sm_100a:
 //   scene bounds  -> Morton codes (+ all radix-digit histograms in the same pass)
-//   -> onesweep LSD radix sort of (key, triangle index)
+//   -> LSD radix sort of (key, triangle index): tile counts, tile prefixes, scatter
 //   -> one bottom-up pass that builds the Karras radix tree and refits its
 //      boxes at the same time.
 //
@@ -20,13 +20,9 @@ namespace atr {
 namespace {
 
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
+constexpr int kSortItems = 12;
 constexpr int kSortTile = kSortThreads * kSortItems;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr uint32_t kFlagAgg = 0x40000000u;
-constexpr uint32_t kFlagInc = 0x80000000u;
-constexpr uint32_t kValueMask = 0x3fffffffu;
-constexpr uint32_t kLookbackLimit = 1u << 26;
 
 // Digit plan of an LSD sort of K keys with BITS-bit digits.  8-bit digits
 // cover every key bit (4 passes for uint32, 8 for uint64).  10-bit digits are
@@ -38,7 +34,7 @@ struct SortPlan {
     static constexpr int kDigits = 1 << BITS;
     static constexpr int kPasses = BITS == 8 ? (int)sizeof(K) : (sizeof(K) == 4 ? 3 : 7);
     static constexpr int kPerThread = kDigits / kSortThreads;  // digits per thread in tile-wide steps
-    // Dynamic shared memory of one onesweep block: the tile's keys and
+    // Dynamic shared memory of one scatter block: the tile's keys and
     // values, per-warp digit counters, digit starts and global bases.
     static constexpr size_t kSmem = (size_t)kSortTile * (sizeof(K) + 4) + (size_t)(kSortWarps + 2) * kDigits * 4;
 };
@@ -131,12 +127,14 @@ __device__ __forceinline__ uint64_t morton_code<uint64_t>(float cx, float cy, fl
 
 // One block per sort tile (kSortTile triangles of one mesh); histograms of
 // every digit of every pass are accumulated in shared memory and added to the
-// mesh's histograms (P x D per mesh) once per block.  Each mesh is normalised
-// to its own box (6 floats per mesh in `bounds`).
+// mesh's histograms (P x D per mesh) once per block; the block's own counts
+// of the first pass's digits are the sort's first tile counts (D per tile in
+// tile_counts).  Each mesh is normalised to its own box (6 floats per mesh
+// in `bounds`).
 template <typename K, int BITS>
 __global__ void __launch_bounds__(256) k_morton(Segs segs, const float4* __restrict__ v,
                                                  const float* __restrict__ bounds, K* __restrict__ keys,
-                                                 uint32_t* __restrict__ hist) {
+                                                 uint32_t* __restrict__ hist, uint32_t* __restrict__ tile_counts) {
     constexpr int P = SortPlan<K, BITS>::kPasses, D = SortPlan<K, BITS>::kDigits;
     __shared__ uint32_t sh[P * D];
     __shared__ float sb[6];
@@ -162,6 +160,8 @@ __global__ void __launch_bounds__(256) k_morton(Segs segs, const float4* __restr
     __syncthreads();
     for (int j = threadIdx.x; j < P * D; j += blockDim.x)
         if (sh[j]) atomicAdd(&hist[(size_t)m * P * D + j], sh[j]);
+    if (tile_counts)
+        for (int j = threadIdx.x; j < D; j += blockDim.x) tile_counts[(size_t)blockIdx.x * D + j] = sh[j];
 }
 
 // 8-bit digit histograms of arbitrary keys (the generic sort entry point).
@@ -214,23 +214,165 @@ __device__ __forceinline__ void block_exclusive_scan(const uint32_t (&x)[R], uin
     }
 }
 
-// ---- onesweep radix sort pass ------------------------------------------------
-// Stable: keys of one digit keep their input order (tiles are numbered by an
-// atomic ticket so that every tile's predecessors are already running; each
-// warp ranks a contiguous run of the tile in order).  The per-tile digit
-// counts are combined across tiles by decoupled look-back: a tile publishes
-// the counts of all its digits before it waits on any earlier tile, and a
-// wait that does not resolve within kLookbackLimit polls sets
-// kErrSortLookback and gives up.  Segmented: a tile holds keys of one mesh
-// only, the look-back stops at the mesh's first tile and keys move only
-// within their mesh, so each mesh is sorted on its own (hist holds P x D
-// counts per mesh).  Each thread owns R = D / 256 consecutive digits in the
-// tile-wide steps.
+// ---- radix sort pass: tile counts -> tile prefixes -> scatter -----------------
+// A pass over keys already split into tiles of kSortTile (a tile holds keys of
+// one mesh only):
+//   k_tile_counts  every tile's digit counts (pass 0 of an LBVH build takes
+//                  them from k_morton instead);
+//   k_tile_prefix  in place, the exclusive sum of each digit's counts over the
+//                  mesh's earlier tiles (a segmented scan down every digit's
+//                  column);
+//   k_scatter      ranks the tile's keys, adds the tile prefix to the mesh's
+//                  digit start and writes every key to its place.
+// Each scatter block finds its offsets ready, so no tile waits on another
+// (the decoupled look-back this replaces spent a third of every pass walking
+// over the aggregates of the tiles running beside it).
+
+// Tile counts of digit `pass` (D per tile, tile-major).  A thread loads its
+// kSortItems keys at once and counts them with shared atomics into its warp's
+// own histogram (no ranks are needed here); the warps' histograms are summed
+// at the end.
+template <typename K, int BITS>
+__global__ void __launch_bounds__(kSortThreads) k_tile_counts(Segs segs, const K* __restrict__ keys, int pass,
+                                                               uint32_t* __restrict__ counts) {
+    constexpr int D = SortPlan<K, BITS>::kDigits;
+    __shared__ uint32_t sh[kSortWarps][D];
+    const int shift = BITS * pass;
+    const uint32_t tile = blockIdx.x;
+    const uint32_t m = segs.seg_of_tile(tile);
+    const uint32_t base = segs.tri_begin(m) + (tile - segs.tile_begin(m)) * kSortTile;
+    const uint32_t end = min(base + (uint32_t)kSortTile, segs.tri_end(m));
+    for (int j = threadIdx.x; j < kSortWarps * D; j += kSortThreads) (&sh[0][0])[j] = 0;
+    uint32_t dg[kSortItems];
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const uint32_t i = base + r * kSortThreads + threadIdx.x;
+        dg[r] = i < end ? (uint32_t)((keys[i] >> shift) & (D - 1)) : (uint32_t)D;
+    }
+    __syncthreads();
+    uint32_t* const wh = sh[threadIdx.x >> 5];
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r)
+        if (dg[r] < (uint32_t)D) atomicAdd(&wh[dg[r]], 1u);
+    __syncthreads();
+    for (int j = threadIdx.x; j < D; j += kSortThreads) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) c += sh[w][j];
+        counts[(size_t)tile * D + j] = c;
+    }
+}
+
+// In place: counts[t][d] -> the sum of counts[t'][d] over the earlier tiles
+// t' of t's mesh within t's chunk of kPrefixChunk tiles.  Block (x, y) takes
+// 32 digits (one per lane) and chunk y, split into 32 runs of 8 tiles (one
+// per warp): run sums, a segmented scan of the run sums in shared memory (a
+// run holding a mesh's first tile restarts the sum), then each run again from
+// its carry.  The chunk's segmented total (sum since its last mesh start, top
+// bit set when it holds one) goes to chunk_tot; k_chunk_carry turns those
+// into each chunk's carry from earlier chunks, which the scatter adds for a
+// tile whose mesh began before its chunk.
+constexpr int kPrefixRuns = 32;
+constexpr int kPrefixRunTiles = 8;
+constexpr uint32_t kPrefixChunk = kPrefixRuns * kPrefixRunTiles;
+constexpr uint32_t kCutBit = 0x80000000u;
+
+// Tile of the next mesh start after mesh m (none: ~0).
+__device__ __forceinline__ uint32_t next_mesh_tile(const Segs& segs, uint32_t m) {
+    return m + 1 < segs.count ? segs.tile_begin(m + 1) : 0xffffffffu;
+}
+
+template <int D>
+__global__ void __launch_bounds__(32 * kPrefixRuns) k_tile_prefix(Segs segs, uint32_t tiles,
+                                                                   uint32_t* __restrict__ counts,
+                                                                   uint32_t* __restrict__ chunk_tot) {
+    __shared__ uint32_t s_sum[kPrefixRuns][32];
+    __shared__ uint8_t s_cut[kPrefixRuns][32];
+    const int lane = threadIdx.x & 31, run = threadIdx.x >> 5;
+    const uint32_t d = blockIdx.x * 32 + lane;
+    const uint32_t c0 = blockIdx.y * kPrefixChunk;
+    const uint32_t t0 = min(tiles, c0 + run * kPrefixRunTiles), t1 = min(tiles, t0 + kPrefixRunTiles);
+    const uint32_t m0 = t0 < t1 ? segs.seg_of_tile(t0) : 0;
+    const bool starts = t0 < t1 && t0 == segs.tile_begin(m0);  // the run begins a mesh
+    const uint32_t next0 = t0 < t1 ? next_mesh_tile(segs, m0) : 0xffffffffu;
+    uint32_t v[kPrefixRunTiles];
+#pragma unroll
+    for (int u = 0; u < kPrefixRunTiles; ++u) v[u] = t0 + u < t1 ? counts[(size_t)(t0 + u) * D + d] : 0u;
+    uint32_t sum = 0;
+    bool cut = starts;
+    {
+        uint32_t m = m0, next = next0;
+#pragma unroll
+        for (int u = 0; u < kPrefixRunTiles; ++u) {
+            if (t0 + u < t1 && t0 + u == next) {  // a mesh starts here: the run's sum restarts
+                sum = 0;
+                cut = true;
+                next = next_mesh_tile(segs, ++m);
+            }
+            sum += v[u];
+        }
+    }
+    s_sum[run][lane] = sum;
+    s_cut[run][lane] = cut;
+    __syncthreads();
+    // Carry into this run from the chunk's earlier runs, back to the last cut.
+    uint32_t carry = 0;
+    if (!starts)
+        for (int r = run - 1; r >= 0; --r) {
+            carry += s_sum[r][lane];
+            if (s_cut[r][lane]) break;
+        }
+    if (run == kPrefixRuns - 1) {
+        bool any = false;
+        for (int r = 0; r < kPrefixRuns; ++r) any |= s_cut[r][lane] != 0;
+        chunk_tot[(size_t)blockIdx.y * D + d] = (cut ? sum : carry + sum) | (any ? kCutBit : 0u);
+    }
+    uint32_t acc = carry;
+    uint32_t m = m0, next = next0;
+#pragma unroll
+    for (int u = 0; u < kPrefixRunTiles; ++u) {
+        if (t0 + u >= t1) break;
+        if (t0 + u == next) {
+            acc = 0;
+            next = next_mesh_tile(segs, ++m);
+        }
+        counts[(size_t)(t0 + u) * D + d] = acc;
+        acc += v[u];
+    }
+}
+
+// In place over the chunk totals: chunk_tot[y][d] -> the segmented sum of the
+// earlier chunks' totals (what a tile of chunk y whose mesh began before the
+// chunk adds to its prefix).  One thread per digit walks the chunks.
+template <int D>
+__global__ void __launch_bounds__(256) k_chunk_carry(uint32_t chunks, uint32_t* __restrict__ chunk_tot) {
+    const uint32_t d = blockIdx.x * 256 + threadIdx.x;
+    if (d >= (uint32_t)D) return;
+    uint32_t acc = 0;
+    for (uint32_t y0 = 0; y0 < chunks; y0 += 8) {
+        uint32_t v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = y0 + u < chunks ? chunk_tot[(size_t)(y0 + u) * D + d] : 0u;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (y0 + u >= chunks) break;
+            chunk_tot[(size_t)(y0 + u) * D + d] = acc;
+            acc = (v[u] & kCutBit) ? (v[u] & ~kCutBit) : acc + v[u];
+        }
+    }
+}
+
+// Stable scatter of one tile: keys of one digit keep their input order
+// (each warp ranks a contiguous run of the tile in order, warps in order).
+// Segmented: keys move only within their mesh (hist holds P x D counts per
+// mesh, prefix the tile's offsets within its chunk from k_tile_prefix,
+// chunk_carry the chunk's carry for tiles whose mesh began before the chunk).  Each
+// thread owns R = D / 256 consecutive digits in the tile-wide steps.
 template <typename K, bool kIota, int BITS>
-__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(
+__global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 4 : 3) k_scatter(
         Segs segs, const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
         uint32_t* __restrict__ vout, int pass, const uint32_t* __restrict__ hist,
-        uint32_t* __restrict__ status, uint32_t* __restrict__ ticket, uint32_t* __restrict__ err) {
+        const uint32_t* __restrict__ prefix, const uint32_t* __restrict__ chunk_carry) {
     using Plan = SortPlan<K, BITS>;
     constexpr int P = Plan::kPasses, D = Plan::kDigits, R = Plan::kPerThread;
     const int shift = BITS * pass;
@@ -241,17 +383,14 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(
     uint32_t* s_dstart = s_wh + kSortWarps * D;  // [D] digit start within the tile
     uint32_t* s_gbase = s_dstart + D;            // [D] output base minus digit start
     __shared__ uint32_t s_scan[kSortWarps];
-    __shared__ uint32_t s_tile;
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
     for (int j = threadIdx.x; j < kSortWarps * D; j += kSortThreads) s_wh[j] = 0;
     __syncthreads();
-    const uint32_t tile = s_tile;
+    const uint32_t tile = blockIdx.x;
     const uint32_t m = segs.seg_of_tile(tile);
-    const uint32_t first_tile = segs.tile_begin(m);
     const uint32_t seg_start = segs.tri_begin(m), seg_end = segs.tri_end(m);
-    const uint32_t base = seg_start + (tile - first_tile) * kSortTile;
+    const uint32_t base = seg_start + (tile - segs.tile_begin(m)) * kSortTile;
     const uint32_t valid_n = min((uint32_t)kSortTile, seg_end - base);
     const uint32_t end = base + valid_n;
 
@@ -266,6 +405,10 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(
         const bool valid = idx < end;
         key[r] = valid ? kin[idx] : (K)0;
         val[r] = kIota ? (uint32_t)idx : (valid ? vin[idx] : 0u);
+    }
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const bool valid = base + (uint32_t)w * (kSortItems * 32) + r * 32 + lane < end;
         const uint32_t d = valid ? (uint32_t)((key[r] >> shift) & (D - 1)) : (uint32_t)D;
         const uint32_t peers = __match_any_sync(kFull, d);
         const uint32_t before = __popc(peers & lt);
@@ -295,58 +438,13 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(
     }
     block_exclusive_scan<R>(count, dstart, s_scan);
     block_exclusive_scan<R>(hv, gdig, s_scan);
-
-    // Decoupled look-back for each owned digit over this mesh's earlier tiles:
-    // publish every aggregate first, then resolve the prefixes.
-    uint32_t* const st = status + (size_t)tile * D + threadIdx.x * R;
-#pragma unroll
-    for (int r = 0; r < R; ++r) __stcg(st + r, (tile == first_tile ? kFlagInc : kFlagAgg) | count[r]);
+    const uint32_t chunk = tile / kPrefixChunk, chunk0 = chunk * kPrefixChunk;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int d = threadIdx.x * R + r;
-        uint32_t prefix = 0;
-        if (tile != first_tile) {
-            // Eight predecessors per poll (tiles before the mesh's first read
-            // as an inclusive zero): add aggregates in order up to the first
-            // inclusive prefix, or stop at the first tile not yet published.
-            constexpr int kWin = 8;
-            int64_t k = (int64_t)tile - 1;
-            uint32_t polls = 0;
-            bool done = false;
-            while (!done) {
-                uint32_t sv[kWin];
-#pragma unroll
-                for (int u = 0; u < kWin; ++u) {
-                    sv[u] = 0x80000000u;  // kFlagInc with value 0
-                    if (k - u >= (int64_t)first_tile)
-                        sv[u] = *reinterpret_cast<volatile uint32_t*>(status + (size_t)(k - u) * D + d);
-                }
-                int used = 0;
-                bool stop = false;
-#pragma unroll
-                for (int u = 0; u < kWin; ++u) {
-                    if (stop || done) continue;
-                    if (sv[u] & kFlagInc) {
-                        prefix += sv[u] & kValueMask;
-                        done = true;
-                    } else if (sv[u] & kFlagAgg) {
-                        prefix += sv[u] & kValueMask;
-                        ++used;
-                    } else {
-                        stop = true;
-                    }
-                }
-                k -= used;
-                if (!done && used == 0 && ++polls > kLookbackLimit) {
-                    set_error_bits(err, kErrSortLookback);
-                    break;
-                }
-            }
-            __threadfence();
-            __stcg(st + r, kFlagInc | (prefix + count[r]));
-        }
         s_dstart[d] = dstart[r];
-        s_gbase[d] = seg_start + gdig[r] + prefix - dstart[r];
+        const uint32_t carry = segs.tile_begin(m) < chunk0 ? chunk_carry[(size_t)chunk * D + d] : 0u;
+        s_gbase[d] = seg_start + gdig[r] + prefix[(size_t)tile * D + d] + carry - dstart[r];
     }
     __syncthreads();
 
@@ -658,61 +756,70 @@ int grid_for(atr_ctx* ctx, uint64_t work, int per_sm_blocks, int threads) {
 // passes the output lands in a second pair of buffers, which then replaces
 // them (*keys and *vals are then separate ctx->alloc allocations that are
 // released: owned = true); with an even number it lands back in place
-// (required when !owned).  hist holds P x D
-// digit counts per mesh when hist_ready; otherwise (single mesh, 8-bit digits
-// only) it is computed here.  With iota the first pass generates the values
-// (global element indices).
+// (required when !owned).  hist holds P x D digit counts per mesh when
+// hist_ready; otherwise (single mesh, 8-bit digits only) it is computed here.
+// tile_counts0, when given, holds the first pass's tile counts (from
+// k_morton; tiles x D) and is consumed.  With iota the first pass generates
+// the values (global element indices).
 template <typename K, int BITS>
 int sort_pairs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, K** keys, uint32_t** vals, uint32_t* hist,
-               bool hist_ready, bool iota, bool owned) {
+               bool hist_ready, bool iota, bool owned, uint32_t* tile_counts0 = nullptr) {
     using Plan = SortPlan<K, BITS>;
     constexpr int P = Plan::kPasses, D = Plan::kDigits;
     static_assert(BITS == 8 || P % 2 == 1, "10-bit plans have an odd pass count");
     ATR_REQUIRE(owned || P % 2 == 0, ATR_ERR_INVALID_ARG, "sort: odd pass count needs owned buffers");
     ATR_REQUIRE(hist_ready || BITS == 8, ATR_ERR_INVALID_ARG, "sort: 10-bit digits need Morton histograms");
     const uint32_t n = segs.n;
-    const size_t sbytes = (size_t)P * tiles * D * 4;
+    const size_t cbytes = align256((size_t)tiles * D * 4);
+    const uint32_t chunks = (tiles + kPrefixChunk - 1) / kPrefixChunk;
+    const size_t tbytes = align256((size_t)chunks * D * 4);
     void* tmp = nullptr;
     void* k2v = nullptr;
     void* v2v = nullptr;
     const size_t hb = hist ? 0 : align256(P * D * 4);
     ATR_TRY(ctx->alloc(&k2v, (size_t)n * sizeof(K)));
     int st = ctx->alloc(&v2v, (size_t)n * 4);
-    if (st == ATR_OK) st = ctx->alloc(&tmp, align256(sbytes) + 256 + hb);
+    if (st == ATR_OK) st = ctx->alloc(&tmp, (tile_counts0 ? 0 : cbytes) + tbytes + hb);
     if (st != ATR_OK) { ctx->release(k2v); ctx->release(v2v); return st; }
     K* k2 = static_cast<K*>(k2v);
     uint32_t* v2 = static_cast<uint32_t*>(v2v);
     char* p = static_cast<char*>(tmp);
-    uint32_t* status = reinterpret_cast<uint32_t*>(p); p += align256(sbytes);
-    uint32_t* tickets = reinterpret_cast<uint32_t*>(p); p += 256;
+    uint32_t* counts = tile_counts0;
+    if (!counts) { counts = reinterpret_cast<uint32_t*>(p); p += cbytes; }
+    uint32_t* chunk_tot = reinterpret_cast<uint32_t*>(p);
+    p += tbytes;
     if (!hist) hist = reinterpret_cast<uint32_t*>(p);
     cudaStream_t s = ctx->stream;
-    cudaError_t e = cudaMemsetAsync(status, 0, align256(sbytes) + 256, s);
-    if (e != cudaSuccess) {
-        ctx->release(tmp);
-        ctx->release(k2v);
-        ctx->release(v2v);
-        return cuda_fail(e, "cudaMemsetAsync", __FILE__, __LINE__);
-    }
+    cudaError_t e = cudaSuccess;
     if (!hist_ready) {
-        cudaMemsetAsync(hist, 0, P * D * 4, s);
-        k_histogram<K><<<grid_for(ctx, n, 4, 256), 256, 0, s>>>(*keys, n, hist);
+        e = cudaMemsetAsync(hist, 0, P * D * 4, s);
+        if (e == cudaSuccess) k_histogram<K><<<grid_for(ctx, n, 4, 256), 256, 0, s>>>(*keys, n, hist);
+        ctx->launches += 1;
     }
     K* ka = *keys; K* kb2 = k2;
     uint32_t* va = *vals; uint32_t* vb2 = v2;
-    for (int pass = 0; pass < P; ++pass) {
-        uint32_t* stp = status + (size_t)pass * tiles * D;
+    const dim3 prefix_grid((unsigned)(D / 32), chunks);
+    for (int pass = 0; pass < P && e == cudaSuccess; ++pass) {
+        if (pass > 0 || !tile_counts0) {
+            k_tile_counts<K, BITS><<<tiles, kSortThreads, 0, s>>>(segs, ka, pass, counts);
+            ctx->launches += 1;
+        }
+        k_tile_prefix<D><<<prefix_grid, 32 * kPrefixRuns, 0, s>>>(segs, tiles, counts, chunk_tot);
+        if (chunks > 1) {
+            k_chunk_carry<D><<<(D + 255) / 256, 256, 0, s>>>(chunks, chunk_tot);
+            ctx->launches += 1;
+        }
         if (pass == 0 && iota)
-            k_onesweep<K, true, BITS><<<tiles, kSortThreads, Plan::kSmem, s>>>(segs, ka, va, kb2, vb2, pass, hist,
-                                                                               stp, tickets + pass, ctx->d_error);
+            k_scatter<K, true, BITS><<<tiles, kSortThreads, Plan::kSmem, s>>>(segs, ka, va, kb2, vb2, pass, hist,
+                                                                              counts, chunk_tot);
         else
-            k_onesweep<K, false, BITS><<<tiles, kSortThreads, Plan::kSmem, s>>>(segs, ka, va, kb2, vb2, pass, hist,
-                                                                                stp, tickets + pass, ctx->d_error);
+            k_scatter<K, false, BITS><<<tiles, kSortThreads, Plan::kSmem, s>>>(segs, ka, va, kb2, vb2, pass, hist,
+                                                                               counts, chunk_tot);
+        ctx->launches += 2;
         std::swap(ka, kb2);
         std::swap(va, vb2);
+        e = cudaGetLastError();
     }
-    ctx->launches += P + (hist_ready ? 0 : 1);
-    e = cudaGetLastError();
     ctx->release(tmp);
     if (P % 2 == 1) {
         // Output in the second pair: hand it to the caller, release the first.
@@ -724,7 +831,7 @@ int sort_pairs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, K** keys, uint32_
         ctx->release(k2v);
         ctx->release(v2v);
     }
-    if (e != cudaSuccess) return cuda_fail(e, "k_onesweep launch", __FILE__, __LINE__);
+    if (e != cudaSuccess) return cuda_fail(e, "sort launch", __FILE__, __LINE__);
     return ATR_OK;
 }
 
@@ -738,26 +845,34 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
     void* iv = nullptr;
     void* aux = nullptr;
     const size_t hbytes = (size_t)segs.count * P * D * 4;
+    const size_t cbytes = (size_t)tiles * D * 4;
     const size_t inner = n - segs.count;
     ATR_TRY(ctx->alloc(&kv, (size_t)n * sizeof(K)));
     int st = ctx->alloc(&iv, (size_t)n * 4);
     const uint32_t bblocks = (n + kBuildBlock - 1) / kBuildBlock;
     const size_t ebytes = (size_t)bblocks * 2 * sizeof(BuildEdge);
-    if (st == ATR_OK) st = ctx->alloc(&aux, align256(hbytes) + align256(inner * 4) + align256(ebytes));
+    if (st == ATR_OK)
+        st = ctx->alloc(&aux, align256(hbytes) + align256(cbytes) + align256(inner * 4) + align256(ebytes));
     if (st != ATR_OK) { ctx->release(kv); ctx->release(iv); return st; }
     K* keys = static_cast<K*>(kv);
     uint32_t* idx = static_cast<uint32_t*>(iv);
-    uint32_t* hist = static_cast<uint32_t*>(aux);
-    int32_t* slot = reinterpret_cast<int32_t*>(static_cast<char*>(aux) + align256(hbytes));
-    BuildEdge* edges = reinterpret_cast<BuildEdge*>(static_cast<char*>(aux) + align256(hbytes) + align256(inner * 4));
-    cudaMemsetAsync(hist, 0, hbytes, s);
+    char* ap = static_cast<char*>(aux);
+    uint32_t* hist = reinterpret_cast<uint32_t*>(ap); ap += align256(hbytes);
+    uint32_t* tile_counts = reinterpret_cast<uint32_t*>(ap); ap += align256(cbytes);
+    int32_t* slot = reinterpret_cast<int32_t*>(ap); ap += align256(inner * 4);
+    BuildEdge* edges = reinterpret_cast<BuildEdge*>(ap);
+    cudaError_t me = cudaMemsetAsync(hist, 0, hbytes, s);
+    if (me != cudaSuccess) {
+        ctx->release(aux); ctx->release(kv); ctx->release(iv);
+        return cuda_fail(me, "cudaMemsetAsync(hist)", __FILE__, __LINE__);
+    }
 
     ctx->phase_begin("morton");
-    k_morton<K, BITS><<<tiles, 256, 0, s>>>(segs, verts, d_bounds, keys, hist);
+    k_morton<K, BITS><<<tiles, 256, 0, s>>>(segs, verts, d_bounds, keys, hist, tile_counts);
     ctx->phase_end();
     ctx->launches += 1;
     ctx->phase_begin("sort");
-    st = sort_pairs<K, BITS>(ctx, segs, tiles, &keys, &idx, hist, true, true, true);
+    st = sort_pairs<K, BITS>(ctx, segs, tiles, &keys, &idx, hist, true, true, true, tile_counts);
     ctx->phase_end();
     if (st == ATR_OK) {
         ctx->phase_begin("build");
@@ -783,20 +898,20 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
 static_assert(kSortTile == (int)kSortTileSize, "sort tile size");
 
 template <typename K, int BITS>
-cudaError_t onesweep_attrs() {
+cudaError_t scatter_attrs() {
     const int smem = (int)SortPlan<K, BITS>::kSmem;
-    cudaError_t e = cudaFuncSetAttribute(k_onesweep<K, true, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(k_scatter<K, true, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_onesweep<K, false, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        e = cudaFuncSetAttribute(k_scatter<K, false, BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     return e;
 }
 
 // Kernel attributes, set once per context before any capture.
 int lbvh_prepare() {
-    ATR_CUDA((onesweep_attrs<uint32_t, 8>()));
-    ATR_CUDA((onesweep_attrs<uint32_t, 10>()));
-    ATR_CUDA((onesweep_attrs<uint64_t, 8>()));
-    ATR_CUDA((onesweep_attrs<uint64_t, 10>()));
+    ATR_CUDA((scatter_attrs<uint32_t, 8>()));
+    ATR_CUDA((scatter_attrs<uint32_t, 10>()));
+    ATR_CUDA((scatter_attrs<uint64_t, 8>()));
+    ATR_CUDA((scatter_attrs<uint64_t, 10>()));
     return ATR_OK;
 }
 
@@ -822,6 +937,7 @@ int prepass_alloc(atr_ctx* ctx, size_t total_nodes, size_t inner, void** block, 
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds, int morton_bits,
                     atr_tree* t) {
     t->morton_bits = morton_bits;
+    tree_topology_changed(t);
     Segs segs{nullptr, nullptr, 1u, n};
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
     TreeOut out{t->parent, t->left, t->right, t->data, t->bmin, t->bmax, t->area, t->range};
@@ -948,6 +1064,12 @@ int atr_refit(atr_ctx* ctx, atr_tree* tree, const atr_scene* scene) {
     tree->prepass_block = nullptr;
     tree->prepass = BuildPrepass{};
     const TreeOut t{tree->parent, tree->left, tree->right, tree->data, tree->bmin, tree->bmax, tree->area};
+    if (!tree->refit_plan && !tree->no_refit_plan) {
+        const int st = refit_plan_build(ctx, tree->n, t, &tree->refit_plan);
+        if (st == ATR_ERR_UNSUPPORTED) tree->no_refit_plan = true;
+        else if (st != ATR_OK) return st;
+    }
+    if (tree->refit_plan) return refit_plan_run(ctx, *tree->refit_plan, t, scene->verts);
     return refit_arrays(ctx, tree->n, t, scene->verts);
 }
 
@@ -965,10 +1087,10 @@ int atr_device_morton(atr_ctx* ctx, const float* vertices, uint32_t n, const flo
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
     if (morton_bits == 30)
         k_morton<uint32_t, 8><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
-                                                              static_cast<uint32_t*>(keys), nullptr);
+                                                              static_cast<uint32_t*>(keys), nullptr, nullptr);
     else
         k_morton<uint64_t, 8><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
-                                                              static_cast<uint64_t*>(keys), nullptr);
+                                                              static_cast<uint64_t*>(keys), nullptr, nullptr);
     ctx->launches += 1;
     cudaError_t e = cudaStreamSynchronize(ctx->stream);  // h is a stack array
     ctx->release(b);

@@ -163,6 +163,7 @@ int atr_plan_run(atr_ctx* ctx, atr_plan* P, int use_graph) {
     ATR_REQUIRE(ctx == P->ctx, ATR_ERR_INVALID_ARG, "atr_plan_run: the plan belongs to another context");
     atr_tree* t = P->tree;
     // Allocations an earlier eager run left on the tree go before any capture.
+    tree_topology_changed(t);
     ctx->release(t->prepass_block);
     t->prepass_block = nullptr;
     t->prepass = BuildPrepass{};

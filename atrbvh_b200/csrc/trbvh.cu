@@ -355,6 +355,7 @@ extern "C" int atr_optimize_trbvh(atr_ctx* ctx, atr_tree* tree, int tsize, int i
     TreeRefs g{n, tree->parent, tree->left, tree->right, tree->bmin, tree->bmax, tree->area, nullptr};
     Segs segs{nullptr, nullptr, 1u, n};
     tree->karras = false;
+    tree_topology_changed(tree);
     ctx->release(tree->prepass_block);
     tree->prepass_block = nullptr;
     tree->prepass = BuildPrepass{};
