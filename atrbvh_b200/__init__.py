@@ -164,6 +164,8 @@ _SIGS = [
     ("atr_scene_device_vertices", C.c_int, [_p, C.POINTER(_p), C.POINTER(C.c_uint32)]),
     ("atr_scene_set_vertices", C.c_int, [_p, _p, _p, C.c_int]),
     ("atr_build_lbvh", C.c_int, [_p, _p, C.c_int, C.POINTER(_p)]),
+    ("atr_build_lbvh_split", C.c_int, [_p, C.c_uint32, _p, _p, _p, _f32p, _f32p, C.c_int, C.POINTER(_p)]),
+    ("atr_split_triangles", C.c_int, [_p, _p, C.c_float, C.c_uint32, _p, _p, _p, C.POINTER(C.c_uint32)]),
     ("atr_tree_destroy", C.c_int, [_p]),
     ("atr_tree_view_get", C.c_int, [_p, C.POINTER(TreeView)]),
     ("atr_tree_download", C.c_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p]),
@@ -519,6 +521,34 @@ class LBVHBuilder:
         h = C.c_void_p()
         check(lib().atr_build_lbvh(scene.ctx.handle, scene.handle, self.bits, C.byref(h)))
         return BVHTree(scene.ctx, h, scene.n)
+
+
+def split_triangles(scene: SceneWrapper, split_ratio: float = 0.3, max_primitives: int | None = None):
+    """Triangle splitting (atr_split_triangles): up to split_ratio * n extra
+    primitives for the triangles whose boxes waste the most surface.  Returns
+    device tensors (bmin float32 [P, 4], bmax float32 [P, 4], data int32 [P])
+    of the fragments, fragments of one triangle together in triangle order."""
+    import torch
+    cap = max_primitives if max_primitives is not None else scene.n + int(split_ratio * scene.n) + 1
+    bmin = torch.empty((cap, 4), dtype=torch.float32, device="cuda")
+    bmax = torch.empty((cap, 4), dtype=torch.float32, device="cuda")
+    data = torch.empty(cap, dtype=torch.int32, device="cuda")
+    cnt = C.c_uint32()
+    check(lib().atr_split_triangles(scene.ctx.handle, scene.handle, split_ratio, cap, bmin.data_ptr(),
+                                    bmax.data_ptr(), data.data_ptr(), C.byref(cnt)))
+    n = cnt.value
+    return bmin[:n], bmax[:n], data[:n]
+
+
+def build_lbvh_split(ctx: Context, bmin, bmax, data, scene_bmin, scene_bmax, bits: int = 30) -> BVHTree:
+    """The triangle-splitting LBVH (atr_build_lbvh_split) over primitive boxes
+    (contiguous device tensors: float32 [P, 4] twice, int32 [P]) in the box
+    scene_bmin..scene_bmax."""
+    n = int(data.shape[0])
+    h = C.c_void_p()
+    check(lib().atr_build_lbvh_split(ctx.handle, n, bmin.data_ptr(), bmax.data_ptr(), data.data_ptr(),
+                                     _f3(scene_bmin), _f3(scene_bmax), bits, C.byref(h)))
+    return BVHTree(ctx, h, n)
 
 
 class AgglomerativeTreeletOptimizer:

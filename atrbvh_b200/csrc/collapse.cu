@@ -263,6 +263,7 @@ int atr_collapse(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int max
     ctx->phase_begin("collapse");
     if (st == ATR_OK) st = collapse_into(ctx, tree, ci, ct, max_leaf, c, parts);
     ctx->phase_end();
+    c->split = tree->split;
     if (st == ATR_OK && sah) {
         float h[2];
         cudaError_t e = cudaMemcpyAsync(h, parts, 8, cudaMemcpyDeviceToHost, ctx->stream);

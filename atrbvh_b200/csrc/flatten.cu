@@ -444,7 +444,8 @@ extern "C" {
 
 int atr_flatten_compact2(atr_ctx* ctx, const atr_collapsed* c, const atr_scene* scene, atr_compact** out) {
     ATR_REQUIRE(ctx && c && scene && out, ATR_ERR_INVALID_ARG, "atr_flatten_compact2: NULL argument");
-    ATR_REQUIRE(c->n == scene->n, ATR_ERR_INVALID_ARG, "atr_flatten_compact2: tree/scene size mismatch");
+    ATR_REQUIRE(c->n == scene->n || c->split, ATR_ERR_INVALID_ARG,
+                "atr_flatten_compact2: tree/scene size mismatch");
     *out = nullptr;
     const uint32_t n = c->n;
     atr_compact* cp = new atr_compact();

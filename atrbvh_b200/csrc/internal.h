@@ -62,6 +62,17 @@ struct BuildPrepass {
     int gamma = 0;
     const uint8_t* seg_gamma = nullptr;  // per-mesh gamma (device), in place of gamma when set
 };
+// Primitive boxes of a triangle-splitting build (BVHRT-Core/src/LBVH.cu:99-161,
+// 320-428, 572-669): one box per primitive (a triangle or a fragment of one)
+// and the triangle it belongs to.  When bmin is set the LBVH build takes
+// Morton codes from the boxes' centroids, leaf boxes from the boxes and leaf
+// data indices from `data`, in place of the triangles' vertices.
+struct PrimBoxes {
+    const float4* bmin = nullptr;
+    const float4* bmax = nullptr;
+    const uint32_t* data = nullptr;
+};
+
 constexpr float kPrepassCi = 1.2f;  // AgglomerativeTreelet.h:75 defaults
 constexpr float kPrepassCt = 1.0f;
 constexpr int kPrepassGamma = 9;    // AgglomerativeTreeletOptimizer.h:24 default treelet size
@@ -158,16 +169,24 @@ struct atr_tree {
     void* sorted_keys = nullptr;
     uint32_t* sorted_idx = nullptr;
     int morton_bits = 30;
-    // Refit plan of the current topology (built by the first refit; released
+    // Refit plan of the current topology (built by the second refit of the
+    // topology -- a topology refit once never pays for a plan; released
     // whenever the topology changes).  no_refit_plan: the topology has no
     // plan (too deep a top); refits climb instead.
     atr::RefitPlan* refit_plan = nullptr;
     bool no_refit_plan = false;
+    int refits = 0;  // refits of the current topology
+    // Leaves are primitive boxes of a triangle-splitting build (a refit from
+    // whole triangles would not reproduce them).
+    bool split = false;
 };
 
 struct atr_collapsed {
     atr_ctx* ctx = nullptr;
     uint32_t n = 0;
+    // Collapsed from a triangle-splitting build: n counts primitives, and the
+    // data indices name triangles of the scene the primitives were split from.
+    bool split = false;
     void* block = nullptr;
     int32_t *parent = nullptr, *left = nullptr, *right = nullptr, *data = nullptr, *count = nullptr;
     float4 *bmin = nullptr, *bmax = nullptr;
@@ -240,13 +259,14 @@ int collapse_into(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int ma
 
 // Single-mesh LBVH into an allocated tree (keeps the sort output).
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds,
-                    int morton_bits, atr_tree* t);
+                    int morton_bits, atr_tree* t, const PrimBoxes* prims = nullptr);
 // LBVH of every mesh of segs (tiles = sort tiles over all meshes); bounds
 // holds 6 floats per mesh.  keep_keys/keep_idx (may be NULL) receive the
 // sorted keys and global triangle order.
 int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts,
                     const float* d_bounds, int morton_bits, const TreeOut& out, void** keep_keys,
-                    uint32_t** keep_idx, const BuildPrepass* prepass = nullptr);
+                    uint32_t** keep_idx, const BuildPrepass* prepass = nullptr,
+                    const PrimBoxes* prims = nullptr);
 // Allocate the prepass arrays for total_nodes nodes and inner internal nodes
 // in one block (*block receives the allocation).
 int prepass_alloc(atr_ctx* ctx, size_t total_nodes, size_t inner, void** block, BuildPrepass* pp);

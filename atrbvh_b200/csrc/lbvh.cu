@@ -134,7 +134,8 @@ __device__ __forceinline__ uint64_t morton_code<uint64_t>(float cx, float cy, fl
 template <typename K, int BITS>
 __global__ void __launch_bounds__(256) k_morton(Segs segs, const float4* __restrict__ v,
                                                  const float* __restrict__ bounds, K* __restrict__ keys,
-                                                 uint32_t* __restrict__ hist, uint32_t* __restrict__ tile_counts) {
+                                                 uint32_t* __restrict__ hist, uint32_t* __restrict__ tile_counts,
+                                                 PrimBoxes pr) {
     constexpr int P = SortPlan<K, BITS>::kPasses, D = SortPlan<K, BITS>::kDigits;
     __shared__ uint32_t sh[P * D];
     __shared__ float sb[6];
@@ -145,10 +146,20 @@ __global__ void __launch_bounds__(256) k_morton(Segs segs, const float4* __restr
     if (threadIdx.x < 6) sb[threadIdx.x] = bounds[6 * m + threadIdx.x];
     __syncthreads();
     for (uint32_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
-        const float4 a = __ldg(v + 3 * (size_t)t), b = __ldg(v + 3 * (size_t)t + 1), c = __ldg(v + 3 * (size_t)t + 2);
-        const float cx = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.x, b.x), c.x), fminf(fminf(a.x, b.x), c.x)), 0.5f);
-        const float cy = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.y, b.y), c.y), fminf(fminf(a.y, b.y), c.y)), 0.5f);
-        const float cz = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.z, b.z), c.z), fminf(fminf(a.z, b.z), c.z)), 0.5f);
+        float cx, cy, cz;
+        if (pr.bmin) {
+            // A primitive box's centroid, (min + max) / 2 (LBVH.cu:41-49; the
+            // halving is exact, so it equals the product by 0.5).
+            const float4 lo = __ldg(pr.bmin + t), hi = __ldg(pr.bmax + t);
+            cx = __fmul_rn(__fadd_rn(lo.x, hi.x), 0.5f);
+            cy = __fmul_rn(__fadd_rn(lo.y, hi.y), 0.5f);
+            cz = __fmul_rn(__fadd_rn(lo.z, hi.z), 0.5f);
+        } else {
+            const float4 a = __ldg(v + 3 * (size_t)t), b = __ldg(v + 3 * (size_t)t + 1), c = __ldg(v + 3 * (size_t)t + 2);
+            cx = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.x, b.x), c.x), fminf(fminf(a.x, b.x), c.x)), 0.5f);
+            cy = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.y, b.y), c.y), fminf(fminf(a.y, b.y), c.y)), 0.5f);
+            cz = __fmul_rn(__fadd_rn(fmaxf(fmaxf(a.z, b.z), c.z), fminf(fminf(a.z, b.z), c.z)), 0.5f);
+        }
         const K code = morton_code<K>(cx, cy, cz, sb);
         keys[t] = code;
         if (hist) {
@@ -535,7 +546,7 @@ template <typename K>
 __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K* __restrict__ keys_all,
                                                              const uint32_t* __restrict__ sidx,
                                                              const float4* __restrict__ verts, BuildOut<K> o,
-                                                             BuildEdge* __restrict__ edges) {
+                                                             BuildEdge* __restrict__ edges, PrimBoxes pr) {
     __shared__ float4 s_lmn[kBuildBlock], s_lmx[kBuildBlock], s_imn[kBuildBlock], s_imx[kBuildBlock];
     __shared__ float s_lns[kBuildBlock], s_ins[kBuildBlock];
     __shared__ int s_ilv[kBuildBlock];  // prepass levels of the block's finished internal nodes
@@ -563,14 +574,27 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
         last = (int)n - 1;
         keys = keys_all + s0;
         const uint32_t gtri = sidx[gi];
-        const float4 a = __ldg(verts + 3 * (size_t)gtri), b = __ldg(verts + 3 * (size_t)gtri + 1),
-                     c = __ldg(verts + 3 * (size_t)gtri + 2);
-        mn = make_float4(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z), 0.0f);
-        mx = make_float4(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z), 0.0f);
+        int32_t dat;
+        if (pr.bmin) {
+            // A primitive's leaf: its box and its triangle (LBVH.cu:372-397,
+            // :600-611 through the routing index).
+            const float4 lo = __ldg(pr.bmin + gtri), hi = __ldg(pr.bmax + gtri);
+            mn = make_float4(lo.x, lo.y, lo.z, 0.0f);
+            mx = make_float4(hi.x, hi.y, hi.z, 0.0f);
+            dat = (int32_t)__ldg(pr.data + gtri);
+        } else {
+            const float4 a = __ldg(verts + 3 * (size_t)gtri), b = __ldg(verts + 3 * (size_t)gtri + 1),
+                         c = __ldg(verts + 3 * (size_t)gtri + 2);
+            mn = make_float4(fminf(fminf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z),
+                             0.0f);
+            mx = make_float4(fmaxf(fmaxf(a.x, b.x), c.x), fmaxf(fmaxf(a.y, b.y), c.y), fmaxf(fmaxf(a.z, b.z), c.z),
+                             0.0f);
+            dat = (int32_t)(gtri - s0);
+        }
         const int leaf = (int)i + last;
         o.left[nb + leaf] = -1;
         o.right[nb + leaf] = -1;
-        o.data[nb + leaf] = (int32_t)(gtri - s0);
+        o.data[nb + leaf] = dat;
         o.bmin[nb + leaf] = mn;
         o.bmax[nb + leaf] = mx;
         const float my_area = box_area(mn, mx);
@@ -837,7 +861,8 @@ int sort_pairs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, K** keys, uint32_
 
 template <typename K, int BITS>
 int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts, const float* d_bounds,
-                const TreeOut& t, void** keep_keys, uint32_t** keep_idx, const BuildPrepass* prepass) {
+                const TreeOut& t, void** keep_keys, uint32_t** keep_idx, const BuildPrepass* prepass,
+                const PrimBoxes& pr) {
     constexpr int P = SortPlan<K, BITS>::kPasses, D = SortPlan<K, BITS>::kDigits;
     const uint32_t n = segs.n;
     cudaStream_t s = ctx->stream;
@@ -868,7 +893,7 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
     }
 
     ctx->phase_begin("morton");
-    k_morton<K, BITS><<<tiles, 256, 0, s>>>(segs, verts, d_bounds, keys, hist, tile_counts);
+    k_morton<K, BITS><<<tiles, 256, 0, s>>>(segs, verts, d_bounds, keys, hist, tile_counts, pr);
     ctx->phase_end();
     ctx->launches += 1;
     ctx->phase_begin("sort");
@@ -879,7 +904,7 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
         const BuildOut<K> o{t.parent, t.left,  t.right, t.data,
                             t.bmin,   t.bmax,  t.area,  slot,
                             t.range,  prepass ? *prepass : BuildPrepass{}};
-        k_build_block<K><<<bblocks, kBuildBlock, 0, s>>>(segs, keys, idx, verts, o, edges);
+        k_build_block<K><<<bblocks, kBuildBlock, 0, s>>>(segs, keys, idx, verts, o, edges, pr);
         k_build_top<K><<<(2 * bblocks + 255) / 256, 256, 0, s>>>(segs, keys, o, edges, 2 * bblocks);
         ctx->phase_end();
         ctx->launches += 2;
@@ -917,13 +942,14 @@ int lbvh_prepare() {
 
 int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* verts, const float* d_bounds,
                     int morton_bits, const TreeOut& out, void** keep_keys, uint32_t** keep_idx,
-                    const BuildPrepass* pp) {
+                    const BuildPrepass* pp, const PrimBoxes* prims) {
     const bool ten = ctx->sort_bits == 10;
+    const PrimBoxes pr = prims ? *prims : PrimBoxes{};
     if (morton_bits == 30)
-        return ten ? build_typed<uint32_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp)
-                   : build_typed<uint32_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp);
-    return ten ? build_typed<uint64_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp)
-               : build_typed<uint64_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp);
+        return ten ? build_typed<uint32_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp, pr)
+                   : build_typed<uint32_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp, pr);
+    return ten ? build_typed<uint64_t, 10>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp, pr)
+               : build_typed<uint64_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp, pr);
 }
 
 int prepass_alloc(atr_ctx* ctx, size_t total_nodes, size_t inner, void** block, BuildPrepass* pp) {
@@ -935,8 +961,9 @@ int prepass_alloc(atr_ctx* ctx, size_t total_nodes, size_t inner, void** block, 
 }
 
 int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* d_bounds, int morton_bits,
-                    atr_tree* t) {
+                    atr_tree* t, const PrimBoxes* prims) {
     t->morton_bits = morton_bits;
+    t->split = prims != nullptr;
     tree_topology_changed(t);
     Segs segs{nullptr, nullptr, 1u, n};
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
@@ -950,7 +977,7 @@ int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* 
     if (ctx->atr_levels > 0)
         ATR_TRY(prepass_alloc(ctx, 2 * (size_t)n - 1, n - 1, &t->prepass_block, &t->prepass));
     ATR_TRY(lbvh_build_segs(ctx, segs, tiles, verts, d_bounds, morton_bits, out, &keys, &idx,
-                            t->prepass_block ? &t->prepass : nullptr));
+                            t->prepass_block ? &t->prepass : nullptr, prims));
     ctx->release(t->sorted_keys);
     ctx->release(t->sorted_idx);
     t->sorted_keys = keys;
@@ -1055,8 +1082,37 @@ int atr_build_lbvh(atr_ctx* ctx, const atr_scene* scene, int morton_bits, atr_tr
     return ATR_OK;
 }
 
+int atr_build_lbvh_split(atr_ctx* ctx, uint32_t num_primitives, const float* prim_bmin, const float* prim_bmax,
+                         const uint32_t* data_indices, const float* scene_bmin, const float* scene_bmax,
+                         int morton_bits, atr_tree** out) {
+    ATR_REQUIRE(ctx && prim_bmin && prim_bmax && data_indices && scene_bmin && scene_bmax && out,
+                ATR_ERR_INVALID_ARG, "atr_build_lbvh_split: NULL argument");
+    ATR_REQUIRE(num_primitives >= 2 && num_primitives < (1u << 30), ATR_ERR_INVALID_ARG,
+                "atr_build_lbvh_split: primitive count %u outside [2, 2^30)", num_primitives);
+    ATR_REQUIRE(morton_bits == 30 || morton_bits == 63, ATR_ERR_UNSUPPORTED,
+                "atr_build_lbvh_split: morton_bits must be 30 or 63 (got %d)", morton_bits);
+    *out = nullptr;
+    atr_tree* t = nullptr;
+    ATR_TRY(tree_alloc(ctx, num_primitives, &t));
+    float* d_bounds = nullptr;
+    int st = ctx->alloc(reinterpret_cast<void**>(&d_bounds), 256);
+    if (st != ATR_OK) { atr_tree_destroy(t); return st; }
+    k_set_bounds<<<1, 1, 0, ctx->stream>>>(d_bounds, scene_bmin[0], scene_bmin[1], scene_bmin[2], scene_bmax[0],
+                                           scene_bmax[1], scene_bmax[2]);
+    ctx->launches += 1;
+    const PrimBoxes pr{reinterpret_cast<const float4*>(prim_bmin), reinterpret_cast<const float4*>(prim_bmax),
+                       data_indices};
+    st = lbvh_build_into(ctx, nullptr, num_primitives, d_bounds, morton_bits, t, &pr);
+    ctx->release(d_bounds);
+    if (st != ATR_OK) { atr_tree_destroy(t); return st; }
+    *out = t;
+    return ATR_OK;
+}
+
 int atr_refit(atr_ctx* ctx, atr_tree* tree, const atr_scene* scene) {
     ATR_REQUIRE(ctx && tree && scene, ATR_ERR_INVALID_ARG, "atr_refit: NULL argument");
+    ATR_REQUIRE(!tree->split, ATR_ERR_UNSUPPORTED,
+                "atr_refit: the tree's leaves are primitive boxes of a triangle-splitting build (rebuild it)");
     ATR_REQUIRE(tree->n == scene->n, ATR_ERR_INVALID_ARG, "atr_refit: tree has %u triangles, scene %u",
                 tree->n, scene->n);
     // New boxes make the build's prepass (areas, costs) stale.
@@ -1064,7 +1120,7 @@ int atr_refit(atr_ctx* ctx, atr_tree* tree, const atr_scene* scene) {
     tree->prepass_block = nullptr;
     tree->prepass = BuildPrepass{};
     const TreeOut t{tree->parent, tree->left, tree->right, tree->data, tree->bmin, tree->bmax, tree->area};
-    if (!tree->refit_plan && !tree->no_refit_plan) {
+    if (!tree->refit_plan && !tree->no_refit_plan && ++tree->refits >= 2) {
         const int st = refit_plan_build(ctx, tree->n, t, &tree->refit_plan);
         if (st == ATR_ERR_UNSUPPORTED) tree->no_refit_plan = true;
         else if (st != ATR_OK) return st;
@@ -1087,10 +1143,12 @@ int atr_device_morton(atr_ctx* ctx, const float* vertices, uint32_t n, const flo
     const uint32_t tiles = (n + kSortTile - 1) / kSortTile;
     if (morton_bits == 30)
         k_morton<uint32_t, 8><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
-                                                              static_cast<uint32_t*>(keys), nullptr, nullptr);
+                                                              static_cast<uint32_t*>(keys), nullptr, nullptr,
+                                                              PrimBoxes{});
     else
         k_morton<uint64_t, 8><<<tiles, 256, 0, ctx->stream>>>(segs, v, static_cast<float*>(b),
-                                                              static_cast<uint64_t*>(keys), nullptr, nullptr);
+                                                              static_cast<uint64_t*>(keys), nullptr, nullptr,
+                                                              PrimBoxes{});
     ctx->launches += 1;
     cudaError_t e = cudaStreamSynchronize(ctx->stream);  // h is a stack array
     ctx->release(b);

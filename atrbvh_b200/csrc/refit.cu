@@ -20,10 +20,11 @@
 // climb over global memory (the same unions of the same boxes; min/max are
 // exact) and the areas are computed from them in the same order.
 //
-// A plan depends only on the topology.  It is built on the first refit after
+// A plan depends only on the topology.  It is built on the second refit after
 // a build or an optimiser changed the topology (that call synchronises the
-// context's stream while it builds the plan) and reused by every later
-// refit of the same tree.
+// context's stream while it builds the plan; the first refit climbs over
+// global memory, so a topology refit only once never pays for a plan) and
+// reused by every later refit of the same tree.
 
 #include <vector>
 
@@ -319,6 +320,7 @@ void tree_topology_changed(atr_tree* t) {
     refit_plan_free(t->ctx, t->refit_plan);
     t->refit_plan = nullptr;
     t->no_refit_plan = false;
+    t->refits = 0;
 }
 
 void refit_plan_free(atr_ctx* ctx, RefitPlan* p) {

@@ -55,6 +55,7 @@ WORKLOAD = ("clustered scene 4,194,304 tris (75% 64-Gaussian mixture, 25% 1024x5
 # writes subtree count and nodesSah (8 B x 2) and a child record and counter per
 # internal node (24 B).
 BYTES_PER_TRI = {"morton": 56.0, "sort": 4.0 + 16.0 * 4, "build": 40.0 + 180.0, "atrbvh": 2 * 136.0}
+REFIT_BYTES_PER_TRI = 180.0  # vertex gather 48, dataIndex 4, parents 8, boxes 64, areas 8, counters 8, siblings 32, children 8
 # DRAM bytes per triangle of the ATRBVH phase (both iterations) from an ncu
 # capture of this bench step at 2,097,152 triangles (dram__bytes_read.sum +
 # dram__bytes_write.sum: k_levels_pp_hist 111.8 MB, k_level_hist 19.3,
@@ -326,6 +327,11 @@ def run_ours(args, world, rank, local):
                      "equal": bool(np.float32(got_tree) == np.float32(gold["tree_sah"])
                                    and np.float32(got_col) == np.float32(gold["collapsed_sah"]))}
 
+    # ---- standalone refit of a resident LBVH + ATRBVH(9,2) tree (the serving
+    # primitive): atr_refit from the scene's device vertices, K repetitions
+    # after warm-up (the first refit builds the topology's refit plan) ----
+    refit = measure_refit(ctx, stream, scene, n_tris, world, reps=max(20, args.steps // 4))
+
     # ---- e2e through the public API from pinned host memory ----
     # Each step: atr_scene_create from pinned host vertices with the host scene
     # box (as the reference's SceneWrapper takes it) -> atr_build_lbvh ->
@@ -437,6 +443,7 @@ def run_ours(args, world, rank, local):
         "clocks": clk,
         "sustained": sustained,
         "sah_check": sah_check,
+        "refit": refit,
     }
     plan.close()
     scene.close()
@@ -453,6 +460,34 @@ def run_ours(args, world, rank, local):
     if rank == 0:
         print(json.dumps(out), flush=True)
     ctx.close()
+
+
+def measure_refit(ctx, stream, scene, n_tris: int, world: int, reps: int) -> dict:
+    """Device time of atr_refit on a resident LBVH + ATRBVH(9,2) tree of the scene
+    (CUDA events on the library's stream, mean of reps after three warm-up
+    refits), as GB/s of the refit's algorithmic bytes."""
+    import torch
+    import atrbvh_b200 as ab
+    tree = ab.LBVHBuilder().BuildTree(scene)
+    ab.AgglomerativeTreeletOptimizer(9, 2).Optimize(tree)
+    for _ in range(3):
+        ab.Refit(tree, scene)
+    ctx.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        ab.Refit(tree, scene)
+    e1.record(stream)
+    ctx.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / reps, world)
+    tree.close()
+    peaks = _read_peaks()
+    gbs = n_tris * REFIT_BYTES_PER_TRI / (ms * 1e-3) / 1e9
+    return {"ms": ms, "mtri_per_s": world * n_tris / (ms * 1e-3) / 1e6, "gbs": gbs,
+            "frac_of_hbm": gbs / peaks["hbm_gbs"], "bytes_per_tri": REFIT_BYTES_PER_TRI, "reps": reps,
+            "tree": "LBVH 30-bit + ATRBVH(9,2) of the workload scene, refit in place from its device vertices"}
 
 
 BATCH_MESHES = 4096

@@ -159,6 +159,35 @@ int atr_scene_set_vertices(atr_ctx* ctx, atr_scene* scene, const float* vertices
  * (BVHRT-Core/src/LBVHBuilder.h:31, LBVHBuilder.cpp:21-130).  morton_bits is
  * 30 (LBVHBuilder(false)) or 63 (LBVHBuilder(true)). */
 int atr_build_lbvh(atr_ctx* ctx, const atr_scene* scene, int morton_bits, atr_tree** out);
+/* The triangle-splitting LBVH: the reference's primitive-box path
+ * (BVHRT-Core/src/LBVH.h:36-68 generateMortonCodes(64)TSKernel, :96-124
+ * buildTreeTSKernel, :140-155 calculateNodeBoundingBoxesTSKernel; LBVH.cu:
+ * 99-161, 320-428, 572-669), which no builder of the reference calls.  One
+ * leaf per primitive: Morton codes from the primitive boxes' centroids
+ * normalised to the scene box, leaf boxes from the primitive boxes, leaf data
+ * indices from data_indices (the triangle each primitive belongs to; several
+ * leaves may name one triangle).  prim_bmin / prim_bmax: num_primitives
+ * float4 each and data_indices: device pointers; scene_bmin / scene_bmax:
+ * 3 host floats.  The tree then optimises, collapses and flattens (with the
+ * scene of the triangles) as any other; atr_refit rejects it
+ * (ATR_ERR_UNSUPPORTED), since its leaves are not whole triangles. */
+int atr_build_lbvh_split(atr_ctx* ctx, uint32_t num_primitives, const float* prim_bmin,
+                         const float* prim_bmax, const uint32_t* data_indices,
+                         const float* scene_bmin, const float* scene_bmax, int morton_bits,
+                         atr_tree** out);
+/* Triangle splitting for atr_build_lbvh_split (no counterpart in the
+ * reference, which has the primitive-box build but no step that makes the
+ * boxes).  Up to split_ratio * n extra primitives (at most max_primitives in
+ * all, at most 8 per triangle) are shared out by how much box surface each
+ * triangle wastes; each split triangle is bisected at the middle of the
+ * longest axis of its largest fragment, and every fragment gets the tight
+ * box of the triangle clipped to its region.  Writes the fragments' boxes
+ * (float4, w = 0) and triangle indices to the device buffers (room for
+ * max_primitives), fragments of one triangle together in triangle order,
+ * and their count to *num_primitives (host; synchronises the context). */
+int atr_split_triangles(atr_ctx* ctx, const atr_scene* scene, float split_ratio,
+                        uint32_t max_primitives, float* prim_bmin, float* prim_bmax,
+                        uint32_t* data_indices, uint32_t* num_primitives);
 int atr_tree_destroy(atr_tree* tree);
 /* BVHTreeInstanceManager::FreeDeviceTree (BVHTreeInstanceManager.h:67). */
 int atr_tree_view_get(const atr_tree* tree, atr_tree_view* view);

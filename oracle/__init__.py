@@ -72,6 +72,10 @@ def lib() -> C.CDLL:
         for f in (L.orc_gen_scene, L.orc_gen_rays_pinhole, L.orc_gen_rays_random, L.orc_gen_batch_sizes,
                   L.orc_gen_batch_scene):
             f.restype = C.c_int
+        L.orc_build_lbvh_split.argtypes = [C.c_uint32, _p, _p, _p, _p, _p, C.c_int] + [_p] * 7 + [C.c_int]
+        L.orc_build_lbvh_split.restype = C.c_int
+        L.orc_split_triangles.argtypes = [_p, C.c_uint32, C.c_float, C.c_uint32, _p, _p, _p]
+        L.orc_split_triangles.restype = C.c_int64
     return _lib
 
 
@@ -157,6 +161,39 @@ def build_lbvh(v: np.ndarray, bbmin, bbmax, bits: int = 30, threads: int = 1):
     if rc != 0:
         raise ValueError(f"orc_build_lbvh rc={rc}")
     return t, sk, si
+
+
+def split_triangles(v: np.ndarray, split_ratio: float, max_prims: int | None = None):
+    """The triangle-splitting pre-pass restated: (bmin float4[P], bmax float4[P],
+    data uint32[P]) of the fragments, in triangle order."""
+    v = np.ascontiguousarray(v, np.float32)
+    n = v.shape[0]
+    cap = max_prims if max_prims is not None else n * 8
+    bmin = np.zeros((cap, 4), np.float32)
+    bmax = np.zeros((cap, 4), np.float32)
+    data = np.zeros(cap, np.uint32)
+    cnt = lib().orc_split_triangles(_ptr(v), n, split_ratio, cap, _ptr(bmin), _ptr(bmax), _ptr(data))
+    if cnt < 0:
+        raise ValueError("orc_split_triangles: no room")
+    return bmin[:cnt].copy(), bmax[:cnt].copy(), data[:cnt].copy()
+
+
+def build_lbvh_split(bmin4: np.ndarray, bmax4: np.ndarray, data: np.ndarray, bbmin, bbmax, bits: int = 30,
+                     threads: int = 1) -> "Tree":
+    """The reference's primitive-box LBVH (LBVH.cu:99-161, 320-428, 572-669)
+    restated: one leaf per primitive box."""
+    bmin4 = np.ascontiguousarray(bmin4, np.float32)
+    bmax4 = np.ascontiguousarray(bmax4, np.float32)
+    data = np.ascontiguousarray(data, np.uint32)
+    n = len(data)
+    t = Tree.empty(n)
+    mn = np.asarray(bbmin, np.float32)
+    mx = np.asarray(bbmax, np.float32)
+    rc = lib().orc_build_lbvh_split(n, _ptr(bmin4), _ptr(bmax4), _ptr(data), _ptr(mn), _ptr(mx), bits, *t.ptrs(),
+                                    threads)
+    if rc != 0:
+        raise ValueError(f"orc_build_lbvh_split rc={rc}")
+    return t
 
 
 def atrbvh(t: Tree, treelet: int = 9, iterations: int = 2, ci: float = 1.2, ct: float = 1.0,
@@ -353,6 +390,8 @@ def ref_host_lib() -> C.CDLL:
             f.restype = C.c_float
         L.ref_host_sah.argtypes = [C.c_uint, _p, C.c_float, C.c_float]
         L.ref_host_sah.restype = C.c_float
+        L.ref_host_lbvh_ts.argtypes = [C.c_uint, _p, _p, _p, _p, _p, C.c_int] + [_p] * 7
+        L.ref_host_lbvh_ts.restype = C.c_int
         _ref_host = L
     return _ref_host
 
@@ -381,6 +420,21 @@ def ref_host_run(v: np.ndarray, bbmin, bbmax, *, use64=False, optimizer=0, treel
     if c is not None:
         c.sah = float(sah_out[0])
     return t, c, times
+
+
+def ref_host_lbvh_split(bmin4: np.ndarray, bmax4: np.ndarray, data: np.ndarray, bbmin, bbmax,
+                        use64: bool = False) -> "Tree":
+    """The reference's own primitive-box LBVH kernels on the host."""
+    bmin4 = np.ascontiguousarray(bmin4, np.float32)
+    bmax4 = np.ascontiguousarray(bmax4, np.float32)
+    data = np.ascontiguousarray(data, np.uint32)
+    n = len(data)
+    t = Tree.empty(n)
+    mn = np.asarray(bbmin, np.float32)
+    mx = np.asarray(bbmax, np.float32)
+    ref_host_lib().ref_host_lbvh_ts(n, _ptr(bmin4), _ptr(bmax4), _ptr(data), _ptr(mn), _ptr(mx),
+                                    1 if use64 else 0, *t.ptrs())
+    return t
 
 
 def ref_host_morton(v: np.ndarray, bbmin, bbmax, bits: int = 30):

@@ -796,6 +796,225 @@ int orc_trbvh(uint32_t n, int32_t* parent, int32_t* left, int32_t* right, int32_
     return 0;
 }
 
+// Triangle-splitting LBVH: the reference's primitive-box kernels.
+// BVHRT-Core/src/LBVH.cu:99-161: Morton codes of each primitive box's
+// centroid (min + max) / 2 normalised to the scene box, routing indices iota;
+// the sort; :320-428: the tree, a leaf's data index dataIndices[routing];
+// :572-669: leaf boxes from the primitive boxes through the routing index,
+// unions above.  pbmin4 / pbmax4: n float4; pdata: n triangle indices.
+int orc_build_lbvh_split(uint32_t n, const float* pbmin4, const float* pbmax4, const uint32_t* pdata,
+                         const float* sbmin, const float* sbmax, int morton_bits, int32_t* parent, int32_t* left,
+                         int32_t* right, int32_t* data, float* bmin4, float* bmax4, float* area, int threads) {
+    if (n < 2 || (morton_bits != 30 && morton_bits != 63)) return 1;
+    const F4* bmn = reinterpret_cast<const F4*>(pbmin4);
+    const F4* bmx = reinterpret_cast<const F4*>(pbmax4);
+    std::vector<uint32_t> route(n), leaf_data(n);
+    auto centroid = [&](uint32_t i, float c[3]) {
+        c[0] = (bmn[i].x + bmx[i].x) / 2.0f;
+        c[1] = (bmn[i].y + bmx[i].y) / 2.0f;
+        c[2] = (bmn[i].z + bmx[i].z) / 2.0f;
+    };
+    if (morton_bits == 30) {
+        std::vector<uint32_t> k(n);
+        for (uint32_t i = 0; i < n; ++i) { float c[3]; centroid(i, c); k[i] = morton30(c, sbmin, sbmax); }
+        orc_sort_pairs32(k.data(), route.data(), n, threads);
+        for (uint32_t i = 0; i < n; ++i) leaf_data[i] = pdata[route[i]];
+        orc_karras(k.data(), nullptr, leaf_data.data(), n, parent, left, right, data, threads);
+    } else {
+        std::vector<uint64_t> k(n);
+        for (uint32_t i = 0; i < n; ++i) { float c[3]; centroid(i, c); k[i] = morton63(c, sbmin, sbmax); }
+        orc_sort_pairs64(k.data(), route.data(), n);
+        for (uint32_t i = 0; i < n; ++i) leaf_data[i] = pdata[route[i]];
+        orc_karras(nullptr, k.data(), leaf_data.data(), n, parent, left, right, data, threads);
+    }
+    Tree t = make_tree(n, parent, left, right, data, bmin4, bmax4, area);
+    for (uint32_t i = 0; i < n; ++i) {
+        const int leaf = (int)i + (int)n - 1;
+        const F4 mn{bmn[route[i]].x, bmn[route[i]].y, bmn[route[i]].z, 0.0f};
+        const F4 mx{bmx[route[i]].x, bmx[route[i]].y, bmx[route[i]].z, 0.0f};
+        t.left[leaf] = -1;
+        t.right[leaf] = -1;
+        t.bmin[leaf] = mn;
+        t.bmax[leaf] = mx;
+        t.area[leaf] = box_area(mn, mx);
+    }
+    auto visit = [&](int x) {
+        const int l = t.left[x], r = t.right[x];
+        F4 mn{fminf(t.bmin[l].x, t.bmin[r].x), fminf(t.bmin[l].y, t.bmin[r].y), fminf(t.bmin[l].z, t.bmin[r].z), 0.0f};
+        F4 mx{fmaxf(t.bmax[l].x, t.bmax[r].x), fmaxf(t.bmax[l].y, t.bmax[r].y), fmaxf(t.bmax[l].z, t.bmax[r].z), 0.0f};
+        t.bmin[x] = mn;
+        t.bmax[x] = mx;
+        t.area[x] = box_area(mn, mx);
+    };
+    run_post_order(t, nthreads_or_max(threads), visit);
+    return 0;
+}
+
+// Triangle splitting (no counterpart in the reference: its primitive-box
+// build above has no step that makes the boxes).  The product's scheme,
+// restated with the same operations in the same order: priority
+// sqrt(max(0, SA(box) - 2 * area)), integer shares floor(p / p_max * 2^16),
+// s_t = min(7, floor(q_t * K / 2^16)) splits with K the largest scale whose
+// splits fit the budget (binary search over the shares' histogram), each bisecting the
+// largest fragment's region at the middle of its tight box's longest axis
+// and clipping the triangle to both halves.  Returns the primitive count, or
+// -1 when max_prims is too small.
+namespace split_detail {
+struct TriV { float v[3][3]; };
+inline float sa_box(const float* mn, const float* mx) {
+    return box_area(mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]);
+}
+float priority(const TriV& T) {
+    float mn[3], mx[3];
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = fminf(fminf(T.v[0][a], T.v[1][a]), T.v[2][a]);
+        mx[a] = fmaxf(fmaxf(T.v[0][a], T.v[1][a]), T.v[2][a]);
+    }
+    const float ux = T.v[1][0] - T.v[0][0], uy = T.v[1][1] - T.v[0][1], uz = T.v[1][2] - T.v[0][2];
+    const float wx = T.v[2][0] - T.v[0][0], wy = T.v[2][1] - T.v[0][1], wz = T.v[2][2] - T.v[0][2];
+    const float cx = uy * wz - uz * wy;
+    const float cy = uz * wx - ux * wz;
+    const float cz = ux * wy - uy * wx;
+    const float len2 = (cx * cx + cy * cy) + cz * cz;
+    const float ar = 0.5f * std::sqrt(len2);
+    const float waste = sa_box(mn, mx) - 2.0f * ar;
+    return waste > 0.0f ? std::sqrt(waste) : 0.0f;
+}
+bool clip_box(const TriV& T, const float* rmn, const float* rmx, float* omn, float* omx) {
+    float P[9][3], Q[9][3];
+    int np = 3;
+    for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a) P[k][a] = T.v[k][a];
+    for (int plane = 0; plane < 6; ++plane) {
+        const int ax = plane >> 1;
+        const bool upper = plane & 1;
+        const float c = upper ? rmx[ax] : rmn[ax];
+        int nq = 0;
+        for (int i = 0; i < np; ++i) {
+            const float* p = P[i];
+            const float* q = P[i + 1 < np ? i + 1 : 0];
+            const bool pin = upper ? p[ax] <= c : p[ax] >= c;
+            const bool qin = upper ? q[ax] <= c : q[ax] >= c;
+            if (pin && nq < 9) { Q[nq][0] = p[0]; Q[nq][1] = p[1]; Q[nq][2] = p[2]; ++nq; }
+            if (pin != qin && nq < 9) {
+                const float t = (c - p[ax]) / (q[ax] - p[ax]);
+                for (int a = 0; a < 3; ++a) Q[nq][a] = a == ax ? c : p[a] + t * (q[a] - p[a]);
+                ++nq;
+            }
+        }
+        np = nq;
+        if (np == 0) return false;
+        for (int i = 0; i < np; ++i) { P[i][0] = Q[i][0]; P[i][1] = Q[i][1]; P[i][2] = Q[i][2]; }
+    }
+    for (int a = 0; a < 3; ++a) {
+        float lo = P[0][a], hi = P[0][a];
+        for (int i = 1; i < np; ++i) { lo = fminf(lo, P[i][a]); hi = fmaxf(hi, P[i][a]); }
+        omn[a] = fmaxf(lo, rmn[a]);
+        omx[a] = fminf(hi, rmx[a]);
+        if (omn[a] > omx[a]) return false;
+    }
+    return true;
+}
+}  // namespace split_detail
+
+int64_t orc_split_triangles(const float* verts, uint32_t n, float split_ratio, uint32_t max_prims,
+                            float* out_bmin4, float* out_bmax4, uint32_t* out_data) {
+    using namespace split_detail;
+    const F4* v = reinterpret_cast<const F4*>(verts);
+    auto tri = [&](uint32_t t) {
+        TriV T;
+        for (int k = 0; k < 3; ++k) {
+            const F4& p = v[3 * (size_t)t + k];
+            T.v[k][0] = p.x; T.v[k][1] = p.y; T.v[k][2] = p.z;
+        }
+        return T;
+    };
+    uint64_t budget = (uint64_t)((double)split_ratio * (double)n);
+    if (budget > (uint64_t)max_prims - n) budget = (uint64_t)max_prims - n;
+    std::vector<float> prio(n);
+    float pmax = 0.0f;
+    for (uint32_t t = 0; t < n; ++t) { prio[t] = priority(tri(t)); pmax = fmaxf(pmax, prio[t]); }
+    std::vector<uint32_t> share(n), count(n), hist(65537, 0u);
+    for (uint32_t t = 0; t < n; ++t) {
+        share[t] = pmax > 0.0f ? (uint32_t)fminf((prio[t] / pmax) * 65536.0f, 65536.0f) : 0u;
+        if (share[t]) hist[share[t]]++;
+    }
+    auto splits_of = [](uint32_t q, uint64_t K) {
+        const uint64_t s = (uint64_t)q * K / 65536u;
+        return (uint32_t)(s < 7 ? s : 7);
+    };
+    auto sum_splits = [&](uint64_t K) {
+        uint64_t s = 0;
+        for (uint32_t q = 1; q <= 65536u; ++q)
+            if (hist[q]) s += (uint64_t)hist[q] * splits_of(q, K);
+        return s;
+    };
+    // The largest scale K whose splits fit the budget.
+    uint64_t lo = 0, hi = 7ull * 65536u + 1;
+    uint64_t K;
+    if (sum_splits(hi) <= budget) {
+        K = hi;
+    } else {
+        while (hi - lo > 1) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (sum_splits(mid) <= budget) lo = mid; else hi = mid;
+        }
+        K = lo;
+    }
+    uint64_t total = 0;
+    for (uint32_t t = 0; t < n; ++t) {
+        count[t] = 1u + splits_of(share[t], K);
+        total += count[t];
+    }
+    if (total > max_prims) return -1;
+    F4* omn = reinterpret_cast<F4*>(out_bmin4);
+    F4* omx = reinterpret_cast<F4*>(out_bmax4);
+    uint64_t o = 0;
+    for (uint32_t t = 0; t < n; ++t) {
+        const TriV T = tri(t);
+        const int c = (int)count[t];
+        float rmn[8][3], rmx[8][3], fmn[8][3], fmx[8][3];
+        for (int a = 0; a < 3; ++a) {
+            fmn[0][a] = rmn[0][a] = fminf(fminf(T.v[0][a], T.v[1][a]), T.v[2][a]);
+            fmx[0][a] = rmx[0][a] = fmaxf(fmaxf(T.v[0][a], T.v[1][a]), T.v[2][a]);
+        }
+        int have = 1;
+        while (have < c) {
+            int b = 0;
+            float bs = sa_box(fmn[0], fmx[0]);
+            for (int k = 1; k < have; ++k) {
+                const float sk = sa_box(fmn[k], fmx[k]);
+                if (sk > bs) { bs = sk; b = k; }
+            }
+            int ax = 0;
+            float ext = fmx[b][0] - fmn[b][0];
+            for (int a = 1; a < 3; ++a) {
+                const float e = fmx[b][a] - fmn[b][a];
+                if (e > ext) { ext = e; ax = a; }
+            }
+            const float mid = (fmn[b][ax] + fmx[b][ax]) * 0.5f;
+            float lmn[3], lmx[3], hmn[3], hmx[3], alo[3], ahi[3], blo[3], bhi[3];
+            for (int a = 0; a < 3; ++a) { lmn[a] = hmn[a] = rmn[b][a]; lmx[a] = hmx[a] = rmx[b][a]; }
+            lmx[ax] = mid;
+            hmn[ax] = mid;
+            if (!(ext > 0.0f) || !clip_box(T, lmn, lmx, alo, ahi) || !clip_box(T, hmn, hmx, blo, bhi)) break;
+            for (int a = 0; a < 3; ++a) {
+                rmn[b][a] = lmn[a]; rmx[b][a] = lmx[a]; fmn[b][a] = alo[a]; fmx[b][a] = ahi[a];
+                rmn[have][a] = hmn[a]; rmx[have][a] = hmx[a]; fmn[have][a] = blo[a]; fmx[have][a] = bhi[a];
+            }
+            ++have;
+        }
+        for (int k = 0; k < c; ++k) {
+            const int f = k < have ? k : have - 1;
+            omn[o + k] = F4{fmn[f][0], fmn[f][1], fmn[f][2], 0.0f};
+            omx[o + k] = F4{fmx[f][0], fmx[f][1], fmx[f][2], 0.0f};
+            out_data[o + k] = t;
+        }
+        o += (uint64_t)c;
+    }
+    return (int64_t)total;
+}
+
 // BVHRT-Core/src/SoABVHTree.cpp:50-74 (sequential float sums in index order).
 float orc_sah(uint32_t n, const float* area, int root, float ci, float ct) {
     const float total = area[root];

@@ -19,6 +19,7 @@
 #include "BVHTreeCollapser.h"
 #include "BVHTreeInstanceManager.h"
 #include "Commons.cuh"
+#include "CubWrapper.h"
 #include "LBVH.h"
 #include "LBVHBuilder.h"
 #include "SceneWrapper.h"
@@ -146,6 +147,82 @@ int ref_host_morton(const float* vertices, unsigned int n, const float* bbmin, c
     }
     if (indices) std::memcpy(indices, idx, n * sizeof(unsigned int));
     cudaFree(idx);
+    return 0;
+}
+
+// The reference's triangle-splitting LBVH kernels (no builder of the
+// reference calls them): LBVH.cu:99-161 DeviceGenerateMortonCodes over
+// primitive boxes, the sort into the *Out buffers, LBVH.cu:320-428
+// DeviceBuildTree with data and routing indices, LBVH.cu:572-669
+// DeviceCalculateInternalNodeBoundingBoxes with counters preset to 0xFF as
+// LBVHBuilder.cpp:90-94 does for the other path.  pbmin4 / pbmax4: n float4;
+// pdata: n triangle indices; the scene box comes from bbmin / bbmax.
+int ref_host_lbvh_ts(unsigned int n, const float* pbmin4, const float* pbmax4, const unsigned int* pdata,
+                     const float* bbmin, const float* bbmax, int use64, int* parent, int* left, int* right,
+                     int* data, float* bmin4, float* bmax4, float* area) {
+    // A scene holding the box: the primitive-box Morton kernel reads only
+    // scene->boundingBoxMin/Max (one placeholder triangle).
+    float4* v = new float4[3];
+    for (int k = 0; k < 3; ++k) v[k] = float4{0.0f, 0.0f, 0.0f, 0.0f};
+    SceneWrapper sw(1, v, f3(bbmin), f3(bbmax));
+    float4 *bmn = nullptr, *bmx = nullptr;
+    unsigned int *route = nullptr, *route_out = nullptr, *dind = nullptr, *counters = nullptr;
+    cudaMalloc(&bmn, n * sizeof(float4));
+    cudaMalloc(&bmx, n * sizeof(float4));
+    cudaMalloc(&route, n * sizeof(unsigned int));
+    cudaMalloc(&route_out, n * sizeof(unsigned int));
+    cudaMalloc(&dind, n * sizeof(unsigned int));
+    cudaMalloc(&counters, (n - 1) * sizeof(unsigned int));
+    std::memcpy(bmn, pbmin4, n * sizeof(float4));
+    std::memcpy(bmx, pbmax4, n * sizeof(float4));
+    std::memcpy(dind, pdata, n * sizeof(unsigned int));
+    BVHTreeInstanceManager mgr;
+    SoABVHTree* dt = mgr.CreateDeviceTree(n);
+    if (use64) {
+        unsigned long long int *k = nullptr, *ko = nullptr;
+        cudaMalloc(&k, n * sizeof(unsigned long long int));
+        cudaMalloc(&ko, n * sizeof(unsigned long long int));
+        DeviceGenerateMortonCodes(n, sw.DeviceScene(), bmn, bmx, k, route);
+        DeviceSort(n, &k, &ko, &route, &route_out);
+        DeviceBuildTree(n, ko, dind, dt, route_out);
+        cudaFree(k);
+        cudaFree(ko);
+    } else {
+        unsigned int *k = nullptr, *ko = nullptr;
+        cudaMalloc(&k, n * sizeof(unsigned int));
+        cudaMalloc(&ko, n * sizeof(unsigned int));
+        DeviceGenerateMortonCodes(n, sw.DeviceScene(), bmn, bmx, k, route);
+        DeviceSort(n, &k, &ko, &route, &route_out);
+        DeviceBuildTree(n, ko, dind, dt, route_out);
+        cudaFree(k);
+        cudaFree(ko);
+    }
+    cudaMemset(counters, 0xFF, (n - 1) * sizeof(unsigned int));
+    DeviceCalculateInternalNodeBoundingBoxes(n, dt, counters, bmn, bmx, route_out);
+    BVHTree* ht = mgr.DeviceToHostTree(dt);
+    for (size_t i = 0; i < 2 * (size_t)n - 1; ++i) {
+        if (parent) parent[i] = ht->ParentIndex((int)i);
+        if (left) left[i] = ht->LeftIndex((int)i);
+        if (right) right[i] = ht->RightIndex((int)i);
+        if (data) data[i] = ht->DataIndex((int)i);
+        if (bmin4) {
+            const float4 b = ht->BoundingBoxMin((int)i);
+            std::memcpy(bmin4 + 4 * i, &b, 16);
+        }
+        if (bmax4) {
+            const float4 b = ht->BoundingBoxMax((int)i);
+            std::memcpy(bmax4 + 4 * i, &b, 16);
+        }
+        if (area) area[i] = ht->Area((int)i);
+    }
+    delete ht;
+    mgr.FreeDeviceTree(dt);
+    cudaFree(bmn);
+    cudaFree(bmx);
+    cudaFree(route);
+    cudaFree(route_out);
+    cudaFree(dind);
+    cudaFree(counters);
     return 0;
 }
 

@@ -27,6 +27,25 @@ def scene_case(name: str) -> np.ndarray:
     if kind == "same":
         v = ab.gen_scene(ab.SCENE_UNIFORM, 1, seed)
         return np.ascontiguousarray(np.repeat(v, n, axis=0))
+    if kind == "sliver":
+        # Long thin triangles along random directions (the case triangle
+        # splitting is for): 90% small triangles of the uniform scene, 10%
+        # slivers of length 0.2-0.6 and width 0.002.
+        v = ab.gen_scene(ab.SCENE_UNIFORM, n, seed).copy()
+        rng = np.random.default_rng(seed)
+        k = n // 10
+        idx = rng.choice(n, size=k, replace=False)
+        p0 = rng.uniform(0.0, 1.0, (k, 3)).astype(np.float32)
+        d = rng.normal(size=(k, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        w = np.cross(d, rng.normal(size=(k, 3)))
+        w /= np.linalg.norm(w, axis=1, keepdims=True)
+        length = rng.uniform(0.2, 0.6, (k, 1))
+        v[idx, 0, :3] = p0
+        v[idx, 1, :3] = (p0 + length * d).astype(np.float32)
+        v[idx, 2, :3] = (p0 + 0.002 * w).astype(np.float32)
+        v[:, :, 3] = 0
+        return np.ascontiguousarray(v)
     raise KeyError(name)
 
 
@@ -44,6 +63,8 @@ CASES = {
     "dupes3000": ("dupes", 3000, 5),
     "flat2000": ("flat", 2000, 6),
     "same64": ("same", 64, 7),
+    "sliver20000": ("sliver", 20000, 8),
+    "sliver262144": ("sliver", 262144, 9),
 }
 
 

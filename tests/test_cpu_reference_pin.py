@@ -161,3 +161,67 @@ def test_reference_sah_matches_oracle():
         area = np.exp(rng.uniform(-30, 30, 2 * n - 1)).astype(np.float32)
         assert np.float32(R.ref_host_sah(n, O._ptr(area), 1.2, 1.0)) == \
             np.float32(L.orc_sah(n, O._ptr(area), 0, 1.2, 1.0))
+
+
+GOLD_SPLIT = json.loads((Path(__file__).resolve().parent / "golden" / "ref_host_split_golden.json").read_text())
+
+
+def test_oracle_split_build_matches_reference_records():
+    """The oracle's triangle-splitting LBVH (primitive-box Morton codes, tree,
+    boxes) equals the reference's own primitive-box kernels
+    (LBVH.cu:99-161, 320-428, 572-669) on the recorded fragment sets; the
+    fragments themselves are the splitting step's (restated in the oracle)."""
+    assert len(GOLD_SPLIT["records"]) >= 40
+    for rec in GOLD_SPLIT["records"]:
+        v = scene_case(rec["case"])
+        mn, mx = O.scene_aabb(v)
+        b0, b1, d = O.split_triangles(v, rec["split_ratio"])
+        what = f"{rec['case']} split {rec['split_ratio']} {rec['bits']}-bit"
+        assert len(d) == rec["primitives"], what
+        assert digest(np.ascontiguousarray(b0[:, :3])) == rec["fragments"]["bmin"], what
+        assert digest(np.ascontiguousarray(b1[:, :3])) == rec["fragments"]["bmax"], what
+        assert digest(d) == rec["fragments"]["data"], what
+        t = O.build_lbvh_split(b0, b1, d, mn, mx, rec["bits"], threads=0)
+        assert _tdig(t) == rec["tree"], what
+        assert np.float32(O.sah(t)) == np.float32(rec["sah"]), what
+
+
+@needs_ref
+def test_reference_split_kernels_reproduce_records():
+    """The reference's host-model primitive-box kernels give the recorded
+    trees again."""
+    for rec in GOLD_SPLIT["records"]:
+        v = scene_case(rec["case"])
+        mn, mx = O.scene_aabb(v)
+        b0, b1, d = O.split_triangles(v, rec["split_ratio"])
+        t = O.ref_host_lbvh_split(b0, b1, d, mn, mx, rec["bits"] == 63)
+        assert _tdig(t) == rec["tree"], f"{rec['case']} split {rec['split_ratio']} {rec['bits']}-bit"
+
+
+def test_split_ratio_zero_is_the_plain_lbvh():
+    """Without splits every triangle is one primitive with its own box, and the
+    primitive-box build equals the plain LBVH."""
+    for case in ("u1000", "clu4096", "dupes3000"):
+        v = scene_case(case)
+        mn, mx = O.scene_aabb(v)
+        b0, b1, d = O.split_triangles(v, 0.0)
+        assert np.array_equal(d, np.arange(len(v), dtype=np.uint32))
+        t = O.build_lbvh_split(b0, b1, d, mn, mx, 30)
+        base, _, _ = O.build_lbvh(v, mn, mx)
+        assert _tdig(t) == _tdig(base), case
+
+
+def test_split_fragments_cover_their_triangles():
+    """Fragments of a triangle lie inside the triangle's box, and their union
+    is the triangle's box (the clipped pieces cover the triangle)."""
+    v = scene_case("sliver20000")
+    b0, b1, d = O.split_triangles(v, 1.0)
+    tmn = v[:, :, :3].min(axis=1)
+    tmx = v[:, :, :3].max(axis=1)
+    assert (b0[:, :3] >= tmn[d]).all() and (b1[:, :3] <= tmx[d]).all()
+    assert (b0[:, :3] <= b1[:, :3]).all()
+    umn = np.full_like(tmn, np.inf)
+    umx = np.full_like(tmx, -np.inf)
+    np.minimum.at(umn, d, b0[:, :3])
+    np.maximum.at(umx, d, b1[:, :3])
+    assert np.allclose(umn, tmn, atol=1e-6) and np.allclose(umx, tmx, atol=1e-6)
