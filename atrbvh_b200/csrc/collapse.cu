@@ -1,7 +1,10 @@
 // Leaf collapse (BVHRT-Core/src/TreeCollapser.cu:13-285, BVHTreeCollapser.cpp:21-93).
 //
-// A streaming pass copies the tree into the collapsed layout.  Pass 1
-// (bottom-up, one thread per leaf, second arrival continues) computes, per
+// The collapsed tree starts as a copy of the tree (TreeCollapser.cu:13-30),
+// made inside pass 1: each leaf's thread copies its leaf, and the first of
+// the two threads reaching an internal node -- which stops there -- copies
+// that node.  Pass 1 (bottom-up, one thread per leaf, second arrival
+// continues) computes, per
 // node: triangle count, SAH cost (ci*A + cL + cR, or ct*A*count when that is
 // cheaper -- :47-84), the collapse flag, and whether a climbing thread of the
 // reference's emission kernel (:173-237) would pass the node upward.  The reference emits, at every
@@ -45,21 +48,6 @@ struct CollapseRefs {
     uint32_t* emit_cnt;
 };
 
-// The collapsed tree starts as a copy of the tree (TreeCollapser.cu:13-30):
-// a streaming pass over every node of every mesh (data is -1 at internal
-// nodes in both), which also clears the emission counts.
-__global__ void __launch_bounds__(256) k_collapse_copy(CollapseRefs g, uint64_t total_nodes) {
-    const uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (x >= total_nodes) return;
-    g.c_parent[x] = g.parent[x];
-    g.c_left[x] = g.left[x];
-    g.c_right[x] = g.right[x];
-    g.c_data[x] = g.data[x];
-    g.c_bmin[x] = g.bmin[x];
-    g.c_bmax[x] = g.bmax[x];
-    g.emit_cnt[x] = 0u;
-}
-
 // Segmented: thread i starts at the i-th leaf of the batch; node arrays are
 // addressed from the mesh's first node (local indices); each mesh's lists
 // live in its own slice [tri_begin, tri_end) of tri_indices.  A node's area
@@ -90,6 +78,13 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
     int2 mine = make_int2(__float_as_int(__fmul_rn(ct, g.area[nb + ch])), (1 << 1) | 1);
     g.c_count[nb + ch] = 1;
     g.rec[nb + ch] = mine;
+    // The leaf's copy (data >= 0, no children).
+    g.c_parent[nb + ch] = cur;
+    g.c_left[nb + ch] = g.left[nb + ch];
+    g.c_right[nb + ch] = g.right[nb + ch];
+    g.c_data[nb + ch] = g.data[nb + ch];
+    g.c_bmin[nb + ch] = g.bmin[nb + ch];
+    g.c_bmax[nb + ch] = g.bmax[nb + ch];
     if (cur < 0) return;
     int l = g.left[nb + cur], r = g.right[nb + cur], up = g.parent[nb + cur];
     float a = g.area[nb + cur];
@@ -103,7 +98,17 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
             na = g.area[nb + up];
         }
         const unsigned long long other = atomicExch(slot + cur, pack_rec(mine));
-        if (other == 0ull) return;
+        if (other == 0ull) {
+            // First of the two children: the node's copy, then stop.
+            const int x = nb + cur;
+            g.c_parent[x] = up;
+            g.c_left[x] = l;
+            g.c_right[x] = r;
+            g.c_data[x] = g.data[x];
+            g.c_bmin[x] = g.bmin[x];
+            g.c_bmax[x] = g.bmax[x];
+            return;
+        }
         const int2 sib = make_int2((int)(uint32_t)other, (int)(uint32_t)(other >> 32));
         const bool from_left = ch == l;
         const int2 el = from_left ? mine : sib, er = from_left ? sib : mine;
@@ -210,6 +215,7 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
     cudaStream_t s = ctx->stream;
     // The climb reads a zero slot as "no sibling yet": a failed clear must stop here.
     cudaError_t me = cudaMemsetAsync(slots, 0, inner * 8, s);
+    if (me == cudaSuccess) me = cudaMemsetAsync(emit, 0, nn * 4, s);
     if (me == cudaSuccess) me = cudaMemsetAsync(dst.tri_indices, 0xff, (size_t)n * 4, s);
     if (me != cudaSuccess) {
         ctx->release(scratch);
@@ -218,9 +224,8 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
     CollapseRefs r{n, src.area, src.parent, src.left, src.right, src.data, src.bmin, src.bmax, dst.parent, dst.left,
                    dst.right, dst.data, dst.count, dst.bmin, dst.bmax, rec, emit};
     const unsigned blocks = (n + 255) / 256;
-    k_collapse_copy<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(r, nn);
     k_collapse_cost<<<blocks, 256, 0, s>>>(r, segs, slots, ci, ct, max_leaf);
-    ctx->launches += 2;
+    ctx->launches += 1;
     int st = exclusive_scan_u32(ctx, emit, offs, nn, nullptr);
     if (st == ATR_OK) {
         k_collapse_emit<<<blocks, 256, 0, s>>>(r, segs, offs, dst.tri_indices);
