@@ -824,6 +824,126 @@ def run_sweep(args, world, rank, local):
     print(json.dumps(out), flush=True)
 
 
+REFIT_WORKLOAD = ("clustered scene (as the default workload): LBVH 30-bit + ATRBVH(9,2) once, then atr_refit of "
+                  "the resident tree from its device vertices per step (the refit plan is built by the second refit, "
+                  "inside the warm-up)")
+
+
+def run_refit(args, world, rank, local):
+    """Standalone refit of a resident tree: one atr_refit per step."""
+    import torch
+    import atrbvh_b200 as ab
+    torch.cuda.set_device(local)
+    ctx = ab.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    n = args.triangles
+    scene = ab.SceneWrapper(ctx, ab.gen_scene(ab.SCENE_CLUSTERED, n, 0))
+    tree = ab.LBVHBuilder().BuildTree(scene)
+    ab.AgglomerativeTreeletOptimizer(9, 2).Optimize(tree)
+    for _ in range(max(args.warmup, 3)):
+        ab.Refit(tree, scene)
+    ctx.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ab.Refit(tree, scene)
+    e1.record(stream)
+    ctx.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    peaks = _read_peaks()
+    gbs = n * REFIT_BYTES_PER_TRI / (ms * 1e-3) / 1e9
+    if rank == 0:
+        print(json.dumps({"metric": "refit Mtri/s", "value": world * n / (ms * 1e-3) / 1e6, "unit": "Mtri/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                          "data": "synthetic (seeded Philox)",
+                          "config": {"workload": REFIT_WORKLOAD, "triangles": n},
+                          "roofline": {"kernel": "k_refit_level", "bound": "hbm", "achieved": gbs,
+                                       "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": gbs / peaks["hbm_gbs"],
+                                       "peak_src": peaks["src"], "bytes_per_tri": REFIT_BYTES_PER_TRI}}), flush=True)
+    tree.close()
+    scene.close()
+    ctx.close()
+
+
+SPLIT_WORKLOAD = ("sliver scene: the uniform-centroid scene with 10% of its triangles replaced by slivers (length "
+                  "0.2-0.6 along random directions, width 0.002; seeded): triangle splitting at ratios 0-1, "
+                  "primitive-box LBVH 30-bit + ATRBVH(9,2) + collapse, SAH and build times against the plain build")
+
+
+def sliver_scene(n: int, seed: int = 9):
+    import atrbvh_b200 as ab
+    v = ab.gen_scene(ab.SCENE_UNIFORM, n, seed).copy()
+    rng = np.random.default_rng(seed)
+    k = n // 10
+    idx = rng.choice(n, size=k, replace=False)
+    p0 = rng.uniform(0.0, 1.0, (k, 3)).astype(np.float32)
+    d = rng.normal(size=(k, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    w = np.cross(d, rng.normal(size=(k, 3)))
+    w /= np.linalg.norm(w, axis=1, keepdims=True)
+    length = rng.uniform(0.2, 0.6, (k, 1))
+    v[idx, 0, :3] = p0
+    v[idx, 1, :3] = (p0 + length * d).astype(np.float32)
+    v[idx, 2, :3] = (p0 + 0.002 * w).astype(np.float32)
+    v[:, :, 3] = 0
+    return np.ascontiguousarray(v)
+
+
+def run_split(args, world, rank, local):
+    """Triangle splitting on a scene of slivers: SAH and device times of split
+    + primitive-box LBVH + ATRBVH(9,2) + collapse against the plain build."""
+    import torch
+    import atrbvh_b200 as ab
+    torch.cuda.set_device(local)
+    ctx = ab.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    n = args.triangles
+    v = sliver_scene(n)
+    mn, mx = ab.scene_bounds(v)
+    scene = ab.SceneWrapper(ctx, v, mn, mx)
+    rows = []
+    for ratio in (None, 0.1, 0.3, 1.0):
+        times = []
+        for rep in range(args.warmup + args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if ratio is None:
+                tree = ab.LBVHBuilder().BuildTree(scene)
+                prims = n
+            else:
+                bmin, bmax, data = ab.split_triangles(scene, ratio)  # synchronises to read the count
+                tree = ab.build_lbvh_split(ctx, bmin, bmax, data, mn, mx)
+                prims = int(data.shape[0])
+            ab.AgglomerativeTreeletOptimizer(9, 2).Optimize(tree)
+            col, csah = ab.BVHTreeCollapser().Collapse(tree)
+            e1.record(stream)
+            ctx.synchronize()
+            if rep >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+            sah = tree.sah()
+            col.close()
+            tree.close()
+        ms = statistics.median(times)
+        rows.append({"split_ratio": ratio, "primitives": prims, "sah": sah, "collapsed_sah": csah, "ms": ms,
+                     "mtri_per_s": n / (ms * 1e-3) / 1e6})
+    plain = rows[0]
+    for r in rows:
+        r["sah_vs_plain"] = r["sah"] / plain["sah"]
+    best = min(rows[1:], key=lambda r: r["sah"])
+    if rank == 0:
+        print(json.dumps({"metric": "ATRBVH SAH with triangle splitting (lower is better)", "value": best["sah"],
+                          "unit": "SAH", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": best["ms"], "higher_is_better": False, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+                          "config": {"workload": SPLIT_WORKLOAD, "triangles": n}, "rows": rows}), flush=True)
+    scene.close()
+    ctx.close()
+
+
 def run_reference(args, world, rank, local):
     """The host-core pipeline on the whole workload scene, one build per step.
     The reference has no CPU implementation of this path, and its CUDA build
@@ -877,7 +997,8 @@ def main():
                     help="default line: seconds of back-to-back steps timed after the K steps, with their own clocks")
     ap.add_argument("--triangles", type=int, default=N_TRIS,
                     help="scene size (default: the workload's 4,194,304); smaller values are for profiling")
-    ap.add_argument("--workload", default="clustered", choices=["clustered", "batch", "serve", "sweep"],
+    ap.add_argument("--workload", default="clustered", choices=["clustered", "batch", "serve", "sweep", "refit",
+                                                                "split"],
                     help="clustered: 4.2M-triangle build+trace (the default line); batch: 4096-mesh segmented "
                          "build vs per-mesh launches; serve: the request loop; sweep: 16.8M-triangle optimiser sweep")
     ap.add_argument("--meshes", type=int, default=BATCH_MESHES, help="batch: number of meshes")
@@ -901,6 +1022,11 @@ def main():
         elif args.workload == "sweep":
             if rank == 0:
                 run_sweep(args, world, rank, local)
+        elif args.workload == "refit":
+            run_refit(args, world, rank, local)
+        elif args.workload == "split":
+            if rank == 0:
+                run_split(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
