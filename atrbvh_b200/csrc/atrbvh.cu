@@ -57,18 +57,35 @@ struct GroupLayout {
     static constexpr int kFloats = kDistPad + 12 * kLeaves;
 };
 
-// What the treelet code keeps up to date for the next iteration, per mesh, for
-// every node it finishes or rewrites: subtree counts (node-indexed),
-// next-iteration levels (indexed by internal node) under the next
-// iteration's gamma, and next-iteration nodesSah (node-indexed).  The
-// reference recomputes nodesSah bottom-up every iteration as
+// The optimiser's per-node record, node-indexed in the batch layout (one
+// 16-byte load gives a treelet leaf everything but its box):
+//   x  subtree triangle count;
+//   y  nodesSah of even iterations, z  nodesSah of odd iterations -- this
+//      iteration's in component 1 + par (par = iteration & 1), the next
+//      iteration's in the other;
+//   w  big-node level: this iteration's until the node is finished, the next
+//      iteration's after (only the level lists, built before any node is
+//      finished, read this iteration's).
+// The reference recomputes nodesSah bottom-up every iteration as
 // (ci*A + left) + right, while a rewritten node stores the merge cost
 // (left + right) + ci*A; the two can differ in the last bit, so the next
 // iteration's values are kept in the recomputation's order.
+__device__ __forceinline__ int rec_ns_cur(int par) { return 1 + par; }
+__device__ __forceinline__ int rec_ns_next(int par) { return 2 - par; }
+__device__ __forceinline__ float* rec_f(int4* r, int x, int c) { return reinterpret_cast<float*>(r + x) + c; }
+__device__ __forceinline__ int* rec_i(int4* r, int x, int c) { return reinterpret_cast<int*>(r + x) + c; }
+// A record from its fields, the nodesSah values placed by parity.
+__device__ __forceinline__ int4 make_rec(int cnt, float ns_cur, float ns_next, int lvl, int par) {
+    return par ? make_int4(cnt, __float_as_int(ns_next), __float_as_int(ns_cur), lvl)
+               : make_int4(cnt, __float_as_int(ns_cur), __float_as_int(ns_next), lvl);
+}
+
+// What the treelet code keeps up to date, per mesh (rec starts at the mesh's
+// first node): the records of the nodes it finishes or rewrites, the next
+// iteration's gamma for their levels.
 struct NextRefs {
-    int32_t* sub;
-    int32_t* nlv;
-    float* nsn;
+    int4* rec;
+    int par;
     int gamma;
 };
 
@@ -155,7 +172,7 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     float4* const BMN = g.bmin + nb;
     float4* const BMX = g.bmax + nb;
     float* const AR = g.area + nb;
-    float* const NS = g.nsah + nb;
+    const int cur_c = rec_ns_cur(nx.par), next_c = rec_ns_next(nx.par);
 
     // ---- formTreelet (Treelet.cuh:57-114) ----
     // Lane k holds treelet leaf k (node and area).  The child record of an
@@ -233,10 +250,11 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     if (run && gl < tsize) {
         s_mn = ld_cg(BMN + s_node);
         s_mx = ld_cg(BMX + s_node);
-        s_sah = ld_cg(NS + s_node);
-        s_cnt = ld_cg(nx.sub + s_node);
-        s_nsn = ld_cg(nx.nsn + s_node);
-        s_nlv = is_internal(s_node, n) ? ld_cg(nx.nlv + s_node) : 0;
+        const int4 r = __ldcg(nx.rec + s_node);
+        s_cnt = r.x;
+        s_sah = __int_as_float(nx.par ? r.z : r.y);
+        s_nsn = __int_as_float(nx.par ? r.y : r.z);
+        s_nlv = is_internal(s_node, n) ? r.w : 0;
     }
     // Records of leaves that were never expanded may still be in flight into
     // the slots the merge state reuses.
@@ -435,15 +453,12 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
         Rt[ni] = fr;
         P[fl] = ni;
         P[fr] = ni;
-        NS[ni] = f0.w;
         const float4 mn = make_float4(f0.x, f0.y, f0.z, 0.0f);
         const float4 mx = make_float4(f1.x, f1.y, f1.z, 0.0f);
         BMN[ni] = mn;
         BMX[ni] = mx;
         AR[ni] = box_area(mn, mx);
-        nx.sub[ni] = f2.x;
-        nx.nlv[ni] = f2.y;
-        nx.nsn[ni] = __int_as_float(f2.z);
+        nx.rec[ni] = make_rec(f2.x, f0.w, __int_as_float(f2.z), f2.y, nx.par);
     }
     __syncwarp();
     // The rewritten nodes' child records, once every new area is stored.
@@ -452,12 +467,16 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     // its children.
     if (run && !accept && gl == 0) {
         const int lc = ld_cg(Lf + root), rc = ld_cg(Rt + root);
-        const int a = is_internal(lc, n) ? ld_cg(nx.nlv + lc) : 0;
-        const int b = is_internal(rc, n) ? ld_cg(nx.nlv + rc) : 0;
-        nx.nlv[root] = ld_cg(nx.sub + root) >= nx.gamma ? 1 + max(a, b) : 0;
-        nx.nsn[root] = __fadd_rn(__fadd_rn(__fmul_rn(ci, ld_cg(AR + root)), ld_cg(nx.nsn + lc)), ld_cg(nx.nsn + rc));
+        const int4 rl = __ldcg(nx.rec + lc), rr = __ldcg(nx.rec + rc);
+        const int a = is_internal(lc, n) ? rl.w : 0;
+        const int b = is_internal(rc, n) ? rr.w : 0;
+        *rec_i(nx.rec, root, 3) = ld_cg(rec_i(nx.rec, root, 0)) >= nx.gamma ? 1 + max(a, b) : 0;
+        *rec_f(nx.rec, root, next_c) =
+            __fadd_rn(__fadd_rn(__fmul_rn(ci, ld_cg(AR + root)), __int_as_float(next_c == 1 ? rl.y : rl.z)),
+                      __int_as_float(next_c == 1 ? rr.y : rr.z));
     }
     __syncwarp();
+    (void)cur_c;
 }
 
 // One iteration over every mesh of `segs`: thread i starts at the i-th sorted
@@ -465,15 +484,13 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
 // when `seg_tsize`/`seg_iters` are given; a mesh whose iterations are done
 // sits this launch out.
 template <int G, int W>
-__global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs, int32_t* __restrict__ subtree,
+__global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs, int4* __restrict__ rec,
                                                    uint32_t* __restrict__ counters, int4* __restrict__ kids,
                                                    int tsize_all,
                                                    const uint8_t* __restrict__ seg_tsize,
                                                    const uint8_t* __restrict__ seg_iters, int iteration, float ci,
                                                    float ct, int group_min, const uint2* __restrict__ start,
-                                                   const uint32_t* __restrict__ start_count,
-                                                   int32_t* __restrict__ next_lv, float* __restrict__ nsah_next,
-                                                   uint32_t* err) {
+                                                   const uint32_t* __restrict__ start_count, uint32_t* err) {
     constexpr int kWarpFloats = warp_floats<G>();
     __shared__ __align__(16) float s_mem[W][kWarpFloats];
     __shared__ uint16_t s_rc[kMaxDist];
@@ -521,9 +538,8 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
         if (seg_tsize) tsize = seg_tsize[m];
         if (!seg_iters || iteration < (int)seg_iters[m]) {
             const int leaf = base + (int)(i - s0) + (int)nm - 1;
-            subtree[leaf] = 1;
-            g.nsah[leaf] = __fmul_rn(ct, g.area[leaf]);
-            nsah_next[leaf] = g.nsah[leaf];
+            const float ls = __fmul_rn(ct, g.area[leaf]);
+            rec[leaf] = make_int4(1, __float_as_int(ls), __float_as_int(ls), 0);
             cur = g.parent[leaf];
         }
     }
@@ -555,17 +571,20 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
         if (second) {
             const int x = base + cur;
             const int l = base + lc, r = base + rc;
-            cnt = ld_cg(subtree + l) + ld_cg(subtree + r);
-            my_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), ld_cg(g.nsah + l)), ld_cg(g.nsah + r));
-            subtree[x] = cnt;
-            g.nsah[x] = my_sah;
+            const int cc = rec_ns_cur(iteration & 1);
+            const int4 rl = __ldcg(rec + l), rr = __ldcg(rec + r);
+            cnt = rl.x + rr.x;
+            my_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), __int_as_float(cc == 1 ? rl.y : rl.z)),
+                               __int_as_float(cc == 1 ? rr.y : rr.z));
             // Child record for treelet formation: one load yields both
             // children and their areas.
             myk = make_int4(lc, rc, __float_as_int(ld_cg(g.area + l)), __float_as_int(ld_cg(g.area + r)));
             kids[cbase + cur] = myk;
             if (cnt < gamma) {  // not a treelet root now, nor next iteration
-                next_lv[cbase + cur] = 0;
-                nsah_next[x] = my_sah;
+                rec[x] = make_int4(cnt, __float_as_int(my_sah), __float_as_int(my_sah), 0);
+            } else {  // the treelet writes the rest
+                *rec_i(rec, x, 0) = cnt;
+                *rec_f(rec, x, cc) = my_sah;
             }
         }
         unsigned vote = __ballot_sync(kFull, cnt >= gamma);
@@ -588,7 +607,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                 const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)rts : 0u);
                 const int4 rk = make_int4(__shfl_sync(kFull, myk.x, rl), __shfl_sync(kFull, myk.y, rl),
                                           __shfl_sync(kFull, myk.z, rl), __shfl_sync(kFull, myk.w, rl));
-                const NextRefs nx{subtree + rbase, next_lv + rcb, nsah_next + rbase, rts << (iteration + 1)};
+                const NextRefs nx{rec + rbase, iteration & 1, rts << (iteration + 1)};
                 process_group<G>(g, has, rbase, rn, root, rk, kids + rcb, nx, rsah, rts, maxts, ci,
                                  &s_mem[w][0] + (grp < NG ? grp : NG - 1) * GroupLayout<G>::kFloats, s_rc, s_prio, err);
 #pragma unroll
@@ -603,7 +622,7 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
                 const int rts = __shfl_sync(kFull, tsize, rl);
                 const int4 rk = make_int4(__shfl_sync(kFull, myk.x, rl), __shfl_sync(kFull, myk.y, rl),
                                           __shfl_sync(kFull, myk.z, rl), __shfl_sync(kFull, myk.w, rl));
-                const NextRefs nx{subtree + rbase, next_lv + rcb, nsah_next + rbase, rts << (iteration + 1)};
+                const NextRefs nx{rec + rbase, iteration & 1, rts << (iteration + 1)};
                 process_group<32>(g, true, rbase, rn, root, rk, kids + rcb, nx, rsah, rts, rts, ci, &s_mem[w][0],
                                   s_rc, s_prio, err);
                 vote &= vote - 1;
@@ -615,13 +634,13 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs
 
 template <int G>
 cudaError_t launch_atrbvh_g(int warps, uint32_t blocks, cudaStream_t s, const TreeRefs& g, const Segs& segs,
-                            int32_t* subtree, uint32_t* counters, int4* kids, int tsize, const uint8_t* seg_tsize,
+                            int4* rec, uint32_t* counters, int4* kids, int tsize, const uint8_t* seg_tsize,
                             const uint8_t* seg_iters, int it, float ci, float ct, int gmin, const uint2* start,
-                            const uint32_t* start_count, int32_t* next_lv, float* nsah_next, uint32_t* err) {
+                            const uint32_t* start_count, uint32_t* err) {
     switch (warps) {
-        case 2: k_atrbvh<G, 2><<<blocks, 64, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, nsah_next, err); break;
-        case 8: k_atrbvh<G, 8><<<blocks, 256, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, nsah_next, err); break;
-        default: k_atrbvh<G, 4><<<blocks, 128, 0, s>>>(g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, nsah_next, err); break;
+        case 2: k_atrbvh<G, 2><<<blocks, 64, 0, s>>>(g, segs, rec, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, err); break;
+        case 8: k_atrbvh<G, 8><<<blocks, 256, 0, s>>>(g, segs, rec, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, err); break;
+        default: k_atrbvh<G, 4><<<blocks, 128, 0, s>>>(g, segs, rec, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, err); break;
     }
     return cudaGetLastError();
 }
@@ -642,13 +661,10 @@ cudaError_t launch_atrbvh_g(int warps, uint32_t blocks, cudaStream_t s, const Tr
 constexpr int kMaxLevels = 64;  // largest L (ATR_TUNE_ATR_LEVELS)
 
 struct LevelRefs {
-    int32_t* subtree;
+    int4* rec;             // per node (node-indexed): count, nodesSah x 2, level (see NextRefs)
+    int par;               // iteration & 1
     uint32_t* counters;
     int4* kids;
-    int32_t* level;        // per internal node (inner-indexed): this iteration's levels
-    int32_t* next;         // the next iteration's levels, filled as nodes are finished
-    float* nsah;           // this iteration's nodesSah (node-indexed)
-    float* nsah_next;      // the next iteration's nodesSah
     uint32_t* hist;        // [L + 2]: level histogram
     uint32_t* off;         // [L + 2]: per-level offsets into `order` (written by phase B)
     uint32_t* cursor;      // [L + 2]
@@ -690,9 +706,8 @@ __global__ void __launch_bounds__(kLvBlock) k_levels(TreeRefs g, Segs segs, Leve
     const float la = g.area[leaf];
     int my_cnt = 1, my_lvl = 0, my_first = li, child = li + (int)n - 1;
     float my_nsah = __fmul_rn(ct, la), my_area = la;
-    lv.subtree[leaf] = 1;
-    g.nsah[leaf] = my_nsah;
-    lv.nsah_next[leaf] = my_nsah;
+    lv.rec[leaf] = make_int4(1, __float_as_int(my_nsah), __float_as_int(my_nsah), 0);
+    const int cur_c = rec_ns_cur(lv.par);
     int cur = g.parent[leaf];
     while (cur >= 0) {
         const int x = base + cur;
@@ -723,29 +738,27 @@ __global__ void __launch_bounds__(kLvBlock) k_levels(TreeRefs g, Segs segs, Leve
         const int sib = lc == child ? rc : lc;
         if (!local) {
             if (atomic_add_acq_rel_gpu(&lv.counters[cb + cur], 1u) == 0u) return;
-            sib_cnt = ld_cg(lv.subtree + base + sib);
-            sib_lvl = is_internal(sib, n) ? ld_cg(lv.level + cb + sib) : 0;
-            sib_nsah = ld_cg(g.nsah + base + sib);
+            const int4 sr = __ldcg(lv.rec + base + sib);
+            sib_cnt = sr.x;
+            sib_lvl = is_internal(sib, n) ? sr.w : 0;
+            sib_nsah = __int_as_float(cur_c == 1 ? sr.y : sr.z);
             sib_area = ld_cg(g.area + base + sib);
             if (ranges) my_first = min(my_first, ranges[cb + cur].x);
         }
         const bool mine_left = lc == child;
         const int cnt = my_cnt + sib_cnt;
         const float a = ld_cg(g.area + x);
-        lv.subtree[x] = cnt;
         lv.kids[cb + cur] = make_int4(lc, rc, __float_as_int(mine_left ? my_area : sib_area),
                                       __float_as_int(mine_left ? sib_area : my_area));
         int lvl = 0;
         float ns = 0.0f;
         if (cnt < gamma) {
             ns = __fadd_rn(__fadd_rn(__fmul_rn(ci, a), mine_left ? my_nsah : sib_nsah), mine_left ? sib_nsah : my_nsah);
-            g.nsah[x] = ns;
-            lv.nsah_next[x] = ns;
-            lv.level[cb + cur] = 0;
-            lv.next[cb + cur] = 0;
+            lv.rec[x] = make_int4(cnt, __float_as_int(ns), __float_as_int(ns), 0);
         } else {
             lvl = 1 + max(my_lvl, sib_lvl);
-            lv.level[cb + cur] = lvl;
+            *rec_i(lv.rec, x, 0) = cnt;
+            *rec_i(lv.rec, x, 3) = lvl;
         }
         my_cnt = cnt;
         my_lvl = lvl;
@@ -776,9 +789,7 @@ __global__ void __launch_bounds__(256) k_levels_pp(TreeRefs g, Segs segs, LevelR
     const int base = segs.node_base(m), cb = segs.inner_base(m);
     const int gamma = (seg_tsize ? (int)seg_tsize[m] : tsize_all) << iteration;
     const int li = (int)(i - s0);
-    const int leaf = base + li + (int)n - 1;
-    lv.subtree[leaf] = 1;
-    lv.nsah_next[leaf] = g.nsah[leaf];
+    // Leaves: the build's records are final (count 1, both nodesSah, level 0).
     if (li >= (int)n - 1) return;
     auto count = [&](int c) {
         if (!is_internal(c, n)) return 1;
@@ -788,19 +799,17 @@ __global__ void __launch_bounds__(256) k_levels_pp(TreeRefs g, Segs segs, LevelR
     int x = li;
     const int lc = g.left[base + x], rc = g.right[base + x];
     const int cnt = count(x);
-    lv.subtree[base + x] = cnt;
     lv.kids[cb + x] = make_int4(lc, rc, __float_as_int(g.area[base + lc]), __float_as_int(g.area[base + rc]));
     if (cnt < gamma) {
-        lv.level[cb + x] = 0;
-        lv.next[cb + x] = 0;
-        lv.nsah_next[base + x] = g.nsah[base + x];
+        const int ns = *rec_i(lv.rec, base + x, 1);  // the build's nodesSah (even iterations)
+        lv.rec[base + x] = make_int4(cnt, ns, ns, 0);
         return;
     }
-    if (levels_known) return;  // the build left every level in lv.level
+    if (levels_known) return;  // the build left every level in the records
     if (count(lc) >= gamma || count(rc) >= gamma) return;  // not a level-1 root: reached by a climb
     int lvl = 1;
     while (true) {
-        lv.level[cb + x] = lvl;
+        *rec_i(lv.rec, base + x, 3) = lvl;
         const int p = g.parent[base + x];
         if (p < 0) return;
         const int pl = g.left[base + p];
@@ -808,7 +817,7 @@ __global__ void __launch_bounds__(256) k_levels_pp(TreeRefs g, Segs segs, LevelR
         int olvl = 0;
         if (count(o) >= gamma) {
             if (atomic_add_acq_rel_gpu(&lv.counters[cb + p], 1u) == 0u) return;
-            olvl = ld_cg(lv.level + cb + o);
+            olvl = ld_cg(rec_i(lv.rec, base + o, 3));
         }
         lvl = 1 + max(lvl, olvl);
         x = p;
@@ -837,28 +846,24 @@ __global__ void __launch_bounds__(256) k_levels_pp_hist(TreeRefs g, Segs segs, L
             const int base = segs.node_base(m), cb = segs.inner_base(m);
             const int gamma = seg_tsize ? (int)seg_tsize[m] : tsize_all;
             const int li = (int)(i - s0);
-            const int leaf = base + li + (int)n - 1;
-            lv.subtree[leaf] = 1;
-            lv.nsah_next[leaf] = g.nsah[leaf];
+            // The build's records are final for every node below gamma (count,
+            // both nodesSah, level 0) and hold the level of the others.
             if (li < (int)n - 1) {
                 const int x = li;
                 const int lc = g.left[base + x], rc = g.right[base + x];
                 const int2 r = ranges[cb + x];
                 const int cnt = r.y - r.x + 1;
-                lv.subtree[base + x] = cnt;
                 lv.kids[cb + x] =
                     make_int4(lc, rc, __float_as_int(g.area[base + lc]), __float_as_int(g.area[base + rc]));
-                if (cnt < gamma) {
-                    lv.level[cb + x] = 0;
-                    lv.next[cb + x] = 0;
-                    lv.nsah_next[base + x] = g.nsah[base + x];
-                } else {
-                    const int me = lv.level[cb + x];
+                if (cnt >= gamma) {
+                    const int me = *rec_i(lv.rec, base + x, 3);
                     if (me <= L) {
                         atomicAdd(&s_hist[me], 1u);
                     } else {
-                        if ((is_internal(lc, n) ? lv.level[cb + lc] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)lc);
-                        if ((is_internal(rc, n) ? lv.level[cb + rc] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)rc);
+                        if ((is_internal(lc, n) ? *rec_i(lv.rec, base + lc, 3) : 0) <= L)
+                            ent[push++] = make_uint2(m, (uint32_t)lc);
+                        if ((is_internal(rc, n) ? *rec_i(lv.rec, base + rc, 3) : 0) <= L)
+                            ent[push++] = make_uint2(m, (uint32_t)rc);
                     }
                 }
             }
@@ -903,16 +908,19 @@ __global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, con
         const uint32_t li = i - s0;
         if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
             const int cb = segs.inner_base(m), nb = segs.node_base(m);
-            const int me = lv.level[cb + (int)li];
+            const int me = *rec_i(lv.rec, nb + (int)li, 3);
             if (me == 0) {
-                lv.next[cb + (int)li] = 0;
-                lv.nsah_next[nb + (int)li] = lv.nsah[nb + (int)li];
+                // Not a treelet root: its next nodesSah is this one (the level
+                // stays 0).
+                *rec_f(lv.rec, nb + (int)li, rec_ns_next(lv.par)) = *rec_f(lv.rec, nb + (int)li, rec_ns_cur(lv.par));
             } else if (me <= L) {
                 atomicAdd(&s_hist[me], 1u);
             } else {
                 const int4 kd = lv.kids[cb + (int)li];
-                if ((is_internal(kd.x, n) ? lv.level[cb + kd.x] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)kd.x);
-                if ((is_internal(kd.y, n) ? lv.level[cb + kd.y] : 0) <= L) ent[push++] = make_uint2(m, (uint32_t)kd.y);
+                if ((is_internal(kd.x, n) ? *rec_i(lv.rec, nb + kd.x, 3) : 0) <= L)
+                    ent[push++] = make_uint2(m, (uint32_t)kd.x);
+                if ((is_internal(kd.y, n) ? *rec_i(lv.rec, nb + kd.y, 3) : 0) <= L)
+                    ent[push++] = make_uint2(m, (uint32_t)kd.y);
             }
         }
     }
@@ -961,7 +969,7 @@ __global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, 
         const uint32_t n = segs.tri_end(m) - s0;
         li = i - s0;
         if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
-            me = lv.level[segs.inner_base(m) + (int)li];
+            me = *rec_i(lv.rec, segs.node_base(m) + (int)li, 3);
             if (me > L) me = 0;
         }
     }
@@ -1010,7 +1018,7 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
     float4* const BMN = g.bmin + nb;
     float4* const BMX = g.bmax + nb;
     float* const AR = g.area + nb;
-    float* const NS = g.nsah + nb;
+    const int next_c = rec_ns_next(nx.par);
     float* const dist = sm;
     float4* const lmn = reinterpret_cast<float4*>(sm + Lay::kDistPad);
     float4* const lmx = lmn + KL;
@@ -1093,9 +1101,9 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
     // (min.xyz, cost), (max.xyz, left child), (count, next level, next
     // nodesSah, right child).
     // A lane's leaves arrive by cp.async, all in flight at once: boxes into
-    // lmn/lmx, count, next level, next nodesSah into lcn and nodesSah parked
-    // in lcn.w, then moved to lmn.w.  Nothing else in this level pass writes
-    // a treelet leaf's records.
+    // lmn/lmx and the node's record into lcn, which the lane then rearranges
+    // (this iteration's nodesSah to lmn.w).  Nothing else in this level pass
+    // writes a treelet leaf's records.
     {
         int node[3];
 #pragma unroll
@@ -1107,23 +1115,19 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
         for (int q = 0; q < 3; ++q) {
             if (node[q] < 0) continue;
             const int k = gl + 4 * q;
-            int* const c = reinterpret_cast<int*>(lcn + k);
             cp_async16_cg(lmn + k, BMN + node[q]);
             cp_async16_cg(lmx + k, BMX + node[q]);
-            cp_async4_ca(c, nx.sub + node[q]);
-            cp_async4_ca(c + 2, nx.nsn + node[q]);
-            cp_async4_ca(c + 3, NS + node[q]);
-            if (is_internal(node[q], n)) cp_async4_ca(c + 1, nx.nlv + node[q]);
-            else c[1] = 0;
+            cp_async16_cg(lcn + k, nx.rec + node[q]);
         }
         cp_async_wait_all();
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             if (node[q] < 0) continue;
             const int k = gl + 4 * q;
-            lmn[k].w = __int_as_float(lcn[k].w);
+            const int4 r = lcn[k];
+            lmn[k].w = __int_as_float(nx.par ? r.z : r.y);
             lmx[k].w = __int_as_float(node[q]);
-            lcn[k].w = 0;
+            lcn[k] = make_int4(r.x, is_internal(node[q], n) ? r.w : 0, nx.par ? r.y : r.z, 0);
         }
     }
     __syncwarp();
@@ -1289,15 +1293,12 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
             Rt[ni] = fr;
             P[fl] = ni;
             P[fr] = ni;
-            NS[ni] = f0.w;
             const float4 mn = make_float4(f0.x, f0.y, f0.z, 0.0f);
             const float4 mx = make_float4(f1.x, f1.y, f1.z, 0.0f);
             BMN[ni] = mn;
             BMX[ni] = mx;
             AR[ni] = box_area(mn, mx);
-            nx.sub[ni] = f2.x;
-            nx.nlv[ni] = f2.y;
-            nx.nsn[ni] = __int_as_float(f2.z);
+            nx.rec[ni] = make_rec(f2.x, f0.w, __int_as_float(f2.z), f2.y, nx.par);
         }
     }
     __syncwarp();
@@ -1313,10 +1314,13 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
     // A treelet left as it was: its root's next level and next nodesSah.
     if (run && !accept && gl == 0) {
         const int lc = ld_cg(Lf + root), rc = ld_cg(Rt + root);
-        const int a = is_internal(lc, n) ? ld_cg(nx.nlv + lc) : 0;
-        const int b = is_internal(rc, n) ? ld_cg(nx.nlv + rc) : 0;
-        nx.nlv[root] = ld_cg(nx.sub + root) >= nx.gamma ? 1 + max(a, b) : 0;
-        nx.nsn[root] = __fadd_rn(__fadd_rn(__fmul_rn(ci, ld_cg(AR + root)), ld_cg(nx.nsn + lc)), ld_cg(nx.nsn + rc));
+        const int4 rl = __ldcg(nx.rec + lc), rr = __ldcg(nx.rec + rc);
+        const int a = is_internal(lc, n) ? rl.w : 0;
+        const int b = is_internal(rc, n) ? rr.w : 0;
+        *rec_i(nx.rec, root, 3) = ld_cg(rec_i(nx.rec, root, 0)) >= nx.gamma ? 1 + max(a, b) : 0;
+        *rec_f(nx.rec, root, next_c) =
+            __fadd_rn(__fadd_rn(__fmul_rn(ci, ld_cg(AR + root)), __int_as_float(next_c == 1 ? rl.y : rl.z)),
+                      __int_as_float(next_c == 1 ? rr.y : rr.z));
     }
     __syncwarp();
 }
@@ -1352,26 +1356,25 @@ __global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Seg
         int nb = 0, x = 0, tsize = 0;
         uint32_t n = 2;
         int4* kd = lv.kids;
-        int32_t* nl = lv.next;
         float root_sah = 0.0f;
         int4 rk = make_int4(-1, -1, 0, 0);
+        const int cur_c = rec_ns_cur(lv.par);
         if (has) {
             const uint2 q = lv.order[e];
             const uint32_t s0 = segs.tri_begin(q.x);
             n = segs.tri_end(q.x) - s0;
             nb = segs.node_base(q.x);
             kd = lv.kids + segs.inner_base(q.x);
-            nl = lv.next + segs.inner_base(q.x);
             x = (int)q.y;
             tsize = seg_tsize ? (int)seg_tsize[q.x] : tsize_all;
             rk = __ldcg(kd + x);
-            root_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, __ldcg(g.area + nb + x)), __ldcg(g.nsah + nb + rk.x)),
-                                 __ldcg(g.nsah + nb + rk.y));
-            if (lane == grp * gw) g.nsah[nb + x] = root_sah;
+            root_sah = __fadd_rn(__fadd_rn(__fmul_rn(ci, __ldcg(g.area + nb + x)), ld_cg(rec_f(lv.rec, nb + rk.x, cur_c))),
+                                 ld_cg(rec_f(lv.rec, nb + rk.y, cur_c)));
+            if (lane == grp * gw) *rec_f(lv.rec, nb + x, cur_c) = root_sah;
         }
         const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)tsize : 0u);
         __syncwarp();
-        const NextRefs nx{lv.subtree + nb, nl, lv.nsah_next + nb, tsize << (iteration + 1)};
+        const NextRefs nx{lv.rec + nb, lv.par, tsize << (iteration + 1)};
         float* const sm = &s_mem[w][0] + (grp < per ? grp : per - 1) * kGroupFloats;
         if constexpr (QUADS)
             process_quad<kQuadLeaves>(g, has, nb, n, x, rk, kd, nx, root_sah, tsize, maxts, ci, sm, s_rc, s_prio,
@@ -1410,41 +1413,34 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     const int max_ts = seg_tsize ? max_tsize : tsize;
     const int L = ctx->atr_levels;
     void* scratch = nullptr;
-    const size_t b_sub = align256(total_nodes * 4), b_sah = align256(total_nodes * 4), b_ctr = align256(inner * 4);
+    const size_t b_rec = align256(total_nodes * 16), b_ctr = align256(inner * 4);
     const size_t b_kid = align256(inner * 16);
     // Big nodes of levels 1..L number at most the internal nodes; frontier
     // nodes root disjoint subtrees, so they number at most the triangles.
-    // Two level arrays: this iteration's and the next one's.
-    const size_t b_lvl = align256(inner * 4), b_ord = L ? align256(inner * 8) : 0;
+    const size_t b_ord = L ? align256(inner * 8) : 0;
     const size_t b_front = L ? align256((size_t)segs.n * 8) : 0;
     const size_t b_small = L ? align256((size_t)(3 * (L + 2) + 1) * 4) : 0;
-    // The build's prepass (counts, first nodesSah, child records) serves as
-    // those arrays when its constants are this pass's.
-    const bool use_pp = prepass && prepass->nsah && karras_ranges && L > 0 && ci == kPrepassCi && ct == kPrepassCt;
+    // The build's prepass records (counts, first nodesSah, levels) serve as
+    // the optimiser's records when its constants are this pass's.
+    const bool use_pp = prepass && prepass->rec && karras_ranges && L > 0 && ci == kPrepassCi && ct == kPrepassCt;
     // ... and its levels serve as the first iteration's when its gamma is this
     // pass's treelet size (per mesh, when the sizes are per mesh).
-    const bool use_pp_levels = use_pp && prepass->level &&
-                               (seg_tsize ? prepass->seg_gamma == seg_tsize
-                                          : !prepass->seg_gamma && tsize == prepass->gamma);
-    ATR_TRY(ctx->alloc(&scratch, b_sub + (use_pp ? 1 : 2) * b_sah + b_kid + b_ctr + 2 * b_lvl + b_ord + b_front +
-                                     b_small));
+    const bool use_pp_levels = use_pp && (seg_tsize ? prepass->seg_gamma == seg_tsize
+                                                    : !prepass->seg_gamma && tsize == prepass->gamma);
+    ATR_TRY(ctx->alloc(&scratch, (use_pp ? 0 : b_rec) + b_kid + b_ctr + b_ord + b_front + b_small));
     char* p = static_cast<char*>(scratch);
     TreeRefs g = g_in;
-    int32_t* subtree = reinterpret_cast<int32_t*>(p); p += b_sub;
-    int4* kids = reinterpret_cast<int4*>(p); p += b_kid;
-    float* ns[2];  // nodesSah: this iteration's and the next one's
+    int4* rec;
     if (use_pp) {
-        ns[0] = prepass->nsah;
+        rec = prepass->rec;
     } else {
-        ns[0] = reinterpret_cast<float*>(p); p += b_sah;
+        rec = reinterpret_cast<int4*>(p);
+        p += b_rec;
     }
-    ns[1] = reinterpret_cast<float*>(p); p += b_sah;
+    int4* kids = reinterpret_cast<int4*>(p); p += b_kid;
     uint32_t* counters = reinterpret_cast<uint32_t*>(p); p += b_ctr;
-    int32_t* lvl[2];
-    lvl[0] = reinterpret_cast<int32_t*>(p); p += b_lvl;
-    lvl[1] = reinterpret_cast<int32_t*>(p); p += b_lvl;
     LevelRefs lv{};
-    lv.subtree = subtree;
+    lv.rec = rec;
     lv.counters = counters;
     lv.kids = kids;
     if (L) {
@@ -1465,11 +1461,7 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     cudaError_t e = cudaSuccess;
     ctx->phase_begin("atrbvh");
     for (int it = 0; it < iterations && e == cudaSuccess; ++it) {
-        lv.level = it == 0 && use_pp_levels ? prepass->level : lvl[it & 1];
-        lv.next = lvl[(it + 1) & 1];
-        g.nsah = lv.nsah = ns[it & 1];
-        lv.nsah_next = ns[(it + 1) & 1];
-        int32_t* const next_lv = lv.next;
+        lv.par = it & 1;
         const bool hist_done = L && it == 0 && use_pp_levels;
         // Arrival counters: for the first iteration's climbs, else only for
         // the dataflow pass (cleared again below).
@@ -1526,10 +1518,10 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         }
         if (e != cudaSuccess) break;
         switch (gw) {
-            case 8: e = launch_atrbvh_g<8>(warps, blocks, st, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, lv.nsah_next, ctx->d_error); break;
-            case 10: e = launch_atrbvh_g<10>(warps, blocks, st, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, lv.nsah_next, ctx->d_error); break;
-            case 16: e = launch_atrbvh_g<16>(warps, blocks, st, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, lv.nsah_next, ctx->d_error); break;
-            default: e = launch_atrbvh_g<32>(warps, blocks, st, g, segs, subtree, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, next_lv, lv.nsah_next, ctx->d_error); break;
+            case 8: e = launch_atrbvh_g<8>(warps, blocks, st, g, segs, rec, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, ctx->d_error); break;
+            case 10: e = launch_atrbvh_g<10>(warps, blocks, st, g, segs, rec, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, ctx->d_error); break;
+            case 16: e = launch_atrbvh_g<16>(warps, blocks, st, g, segs, rec, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, ctx->d_error); break;
+            default: e = launch_atrbvh_g<32>(warps, blocks, st, g, segs, rec, counters, kids, tsize, seg_tsize, seg_iters, it, ci, ct, gmin, start, start_count, ctx->d_error); break;
         }
         ++ctx->launches;
     }

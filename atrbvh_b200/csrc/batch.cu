@@ -117,7 +117,7 @@ int batch_run(atr_ctx* ctx, atr_batch* b, int optimizer, int tsize, int iteratio
     const bool want_pp = optimizer == 1 && (b->per_mesh_params ? b->max_iters : iterations) > 0 &&
                          ctx->atr_levels > 0 && ci == kPrepassCi && ct == kPrepassCt;
     if (want_pp) {
-        ATR_TRY(prepass_alloc(ctx, b->total_nodes, b->n - b->count, &ppb, &pp));
+        ATR_TRY(prepass_alloc(ctx, b->total_nodes, &ppb, &pp));
         if (b->per_mesh_params) pp.seg_gamma = b->d_tsize;  // first iteration: gamma = each mesh's treelet size
         else pp.gamma = tsize;
     }

@@ -49,16 +49,16 @@ constexpr int kNumSms = 148;  // B200
 // Round up to a multiple of 256 bytes (alignment of every sub-array).
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-// What the LBVH build's climb leaves for the first ATRBVH iteration: every
-// node's nodesSah under the reference's default constants, node-indexed in
-// the batch layout, and every internal node's level among the nodes of at
-// least `gamma` triangles (0 below gamma, else 1 + the larger level of its
-// children; gamma per mesh when seg_gamma is set), indexed by internal node
-// in the batch layout (NULL: not computed).  Subtree counts follow from the
-// radix tree's leaf ranges.
+// What the LBVH build's climb leaves for the first ATRBVH iteration: the
+// optimiser's per-node record (node-indexed in the batch layout) -- subtree
+// triangle count, nodesSah under the reference's default constants, the
+// next iteration's nodesSah (the same value below `gamma` triangles, where the
+// node is not a treelet root; 0 otherwise, until the optimiser writes it) and
+// the node's level among the nodes of at least `gamma` triangles (0 below
+// gamma, else 1 + the larger level of its children; gamma per mesh when
+// seg_gamma is set).
 struct BuildPrepass {
-    float* nsah = nullptr;
-    int32_t* level = nullptr;
+    int4* rec = nullptr;
     int gamma = 0;
     const uint8_t* seg_gamma = nullptr;  // per-mesh gamma (device), in place of gamma when set
 };
@@ -267,9 +267,9 @@ int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4
                     const float* d_bounds, int morton_bits, const TreeOut& out, void** keep_keys,
                     uint32_t** keep_idx, const BuildPrepass* prepass = nullptr,
                     const PrimBoxes* prims = nullptr);
-// Allocate the prepass arrays for total_nodes nodes and inner internal nodes
-// in one block (*block receives the allocation).
-int prepass_alloc(atr_ctx* ctx, size_t total_nodes, size_t inner, void** block, BuildPrepass* pp);
+// Allocate the prepass record for total_nodes nodes (*block receives the
+// allocation).
+int prepass_alloc(atr_ctx* ctx, size_t total_nodes, void** block, BuildPrepass* pp);
 
 int atrbvh_run(atr_ctx* ctx, const TreeRefs& g, const Segs& segs, size_t total_nodes, int tsize,
                int max_tsize, int iterations, const uint8_t* seg_tsize, const uint8_t* seg_iters, float ci,

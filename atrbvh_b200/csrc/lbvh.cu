@@ -536,8 +536,11 @@ __device__ __forceinline__ void write_inner(const BuildOut<K>& o, const Segs& se
     o.bmin[nb + p] = mn;
     o.bmax[nb + p] = mx;
     o.area[nb + p] = pa;
-    if (o.pp.nsah) o.pp.nsah[nb + p] = ns;
-    if (o.pp.level) o.pp.level[segs.inner_base(m) + p] = lvl;
+    if (o.pp.rec) {
+        const int cnt = pr - pl + 1;
+        const int gam = o.pp.seg_gamma ? (int)o.pp.seg_gamma[m] : o.pp.gamma;
+        o.pp.rec[nb + p] = make_int4(cnt, __float_as_int(ns), cnt < gam ? __float_as_int(ns) : 0, lvl);
+    }
 }
 
 constexpr int kBuildBlock = 256;
@@ -602,7 +605,7 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
         // Prepass for the first ATRBVH iteration: this subtree's nodesSah under
         // the default constants, (ci*A + left) + right bottom-up from ct*A at leaves.
         my_ns = __fmul_rn(kPrepassCt, my_area);
-        if (o.pp.nsah) o.pp.nsah[nb + leaf] = my_ns;
+        if (o.pp.rec) o.pp.rec[nb + leaf] = make_int4(1, __float_as_int(my_ns), __float_as_int(my_ns), 0);
         s_lmn[tid] = mn;
         s_lmx[tid] = mx;
         s_lns[tid] = my_ns;
@@ -649,11 +652,9 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
                 p = dr > dl ? pr : pl;
             }
             const float pa = box_area(mn, mx);
-            if (o.pp.nsah) {
+            if (o.pp.rec) {
                 const float sns = sib_leaf ? s_lns[sp] : s_ins[sp];
                 my_ns = __fadd_rn(__fadd_rn(__fmul_rn(kPrepassCi, pa), is_left ? my_ns : sns), is_left ? sns : my_ns);
-            }
-            if (o.pp.level) {
                 const int gam = o.pp.seg_gamma ? (int)o.pp.seg_gamma[m] : o.pp.gamma;
                 my_lv = pr - pl + 1 >= gam ? 1 + max(my_lv, sib_leaf ? 0 : s_ilv[sp]) : 0;
             }
@@ -689,9 +690,13 @@ __global__ void __launch_bounds__(256) k_build_top(Segs segs, const K* __restric
     const K* keys = keys_all + s0;
     int32_t* slot = o.slot + segs.inner_base(m);
     float4 mn = ld_cg(o.bmin + nb + e.node), mx = ld_cg(o.bmax + nb + e.node);
-    float my_ns = o.pp.nsah ? ld_cg(o.pp.nsah + nb + e.node) : 0.0f;
-    const int32_t* const plv = o.pp.level + segs.inner_base(m);
-    int my_lv = o.pp.level && e.node < last ? ld_cg(plv + e.node) : 0;
+    float my_ns = 0.0f;
+    int my_lv = 0;
+    if (o.pp.rec) {
+        const int4 r0 = __ldcg(o.pp.rec + nb + e.node);
+        my_ns = __int_as_float(r0.y);
+        my_lv = r0.w;  // 0 at a leaf
+    }
     int l = e.l, r = e.r;
     int dl = l > 0 ? delta_adj(keys, l - 1) : -1;
     int dr = r < last ? delta_adj(keys, r) : -1;
@@ -716,14 +721,13 @@ __global__ void __launch_bounds__(256) k_build_top(Segs segs, const K* __restric
             p = dr > dl ? pr : pl;
         }
         const float pa = box_area(mn, mx);
-        if (o.pp.nsah) {
-            const float sns = ld_cg(o.pp.nsah + nb + sib);
+        if (o.pp.rec) {
+            const int4 sr = __ldcg(o.pp.rec + nb + sib);
+            const float sns = __int_as_float(sr.y);
             my_ns = __fadd_rn(__fadd_rn(__fmul_rn(kPrepassCi, pa), is_left ? my_ns : sns), is_left ? sns : my_ns);
+            my_lv = pr - pl + 1 >= (o.pp.seg_gamma ? (int)o.pp.seg_gamma[m] : o.pp.gamma) ? 1 + max(my_lv, sr.w)
+                                                                                          : 0;
         }
-        if (o.pp.level)
-            my_lv = pr - pl + 1 >= (o.pp.seg_gamma ? (int)o.pp.seg_gamma[m] : o.pp.gamma)
-                        ? 1 + max(my_lv, sib < last ? ld_cg(plv + sib) : 0)
-                        : 0;
         write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns, my_lv);
         if (root) {
             o.parent[nb] = -1;
@@ -952,10 +956,9 @@ int lbvh_build_segs(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4
                : build_typed<uint64_t, 8>(ctx, segs, tiles, verts, d_bounds, out, keep_keys, keep_idx, pp, pr);
 }
 
-int prepass_alloc(atr_ctx* ctx, size_t total_nodes, size_t inner, void** block, BuildPrepass* pp) {
-    ATR_TRY(ctx->alloc(block, align256(total_nodes * 4) + inner * 4));
-    pp->nsah = static_cast<float*>(*block);
-    pp->level = reinterpret_cast<int32_t*>(static_cast<char*>(*block) + align256(total_nodes * 4));
+int prepass_alloc(atr_ctx* ctx, size_t total_nodes, void** block, BuildPrepass* pp) {
+    ATR_TRY(ctx->alloc(block, total_nodes * 16));
+    pp->rec = static_cast<int4*>(*block);
     pp->gamma = kPrepassGamma;
     return ATR_OK;
 }
@@ -975,7 +978,7 @@ int lbvh_build_into(atr_ctx* ctx, const float4* verts, uint32_t n, const float* 
     t->prepass_block = nullptr;
     t->prepass = BuildPrepass{};
     if (ctx->atr_levels > 0)
-        ATR_TRY(prepass_alloc(ctx, 2 * (size_t)n - 1, n - 1, &t->prepass_block, &t->prepass));
+        ATR_TRY(prepass_alloc(ctx, 2 * (size_t)n - 1, &t->prepass_block, &t->prepass));
     ATR_TRY(lbvh_build_segs(ctx, segs, tiles, verts, d_bounds, morton_bits, out, &keys, &idx,
                             t->prepass_block ? &t->prepass : nullptr, prims));
     ctx->release(t->sorted_keys);
