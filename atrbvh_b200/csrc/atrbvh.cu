@@ -151,6 +151,146 @@ __device__ __forceinline__ float union_area3(float ax0, float ay0, float az0, fl
                __fsub_rn(fmaxf(az1, bz1), fminf(az0, bz0)));
 }
 
+// Treelets of at most kRegTreelet leaves on a whole warp (the dataflow
+// pass's single treelets, whose latency is the pass's critical path): the
+// merge and rewrite with every slot in its lane's registers and the distance
+// matrix in two registers per lane (pair j in lane j % 32, register j / 32),
+// exchanged by shuffles instead of shared memory.  Same choices, same
+// arithmetic as the shared-memory merge below (AgglomerativeTreelet.cu:
+// 101-212, 476-532); lane k < tsize enters holding leaf k.
+constexpr int kRegTreelet = 11;  // 55 pairs fit two registers per lane
+
+struct RegSlot {
+    Box b;
+    float sah;   // nodesSah, or the merge cost of a new node
+    int node;    // node id; a retired slot's left child
+    int cnt;     // subtree triangle count
+    int nlv;     // next-iteration level
+    float nsn;   // next-iteration nodesSah
+};
+
+__device__ __forceinline__ RegSlot shfl_slot(const RegSlot& s, int src) {
+    RegSlot o;
+    o.b = shfl_box(s.b, src);
+    o.sah = __shfl_sync(kFull, s.sah, src);
+    o.node = __shfl_sync(kFull, s.node, src);
+    o.cnt = __shfl_sync(kFull, s.cnt, src);
+    o.nlv = __shfl_sync(kFull, s.nlv, src);
+    o.nsn = __shfl_sync(kFull, s.nsn, src);
+    return o;
+}
+
+__device__ __forceinline__ void merge_rewrite_regs(const TreeRefs& g, int nb, uint32_t n, int root, RegSlot sl,
+                                                   int internal_node, int4* KD, const NextRefs& nx,
+                                                   float root_sah, int tsize, float ci,
+                                                   const uint16_t* __restrict__ s_rc) {
+    const int lane = threadIdx.x & 31;
+    int32_t* const P = g.parent + nb;
+    int32_t* const Lf = g.left + nb;
+    int32_t* const Rt = g.right + nb;
+    float4* const BMN = g.bmin + nb;
+    float4* const BMX = g.bmax + nb;
+    float* const AR = g.area + nb;
+    const int next_c = rec_ns_next(nx.par);
+    // Pair coordinates (row > column) of this lane's two pairs.
+    const uint32_t rc0 = s_rc[lane], rc1 = s_rc[lane + 32];
+    const int r0 = (int)(rc0 >> 8), c0 = (int)(rc0 & 255u), r1 = (int)(rc1 >> 8), c1 = (int)(rc1 & 255u);
+    float d0, d1;
+    {
+        const Box a0 = shfl_box(sl.b, r0), b0 = shfl_box(sl.b, c0);
+        const Box a1 = shfl_box(sl.b, r1), b1 = shfl_box(sl.b, c1);
+        d0 = union_area(a0, b0);
+        d1 = union_area(a1, b1);
+    }
+    int right = 0;  // a retired slot's right child
+    for (int last = tsize - 1; last >= 1; --last) {
+        // The minimum distance over pairs j < last (last + 1) / 2, then the
+        // lowest (brev5(j % 32), j) among the pairs holding it -- the lane-
+        // strided scan's choice.
+        const int msize = last * (last + 1) / 2;
+        float bd = FLT_MAX;
+        int bj = -1;
+        if (lane < msize && d0 < bd) { bd = d0; bj = lane; }
+        if (lane + 32 < msize && d1 < bd) { bd = d1; bj = lane + 32; }
+        const uint32_t db = bj >= 0 ? __float_as_uint(bd) : 0xffffffffu;
+        const uint32_t dmin = __reduce_min_sync(kFull, db);
+        const uint32_t tk =
+            (bj >= 0 && db == dmin) ? (((__brev((uint32_t)lane) >> 27) << 8) | (uint32_t)bj) : 0xffffffffu;
+        const uint32_t kmin = __reduce_min_sync(kFull, tk);
+        const int mi = dmin == 0xffffffffu ? 0 : (int)(kmin & 255u);
+        const uint32_t rc = s_rc[mi];
+        const int jr = (int)(rc >> 8), jc = (int)(rc & 255u);
+        const RegSlot r = shfl_slot(sl, jr), c = shfl_slot(sl, jc), z = shfl_slot(sl, last);
+        const int new_internal = __shfl_sync(kFull, internal_node, last - 1);
+        // updateState (:101-150): the new node (rows jr and jc) takes slot jc,
+        // slot `last` moves to slot jr, slot `last` retires holding the new
+        // node (left child row jr's node, right child row jc's).
+        RegSlot nw;
+        nw.b.mnx = fminf(c.b.mnx, r.b.mnx); nw.b.mny = fminf(c.b.mny, r.b.mny); nw.b.mnz = fminf(c.b.mnz, r.b.mnz);
+        nw.b.mxx = fmaxf(c.b.mxx, r.b.mxx); nw.b.mxy = fmaxf(c.b.mxy, r.b.mxy); nw.b.mxz = fmaxf(c.b.mxz, r.b.mxz);
+        const float area_new = box_area(nw.b.mnx, nw.b.mny, nw.b.mnz, nw.b.mxx, nw.b.mxy, nw.b.mxz);
+        nw.sah = __fadd_rn(__fadd_rn(r.sah, c.sah), __fmul_rn(ci, area_new));
+        nw.cnt = r.cnt + c.cnt;
+        nw.nlv = nw.cnt >= nx.gamma ? 1 + max(r.nlv, c.nlv) : 0;
+        nw.nsn = __fadd_rn(__fadd_rn(__fmul_rn(ci, area_new), r.nsn), c.nsn);
+        nw.node = new_internal;
+        if (lane == jc) sl = nw;
+        if (lane == jr) sl = z;
+        if (lane == last) {
+            sl = nw;
+            sl.node = r.node;
+            right = c.node;
+        }
+        // updateDistancesMatrix (:152-188): pairs (jc, k) take the union with
+        // the new node (lane k computes it), pairs (jr, k) take the distance
+        // of pair (last, k) as the step began.
+        const float u = union_area(nw.b, sl.b);
+        const int o0 = r0 + c0 - (r0 == jc || c0 == jc ? jc : jr);
+        const int o1 = r1 + c1 - (r1 == jc || c1 == jc ? jc : jr);
+        const int t0 = trm_idx(last, min(o0, last - 1)), t1 = trm_idx(last, min(o1, last - 1));
+        const float u0 = __shfl_sync(kFull, u, o0 & 31), u1 = __shfl_sync(kFull, u, o1 & 31);
+        const float m00 = __shfl_sync(kFull, d0, t0 & 31), m01 = __shfl_sync(kFull, d1, t0 & 31);
+        const float m10 = __shfl_sync(kFull, d0, t1 & 31), m11 = __shfl_sync(kFull, d1, t1 & 31);
+        if (r0 < last) {
+            if (r0 == jc || c0 == jc) d0 = u0;
+            else if (r0 == jr || c0 == jr) d0 = t0 >= 32 ? m01 : m00;
+        }
+        if (r1 < last) {
+            if (r1 == jc || c1 == jc) d1 = u1;
+            else if (r1 == jr || c1 == jr) d1 = t1 >= 32 ? m11 : m10;
+        }
+    }
+    // ---- updateTreelet (:190-212): slot k >= 1 holds the k-th new node ----
+    const int ni = __shfl_sync(kFull, internal_node, lane > 0 ? lane - 1 : 0);
+    const bool accept = __shfl_sync(kFull, sl.sah, 1) < root_sah;
+    const bool wr = accept && lane >= 1 && lane < tsize;
+    if (wr) {
+        Lf[ni] = sl.node;
+        Rt[ni] = right;
+        P[sl.node] = ni;
+        P[right] = ni;
+        const float4 mn = make_float4(sl.b.mnx, sl.b.mny, sl.b.mnz, 0.0f);
+        const float4 mx = make_float4(sl.b.mxx, sl.b.mxy, sl.b.mxz, 0.0f);
+        BMN[ni] = mn;
+        BMX[ni] = mx;
+        AR[ni] = box_area(mn, mx);
+        nx.rec[ni] = make_rec(sl.cnt, sl.sah, sl.nsn, sl.nlv, nx.par);
+    }
+    __syncwarp();
+    if (wr) KD[ni] = make_int4(sl.node, right, __float_as_int(__ldcg(AR + sl.node)), __float_as_int(__ldcg(AR + right)));
+    if (!accept && lane == 0) {
+        const int lc = ld_cg(Lf + root), rc = ld_cg(Rt + root);
+        const int4 rl = __ldcg(nx.rec + lc), rr = __ldcg(nx.rec + rc);
+        const int a = is_internal(lc, n) ? rl.w : 0;
+        const int b = is_internal(rc, n) ? rr.w : 0;
+        *rec_i(nx.rec, root, 3) = ld_cg(rec_i(nx.rec, root, 0)) >= nx.gamma ? 1 + max(a, b) : 0;
+        *rec_f(nx.rec, root, next_c) =
+            __fadd_rn(__fadd_rn(__fmul_rn(ci, ld_cg(AR + root)), __int_as_float(next_c == 1 ? rl.y : rl.z)),
+                      __int_as_float(next_c == 1 ? rr.y : rr.z));
+    }
+    __syncwarp();
+}
+
 // One treelet per lane group.  Lanes of a group hold the same root/mesh
 // arguments; `active` is false for groups without a treelet (and for lanes
 // outside every group).  maxts is the largest treelet size of the active
@@ -260,6 +400,19 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     // the slots the merge state reuses.
     cp_async_wait_all();
     __syncwarp();
+    if constexpr (G == 32) {
+        if (run && tsize <= kRegTreelet) {
+            RegSlot sl;
+            sl.b = Box{s_mn.x, s_mn.y, s_mn.z, s_mx.x, s_mx.y, s_mx.z};
+            sl.sah = s_sah;
+            sl.node = s_node;
+            sl.cnt = s_cnt;
+            sl.nlv = s_nlv;
+            sl.nsn = s_nsn;
+            merge_rewrite_regs(g, nb, n, root, sl, internal_node, KD, nx, root_sah, tsize, ci, s_rc);
+            return;
+        }
+    }
 
     // ---- distance matrix (AgglomerativeTreelet.cu:18-63) ----
     // Slot k: (min.xyz, nodesSah), (max.xyz, node), (count, next level,
@@ -484,7 +637,7 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
 // when `seg_tsize`/`seg_iters` are given; a mesh whose iterations are done
 // sits this launch out.
 template <int G, int W>
-__global__ void __launch_bounds__(W * 32, 32 / W) k_atrbvh(TreeRefs g, Segs segs, int4* __restrict__ rec,
+__global__ void __launch_bounds__(W * 32, 16 / W) k_atrbvh(TreeRefs g, Segs segs, int4* __restrict__ rec,
                                                    uint32_t* __restrict__ counters, int4* __restrict__ kids,
                                                    int tsize_all,
                                                    const uint8_t* __restrict__ seg_tsize,

@@ -121,7 +121,7 @@ def test_refit_bit_exact(ctx, case):
 ATR_CASES = ["u17", "u100", "u1000", "u4097", "clu4096", "dupes3000", "flat2000", "same64"]
 
 
-@pytest.mark.parametrize("treelet,iters", [(3, 1), (5, 1), (7, 2), (9, 2), (9, 3), (12, 2), (16, 1), (20, 1)])
+@pytest.mark.parametrize("treelet,iters", [(3, 1), (5, 1), (7, 2), (9, 2), (9, 3), (10, 1), (11, 2), (12, 2), (16, 1), (20, 1)])
 @pytest.mark.parametrize("case", ATR_CASES)
 def test_atrbvh_bit_exact(ctx, case, treelet, iters):
     v = scene_case(case)
