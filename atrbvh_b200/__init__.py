@@ -36,6 +36,7 @@ TUNE_ATR_GROUP_MIN = 1
 TUNE_SORT_BITS = 2
 TUNE_ATR_LEVELS = 3
 TUNE_QUAD_MIN = 4
+TUNE_WARP_MAX = 5
 
 
 class AtrError(RuntimeError):

@@ -204,6 +204,10 @@ int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value) {
             ATR_REQUIRE(value >= -1, ATR_ERR_INVALID_ARG, "atr_ctx_set_tuning: quad threshold %d below -1", value);
             ctx->atr_quad_min = value;
             return ATR_OK;
+        case ATR_TUNE_WARP_MAX:
+            ATR_REQUIRE(value >= 0, ATR_ERR_INVALID_ARG, "atr_ctx_set_tuning: whole-warp threshold %d below 0", value);
+            ctx->atr_warp_max = value;
+            return ATR_OK;
         default:
             break;
     }
@@ -218,6 +222,7 @@ int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value) {
         case ATR_TUNE_SORT_BITS: *value = ctx->sort_bits; return ATR_OK;
         case ATR_TUNE_ATR_LEVELS: *value = ctx->atr_levels; return ATR_OK;
         case ATR_TUNE_QUAD_MIN: *value = ctx->atr_quad_min; return ATR_OK;
+        case ATR_TUNE_WARP_MAX: *value = ctx->atr_warp_max; return ATR_OK;
         default: break;
     }
     ATR_REQUIRE(false, ATR_ERR_INVALID_ARG, "atr_ctx_get_tuning: unknown knob %d", knob);

@@ -167,6 +167,7 @@ struct RegSlot {
     int cnt;     // subtree triangle count
     int nlv;     // next-iteration level
     float nsn;   // next-iteration nodesSah
+    float area;  // the node's stored area; a retired slot's left child's
 };
 
 __device__ __forceinline__ RegSlot shfl_slot(const RegSlot& s, int src) {
@@ -177,6 +178,7 @@ __device__ __forceinline__ RegSlot shfl_slot(const RegSlot& s, int src) {
     o.cnt = __shfl_sync(kFull, s.cnt, src);
     o.nlv = __shfl_sync(kFull, s.nlv, src);
     o.nsn = __shfl_sync(kFull, s.nsn, src);
+    o.area = __shfl_sync(kFull, s.area, src);
     return o;
 }
 
@@ -202,7 +204,8 @@ __device__ __forceinline__ void merge_rewrite_regs(const TreeRefs& g, int nb, ui
         d0 = union_area(a0, b0);
         d1 = union_area(a1, b1);
     }
-    int right = 0;  // a retired slot's right child
+    int right = 0;       // a retired slot's right child
+    float right_area = 0.0f;  // and its stored area
     for (int last = tsize - 1; last >= 1; --last) {
         // The minimum distance over pairs j < last (last + 1) / 2, then the
         // lowest (brev5(j % 32), j) among the pairs holding it -- the lane-
@@ -234,12 +237,15 @@ __device__ __forceinline__ void merge_rewrite_regs(const TreeRefs& g, int nb, ui
         nw.nlv = nw.cnt >= nx.gamma ? 1 + max(r.nlv, c.nlv) : 0;
         nw.nsn = __fadd_rn(__fadd_rn(__fmul_rn(ci, area_new), r.nsn), c.nsn);
         nw.node = new_internal;
+        nw.area = area_new;  // what the rewrite stores: box_area of the same box
         if (lane == jc) sl = nw;
         if (lane == jr) sl = z;
         if (lane == last) {
             sl = nw;
             sl.node = r.node;
+            sl.area = r.area;
             right = c.node;
+            right_area = c.area;
         }
         // updateDistancesMatrix (:152-188): pairs (jc, k) take the union with
         // the new node (lane k computes it), pairs (jr, k) take the distance
@@ -276,8 +282,10 @@ __device__ __forceinline__ void merge_rewrite_regs(const TreeRefs& g, int nb, ui
         AR[ni] = box_area(mn, mx);
         nx.rec[ni] = make_rec(sl.cnt, sl.sah, sl.nsn, sl.nlv, nx.par);
     }
-    __syncwarp();
-    if (wr) KD[ni] = make_int4(sl.node, right, __float_as_int(__ldcg(AR + sl.node)), __float_as_int(__ldcg(AR + right)));
+    // The rewritten nodes' child records: children and their stored areas
+    // (new nodes' as just stored, the treelet leaves' as their parents'
+    // records held them).
+    if (wr) KD[ni] = make_int4(sl.node, right, __float_as_int(sl.area), __float_as_int(right_area));
     if (!accept && lane == 0) {
         const int lc = ld_cg(Lf + root), rc = ld_cg(Rt + root);
         const int4 rl = __ldcg(nx.rec + lc), rr = __ldcg(nx.rec + rc);
@@ -342,13 +350,18 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
         int largest;
         if constexpr (G == 32) {
             // Largest value (internal nodes' areas as bits + 1, which order like
-            // the areas; other leaves 0, the reference's -FLT_MAX), then the
-            // first lane in the tree's tie order.
+            // the areas; other leaves 0, the reference's -FLT_MAX), then, among
+            // several lanes holding it, the first in the tree's tie order.
             const uint32_t ev = (gl < m && is_internal(s_node, n)) ? __float_as_uint(s_area) + 1u : 0u;
             const uint32_t vmax = __reduce_max_sync(kFull, ev);
-            const uint32_t pk = (gl < m && ev == vmax) ? (uint32_t)s_prio[m * 32 + gl] : 255u;
-            const uint32_t pmin = __reduce_min_sync(kFull, pk);
-            largest = __ffs(__ballot_sync(kFull, pk == pmin)) - 1;
+            const uint32_t tied = __ballot_sync(kFull, gl < m && ev == vmax);
+            if (__popc(tied) == 1) {
+                largest = __ffs(tied) - 1;
+            } else {
+                const uint32_t pk = ((tied >> gl) & 1u) ? (uint32_t)s_prio[m * 32 + gl] : 255u;
+                const uint32_t pmin = __reduce_min_sync(kFull, pk);
+                largest = __ffs(__ballot_sync(kFull, pk == pmin)) - 1;
+            }
         } else {
             float v = (gl < m && is_internal(s_node, n)) ? s_area : -FLT_MAX;
             int ix = gl;
@@ -409,6 +422,7 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
             sl.cnt = s_cnt;
             sl.nlv = s_nlv;
             sl.nsn = s_nsn;
+            sl.area = s_area;
             merge_rewrite_regs(g, nb, n, root, sl, internal_node, KD, nx, root_sah, tsize, ci, s_rc);
             return;
         }
@@ -1481,7 +1495,7 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
 // Phase C: every treelet root of level `lev`.  Each warp takes `per` roots
 // at a time: 32/G in lane groups of G, or (QUADS) eight in four-lane groups.
 template <int G, int W, bool QUADS>
-__global__ void __launch_bounds__(W * 32, 32 / W) k_level_groups(TreeRefs g, Segs segs, LevelRefs lv, int lev,
+__global__ void __launch_bounds__(W * 32, (G == 32 ? 16 : 32) / W) k_level_groups(TreeRefs g, Segs segs, LevelRefs lv, int lev,
                                                                  int tsize_all, const uint8_t* __restrict__ seg_tsize,
                                                                  int iteration, float ci, uint32_t* err) {
     constexpr int per = QUADS ? 8 : GroupLayout<G>::kGroups;
@@ -1647,13 +1661,18 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
             const unsigned lg = (unsigned)ctx->num_sms * (256 / threads) * 4;
             // Roots per level fall by about 0.62 per level from n / (1.5 gamma)
             // at level 1 (gamma = tsize << it); levels expected to hold at
-            // least atr_quad_min roots run in four-lane groups.
+            // least atr_quad_min roots run in four-lane groups, levels expected
+            // to hold at most atr_warp_max one treelet per warp (the shortest
+            // latency per treelet, for levels too narrow to fill the GPU).
             const double gamma = (double)(tsize << it);
             double expect = (double)segs.n / (1.5 * gamma);
             for (int lev = 1; lev <= L; ++lev, expect *= 0.62) {
                 const bool quads = max_ts <= kQuadLeaves && ctx->atr_quad_min >= 0 && expect >= ctx->atr_quad_min;
+                const bool whole = !quads && max_ts <= kRegTreelet && expect <= (double)ctx->atr_warp_max;
                 if (quads) {
                     launch_level_g<8, true>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error);
+                } else if (whole) {
+                    launch_level_g<32, false>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error);
                 } else {
                     switch (gw) {
                         case 8: launch_level_g<8, false>(warps, lg, st, g, segs, lv, lev, tsize, seg_tsize, it, ci, ctx->d_error); break;

@@ -38,7 +38,7 @@ struct atr_batch {
     void* block = nullptr;
     atr::TreeOut tree{};
     cudaGraphExec_t graph = nullptr;
-    int graph_key[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // build parameters and launch tuning of the graph
+    int graph_key[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // build parameters and launch tuning of the graph
     float graph_cf[2] = {0, 0};
     uint64_t graph_launches = 0;
     // Collapsed trees and Compact2 layouts (allocated on first use).
@@ -259,9 +259,9 @@ int atr_batch_build(atr_ctx* ctx, atr_batch* b, int optimizer, int treelet_size,
     ATR_REQUIRE(iterations >= 0 && iterations <= 24, ATR_ERR_INVALID_ARG, "atr_batch_build: iterations %d",
                 iterations);
     if (!use_graph) return batch_run(ctx, b, optimizer, treelet_size, iterations, ci, ct);
-    const int key[9] = {optimizer,        treelet_size,       iterations,      b->per_mesh_params ? 1 : 0,
-                        ctx->atr_warps,   ctx->atr_group_min, ctx->sort_bits,  ctx->atr_levels,
-                        ctx->atr_quad_min};
+    const int key[10] = {optimizer,        treelet_size,       iterations,      b->per_mesh_params ? 1 : 0,
+                         ctx->atr_warps,   ctx->atr_group_min, ctx->sort_bits,  ctx->atr_levels,
+                         ctx->atr_quad_min, ctx->atr_warp_max};
     const bool same = b->graph && std::memcmp(key, b->graph_key, sizeof(key)) == 0 && b->graph_cf[0] == ci &&
                       b->graph_cf[1] == ct;
     if (!same) {

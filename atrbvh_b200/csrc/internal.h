@@ -101,6 +101,7 @@ struct atr_ctx {
     // A level pass over at least this many treelet roots restructures them in
     // four-lane groups (eight per warp); -1 = never.
     int atr_quad_min = 50000;
+    int atr_warp_max = 4096;
     struct Phase {
         std::string name;
         cudaEvent_t a, b;

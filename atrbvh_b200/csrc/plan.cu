@@ -33,7 +33,7 @@ struct atr_plan {
     float* d_sah = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // start, collapsed, end
     cudaGraphExec_t graph = nullptr;
-    int graph_key[5] = {0, 0, 0, 0, 0};
+    int graph_key[6] = {0, 0, 0, 0, 0, 0};
     uint64_t graph_launches = 0;
     bool ran = false;
     bool sizes_read = false;
@@ -47,12 +47,13 @@ struct atr_plan {
 namespace atr {
 namespace {
 
-void plan_tuning_key(const atr_ctx* ctx, int key[5]) {
+void plan_tuning_key(const atr_ctx* ctx, int key[6]) {
     key[0] = ctx->atr_warps;
     key[1] = ctx->atr_group_min;
     key[2] = ctx->sort_bits;
     key[3] = ctx->atr_levels;
     key[4] = ctx->atr_quad_min;
+    key[5] = ctx->atr_warp_max;
 }
 
 // Marks a point of the run; while capturing, as an external record node so
@@ -179,7 +180,7 @@ int atr_plan_run(atr_ctx* ctx, atr_plan* P, int use_graph) {
         P->ran = st == ATR_OK;
         return st;
     }
-    int key[5];
+    int key[6];
     plan_tuning_key(ctx, key);
     if (!P->graph || std::memcmp(key, P->graph_key, sizeof(key)) != 0) {
         if (P->graph) {

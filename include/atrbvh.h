@@ -119,13 +119,19 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
  *   ATR_TUNE_QUAD_MIN       fewest treelet roots of one level that the level
  *                           pass restructures in four-lane groups, eight per
  *                           warp, instead of 32/G per warp (-1 = never;
- *                           default 50000). */
+ *                           default 50000).
+ *   ATR_TUNE_WARP_MAX       most treelet roots of one level that the level
+ *                           pass restructures one per warp, with the
+ *                           treelet's slots and distances in registers
+ *                           (treelets of at most 11 leaves; 0 = never;
+ *                           default 4096). */
 enum atr_tune_knob {
     ATR_TUNE_ATR_WARPS = 0,
     ATR_TUNE_ATR_GROUP_MIN = 1,
     ATR_TUNE_SORT_BITS = 2,
     ATR_TUNE_ATR_LEVELS = 3,
-    ATR_TUNE_QUAD_MIN = 4
+    ATR_TUNE_QUAD_MIN = 4,
+    ATR_TUNE_WARP_MAX = 5
 };
 int atr_ctx_set_tuning(atr_ctx* ctx, int knob, int value);
 int atr_ctx_get_tuning(atr_ctx* ctx, int knob, int* value);

@@ -34,15 +34,18 @@ def test_ten_bit_sort_digits_bit_exact(tuned_ctx, case, bits):
     assert_trees_equal(ab.BVHTreeInstanceManager().DeviceToHostTree(tree), want, f"{case}/{bits} 10-bit digits")
 
 
-@pytest.mark.parametrize("warps,gmin,levels,qmin", [(2, 2, 16, 0), (8, 2, 16, 0), (4, 3, 0, 0), (4, 33, 0, -1),
-                                                    (4, 2, 1, 0), (4, 2, 4, -1), (2, 2, 64, 0), (4, 2, 16, 0),
-                                                    (4, 2, 16, -1), (8, 2, 64, 1000)])
-@pytest.mark.parametrize("treelet,iters", [(3, 1), (5, 2), (9, 2), (10, 3), (12, 1), (20, 1)])
-def test_atrbvh_launch_tuning_bit_exact(tuned_ctx, warps, gmin, levels, qmin, treelet, iters):
+@pytest.mark.parametrize("warps,gmin,levels,qmin,wmax", [(2, 2, 16, 0, 0), (8, 2, 16, 0, 0), (4, 3, 0, 0, 0),
+                                                         (4, 33, 0, -1, 0), (4, 2, 1, 0, 0), (4, 2, 4, -1, 0),
+                                                         (2, 2, 64, 0, 0), (4, 2, 16, 0, 0), (4, 2, 16, -1, 0),
+                                                         (8, 2, 64, 1000, 0), (8, 2, 12, -1, 1 << 30),
+                                                         (2, 2, 16, 1000, 500), (8, 2, 12, 50000, 8192)])
+@pytest.mark.parametrize("treelet,iters", [(3, 1), (5, 2), (9, 2), (10, 3), (11, 2), (12, 1), (20, 1)])
+def test_atrbvh_launch_tuning_bit_exact(tuned_ctx, warps, gmin, levels, qmin, wmax, treelet, iters):
     tuned_ctx.set_tuning(ab.TUNE_ATR_WARPS, warps)
     tuned_ctx.set_tuning(ab.TUNE_ATR_GROUP_MIN, gmin)
     tuned_ctx.set_tuning(ab.TUNE_ATR_LEVELS, levels)
     tuned_ctx.set_tuning(ab.TUNE_QUAD_MIN, qmin)
+    tuned_ctx.set_tuning(ab.TUNE_WARP_MAX, wmax)
     v = scene_case("clu65536")
     mn, mx = O.scene_aabb(v)
     base, _, _ = O.build_lbvh(v, mn, mx, threads=8)
@@ -51,12 +54,13 @@ def test_atrbvh_launch_tuning_bit_exact(tuned_ctx, warps, gmin, levels, qmin, tr
     tree = ab.LBVHBuilder().BuildTree(scene)
     ab.AgglomerativeTreeletOptimizer(treelet, iters).Optimize(tree)
     assert_trees_equal(ab.BVHTreeInstanceManager().DeviceToHostTree(tree), want,
-                       f"ATRBVH({treelet},{iters}) warps {warps} group_min {gmin} levels {levels} quads {qmin}")
+                       f"ATRBVH({treelet},{iters}) warps {warps} group_min {gmin} levels {levels} quads {qmin} "
+                       f"whole-warp {wmax}")
 
 
 def test_tuning_rejects_bad_values(tuned_ctx):
     for knob, bad in [(ab.TUNE_ATR_WARPS, 3), (ab.TUNE_ATR_GROUP_MIN, 1), (ab.TUNE_SORT_BITS, 9),
-                      (ab.TUNE_ATR_LEVELS, 65), (ab.TUNE_ATR_LEVELS, -1), (ab.TUNE_QUAD_MIN, -2), (7, 1)]:
+                      (ab.TUNE_ATR_LEVELS, 65), (ab.TUNE_ATR_LEVELS, -1), (ab.TUNE_QUAD_MIN, -2), (ab.TUNE_WARP_MAX, -1), (7, 1)]:
         with pytest.raises(ab.AtrError):
             tuned_ctx.set_tuning(knob, bad)
 
