@@ -826,6 +826,8 @@ cudaError_t launch_atrbvh_g(int warps, uint32_t blocks, cudaStream_t s, const Tr
 // below the levels above L.
 
 constexpr int kMaxLevels = 64;  // largest L (ATR_TUNE_ATR_LEVELS)
+constexpr int kListPer = 8;                  // nodes per thread of the level-list kernels
+constexpr int kListBlock = 256 * kListPer;  // nodes per block of those kernels
 
 struct LevelRefs {
     int4* rec;             // per node (node-indexed): count, nodesSah x 2, level (see NextRefs)
@@ -1002,51 +1004,53 @@ __global__ void __launch_bounds__(256) k_levels_pp_hist(TreeRefs g, Segs segs, L
     __shared__ uint32_t s_hist[kMaxLevels + 2];
     for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_hist[k] = 0;
     __syncthreads();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    int push = 0;
-    uint2 ent[2];
-    if (i < segs.n) {
-        const uint32_t m = segs.seg_of_tri(i);
-        const uint32_t s0 = segs.tri_begin(m);
-        const uint32_t n = segs.tri_end(m) - s0;
-        if (!seg_iters || 0 < (int)seg_iters[m]) {
-            const int base = segs.node_base(m), cb = segs.inner_base(m);
-            const int gamma = seg_tsize ? (int)seg_tsize[m] : tsize_all;
-            const int li = (int)(i - s0);
-            // The build's records are final for every node below gamma (count,
-            // both nodesSah, level 0) and hold the level of the others.
-            if (li < (int)n - 1) {
-                const int x = li;
-                const int lc = g.left[base + x], rc = g.right[base + x];
-                const int2 r = ranges[cb + x];
-                const int cnt = r.y - r.x + 1;
-                lv.kids[cb + x] =
-                    make_int4(lc, rc, __float_as_int(g.area[base + lc]), __float_as_int(g.area[base + rc]));
-                if (cnt >= gamma) {
-                    const int me = *rec_i(lv.rec, base + x, 3);
-                    if (me <= L) {
-                        atomicAdd(&s_hist[me], 1u);
-                    } else {
-                        if ((is_internal(lc, n) ? *rec_i(lv.rec, base + lc, 3) : 0) <= L)
-                            ent[push++] = make_uint2(m, (uint32_t)lc);
-                        if ((is_internal(rc, n) ? *rec_i(lv.rec, base + rc, 3) : 0) <= L)
-                            ent[push++] = make_uint2(m, (uint32_t)rc);
+    for (int q = 0; q < kListPer; ++q) {
+        const uint32_t i = blockIdx.x * kListBlock + q * 256 + threadIdx.x;
+        int push = 0;
+        uint2 ent[2];
+        if (i < segs.n) {
+            const uint32_t m = segs.seg_of_tri(i);
+            const uint32_t s0 = segs.tri_begin(m);
+            const uint32_t n = segs.tri_end(m) - s0;
+            if (!seg_iters || 0 < (int)seg_iters[m]) {
+                const int base = segs.node_base(m), cb = segs.inner_base(m);
+                const int gamma = seg_tsize ? (int)seg_tsize[m] : tsize_all;
+                const int li = (int)(i - s0);
+                // The build's records are final for every node below gamma (count,
+                // both nodesSah, level 0) and hold the level of the others.
+                if (li < (int)n - 1) {
+                    const int x = li;
+                    const int lc = g.left[base + x], rc = g.right[base + x];
+                    const int2 r = ranges[cb + x];
+                    const int cnt = r.y - r.x + 1;
+                    lv.kids[cb + x] =
+                        make_int4(lc, rc, __float_as_int(g.area[base + lc]), __float_as_int(g.area[base + rc]));
+                    if (cnt >= gamma) {
+                        const int me = *rec_i(lv.rec, base + x, 3);
+                        if (me <= L) {
+                            atomicAdd(&s_hist[me], 1u);
+                        } else {
+                            if ((is_internal(lc, n) ? *rec_i(lv.rec, base + lc, 3) : 0) <= L)
+                                ent[push++] = make_uint2(m, (uint32_t)lc);
+                            if ((is_internal(rc, n) ? *rec_i(lv.rec, base + rc, 3) : 0) <= L)
+                                ent[push++] = make_uint2(m, (uint32_t)rc);
+                        }
                     }
                 }
             }
         }
+        // Frontier entries: one atomic per warp.
+        uint32_t incl = push;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, o);
+            if ((threadIdx.x & 31) >= o) incl += y;
+        }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        uint32_t at = 0;
+        if ((threadIdx.x & 31) == 31 && total) at = atomicAdd(lv.n_frontier, total);
+        at = __shfl_sync(kFull, at, 31) + incl - push;
+        for (int k = 0; k < push; ++k) lv.frontier[at + k] = ent[k];
     }
-    // Frontier entries: one atomic per warp.
-    uint32_t incl = push;
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(kFull, incl, o);
-        if ((threadIdx.x & 31) >= o) incl += y;
-    }
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    uint32_t at = 0;
-    if ((threadIdx.x & 31) == 31 && total) at = atomicAdd(lv.n_frontier, total);
-    at = __shfl_sync(kFull, at, 31) + incl - push;
-    for (int k = 0; k < push; ++k) lv.frontier[at + k] = ent[k];
     // Level counts: one global atomic per level present in the block.
     __syncthreads();
     for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
@@ -1064,51 +1068,54 @@ __global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, con
     __shared__ uint32_t s_hist[kMaxLevels + 2];
     for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_hist[k] = 0;
     __syncthreads();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    int push = 0;
-    uint32_t m = 0;
-    uint2 ent[2];
-    if (i < segs.n) {
-        m = segs.seg_of_tri(i);
-        const uint32_t s0 = segs.tri_begin(m);
-        const uint32_t n = segs.tri_end(m) - s0;
-        const uint32_t li = i - s0;
-        if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
-            const int cb = segs.inner_base(m), nb = segs.node_base(m);
-            const int me = *rec_i(lv.rec, nb + (int)li, 3);
-            if (me == 0) {
-                // Not a treelet root: its next nodesSah is this one (the level
-                // stays 0).
-                *rec_f(lv.rec, nb + (int)li, rec_ns_next(lv.par)) = *rec_f(lv.rec, nb + (int)li, rec_ns_cur(lv.par));
-            } else if (me <= L) {
-                atomicAdd(&s_hist[me], 1u);
-            } else {
-                const int4 kd = lv.kids[cb + (int)li];
-                if ((is_internal(kd.x, n) ? *rec_i(lv.rec, nb + kd.x, 3) : 0) <= L)
-                    ent[push++] = make_uint2(m, (uint32_t)kd.x);
-                if ((is_internal(kd.y, n) ? *rec_i(lv.rec, nb + kd.y, 3) : 0) <= L)
-                    ent[push++] = make_uint2(m, (uint32_t)kd.y);
+    for (int q = 0; q < kListPer; ++q) {
+        const uint32_t i = blockIdx.x * kListBlock + q * 256 + threadIdx.x;
+        int push = 0;
+        uint32_t m = 0;
+        uint2 ent[2];
+        if (i < segs.n) {
+            m = segs.seg_of_tri(i);
+            const uint32_t s0 = segs.tri_begin(m);
+            const uint32_t n = segs.tri_end(m) - s0;
+            const uint32_t li = i - s0;
+            if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
+                const int cb = segs.inner_base(m), nb = segs.node_base(m);
+                const int me = *rec_i(lv.rec, nb + (int)li, 3);
+                if (me == 0) {
+                    // Not a treelet root: its next nodesSah is this one (the level
+                    // stays 0).
+                    *rec_f(lv.rec, nb + (int)li, rec_ns_next(lv.par)) = *rec_f(lv.rec, nb + (int)li, rec_ns_cur(lv.par));
+                } else if (me <= L) {
+                    atomicAdd(&s_hist[me], 1u);
+                } else {
+                    const int4 kd = lv.kids[cb + (int)li];
+                    if ((is_internal(kd.x, n) ? *rec_i(lv.rec, nb + kd.x, 3) : 0) <= L)
+                        ent[push++] = make_uint2(m, (uint32_t)kd.x);
+                    if ((is_internal(kd.y, n) ? *rec_i(lv.rec, nb + kd.y, 3) : 0) <= L)
+                        ent[push++] = make_uint2(m, (uint32_t)kd.y);
+                }
             }
         }
+        // Frontier entries: one atomic per warp.
+        uint32_t incl = push;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(kFull, incl, o);
+            if ((threadIdx.x & 31) >= o) incl += y;
+        }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        uint32_t at = 0;
+        if ((threadIdx.x & 31) == 31 && total) at = atomicAdd(lv.n_frontier, total);
+        at = __shfl_sync(kFull, at, 31) + incl - push;
+        for (int k = 0; k < push; ++k) lv.frontier[at + k] = ent[k];
     }
-    // Frontier entries: one atomic per warp.
-    uint32_t incl = push;
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(kFull, incl, o);
-        if ((threadIdx.x & 31) >= o) incl += y;
-    }
-    const uint32_t total = __shfl_sync(kFull, incl, 31);
-    uint32_t at = 0;
-    if ((threadIdx.x & 31) == 31 && total) at = atomicAdd(lv.n_frontier, total);
-    at = __shfl_sync(kFull, at, 31) + incl - push;
-    for (int k = 0; k < push; ++k) lv.frontier[at + k] = ent[k];
     // Level counts: one global atomic per level present in the block.
     __syncthreads();
     for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
         if (s_hist[k]) atomicAdd(&lv.hist[k], s_hist[k]);
 }
 
-// Exclusive scan of the level histogram into offsets (one small block).
+// Phase B: the level lists.  Every block scans the (small) level histogram
+// into list offsets, then files its nodes of levels 1..L into the lists.
 __global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, const uint8_t* __restrict__ seg_iters,
                                                        int iteration, int L) {
     __shared__ uint32_t s_cnt[kMaxLevels + 2];
@@ -1127,26 +1134,50 @@ __global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, 
     __syncthreads();
     if (blockIdx.x == 0)
         for (int k = threadIdx.x; k < L + 2; k += blockDim.x) lv.off[k] = s_off[k];
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    int me = 0;
-    uint32_t m = 0, li = 0, rank = 0;
-    if (i < segs.n) {
-        m = segs.seg_of_tri(i);
-        const uint32_t s0 = segs.tri_begin(m);
-        const uint32_t n = segs.tri_end(m) - s0;
-        li = i - s0;
-        if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
-            me = *rec_i(lv.rec, segs.node_base(m) + (int)li, 3);
-            if (me > L) me = 0;
+    // kListPer nodes per thread: levels first (independent loads), then each
+    // node's rank among the block's nodes of its level, one shared atomic per
+    // level present in the warp.
+    const int lane = threadIdx.x & 31;
+    int me[kListPer];
+    uint2 ent[kListPer];
+#pragma unroll
+    for (int q = 0; q < kListPer; ++q) {
+        const uint32_t i = blockIdx.x * kListBlock + q * 256 + threadIdx.x;
+        me[q] = 0;
+        ent[q] = make_uint2(0u, 0u);
+        if (i < segs.n) {
+            const uint32_t m = segs.seg_of_tri(i);
+            const uint32_t s0 = segs.tri_begin(m);
+            const uint32_t n = segs.tri_end(m) - s0;
+            const uint32_t li = i - s0;
+            ent[q] = make_uint2(m, li);
+            if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
+                const int lvl = *rec_i(lv.rec, segs.node_base(m) + (int)li, 3);
+                me[q] = lvl <= L ? lvl : 0;
+            }
         }
     }
-    if (me > 0) rank = atomicAdd(&s_cnt[me], 1u);
+    uint32_t key[kListPer];
+#pragma unroll
+    for (int q = 0; q < kListPer; ++q) {
+        const uint32_t peers = __match_any_sync(kFull, me[q]);
+        const int leader = __ffs(peers) - 1;
+        uint32_t b = 0;
+        if (lane == leader && me[q] > 0) b = atomicAdd(&s_cnt[me[q]], (uint32_t)__popc(peers));
+        b = __shfl_sync(kFull, b, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+        key[q] = me[q] > 0 ? ((uint32_t)me[q] << 16) | b : 0u;  // rank < kListBlock
+    }
     __syncthreads();
     // One global reservation per level present in the block.
     for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
         s_base[k] = s_cnt[k] ? atomicAdd(&lv.cursor[k], s_cnt[k]) : 0u;
     __syncthreads();
-    if (me > 0) lv.order[s_off[me] + s_base[me] + rank] = make_uint2(m, li);
+#pragma unroll
+    for (int q = 0; q < kListPer; ++q)
+        if (key[q]) {
+            const uint32_t l = key[q] >> 16;
+            lv.order[s_off[l] + s_base[l] + (key[q] & 0xffffu)] = ent[q];
+        }
 }
 
 // ---- quads: eight treelets per warp ----------------------------------------
@@ -1639,8 +1670,9 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         if (L && e == cudaSuccess) {
             e = cudaMemsetAsync(lv.hist, 0, b_small, st);
             const unsigned gb = (segs.n + 255) / 256;
+            const unsigned gbl = (segs.n + kListBlock - 1) / kListBlock;
             if (hist_done)
-                k_levels_pp_hist<<<gb, 256, 0, st>>>(g, segs, lv, karras_ranges, tsize, seg_tsize, seg_iters, L);
+                k_levels_pp_hist<<<gbl, 256, 0, st>>>(g, segs, lv, karras_ranges, tsize, seg_tsize, seg_iters, L);
             else if (it == 0 && use_pp)
                 k_levels_pp<<<gb, 256, 0, st>>>(g, segs, lv, karras_ranges, tsize, seg_tsize, seg_iters, it,
                                                 use_pp_levels);
@@ -1653,10 +1685,10 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
             // first iteration's climb, or from the levels the previous
             // iteration left).
             if (!hist_done) {
-                k_level_hist<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
+                k_level_hist<<<gbl, 256, 0, st>>>(segs, lv, seg_iters, it, L);
                 ++ctx->launches;
             }
-            k_level_scatter<<<gb, 256, 0, st>>>(segs, lv, seg_iters, it, L);
+            k_level_scatter<<<gbl, 256, 0, st>>>(segs, lv, seg_iters, it, L);
             ++ctx->launches;
             const unsigned lg = (unsigned)ctx->num_sms * (256 / threads) * 4;
             // Roots per level fall by about 0.62 per level from n / (1.5 gamma)
