@@ -10,6 +10,7 @@
 // follows Karras (a node covering [l, r] is stored at r when it is its
 // parent's left child and at l when it is the right child; the root at 0).
 
+#include <climits>
 #include <cstdio>
 #include <utility>
 
@@ -522,7 +523,8 @@ struct BuildOut {
     BuildPrepass pp;
 };
 
-// Record of the internal node p over leaves [pl, pr] with children lc, rc.
+// Record of the internal node p over leaves [pl, pr] with children lc, rc
+// (the children's parent links are the caller's).
 template <typename K>
 __device__ __forceinline__ void write_inner(const BuildOut<K>& o, const Segs& segs, uint32_t m, int nb, int p, int pl,
                                             int pr, int lc, int rc, float4 mn, float4 mx, float pa, float ns,
@@ -531,8 +533,6 @@ __device__ __forceinline__ void write_inner(const BuildOut<K>& o, const Segs& se
     o.right[nb + p] = rc;
     o.data[nb + p] = -1;
     if (o.range) o.range[segs.inner_base(m) + p] = make_int2(pl, pr);
-    o.parent[nb + lc] = p;
-    o.parent[nb + rc] = p;
     o.bmin[nb + p] = mn;
     o.bmax[nb + p] = mx;
     o.area[nb + p] = pa;
@@ -555,11 +555,21 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
     __shared__ int s_ilv[kBuildBlock];  // prepass levels of the block's finished internal nodes
     __shared__ int s_slot[kBuildBlock];
     __shared__ int s_delta[kBuildBlock + 1];  // delta at sorted position B0 - 1 + k
+    // Records of the internal nodes the block finishes, by block position
+    // (internal node p of a mesh sits at its sorted position p), and the
+    // parents it assigns: written out coalesced once the block's climbs end.
+    __shared__ int s_left[kBuildBlock], s_right[kBuildBlock];  // kUnset: not finished here
+    __shared__ int2 s_rng[kBuildBlock];
+    __shared__ int s_ipar[kBuildBlock], s_lpar[kBuildBlock];   // parents of internal node / leaf
+    constexpr int kUnset = INT_MIN;
     const int tid = threadIdx.x;
     const uint32_t B0 = blockIdx.x * kBuildBlock;
     const uint32_t gi = B0 + tid;
     const bool live = gi < segs.n;
     s_slot[tid] = -1;
+    s_left[tid] = kUnset;
+    s_ipar[tid] = kUnset;
+    s_lpar[tid] = kUnset;
     if (tid < 2) edges[2 * blockIdx.x + tid] = BuildEdge{-1, -1, -1, -1};
     uint32_t m = 0, s0 = 0, n = 1, i = 0;
     int nb = 0, last = 0;
@@ -658,13 +668,18 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
                 const int gam = o.pp.seg_gamma ? (int)o.pp.seg_gamma[m] : o.pp.gamma;
                 my_lv = pr - pl + 1 >= gam ? 1 + max(my_lv, sib_leaf ? 0 : s_ilv[sp]) : 0;
             }
-            write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns, my_lv);
+            s_left[off + p] = lc;
+            s_right[off + p] = rc;
+            s_rng[off + p] = make_int2(pl, pr);
+            // The left child sits at position split, the right at split + 1.
+            (split == pl ? s_lpar : s_ipar)[off + split] = p;
+            (split + 1 == pr ? s_lpar : s_ipar)[off + split + 1] = p;
             s_imn[off + p] = mn;
             s_imx[off + p] = mx;
             s_ins[off + p] = my_ns;
             s_ilv[off + p] = my_lv;
             if (root) {
-                o.parent[nb] = -1;
+                s_ipar[off] = -1;
                 break;
             }
             node = p;
@@ -673,7 +688,16 @@ __global__ void __launch_bounds__(kBuildBlock) k_build_block(Segs segs, const K*
         }
     }
     __syncthreads();
-    if (live && (int)i < last) o.slot[segs.inner_base(m) + i] = s_slot[tid];
+    if (live) {
+        if (s_left[tid] != kUnset) {  // internal node i, finished by this block
+            const int2 rg = s_rng[tid];
+            write_inner(o, segs, m, nb, (int)i, rg.x, rg.y, s_left[tid], s_right[tid], s_imn[tid], s_imx[tid],
+                        box_area(s_imn[tid], s_imx[tid]), s_ins[tid], s_ilv[tid]);
+        }
+        if (s_ipar[tid] != kUnset) o.parent[nb + (int)i] = s_ipar[tid];
+        if (s_lpar[tid] != kUnset) o.parent[nb + (int)i + last] = s_lpar[tid];
+        if ((int)i < last) o.slot[segs.inner_base(m) + i] = s_slot[tid];
+    }
 }
 
 template <typename K>
@@ -729,6 +753,8 @@ __global__ void __launch_bounds__(256) k_build_top(Segs segs, const K* __restric
                                                                                           : 0;
         }
         write_inner(o, segs, m, nb, p, pl, pr, lc, rc, mn, mx, pa, my_ns, my_lv);
+        o.parent[nb + lc] = p;
+        o.parent[nb + rc] = p;
         if (root) {
             o.parent[nb] = -1;
             return;
