@@ -294,57 +294,108 @@ __global__ void __launch_bounds__(256) k_flat_slots(FlatRefs t, Segs segs, const
 }
 
 // One thread per reachable inner node: its 64-byte record in the mesh's node
-// slice (first node 4 * cb in float4 units) and its leaf children's Woop
-// triangles in the mesh's Woop slice (first entry 4 * s0).
-__global__ void __launch_bounds__(128) k_flat_write(FlatRefs t, Segs segs, const float4* __restrict__ verts,
+// slice (first node 4 * cb in float4 units), the terminators of its leaf
+// children's Woop lists in the mesh's Woop slice (first entry 4 * s0).  The
+// Woop triangles of a warp's leaf children are then spread over the warp's
+// lanes (an exclusive scan of the nodes' triangle counts in shared memory,
+// item u to the node whose range holds it), so a node with long leaf lists
+// does not hold the warp while the others idle.
+constexpr int kWriteThreads = 128;
+
+__global__ void __launch_bounds__(kWriteThreads) k_flat_write(FlatRefs t, Segs segs, const float4* __restrict__ verts,
                                                      const int2* __restrict__ acc,
                                                      const uint32_t* __restrict__ w_by_rank,
                                                      const int* __restrict__ slot_of, int4* __restrict__ nodes,
                                                      float4* __restrict__ woop, int32_t* __restrict__ tri_index) {
+    constexpr int W = kWriteThreads / 32;
+    __shared__ uint32_t s_pre[W][32], s_n0[W][32], s_w[W][2][32], s_s0[W][32];
+    __shared__ int32_t s_d[W][2][32];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gi >= segs.n) return;
-    const SegPos q = seg_pos(segs, gi);
-    if (q.li >= q.n - 1) return;
-    const int x = (int)q.li;
-    const int2 a = acc[q.cb + x];
-    if (a.y & (1 << 30)) return;
-    const float4* mv = verts + 3 * (size_t)q.s0;
-    float4* mw = woop + 4 * (size_t)q.s0;
-    int32_t* mt = tri_index + 4 * (size_t)q.s0;
-    const int ch[2] = {t.left[q.nb + x], t.right[q.nb + x]};
-    int cref[2];
-    uint32_t w = w_by_rank[q.cb + a.x] - w_by_rank[q.cb];
+    uint32_t items[2] = {0u, 0u}, wk[2] = {0u, 0u};
+    int32_t dk[2] = {0, 0};
+    uint32_t s0 = 0;
+    bool multi[2] = {false, false};
+    if (gi < segs.n) {
+        const SegPos q = seg_pos(segs, gi);
+        s0 = q.s0;
+        const int x = (int)q.li;
+        const int2 a = q.li < q.n - 1 ? acc[q.cb + x] : make_int2(0, 1 << 30);
+        if (!(a.y & (1 << 30))) {
+            float4* mw = woop + 4 * (size_t)q.s0;
+            int32_t* mt = tri_index + 4 * (size_t)q.s0;
+            const int ch[2] = {t.left[q.nb + x], t.right[q.nb + x]};
+            int cref[2];
+            uint32_t w = w_by_rank[q.cb + a.x] - w_by_rank[q.cb];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const int c = ch[k];
-        if (!c_leaf(t, q.nb, c)) {
-            cref[k] = 4 * slot_of[q.cb + c];
-            continue;
+            for (int k = 0; k < 2; ++k) {
+                const int c = ch[k];
+                if (!c_leaf(t, q.nb, c)) {
+                    cref[k] = 4 * slot_of[q.cb + c];
+                    continue;
+                }
+                cref[k] = ~(int)w;
+                const int cnt = t.count[q.nb + c];
+                multi[k] = cnt > 1;
+                items[k] = (uint32_t)(cnt > 1 ? cnt : 1);
+                wk[k] = w;
+                dk[k] = t.data[q.nb + c];
+                w += 3u * items[k];
+                const float term = __int_as_float((int)0x80000000u);
+                mw[w] = make_float4(term, term, term, term);
+                mt[w] = 0;
+                w += 1;
+            }
+            const float4 lm = t.bmin[q.nb + ch[0]], lx = t.bmax[q.nb + ch[0]];
+            const float4 rm = t.bmin[q.nb + ch[1]], rx = t.bmax[q.nb + ch[1]];
+            int4* dst = nodes + 4 * ((size_t)q.cb + (size_t)slot_of[q.cb + x]);
+            dst[0] = make_int4(__float_as_int(lm.x), __float_as_int(lx.x), __float_as_int(lm.y), __float_as_int(lx.y));
+            dst[1] = make_int4(__float_as_int(rm.x), __float_as_int(rx.x), __float_as_int(rm.y), __float_as_int(rx.y));
+            dst[2] = make_int4(__float_as_int(lm.z), __float_as_int(lx.z), __float_as_int(rm.z), __float_as_int(rx.z));
+            dst[3] = make_int4(cref[0], cref[1], 0, 0);
         }
-        cref[k] = ~(int)w;
-        const int cnt = t.count[q.nb + c];
-        const int d = t.data[q.nb + c];
-        const int mcount = cnt > 1 ? cnt : 1;
-        for (int j = 0; j < mcount; ++j) {
-            const int tri = cnt > 1 ? t.tri[q.s0 + d + j] : d;
-            woopify(mv, tri, mw + w);
-            mt[w] = tri;
-            mt[w + 1] = 0;
-            mt[w + 2] = 0;
-            w += 3;
-        }
-        const float term = __int_as_float((int)0x80000000u);
-        mw[w] = make_float4(term, term, term, term);
-        mt[w] = 0;
-        w += 1;
     }
-    const float4 lm = t.bmin[q.nb + ch[0]], lx = t.bmax[q.nb + ch[0]];
-    const float4 rm = t.bmin[q.nb + ch[1]], rx = t.bmax[q.nb + ch[1]];
-    int4* dst = nodes + 4 * ((size_t)q.cb + (size_t)slot_of[q.cb + x]);
-    dst[0] = make_int4(__float_as_int(lm.x), __float_as_int(lx.x), __float_as_int(lm.y), __float_as_int(lx.y));
-    dst[1] = make_int4(__float_as_int(rm.x), __float_as_int(rx.x), __float_as_int(rm.y), __float_as_int(rx.y));
-    dst[2] = make_int4(__float_as_int(lm.z), __float_as_int(lx.z), __float_as_int(rm.z), __float_as_int(rx.z));
-    dst[3] = make_int4(cref[0], cref[1], 0, 0);
+    // Items of this lane: items[0] triangles of the left leaf child, then
+    // items[1] of the right.
+    const uint32_t mine = items[0] + items[1];
+    uint32_t incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(kFull, incl, 31);
+    s_pre[wp][lane] = incl - mine;
+    s_n0[wp][lane] = items[0];
+    s_w[wp][0][lane] = wk[0];
+    s_w[wp][1][lane] = wk[1];
+    // A single-triangle leaf's data is the triangle (sign bit set here);
+    // a list leaf's data is its list offset.
+    s_d[wp][0][lane] = dk[0] | (multi[0] ? 0 : (int32_t)0x80000000);
+    s_d[wp][1][lane] = dk[1] | (multi[1] ? 0 : (int32_t)0x80000000);
+    s_s0[wp][lane] = s0;
+    __syncwarp();
+    for (uint32_t u = lane; u < total; u += 32) {
+        // The node holding item u: the last lane whose range starts at or
+        // before u (lanes without items share the next lane's start).
+        int o = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1)
+            if (s_pre[wp][o + step] <= u) o += step;
+        const uint32_t loc = u - s_pre[wp][o];
+        const int k = loc < s_n0[wp][o] ? 0 : 1;
+        const uint32_t j = loc - (k ? s_n0[wp][o] : 0u);
+        const int32_t dd = s_d[wp][k][o];
+        const uint32_t ms0 = s_s0[wp][o];
+        const int d = dd & 0x7fffffff;
+        const int tri = dd >= 0 ? t.tri[ms0 + (uint32_t)d + j] : d;
+        const uint32_t w = s_w[wp][k][o] + 3u * j;
+        woopify(verts + 3 * (size_t)ms0, tri, woop + 4 * (size_t)ms0 + w);
+        int32_t* mt = tri_index + 4 * (size_t)ms0;
+        mt[w] = tri;
+        mt[w + 1] = 0;
+        mt[w + 2] = 0;
+    }
 }
 
 // Per-mesh sizes: inner nodes = 1 + inner children, Woop entries.
@@ -426,7 +477,8 @@ int flatten_segs(atr_ctx* ctx, const Segs& segs, const CollapsedOut& c, const fl
     if (st == ATR_OK) st = exclusive_scan_u32(ctx, tw_r, tw_r, m, flags + 3);
     if (st == ATR_OK) {
         k_flat_slots<<<gb, 256, 0, s>>>(t, segs, ai, ic_r, slot_of);
-        k_flat_write<<<(n + 127) / 128, 128, 0, s>>>(t, segs, verts, ai, tw_r, slot_of, nodes, woop, tri_index);
+        k_flat_write<<<(n + kWriteThreads - 1) / kWriteThreads, kWriteThreads, 0, s>>>(t, segs, verts, ai, tw_r,
+                                                                                       slot_of, nodes, woop, tri_index);
         k_flat_sizes<<<(segs.count + 255) / 256, 256, 0, s>>>(segs, ic_r, tw_r, flags + 2,
                                                              reinterpret_cast<const int*>(flags + 1), d_sizes,
                                                              d_sizes + segs.count, d_sizes + 2 * segs.count);
