@@ -58,10 +58,10 @@ BYTES_PER_TRI = {"morton": 56.0, "sort": 4.0 + 16.0 * 4, "build": 40.0 + 180.0, 
 REFIT_BYTES_PER_TRI = 180.0  # vertex gather 48, dataIndex 4, parents 8, boxes 64, areas 8, counters 8, siblings 32, children 8
 # DRAM bytes per triangle of the ATRBVH phase (both iterations) from an ncu
 # capture of this bench step at 2,097,152 triangles (dram__bytes_read.sum +
-# dram__bytes_write.sum: k_levels_pp_hist 111.8 MB, k_level_hist 19.3,
-# k_level_scatter 16.8, k_level_groups 1896.6, k_atrbvh 13.0), scaled by
-# triangle count.
-ATRBVH_DRAM_BYTES_PER_TRI = (111.3 + 19.3 + 16.8 + 1923.6 + 12.9) * 1e6 / 2097152
+# dram__bytes_write.sum per step: k_levels_pp_hist 87.7 MB, k_level_hist 33.7,
+# k_level_scatter 67.2, k_level_groups 951.0 + 709.6 + 54.5, k_atrbvh 8.4),
+# scaled by triangle count.
+ATRBVH_DRAM_BYTES_PER_TRI = (87.7 + 33.7 + 67.2 + 951.0 + 709.6 + 54.5 + 8.4) * 1e6 / 2097152
 
 
 def _read_peaks() -> dict:
