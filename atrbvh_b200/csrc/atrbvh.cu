@@ -87,6 +87,7 @@ struct NextRefs {
     int4* rec;
     int par;
     int gamma;
+    float ct;  // a triangle leaf's record is (1, ct * area, ct * area, 0), never rewritten
 };
 
 template <int G>
@@ -403,11 +404,16 @@ __device__ __forceinline__ void process_group(const TreeRefs& g, bool active, in
     if (run && gl < tsize) {
         s_mn = ld_cg(BMN + s_node);
         s_mx = ld_cg(BMX + s_node);
-        const int4 r = __ldcg(nx.rec + s_node);
-        s_cnt = r.x;
-        s_sah = __int_as_float(nx.par ? r.z : r.y);
-        s_nsn = __int_as_float(nx.par ? r.y : r.z);
-        s_nlv = is_internal(s_node, n) ? r.w : 0;
+        if (is_internal(s_node, n)) {
+            const int4 r = __ldcg(nx.rec + s_node);
+            s_cnt = r.x;
+            s_sah = __int_as_float(nx.par ? r.z : r.y);
+            s_nsn = __int_as_float(nx.par ? r.y : r.z);
+            s_nlv = r.w;
+        } else {  // a triangle: its record follows from its area (the parent's child record's)
+            s_cnt = 1;
+            s_sah = s_nsn = __fmul_rn(nx.ct, s_area);
+        }
     }
     // Records of leaves that were never expanded may still be in flight into
     // the slots the merge state reuses.
@@ -774,7 +780,7 @@ __global__ void __launch_bounds__(W * 32, 16 / W) k_atrbvh(TreeRefs g, Segs segs
                 const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)rts : 0u);
                 const int4 rk = make_int4(__shfl_sync(kFull, myk.x, rl), __shfl_sync(kFull, myk.y, rl),
                                           __shfl_sync(kFull, myk.z, rl), __shfl_sync(kFull, myk.w, rl));
-                const NextRefs nx{rec + rbase, iteration & 1, rts << (iteration + 1)};
+                const NextRefs nx{rec + rbase, iteration & 1, rts << (iteration + 1), ct};
                 process_group<G>(g, has, rbase, rn, root, rk, kids + rcb, nx, rsah, rts, maxts, ci,
                                  &s_mem[w][0] + (grp < NG ? grp : NG - 1) * GroupLayout<G>::kFloats, s_rc, s_prio, err);
 #pragma unroll
@@ -789,7 +795,7 @@ __global__ void __launch_bounds__(W * 32, 16 / W) k_atrbvh(TreeRefs g, Segs segs
                 const int rts = __shfl_sync(kFull, tsize, rl);
                 const int4 rk = make_int4(__shfl_sync(kFull, myk.x, rl), __shfl_sync(kFull, myk.y, rl),
                                           __shfl_sync(kFull, myk.z, rl), __shfl_sync(kFull, myk.w, rl));
-                const NextRefs nx{rec + rbase, iteration & 1, rts << (iteration + 1)};
+                const NextRefs nx{rec + rbase, iteration & 1, rts << (iteration + 1), ct};
                 process_group<32>(g, true, rbase, rn, root, rk, kids + rcb, nx, rsah, rts, rts, ci, &s_mem[w][0],
                                   s_rc, s_prio, err);
                 vote &= vote - 1;
@@ -832,6 +838,7 @@ constexpr int kListBlock = 256 * kListPer;  // nodes per block of those kernels
 struct LevelRefs {
     int4* rec;             // per node (node-indexed): count, nodesSah x 2, level (see NextRefs)
     int par;               // iteration & 1
+    float ct;              // the leaf cost constant (triangle leaves' records)
     uint32_t* counters;
     int4* kids;
     uint32_t* hist;        // [L + 2]: level histogram
@@ -1304,10 +1311,12 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
     // writes a treelet leaf's records.
     {
         int node[3];
+        float area[3];
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             const int k = gl + 4 * q;
             node[q] = run && k < tsize ? __float_as_int(lmx[k].w) : -1;
+            area[q] = node[q] >= 0 ? lmn[k].w : 0.0f;
         }
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
@@ -1315,17 +1324,24 @@ __device__ __forceinline__ void process_quad(const TreeRefs& g, bool active, int
             const int k = gl + 4 * q;
             cp_async16_cg(lmn + k, BMN + node[q]);
             cp_async16_cg(lmx + k, BMX + node[q]);
-            cp_async16_cg(lcn + k, nx.rec + node[q]);
+            // A triangle's record follows from its area: not fetched.
+            if (is_internal(node[q], n)) cp_async16_cg(lcn + k, nx.rec + node[q]);
         }
         cp_async_wait_all();
 #pragma unroll
         for (int q = 0; q < 3; ++q) {
             if (node[q] < 0) continue;
             const int k = gl + 4 * q;
-            const int4 r = lcn[k];
-            lmn[k].w = __int_as_float(nx.par ? r.z : r.y);
             lmx[k].w = __int_as_float(node[q]);
-            lcn[k] = make_int4(r.x, is_internal(node[q], n) ? r.w : 0, nx.par ? r.y : r.z, 0);
+            if (is_internal(node[q], n)) {
+                const int4 r = lcn[k];
+                lmn[k].w = __int_as_float(nx.par ? r.z : r.y);
+                lcn[k] = make_int4(r.x, r.w, nx.par ? r.y : r.z, 0);
+            } else {
+                const float ns = __fmul_rn(nx.ct, area[q]);
+                lmn[k].w = ns;
+                lcn[k] = make_int4(1, 0, __float_as_int(ns), 0);
+            }
         }
     }
     __syncwarp();
@@ -1572,7 +1588,7 @@ __global__ void __launch_bounds__(W * 32, (G == 32 ? 16 : 32) / W) k_level_group
         }
         const int maxts = (int)__reduce_max_sync(kFull, has ? (unsigned)tsize : 0u);
         __syncwarp();
-        const NextRefs nx{lv.rec + nb, lv.par, tsize << (iteration + 1)};
+        const NextRefs nx{lv.rec + nb, lv.par, tsize << (iteration + 1), lv.ct};
         float* const sm = &s_mem[w][0] + (grp < per ? grp : per - 1) * kGroupFloats;
         if constexpr (QUADS)
             process_quad<kQuadLeaves>(g, has, nb, n, x, rk, kd, nx, root_sah, tsize, maxts, ci, sm, s_rc, s_prio,
@@ -1660,6 +1676,7 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     ctx->phase_begin("atrbvh");
     for (int it = 0; it < iterations && e == cudaSuccess; ++it) {
         lv.par = it & 1;
+        lv.ct = ct;
         const bool hist_done = L && it == 0 && use_pp_levels;
         // Arrival counters: for the first iteration's climbs, else only for
         // the dataflow pass (cleared again below).
