@@ -100,7 +100,7 @@ struct atr_ctx {
     int atr_levels = 12;
     // A level pass over at least this many treelet roots restructures them in
     // four-lane groups (eight per warp); -1 = never.
-    int atr_quad_min = 50000;
+    int atr_quad_min = 20000;
     int atr_warp_max = 4096;
     struct Phase {
         std::string name;

@@ -119,7 +119,7 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
  *   ATR_TUNE_QUAD_MIN       fewest treelet roots of one level that the level
  *                           pass restructures in four-lane groups, eight per
  *                           warp, instead of 32/G per warp (-1 = never;
- *                           default 50000).
+ *                           default 20000).
  *   ATR_TUNE_WARP_MAX       most treelet roots of one level that the level
  *                           pass restructures one per warp, with the
  *                           treelet's slots and distances in registers

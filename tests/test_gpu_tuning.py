@@ -38,7 +38,7 @@ def test_ten_bit_sort_digits_bit_exact(tuned_ctx, case, bits):
                                                          (4, 33, 0, -1, 0), (4, 2, 1, 0, 0), (4, 2, 4, -1, 0),
                                                          (2, 2, 64, 0, 0), (4, 2, 16, 0, 0), (4, 2, 16, -1, 0),
                                                          (8, 2, 64, 1000, 0), (8, 2, 12, -1, 1 << 30),
-                                                         (2, 2, 16, 1000, 500), (8, 2, 12, 50000, 8192)])
+                                                         (2, 2, 16, 1000, 500), (8, 2, 12, 50000, 8192), (8, 2, 12, 20000, 4096)])
 @pytest.mark.parametrize("treelet,iters", [(3, 1), (5, 2), (9, 2), (10, 3), (11, 2), (12, 1), (20, 1)])
 def test_atrbvh_launch_tuning_bit_exact(tuned_ctx, warps, gmin, levels, qmin, wmax, treelet, iters):
     tuned_ctx.set_tuning(ab.TUNE_ATR_WARPS, warps)
