@@ -11,6 +11,7 @@
 // replayed.
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
@@ -50,7 +51,7 @@ struct atr_batch {
     int32_t* cp_tri = nullptr;
     int64_t* d_sizes = nullptr;  // per mesh: nodes then woop entries
     std::vector<int64_t> h_sizes;
-    int32_t max_depth = 0;
+    std::atomic<int32_t> max_depth{0};  // refits of different meshes may raise it from several lanes
     bool flattened = false;
     // Parameters of the last atr_batch_collapse (reused when one mesh is refit).
     float col_ci = 1.2f, col_ct = 1.0f;
@@ -507,7 +508,8 @@ int batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* ver
     }
     b->h_sizes[mesh] = h[0];
     b->h_sizes[b->count + mesh] = h[1];
-    b->max_depth = std::max(b->max_depth, (int32_t)h[2]);
+    for (int32_t d = b->max_depth.load(); (int32_t)h[2] > d && !b->max_depth.compare_exchange_weak(d, (int32_t)h[2]);) {
+    }
     return ATR_OK;
 }
 

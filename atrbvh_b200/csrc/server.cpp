@@ -47,6 +47,8 @@ constexpr uint64_t kBuildBytesPerTri = 460;
 constexpr uint64_t kResidentBytesPerTri = 404;
 constexpr uint64_t kRayBytes = 48;  // ray (32) + result (16)
 
+struct BatchRec;
+
 struct Request {
     uint64_t ticket = 0;
     atr_request req{};
@@ -58,13 +60,16 @@ struct Request {
     uint32_t batch_requests = 0, lane = 0;
     uint64_t bytes = 0;  // admission estimate while in flight
     std::string error;
+    std::shared_ptr<BatchRec> refit_rec;  // a refit: the resident batch it holds busy
+    uint32_t refit_index = 0;             // and the mesh's index in it
+    uint32_t refit_n = 0;                 // and its triangle count
 };
 
 struct BatchRec {
     atr_batch* batch = nullptr;
     uint64_t bytes = 0;
     uint32_t live = 0;   // resident meshes still referring to it
-    int busy_lane = -1;  // lane using it, or -1
+    uint32_t busy = 0;   // refits of its meshes in flight (on any lanes)
     uint64_t last_use = 0;
 };
 
@@ -72,6 +77,7 @@ struct Resident {
     std::shared_ptr<BatchRec> rec;
     uint32_t index = 0;
     uint32_t n = 0;
+    int busy_lane = -1;  // lane refitting this mesh, or -1
 };
 
 struct Lane {
@@ -196,7 +202,7 @@ struct atr_server {
         maybe_free(rec);
     }
     void maybe_free(const std::shared_ptr<BatchRec>& rec) {
-        if (rec->live || rec->busy_lane >= 0 || !rec->batch) return;
+        if (rec->live || rec->busy || !rec->batch) return;
         atr_batch_destroy(rec->batch);
         rec->batch = nullptr;
         resident_bytes -= rec->bytes;
@@ -210,7 +216,7 @@ struct atr_server {
         if (inflight_bytes + resident_bytes + need <= budget) return true;
         std::vector<std::shared_ptr<BatchRec>> idle;
         for (auto& b : batches)
-            if (b->busy_lane < 0 && b->live) idle.push_back(b);
+            if (!b->busy && b->live) idle.push_back(b);
         std::sort(idle.begin(), idle.end(), [](auto& a, auto& b) { return a->last_use < b->last_use; });
         for (auto& b : idle) {
             bool wanted = false;
@@ -265,8 +271,10 @@ struct atr_server {
                     cv_done.notify_all();
                     continue;
                 }
-                auto& rec = res->second.rec;
-                if (rec->busy_lane >= 0 && rec->busy_lane != lane) { ++it; continue; }
+                // Refits of one mesh run on one lane at a time; refits of other
+                // meshes of the same resident batch touch only their own slices
+                // and may run on other lanes meanwhile.
+                if (res->second.busy_lane >= 0 && res->second.busy_lane != lane) { ++it; continue; }
                 need += 64ull * res->second.n;  // re-collapse / re-flatten scratch
             } else {
                 if (!out.empty() && tris + r->req.num_triangles > cfg.max_batch_triangles) { ++it; continue; }
@@ -282,8 +290,12 @@ struct atr_server {
                 break;  // wait for memory to free up (keeps arrival order)
             }
             if (r->req.kind == ATR_REQ_REFIT) {
-                auto& rec = resident.find(r->req.mesh_id)->second.rec;
-                rec->busy_lane = lane;
+                Resident& res = resident.find(r->req.mesh_id)->second;
+                res.busy_lane = lane;
+                r->refit_rec = res.rec;
+                r->refit_index = res.index;
+                r->refit_n = res.n;
+                ++res.rec->busy;
             } else {
                 tris += r->req.num_triangles;
             }
@@ -347,26 +359,16 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
     // Pageable refit vertices go to their own staging buffer (copied before any launch).
     uint64_t refit_tris = 0;
     std::vector<size_t> refit_at(work.size(), 0);
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        for (size_t i = 0; i < work.size(); ++i) {
-            if (work[i]->req.kind != ATR_REQ_REFIT || verts_pinned[i]) continue;
-            auto f = resident.find(work[i]->req.mesh_id);
-            if (f == resident.end()) continue;
-            refit_at[i] = refit_tris;
-            refit_tris += f->second.n;
-        }
+    for (size_t i = 0; i < work.size(); ++i) {
+        if (work[i]->req.kind != ATR_REQ_REFIT || verts_pinned[i] || !work[i]->refit_rec) continue;
+        refit_at[i] = refit_tris;
+        refit_tris += work[i]->refit_n;
     }
     if (refit_tris) ATR_TRY(grow_pinned(&L.h_rverts, &L.h_rverts_cap, refit_tris * 48));
-    {
-        std::lock_guard<std::mutex> lock(mu);
-        for (size_t i = 0; i < work.size(); ++i) {
-            if (work[i]->req.kind != ATR_REQ_REFIT || verts_pinned[i]) continue;
-            auto f = resident.find(work[i]->req.mesh_id);
-            if (f == resident.end()) continue;
-            jobs.push_back({static_cast<char*>(L.h_rverts) + refit_at[i] * 48, work[i]->req.vertices,
-                            (size_t)f->second.n * 48});
-        }
+    for (size_t i = 0; i < work.size(); ++i) {
+        if (work[i]->req.kind != ATR_REQ_REFIT || verts_pinned[i] || !work[i]->refit_rec) continue;
+        jobs.push_back({static_cast<char*>(L.h_rverts) + refit_at[i] * 48, work[i]->req.vertices,
+                        (size_t)work[i]->refit_n * 48});
     }
     par_copy(jobs);
     double copy_ms = ms_between(t_start, Clock::now());
@@ -490,13 +492,16 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
 
     // 2. Refits of resident meshes, each traced against its own batch.
     for (Request* r : refits) {
+        // The batch taken for this refit, held busy (not evicted) until the
+        // lane releases it.
         Resident res;
-        {
-            std::lock_guard<std::mutex> lock(mu);
-            auto f = resident.find(r->req.mesh_id);
-            if (f == resident.end()) { r->status = ATR_ERR_NOT_RESIDENT; r->error = "refit: mesh was released"; continue; }
-            res = f->second;
+        if (!r->refit_rec || !r->refit_rec->batch) {
+            r->status = ATR_ERR_NOT_RESIDENT;
+            r->error = "refit: mesh was released";
+            continue;
         }
+        res.rec = r->refit_rec;
+        res.index = r->refit_index;
         float sah = 0.0f;
         const size_t p = work_pos(r);
         const float* src = verts_pinned[p]
@@ -604,14 +609,12 @@ void atr_server::lane_loop(Lane* L) {
         }
         for (Request* r : work) {
             inflight_bytes -= r->bytes;
-            if (r->req.kind == ATR_REQ_REFIT) {
+            if (r->req.kind == ATR_REQ_REFIT && r->refit_rec) {
                 auto f = resident.find(r->req.mesh_id);
-                if (f != resident.end()) {
-                    f->second.rec->busy_lane = -1;
-                    f->second.rec->last_use = use_clock;
-                }
-                for (auto& b : batches)
-                    if (b->busy_lane == L->id) b->busy_lane = -1;
+                if (f != resident.end() && f->second.busy_lane == L->id) f->second.busy_lane = -1;
+                --r->refit_rec->busy;
+                r->refit_rec->last_use = use_clock;
+                r->refit_rec.reset();
             }
             if (s != ATR_OK) {
                 finish(r, s, msg.c_str());
@@ -680,6 +683,16 @@ int atr_server_create(int device, const atr_server_config* cfg, atr_server** out
             atr::set_error("%s", msg.c_str());
             return st;
         }
+        // A lane's stream-ordered pool keeps what it frees.  Reserving part of
+        // the budget up front keeps the first large batches from growing the
+        // pool, which maps new device memory while their requests wait.
+        const uint64_t prime = std::min<uint64_t>(cfg->hbm_budget_bytes / (4ull * cfg->lanes), 4ull << 30);
+        void* p = nullptr;
+        if (prime && L->ctx->alloc(&p, prime) == ATR_OK) {
+            L->ctx->release(p);
+            cudaStreamSynchronize(L->ctx->stream);
+        }
+        cudaGetLastError();
         s->lanes.push_back(std::move(L));
     }
     for (auto& L : s->lanes) L->thread = std::thread(&atr_server::lane_loop, s, L.get());
