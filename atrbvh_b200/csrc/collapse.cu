@@ -46,6 +46,9 @@ struct CollapseRefs {
     // record so a climbing thread reads each child with one load.
     int2* rec;
     uint32_t* emit_cnt;
+    // False when the collapsed tree shares the source tree's links and boxes
+    // (a collapse leaves them as they are): only data and counts are written.
+    bool copy;
 };
 
 // Segmented: thread i starts at the i-th leaf of the batch; node arrays are
@@ -79,12 +82,14 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
     g.c_count[nb + ch] = 1;
     g.rec[nb + ch] = mine;
     // The leaf's copy (data >= 0, no children).
-    g.c_parent[nb + ch] = cur;
-    g.c_left[nb + ch] = g.left[nb + ch];
-    g.c_right[nb + ch] = g.right[nb + ch];
     g.c_data[nb + ch] = g.data[nb + ch];
-    g.c_bmin[nb + ch] = g.bmin[nb + ch];
-    g.c_bmax[nb + ch] = g.bmax[nb + ch];
+    if (g.copy) {
+        g.c_parent[nb + ch] = cur;
+        g.c_left[nb + ch] = g.left[nb + ch];
+        g.c_right[nb + ch] = g.right[nb + ch];
+        g.c_bmin[nb + ch] = g.bmin[nb + ch];
+        g.c_bmax[nb + ch] = g.bmax[nb + ch];
+    }
     if (cur < 0) return;
     int l = g.left[nb + cur], r = g.right[nb + cur], up = g.parent[nb + cur];
     float a = g.area[nb + cur];
@@ -101,12 +106,14 @@ __global__ void __launch_bounds__(256) k_collapse_cost(CollapseRefs g, Segs segs
         if (other == 0ull) {
             // First of the two children: the node's copy, then stop.
             const int x = nb + cur;
-            g.c_parent[x] = up;
-            g.c_left[x] = l;
-            g.c_right[x] = r;
             g.c_data[x] = g.data[x];
-            g.c_bmin[x] = g.bmin[x];
-            g.c_bmax[x] = g.bmax[x];
+            if (g.copy) {
+                g.c_parent[x] = up;
+                g.c_left[x] = l;
+                g.c_right[x] = r;
+                g.c_bmin[x] = g.bmin[x];
+                g.c_bmax[x] = g.bmax[x];
+            }
             return;
         }
         const int2 sib = make_int2((int)(uint32_t)other, (int)(uint32_t)(other >> 32));
@@ -194,6 +201,32 @@ int collapsed_alloc(atr_ctx* ctx, uint32_t n, atr_collapsed** out) {
     return ATR_OK;
 }
 
+// A collapsed tree that shares `tree`'s links and boxes (parent, left, right,
+// bmin, bmax: a collapse leaves them as they are) and owns only its data,
+// counts and leaf lists -- for a holder of both that never changes the tree
+// without collapsing again (a build plan).
+int collapsed_alloc_sharing(atr_ctx* ctx, const atr_tree* tree, atr_collapsed** out) {
+    const uint32_t n = tree->n;
+    const size_t nn = 2 * (size_t)n - 1;
+    const size_t b4 = align256(nn * 4);
+    atr_collapsed* c = new atr_collapsed();
+    c->ctx = ctx;
+    c->n = n;
+    int s = ctx->alloc(&c->block, 2 * b4 + align256((size_t)n * 4));
+    if (s != ATR_OK) { delete c; return s; }
+    char* p = static_cast<char*>(c->block);
+    c->data = reinterpret_cast<int32_t*>(p); p += b4;
+    c->count = reinterpret_cast<int32_t*>(p); p += b4;
+    c->tri_indices = reinterpret_cast<int32_t*>(p);
+    c->parent = tree->parent;
+    c->left = tree->left;
+    c->right = tree->right;
+    c->bmin = tree->bmin;
+    c->bmax = tree->bmax;
+    *out = c;
+    return ATR_OK;
+}
+
 // Collapse every mesh of segs (total_nodes = sum of 2n_m - 1).  src holds the
 // optimised trees, dst the collapsed arrays; d_sah_parts (optional) receives
 // cost[root] and area[root] of every mesh (2 floats per mesh).
@@ -221,8 +254,11 @@ int collapse_segs(atr_ctx* ctx, const Segs& segs, size_t total_nodes, const Tree
         ctx->release(scratch);
         return cuda_fail(me, "collapse scratch clear", __FILE__, __LINE__);
     }
-    CollapseRefs r{n, src.area, src.parent, src.left, src.right, src.data, src.bmin, src.bmax, dst.parent, dst.left,
-                   dst.right, dst.data, dst.count, dst.bmin, dst.bmax, rec, emit};
+    const bool shared = dst.parent == src.parent && dst.left == src.left && dst.right == src.right &&
+                        dst.bmin == src.bmin && dst.bmax == src.bmax;
+    CollapseRefs r{n,        src.area,  src.parent, src.left,  src.right, src.data, src.bmin, src.bmax,
+                   dst.parent, dst.left, dst.right, dst.data, dst.count, dst.bmin, dst.bmax, rec,
+                   emit,     !shared};
     const unsigned blocks = (n + 255) / 256;
     k_collapse_cost<<<blocks, 256, 0, s>>>(r, segs, slots, ci, ct, max_leaf);
     ctx->launches += 1;

@@ -131,7 +131,9 @@ int atr_plan_create(atr_ctx* ctx, const atr_scene* scene, const atr_plan_params*
     P->p = p;
     const uint32_t n = scene->n;
     int st = tree_alloc(ctx, n, &P->tree);
-    if (st == ATR_OK) st = collapsed_alloc(ctx, n, &P->col);
+    // The plan's collapsed tree shares its tree's links and boxes: the plan
+    // rewrites both on every run and hands out neither for writing.
+    if (st == ATR_OK) st = collapsed_alloc_sharing(ctx, P->tree, &P->col);
     if (st == ATR_OK) st = ctx->alloc(&P->block, 256);
     if (st == ATR_OK && p.flatten) {
         // Upper bounds: every inner node; three entries and a terminator per triangle.

@@ -296,7 +296,10 @@ int atr_trace(atr_ctx* ctx, const atr_compact* compact, const float* rays, int64
  * deforming mesh.  The results are read through atr_plan_tree /
  * atr_plan_collapsed / atr_plan_compact (the last reads the layout sizes and
  * synchronises) and atr_plan_sah; atr_plan_times gives the device time of the
- * last run's build (Morton through collapse) and flatten. */
+ * last run's build (Morton through collapse) and flatten.  The plan's
+ * collapsed tree shares the plan's tree's links and boxes (parent, left,
+ * right, bmin, bmax; a collapse leaves them unchanged) and owns its data,
+ * counts and leaf lists: both are read-only views, rewritten by each run. */
 typedef struct atr_plan_params {
     int32_t morton_bits;   /* 30 or 63 */
     int32_t optimizer;     /* 0 none, 1 ATRBVH, 2 TRBVH */
