@@ -683,10 +683,12 @@ int atr_server_create(int device, const atr_server_config* cfg, atr_server** out
             atr::set_error("%s", msg.c_str());
             return st;
         }
-        // A lane's stream-ordered pool keeps what it frees.  Reserving part of
-        // the budget up front keeps the first large batches from growing the
-        // pool, which maps new device memory while their requests wait.
-        const uint64_t prime = std::min<uint64_t>(cfg->hbm_budget_bytes / (4ull * cfg->lanes), 4ull << 30);
+        // A lane's stream-ordered pool keeps what it frees.  Growing it maps
+        // new device memory while the batch's requests wait (a few ms per GB,
+        // measured): reserve up front what the lane's largest batch needs,
+        // within half the budget's share per lane.
+        const uint64_t prime = std::min<uint64_t>(cfg->max_batch_triangles * kBuildBytesPerTri,
+                                                  cfg->hbm_budget_bytes / (2ull * cfg->lanes));
         void* p = nullptr;
         if (prime && L->ctx->alloc(&p, prime) == ATR_OK) {
             L->ctx->release(p);
