@@ -1685,7 +1685,7 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         const uint32_t* start_count = nullptr;
         uint32_t blocks = leaf_blocks;
         if (L && e == cudaSuccess) {
-            e = cudaMemsetAsync(lv.hist, 0, b_small, st);
+            if (zero_words_async(ctx, lv.hist, b_small / 4) != ATR_OK) e = cudaErrorLaunchFailure;
             const unsigned gb = (segs.n + 255) / 256;
             const unsigned gbl = (segs.n + kListBlock - 1) / kListBlock;
             if (hist_done)

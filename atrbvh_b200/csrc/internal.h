@@ -256,6 +256,7 @@ int batch_refit_mesh(atr_ctx* ctx, atr_batch* b, uint32_t mesh, const float* ver
 // collapse into them (d_sah_parts, may be NULL: cost and area of the root).
 int collapsed_alloc(atr_ctx* ctx, uint32_t n, atr_collapsed** out);
 int collapsed_alloc_sharing(atr_ctx* ctx, const atr_tree* tree, atr_collapsed** out);
+int zero_words_async(atr_ctx* ctx, uint32_t* p, size_t words);
 int collapse_into(atr_ctx* ctx, const atr_tree* tree, float ci, float ct, int max_leaf, atr_collapsed* c,
                   float* d_sah_parts);
 

@@ -916,10 +916,10 @@ int build_typed(atr_ctx* ctx, const Segs& segs, uint32_t tiles, const float4* ve
     uint32_t* tile_counts = reinterpret_cast<uint32_t*>(ap); ap += align256(cbytes);
     int32_t* slot = reinterpret_cast<int32_t*>(ap); ap += align256(inner * 4);
     BuildEdge* edges = reinterpret_cast<BuildEdge*>(ap);
-    cudaError_t me = cudaMemsetAsync(hist, 0, hbytes, s);
-    if (me != cudaSuccess) {
+    const int zs = zero_words_async(ctx, hist, hbytes / 4);
+    if (zs != ATR_OK) {
         ctx->release(aux); ctx->release(kv); ctx->release(iv);
-        return cuda_fail(me, "cudaMemsetAsync(hist)", __FILE__, __LINE__);
+        return zs;
     }
 
     ctx->phase_begin("morton");

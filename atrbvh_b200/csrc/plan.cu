@@ -34,6 +34,7 @@ struct atr_plan {
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // start, collapsed, end
     cudaGraphExec_t graph = nullptr;
     int graph_key[6] = {0, 0, 0, 0, 0, 0};
+    bool graph_phases = false;  // the graph records per-phase marks
     uint64_t graph_launches = 0;
     bool ran = false;
     bool sizes_read = false;
@@ -184,7 +185,10 @@ int atr_plan_run(atr_ctx* ctx, atr_plan* P, int use_graph) {
     }
     int key[6];
     plan_tuning_key(ctx, key);
-    if (!P->graph || std::memcmp(key, P->graph_key, sizeof(key)) != 0) {
+    // Per-phase marks are captured when the context times phases: each is an
+    // event node at a stage boundary, which leaves the device idle for several
+    // microseconds, so a graph captured without them is a little faster.
+    if (!P->graph || std::memcmp(key, P->graph_key, sizeof(key)) != 0 || P->graph_phases != ctx->timing) {
         if (P->graph) {
             cudaGraphExecDestroy(P->graph);
             P->graph = nullptr;
@@ -194,11 +198,11 @@ int atr_plan_run(atr_ctx* ctx, atr_plan* P, int use_graph) {
             cudaEventDestroy(ph.b);
         }
         P->phases.clear();
-        // The capture records its own phase marks (kept by the plan).
+        // The capture records its own phase marks (kept by the plan) when the
+        // context times phases.
         const bool timing = ctx->timing;
         std::vector<atr_ctx::Phase> outer;
         outer.swap(ctx->phases);
-        ctx->timing = true;
         ctx->capture_marks = true;
         const uint64_t l0 = ctx->launches;
         cudaGraph_t graph = nullptr;
@@ -223,6 +227,7 @@ int atr_plan_run(atr_ctx* ctx, atr_plan* P, int use_graph) {
         P->graph_launches = ctx->launches - l0;
         ctx->launches = l0;
         std::memcpy(P->graph_key, key, sizeof(key));
+        P->graph_phases = timing;
     }
     ctx->phase_begin("plan");
     ATR_CUDA(cudaGraphLaunch(P->graph, ctx->stream));

@@ -296,7 +296,10 @@ int atr_trace(atr_ctx* ctx, const atr_compact* compact, const float* rays, int64
  * deforming mesh.  The results are read through atr_plan_tree /
  * atr_plan_collapsed / atr_plan_compact (the last reads the layout sizes and
  * synchronises) and atr_plan_sah; atr_plan_times gives the device time of the
- * last run's build (Morton through collapse) and flatten.  The plan's
+ * last run's build (Morton through collapse) and flatten; atr_plan_phase_times
+ * the per-phase device times of the last replay when the graph was captured
+ * with the context's phase timing on (atr_ctx_set_timing; the graph is captured
+ * again when that setting changes), else none.  The plan's
  * collapsed tree shares the plan's tree's links and boxes (parent, left,
  * right, bmin, bmax; a collapse leaves them unchanged) and owns its data,
  * counts and leaf lists: both are read-only views, rewritten by each run. */

@@ -1,6 +1,6 @@
-"""Phase marks recorded inside a build plan's graph: one device time per
-phase of the last replay, positive, and summing to about the build time
-measured around the same phases."""
+"""Phase marks recorded inside a build plan's graph when the context times
+phases: one device time per phase of the last replay, positive, and summing to
+about the build time measured around the same phases; none without."""
 import pytest
 
 import atrbvh_b200 as ab
@@ -17,9 +17,15 @@ def test_plan_phase_times_after_replay(ctx):
     plan = ab.BuildPlan(scene)
     with pytest.raises(ab.AtrError):
         plan.phase_times()  # no replay yet
-    for _ in range(3):
-        plan.run(graph=True)
-    ph = dict(plan.phase_times())
+    plan.run(graph=True)
+    assert plan.phase_times() == []  # captured without phase timing: no marks
+    ctx.set_timing(True)  # the next replay captures the graph again, with marks
+    try:
+        for _ in range(3):
+            plan.run(graph=True)
+        ph = dict(plan.phase_times())
+    finally:
+        ctx.set_timing(False)
     assert set(ph) == {"morton", "sort", "build", "atrbvh", "collapse", "flatten"}, ph
     assert all(t > 0 for t in ph.values())
     build_ms, flatten_ms = plan.times()
