@@ -15,8 +15,8 @@ Builds the checkers:
 
 The reference's own sources are located through the ATRBVH_REFERENCE
 environment variable (the root of the leonardo-domingues/atrbvh tree; default
-/root/reference, where this build's container mounts it read-only).  Nothing
-here runs the reference's CUDA kernels.
+/root/reference, a read-only checkout).  Nothing here runs the reference's CUDA
+kernels.
 Run as ``python -m oracle.build``.
 """
 from __future__ import annotations
