@@ -826,10 +826,11 @@ cudaError_t launch_atrbvh_g(int warps, uint32_t blocks, cudaStream_t s, const Tr
 // Phase A finishes every node that is not big (subtree count, nodesSah, child
 // record) and levels the big ones: k_levels climbs once from every leaf;
 // k_levels_pp and k_levels_pp_hist take counts, nodesSah (and levels) from
-// the LBVH build.  Phase B sorts big nodes of levels 1..L into per-level
-// lists; phase C restructures each level's treelets in one launch, several
-// per warp in lane groups; the dataflow kernel then climbs from the frontier
-// below the levels above L.
+// the LBVH build.  Phase B files big nodes of levels 1..L into per-level
+// lists (in the same pass as the level counts: k_levels_pp_hist for the first
+// iteration, k_level_hist for the others); phase C restructures each level's
+// treelets in one launch, several per warp in lane groups; the dataflow kernel
+// then climbs from the frontier below the levels above L.
 
 constexpr int kMaxLevels = 64;  // largest L (ATR_TUNE_ATR_LEVELS)
 constexpr int kListPer = 8;                  // nodes per thread of the level-list kernels
@@ -841,12 +842,12 @@ struct LevelRefs {
     float ct;              // the leaf cost constant (triangle leaves' records)
     uint32_t* counters;
     int4* kids;
-    uint32_t* hist;        // [L + 2]: level histogram
-    uint32_t* off;         // [L + 2]: per-level offsets into `order` (written by phase B)
-    uint32_t* cursor;      // [L + 2]
-    uint2* order;          // (mesh, local node) of big nodes by level
+    uint32_t* cursor;      // [L + 2]: entries filed per level (the level's count)
+    uint2* order;          // (mesh, local node) of big nodes: level l's list at (l - 1) * cap
+    uint32_t cap;          // entries per level list (at most n / gamma nodes share a level)
     uint2* frontier;       // climb starts of the dataflow pass
     uint32_t* n_frontier;
+    uint32_t* err;
 };
 
 constexpr int kLvBlock = 512;  // threads (leaves) per block of the phase-A climb
@@ -1004,17 +1005,58 @@ __global__ void __launch_bounds__(256) k_levels_pp(TreeRefs g, Segs segs, LevelR
 // one streaming pass writes the counts, child records and next-iteration
 // values of the nodes that are not big, counts the levels 1..L and lists
 // the frontier below the levels above L (k_level_hist's work as well).
+// Files a block's nodes of levels 1..L into the level lists: thread-held
+// levels me[q] (0: none) and entries ent[q].  Ranks within the block come from
+// one shared atomic per level present in a warp (__match_any_sync), then one
+// global reservation per level per block on lv.cursor (which ends as the
+// level's count).  Nodes of one level have disjoint subtrees of at least gamma
+// triangles each, so a list holds at most lv.cap of them; a reservation past
+// that sets kErrLevelList and writes nothing.  Every thread of the block calls
+// it; s_cnt holds L + 2 zeroed counters.
+__device__ __forceinline__ void file_levels(const LevelRefs& lv, int L, const int (&me)[kListPer],
+                                            const uint2 (&ent)[kListPer], uint32_t* s_cnt, uint32_t* s_base) {
+    const int lane = threadIdx.x & 31;
+    uint32_t key[kListPer];
+#pragma unroll
+    for (int q = 0; q < kListPer; ++q) {
+        const uint32_t peers = __match_any_sync(kFull, me[q]);
+        const int leader = __ffs(peers) - 1;
+        uint32_t b = 0;
+        if (lane == leader && me[q] > 0) b = atomicAdd(&s_cnt[me[q]], (uint32_t)__popc(peers));
+        b = __shfl_sync(kFull, b, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+        key[q] = me[q] > 0 ? ((uint32_t)me[q] << 16) | b : 0u;  // rank < kListBlock
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
+        s_base[k] = s_cnt[k] ? atomicAdd(&lv.cursor[k], s_cnt[k]) : 0u;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kListPer; ++q)
+        if (key[q]) {
+            const uint32_t l = key[q] >> 16;
+            const uint32_t at = s_base[l] + (key[q] & 0xffffu);
+            if (at < lv.cap) lv.order[(size_t)(l - 1) * lv.cap + at] = ent[q];
+            else set_error_bits(lv.err, kErrLevelList);
+        }
+}
+
 __global__ void __launch_bounds__(256) k_levels_pp_hist(TreeRefs g, Segs segs, LevelRefs lv,
                                                         const int2* __restrict__ ranges, int tsize_all,
                                                         const uint8_t* __restrict__ seg_tsize,
                                                         const uint8_t* __restrict__ seg_iters, int L) {
-    __shared__ uint32_t s_hist[kMaxLevels + 2];
-    for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_hist[k] = 0;
+    __shared__ uint32_t s_cnt[kMaxLevels + 2];
+    __shared__ uint32_t s_base[kMaxLevels + 2];
+    for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_cnt[k] = 0;
     __syncthreads();
+    int lvl[kListPer];
+    uint2 lent[kListPer];
+#pragma unroll
     for (int q = 0; q < kListPer; ++q) {
         const uint32_t i = blockIdx.x * kListBlock + q * 256 + threadIdx.x;
         int push = 0;
         uint2 ent[2];
+        lvl[q] = 0;
+        lent[q] = make_uint2(0u, 0u);
         if (i < segs.n) {
             const uint32_t m = segs.seg_of_tri(i);
             const uint32_t s0 = segs.tri_begin(m);
@@ -1035,7 +1077,8 @@ __global__ void __launch_bounds__(256) k_levels_pp_hist(TreeRefs g, Segs segs, L
                     if (cnt >= gamma) {
                         const int me = *rec_i(lv.rec, base + x, 3);
                         if (me <= L) {
-                            atomicAdd(&s_hist[me], 1u);
+                            lvl[q] = me;
+                            lent[q] = make_uint2(m, (uint32_t)x);
                         } else {
                             if ((is_internal(lc, n) ? *rec_i(lv.rec, base + lc, 3) : 0) <= L)
                                 ent[push++] = make_uint2(m, (uint32_t)lc);
@@ -1058,10 +1101,7 @@ __global__ void __launch_bounds__(256) k_levels_pp_hist(TreeRefs g, Segs segs, L
         at = __shfl_sync(kFull, at, 31) + incl - push;
         for (int k = 0; k < push; ++k) lv.frontier[at + k] = ent[k];
     }
-    // Level counts: one global atomic per level present in the block.
-    __syncthreads();
-    for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
-        if (s_hist[k]) atomicAdd(&lv.hist[k], s_hist[k]);
+    file_levels(lv, L, lvl, lent, s_cnt, s_base);
 }
 
 // Phase A of iterations after the first: the previous iteration left every
@@ -1072,14 +1112,20 @@ __global__ void __launch_bounds__(256) k_levels_pp_hist(TreeRefs g, Segs segs, L
 // one too, and list the frontier below the levels above L.
 __global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, const uint8_t* __restrict__ seg_iters,
                                                     int iteration, int L) {
-    __shared__ uint32_t s_hist[kMaxLevels + 2];
-    for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_hist[k] = 0;
+    __shared__ uint32_t s_cnt[kMaxLevels + 2];
+    __shared__ uint32_t s_base[kMaxLevels + 2];
+    for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_cnt[k] = 0;
     __syncthreads();
+    int lvl[kListPer];
+    uint2 lent[kListPer];
+#pragma unroll
     for (int q = 0; q < kListPer; ++q) {
         const uint32_t i = blockIdx.x * kListBlock + q * 256 + threadIdx.x;
         int push = 0;
         uint32_t m = 0;
         uint2 ent[2];
+        lvl[q] = 0;
+        lent[q] = make_uint2(0u, 0u);
         if (i < segs.n) {
             m = segs.seg_of_tri(i);
             const uint32_t s0 = segs.tri_begin(m);
@@ -1093,7 +1139,8 @@ __global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, con
                     // stays 0).
                     *rec_f(lv.rec, nb + (int)li, rec_ns_next(lv.par)) = *rec_f(lv.rec, nb + (int)li, rec_ns_cur(lv.par));
                 } else if (me <= L) {
-                    atomicAdd(&s_hist[me], 1u);
+                    lvl[q] = me;
+                    lent[q] = make_uint2(m, li);
                 } else {
                     const int4 kd = lv.kids[cb + (int)li];
                     if ((is_internal(kd.x, n) ? *rec_i(lv.rec, nb + kd.x, 3) : 0) <= L)
@@ -1115,76 +1162,7 @@ __global__ void __launch_bounds__(256) k_level_hist(Segs segs, LevelRefs lv, con
         at = __shfl_sync(kFull, at, 31) + incl - push;
         for (int k = 0; k < push; ++k) lv.frontier[at + k] = ent[k];
     }
-    // Level counts: one global atomic per level present in the block.
-    __syncthreads();
-    for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
-        if (s_hist[k]) atomicAdd(&lv.hist[k], s_hist[k]);
-}
-
-// Phase B: the level lists.  Every block scans the (small) level histogram
-// into list offsets, then files its nodes of levels 1..L into the lists.
-__global__ void __launch_bounds__(256) k_level_scatter(Segs segs, LevelRefs lv, const uint8_t* __restrict__ seg_iters,
-                                                       int iteration, int L) {
-    __shared__ uint32_t s_cnt[kMaxLevels + 2];
-    __shared__ uint32_t s_base[kMaxLevels + 2];
-    __shared__ uint32_t s_off[kMaxLevels + 2];
-    for (int k = threadIdx.x; k < L + 2; k += blockDim.x) s_cnt[k] = 0;
-    // Offsets of the level lists: every block scans the (small) histogram;
-    // block 0 publishes them for the level passes.
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int l = 0; l <= L + 1; ++l) {
-            s_off[l] = run;
-            run += lv.hist[l];
-        }
-    }
-    __syncthreads();
-    if (blockIdx.x == 0)
-        for (int k = threadIdx.x; k < L + 2; k += blockDim.x) lv.off[k] = s_off[k];
-    // kListPer nodes per thread: levels first (independent loads), then each
-    // node's rank among the block's nodes of its level, one shared atomic per
-    // level present in the warp.
-    const int lane = threadIdx.x & 31;
-    int me[kListPer];
-    uint2 ent[kListPer];
-#pragma unroll
-    for (int q = 0; q < kListPer; ++q) {
-        const uint32_t i = blockIdx.x * kListBlock + q * 256 + threadIdx.x;
-        me[q] = 0;
-        ent[q] = make_uint2(0u, 0u);
-        if (i < segs.n) {
-            const uint32_t m = segs.seg_of_tri(i);
-            const uint32_t s0 = segs.tri_begin(m);
-            const uint32_t n = segs.tri_end(m) - s0;
-            const uint32_t li = i - s0;
-            ent[q] = make_uint2(m, li);
-            if ((!seg_iters || iteration < (int)seg_iters[m]) && li < n - 1) {
-                const int lvl = *rec_i(lv.rec, segs.node_base(m) + (int)li, 3);
-                me[q] = lvl <= L ? lvl : 0;
-            }
-        }
-    }
-    uint32_t key[kListPer];
-#pragma unroll
-    for (int q = 0; q < kListPer; ++q) {
-        const uint32_t peers = __match_any_sync(kFull, me[q]);
-        const int leader = __ffs(peers) - 1;
-        uint32_t b = 0;
-        if (lane == leader && me[q] > 0) b = atomicAdd(&s_cnt[me[q]], (uint32_t)__popc(peers));
-        b = __shfl_sync(kFull, b, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
-        key[q] = me[q] > 0 ? ((uint32_t)me[q] << 16) | b : 0u;  // rank < kListBlock
-    }
-    __syncthreads();
-    // One global reservation per level present in the block.
-    for (int k = threadIdx.x; k < L + 2; k += blockDim.x)
-        s_base[k] = s_cnt[k] ? atomicAdd(&lv.cursor[k], s_cnt[k]) : 0u;
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < kListPer; ++q)
-        if (key[q]) {
-            const uint32_t l = key[q] >> 16;
-            lv.order[s_off[l] + s_base[l] + (key[q] & 0xffffu)] = ent[q];
-        }
+    file_levels(lv, L, lvl, lent, s_cnt, s_base);
 }
 
 // ---- quads: eight treelets per warp ----------------------------------------
@@ -1550,7 +1528,8 @@ __global__ void __launch_bounds__(W * 32, (G == 32 ? 16 : 32) / W) k_level_group
     __shared__ __align__(16) float s_mem[W][kGroupFloats * per];
     __shared__ uint16_t s_rc[kMaxDist];
     __shared__ __align__(4) uint8_t s_prio[(kMaxTreelet + 1) * 32];
-    const uint32_t beg = lv.off[lev], end = lv.off[lev + 1];
+    const uint32_t beg = (uint32_t)(lev - 1) * lv.cap;
+    const uint32_t end = beg + min(lv.cursor[lev], lv.cap);
     if (beg + blockIdx.x * (uint32_t)(W * per) >= end) return;  // no root for this block
     for (int k = threadIdx.x; k < kMaxDist; k += blockDim.x) {
         int r, c;
@@ -1629,11 +1608,15 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     void* scratch = nullptr;
     const size_t b_rec = align256(total_nodes * 16), b_ctr = align256(inner * 4);
     const size_t b_kid = align256(inner * 16);
-    // Big nodes of levels 1..L number at most the internal nodes; frontier
-    // nodes root disjoint subtrees, so they number at most the triangles.
-    const size_t b_ord = L ? align256(inner * 8) : 0;
+    // Big nodes of one level root disjoint subtrees of at least gamma
+    // triangles (the first iteration's gamma, the smallest; 3 bounds per-mesh
+    // sizes), so each level's list holds at most n / gamma; frontier nodes
+    // root disjoint subtrees too, so they number at most the triangles.
+    const uint32_t gamma0 = seg_tsize ? 3u : (uint32_t)tsize;
+    const uint32_t cap = (segs.n + gamma0 - 1) / gamma0;
+    const size_t b_ord = L ? align256((size_t)L * cap * 8) : 0;
     const size_t b_front = L ? align256((size_t)segs.n * 8) : 0;
-    const size_t b_small = L ? align256((size_t)(3 * (L + 2) + 1) * 4) : 0;
+    const size_t b_small = L ? align256((size_t)((L + 2) + 1) * 4) : 0;
     // The build's prepass records (counts, first nodesSah, levels) serve as
     // the optimiser's records when its constants are this pass's.
     const bool use_pp = prepass && prepass->rec && karras_ranges && L > 0 && ci == kPrepassCi && ct == kPrepassCt;
@@ -1659,10 +1642,10 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
     lv.kids = kids;
     if (L) {
         lv.order = reinterpret_cast<uint2*>(p); p += b_ord;
+        lv.cap = cap;
+        lv.err = ctx->d_error;
         lv.frontier = reinterpret_cast<uint2*>(p); p += b_front;
-        lv.hist = reinterpret_cast<uint32_t*>(p);
-        lv.off = lv.hist + (L + 2);
-        lv.cursor = lv.off + (L + 2);
+        lv.cursor = reinterpret_cast<uint32_t*>(p);
         lv.n_frontier = lv.cursor + (L + 2);
     }
     const int warps = ctx->atr_warps == 2 || ctx->atr_warps == 4 ? ctx->atr_warps : 8;
@@ -1685,7 +1668,7 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
         const uint32_t* start_count = nullptr;
         uint32_t blocks = leaf_blocks;
         if (L && e == cudaSuccess) {
-            if (zero_words_async(ctx, lv.hist, b_small / 4) != ATR_OK) e = cudaErrorLaunchFailure;
+            if (zero_words_async(ctx, lv.cursor, b_small / 4) != ATR_OK) e = cudaErrorLaunchFailure;
             const unsigned gb = (segs.n + 255) / 256;
             const unsigned gbl = (segs.n + kListBlock - 1) / kListBlock;
             if (hist_done)
@@ -1705,8 +1688,6 @@ int atrbvh_run(atr_ctx* ctx, const TreeRefs& g_in, const Segs& segs, size_t tota
                 k_level_hist<<<gbl, 256, 0, st>>>(segs, lv, seg_iters, it, L);
                 ++ctx->launches;
             }
-            k_level_scatter<<<gbl, 256, 0, st>>>(segs, lv, seg_iters, it, L);
-            ++ctx->launches;
             const unsigned lg = (unsigned)ctx->num_sms * (256 / threads) * 4;
             // Roots per level fall by about 0.62 per level from n / (1.5 gamma)
             // at level 1 (gamma = tsize << it); levels expected to hold at

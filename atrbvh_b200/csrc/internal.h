@@ -42,6 +42,7 @@ enum : uint32_t {
     kErrTreeletClimb = 4u,
     kErrTraceStack = 8u,
     kErrCollapse = 16u,
+    kErrLevelList = 32u,  // a level list would overflow its capacity (entries dropped)
 };
 
 constexpr int kNumSms = 148;  // B200

@@ -456,7 +456,9 @@ int atr_server::run_batch(Lane& L, std::vector<Request*>& work, std::shared_ptr<
             s = atr_batch_create(ctx, static_cast<const float*>(L.h_verts), off.data(), (uint32_t)builds.size(),
                                  nullptr, 0, &b);
         }
-        if (s == ATR_OK) s = atr_batch_set_params(ctx, b, ts.data(), it.data());
+        // Per-mesh parameters only with size classes; otherwise every mesh
+        // takes the configuration's, passed to the build directly.
+        if (s == ATR_OK && have_classes) s = atr_batch_set_params(ctx, b, ts.data(), it.data());
         if (s == ATR_OK) s = atr_batch_build(ctx, b, 1, cfg.treelet_size, cfg.iterations, 1.2f, 1.0f, 0);
         std::vector<float> sah(builds.size(), 0.0f);
         if (s == ATR_OK) s = atr_batch_collapse(ctx, b, 1.2f, 1.0f, cfg.max_leaf, sah.data());
