@@ -58,10 +58,9 @@ BYTES_PER_TRI = {"morton": 56.0, "sort": 4.0 + 16.0 * 4, "build": 40.0 + 180.0, 
 REFIT_BYTES_PER_TRI = 180.0  # vertex gather 48, dataIndex 4, parents 8, boxes 64, areas 8, counters 8, siblings 32, children 8
 # DRAM bytes per triangle of the ATRBVH phase (both iterations) from an ncu
 # capture of this bench step at 2,097,152 triangles (dram__bytes_read.sum +
-# dram__bytes_write.sum per step: k_levels_pp_hist 87.7 MB, k_level_hist 33.7,
-# k_level_scatter 67.2, k_level_groups 951.0 + 709.6 + 54.5, k_atrbvh 8.4),
-# scaled by triangle count.
-ATRBVH_DRAM_BYTES_PER_TRI = (87.7 + 33.7 + 67.2 + 951.0 + 709.6 + 54.5 + 8.4) * 1e6 / 2097152
+# dram__bytes_write.sum per step: k_levels_pp_hist 88.2 MB, k_level_hist 33.7,
+# k_level_groups 1325.9 + 263.4 + 54.4, k_atrbvh 8.4), scaled by triangle count.
+ATRBVH_DRAM_BYTES_PER_TRI = (88.2 + 33.7 + 1325.9 + 263.4 + 54.4 + 8.4) * 1e6 / 2097152
 
 
 def _read_peaks() -> dict:
