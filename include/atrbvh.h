@@ -114,8 +114,7 @@ int atr_ctx_get_stream(atr_ctx* ctx, void** stream);
  *                           (3 and 7 passes).
  *   ATR_TUNE_ATR_LEVELS     ATRBVH levels of treelet roots restructured level
  *                           by level in lane groups (0..64; default 12; 0 =
- *                           all by the bottom-up warp pass); used when every
- *                           treelet size is at most 10.
+ *                           all by the bottom-up warp pass).
  *   ATR_TUNE_QUAD_MIN       fewest treelet roots of one level that the level
  *                           pass restructures in four-lane groups, eight per
  *                           warp, instead of 32/G per warp (-1 = never;
